@@ -1,0 +1,136 @@
+"""Python front end of libdiablo_gpu, mirroring the reference's step surface.
+
+``Channel`` owns one device context.  Its methods keep the reference's
+routine names and argument meaning:
+
+* ``fft_xz_to_fourier(v, vv)`` / ``fft_xz_to_physical(vv, v)``
+  (``for/fft.f90:247,319``) take arrays in the reference layout; passing the
+  same array twice reproduces the reference's in-place aliasing.
+* ``rk_chan_1(rk_step)`` (``for/channel.f90:10``), ``step(n)``
+  (``for/diablo.f90:104-108``), ``pre_first_step`` (``for/advance.f90:17``)
+  and ``apply_bc_post`` (``for/boundary.f90:824-855``).
+
+Arrays are numpy (host) arrays in the reference's Fortran memory order: a
+physical field has numpy shape ``(Ny+2, Nz+2, Nx+2)`` float64 (index
+``[j, k, i]``) and a Fourier field the complex128 view of the same bytes,
+shape ``(Ny+2, Nz+2, Nx/2+1)``.  Torch CUDA tensors of those shapes may be
+passed instead; their device pointers are used directly.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import ChannelParams
+
+
+def _ptr(a):
+    """Data pointer of a contiguous numpy array or torch tensor."""
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous (the reference's Fortran order)")
+        return a.ctypes.data_as(ctypes.c_void_p)
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr())
+    raise TypeError(f"unsupported array type {type(a)!r}")
+
+
+class Channel:
+    def __init__(self, params: ChannelParams, gy):
+        self.params = params
+        self.lib = _lib.load()
+        self._c = params.to_c()
+        gy = np.ascontiguousarray(gy, dtype=np.float64)
+        if gy.size != params.ny + 1:
+            raise ValueError(f"gy must hold Ny+1 = {params.ny + 1} points")
+        self._gy = gy
+        st = ctypes.c_int(0)
+        self.ctx = self.lib.diablo_create(ctypes.byref(self._c), gy.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.byref(st))
+        if not self.ctx:
+            raise _lib.DiabloError(st.value, "diablo_create")
+        self.shape_phys = (params.ny + 2, params.nz + 2, params.nx + 2)
+        self.shape_four = (params.ny + 2, params.nz + 2, params.nx // 2 + 1)
+
+    # -- lifetime ------------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.diablo_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- arrays --------------------------------------------------------
+    def new_field(self) -> np.ndarray:
+        """A zeroed reference-layout buffer (physical view)."""
+        return np.zeros(self.shape_phys, dtype=np.float64)
+
+    def upload(self, field: int, buf, layout: int = _lib.LAYOUT_FOURIER):
+        _lib.check(self.lib.diablo_upload_state(self.ctx, field, _ptr(buf), layout), "upload_state")
+
+    def download(self, field: int, layout: int = _lib.LAYOUT_FOURIER, out=None) -> np.ndarray:
+        if out is None:
+            out = self.new_field()
+        _lib.check(self.lib.diablo_download_state(self.ctx, field, _ptr(out), layout), "download_state")
+        return out
+
+    # -- reference surface ---------------------------------------------
+    def fft_xz_to_fourier(self, v, vv):
+        _lib.check(self.lib.diablo_fft_xz_to_fourier(self.ctx, _ptr(v), _ptr(vv)), "fft_xz_to_fourier")
+
+    def fft_xz_to_physical(self, vv, v):
+        _lib.check(self.lib.diablo_fft_xz_to_physical(self.ctx, _ptr(vv), _ptr(v)), "fft_xz_to_physical")
+
+    def rk_chan_1(self, rk_step: int):
+        _lib.check(self.lib.diablo_rk_substep(self.ctx, rk_step), "rk_substep")
+
+    def step(self, nsteps: int = 1):
+        _lib.check(self.lib.diablo_step(self.ctx, nsteps), "step")
+
+    def pre_first_step(self, compute_pressure: bool = False):
+        _lib.check(self.lib.diablo_pre_first_step(self.ctx, int(compute_pressure)), "pre_first_step")
+
+    def apply_bc_post(self):
+        _lib.check(self.lib.diablo_apply_bc_post(self.ctx), "apply_bc_post")
+
+    def set_precision(self, precision: int):
+        _lib.check(self.lib.diablo_set_precision(self.ctx, precision), "set_precision")
+
+    def synchronize(self):
+        _lib.check(self.lib.diablo_synchronize(self.ctx), "synchronize")
+
+    def check_finite(self) -> bool:
+        st = self.lib.diablo_check_finite(self.ctx)
+        if st == _lib.ERR_NONFINITE:
+            return False
+        _lib.check(st, "check_finite")
+        return True
+
+    @property
+    def time(self):
+        t = ctypes.c_double(0)
+        n = ctypes.c_int(0)
+        dt = ctypes.c_double(0)
+        _lib.check(self.lib.diablo_get_time(self.ctx, ctypes.byref(t), ctypes.byref(n), ctypes.byref(dt)),
+                   "get_time")
+        return t.value, n.value, dt.value
+
+    def set_time(self, time: float, time_step: int, delta_t: float):
+        _lib.check(self.lib.diablo_set_time(self.ctx, time, time_step, delta_t), "set_time")
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.diablo_kernel_launches(self.ctx))

@@ -1,0 +1,827 @@
+// libdiablo_gpu: context, device memory, kernel orchestration and the C ABI
+// declared in include/diablo_gpu.h.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/diablo_gpu.h"
+#include "common.cuh"
+#include "fft.cuh"
+#include "kernels_layout.cuh"
+#include "kernels_solve.cuh"
+
+static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
+static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
+
+// ``pi = 4.*atan(1.0)`` in for/fft.f90:152 is evaluated in default (single)
+// precision -- the reference build has no -fdefault-real-8 -- so its
+// wavenumbers kx = i*2*pi/Lx use float32(pi) widened to double.
+static const double PI_REF = 3.1415927410125732421875;
+
+// RK3 coefficients (for/flow.f90:78-86)
+static const double H_FRAC[3] = {8.0 / 15.0, 2.0 / 15.0, 5.0 / 15.0};
+static const double BETA_BAR[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0};
+static const double ZETA_BAR[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e__ = (call);                     \
+    if (e__ != cudaSuccess) {                     \
+      ctx->last_cuda = (int)e__;                  \
+      return DIABLO_ERR_CUDA;                     \
+    }                                             \
+  } while (0)
+
+struct diablo_ctx {
+  diablo_params p;
+  int nx, ny, nz, nth, nf;
+  int nxp, nkx, nkz, nkx1, nk2, kp, nyp2, M;
+  Geom g;
+  double nu, ro_inv;
+  int jstart, jend, jst[DIABLO_MAX_TH], jet[DIABLO_MAX_TH];
+  double time, delta_t, h_bar[3];
+  int time_step;
+  double w_top_transient;
+  int precision;
+  int last_cuda;
+  long long launches;
+  cudaStream_t stream, own_stream;
+  // grid metrics and wavenumbers (device)
+  double *d_dy, *d_dyf, *d_gy, *d_gyf, *d_kx, *d_kz;
+  std::vector<double> h_dy, h_dyf, h_gy, h_gyf;
+  // twiddles: exp(-2 pi i m/N) for N = Nz, M = Nx/2, Nx
+  double2 *tz64, *tm64, *tx64;
+  float2 *tz32, *tm32, *tx32;
+  // Fourier state, double buffered: [u1, u2, u3, p, th0..]
+  double2* st[2][3 + DIABLO_MAX_TH];
+  double2* cf[2][3 + DIABLO_MAX_TH];
+  int cur;      // index of the current state buffer
+  int cf_cur;   // index of the buffer holding the last substep's cf
+  // nonlinear terms and step scratch
+  void* nl[3 + DIABLO_MAX_TH];
+  void* phys[3 + DIABLO_MAX_TH];
+  void* xs[2 * (3 + DIABLO_MAX_TH)];
+  int scratch_prec;   // precision the scratch was sized for (-1 = none)
+  // boundary-call scratch (FP64): one field in each internal layout + one reference array
+  double* b_phys;
+  double2* b_xs;
+  double2* b_four;
+  double* b_ref;
+  int* d_flag;
+  std::vector<void*> allocs;
+};
+
+#include "fft_launch.h"
+
+// ---- column solve ----
+template <int R>
+static void launch_solve_t(const SolveArgs& a, bool project_only, cudaStream_t s) {
+  const int warps = 4;
+  dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
+  if (project_only) k_rem_div<R><<<grd, blk, 0, s>>>(a);
+  else k_column_solve<R><<<grd, blk, 0, s>>>(a);
+}
+static int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s) {
+  int R = (a.n + 31) / 32;
+  if (R < 3) R = 3;
+  switch (R) {
+#define X(r) case r: launch_solve_t<r>(a, project_only, s); return 0;
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return DIABLO_ERR_SIZE;
+  }
+}
+
+// --------------------------------------------------------------------------
+static int dev_alloc(diablo_ctx* ctx, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    ctx->last_cuda = (int)e;
+    cudaGetLastError();
+    return DIABLO_ERR_NOMEM;
+  }
+  ctx->allocs.push_back(*p);
+  e = cudaMemsetAsync(*p, 0, bytes, ctx->stream);
+  if (e != cudaSuccess) { ctx->last_cuda = (int)e; return DIABLO_ERR_CUDA; }
+  return 0;
+}
+
+static void twiddles(int n, int count, std::vector<double2>& d, std::vector<float2>& f) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  d.resize(count);
+  f.resize(count);
+  for (int m = 0; m < count; ++m) {
+    long double ang = 2.0L * pi * (long double)m / (long double)n;
+    double c = (double)cosl(ang), s = (double)-sinl(ang);
+    d[m] = make_double2(c, s);
+    f[m] = make_float2((float)cosl(ang), (float)-sinl(ang));
+  }
+}
+
+static int upload_tw(diablo_ctx* ctx, int n, int count, double2** d, float2** f) {
+  std::vector<double2> hd;
+  std::vector<float2> hf;
+  twiddles(n, count, hd, hf);
+  int rc = dev_alloc(ctx, (void**)d, count * sizeof(double2));
+  if (rc) return rc;
+  rc = dev_alloc(ctx, (void**)f, count * sizeof(float2));
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(*d, hd.data(), count * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(*f, hf.data(), count * sizeof(float2), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+static size_t four_elems(const diablo_ctx* c) { return (size_t)c->nyp2 * c->nkx1 * c->kp; }
+static size_t xs_elems(const diablo_ctx* c) { return (size_t)c->nyp2 * c->nkx1 * c->nz; }
+static size_t phys_elems(const diablo_ctx* c) { return (size_t)c->nyp2 * c->nz * c->nx; }
+static size_t ref_doubles(const diablo_ctx* c) { return (size_t)c->nyp2 * (c->nz + 2) * (c->nx + 2); }
+
+static int ensure_scratch(diablo_ctx* ctx) {
+  if (ctx->scratch_prec == ctx->precision) return 0;
+  if (ctx->scratch_prec >= 0) return DIABLO_ERR_UNSUPPORTED;  // resized below on first use only
+  const size_t cs = ctx->precision == DIABLO_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t rs = cs / 2;
+  for (int f = 0; f < ctx->nf; ++f) {
+    int rc = dev_alloc(ctx, &ctx->nl[f], four_elems(ctx) * cs);
+    if (rc) return rc;
+    rc = dev_alloc(ctx, &ctx->phys[f], phys_elems(ctx) * rs);
+    if (rc) return rc;
+  }
+  for (int f = 0; f < 2 * ctx->nf; ++f) {
+    int rc = dev_alloc(ctx, &ctx->xs[f], xs_elems(ctx) * cs);
+    if (rc) return rc;
+  }
+  ctx->scratch_prec = ctx->precision;
+  return 0;
+}
+
+static int ensure_bscratch(diablo_ctx* ctx) {
+  if (ctx->b_phys) return 0;
+  int rc;
+  if ((rc = dev_alloc(ctx, (void**)&ctx->b_phys, phys_elems(ctx) * sizeof(double)))) return rc;
+  if ((rc = dev_alloc(ctx, (void**)&ctx->b_xs, xs_elems(ctx) * sizeof(double2)))) return rc;
+  if ((rc = dev_alloc(ctx, (void**)&ctx->b_four, four_elems(ctx) * sizeof(double2)))) return rc;
+  if ((rc = dev_alloc(ctx, (void**)&ctx->b_ref, ref_doubles(ctx) * sizeof(double)))) return rc;
+  return 0;
+}
+
+// --------------------------------------------------------------------------
+// FP64 transforms between internal layouts (one field)
+static int fwd_phys_to_four(diablo_ctx* ctx, const double* phys, double2* xs, double2* four) {
+  XFwdArgs<double> xa;
+  memset(&xa, 0, sizeof(xa));
+  xa.in[0] = phys;
+  xa.outA[0] = xs;
+  xa.j0 = 0;
+  xa.g = ctx->g;
+  xa.twM = ctx->tm64;
+  xa.twX = ctx->tx64;
+  xa.kx = ctx->d_kx;
+  xa.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
+  xa.scale = 1.0 / ctx->nx;
+  int rc = launch_xfwd<double, false>(xa, ctx->M, ctx->nyp2, 1, ctx->stream);
+  if (rc) return rc;
+  ctx->launches++;
+  ZFwdArgs<double2, double2> za;
+  memset(&za, 0, sizeof(za));
+  za.srcA[0] = xs;
+  za.dst[0] = four;
+  za.q0 = 0;
+  za.nseq = ctx->nyp2 * ctx->nkx1;
+  za.g = ctx->g;
+  za.tw = ctx->tz64;
+  za.kz = ctx->d_kz;
+  za.scale = 1.0 / ctx->nz;
+  rc = launch_zfwd<double2, double2, false>(za, ctx->nz, 1, ctx->stream);
+  if (rc) return rc;
+  ctx->launches++;
+  return 0;
+}
+
+static int inv_four_to_phys(diablo_ctx* ctx, const double2* four, double2* xs, double* phys) {
+  ZInvArgs<double2> za;
+  memset(&za, 0, sizeof(za));
+  za.src[0] = four;
+  za.dst[0] = xs;
+  za.q0 = 0;
+  za.nseq = ctx->nyp2 * ctx->nkx1;
+  za.g = ctx->g;
+  za.tw = ctx->tz64;
+  int rc = launch_zinv<double2>(za, ctx->nz, 1, ctx->stream);
+  if (rc) return rc;
+  ctx->launches++;
+  XInvArgs<double2> xa;
+  memset(&xa, 0, sizeof(xa));
+  xa.src[0] = xs;
+  xa.dst[0] = phys;
+  xa.j0 = 0;
+  xa.g = ctx->g;
+  xa.twM = ctx->tm64;
+  xa.twX = ctx->tx64;
+  rc = launch_xinv<double2>(xa, ctx->M, ctx->nyp2, 1, ctx->stream);
+  if (rc) return rc;
+  ctx->launches++;
+  return 0;
+}
+
+static int grid1d(size_t n) { return (int)((n + 255) / 256); }
+
+static bool is_device_ptr(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// --------------------------------------------------------------------------
+static void fill_solve_args(diablo_ctx* ctx, SolveArgs& a, int rk) {
+  memset(&a, 0, sizeof(a));
+  const diablo_params& p = ctx->p;
+  a.nyp = ctx->ny;
+  a.n = ctx->nyp2;
+  a.nkx1 = ctx->nkx1;
+  a.nk2 = ctx->nk2;
+  a.kp = ctx->kp;
+  a.ncol = ctx->nkx1 * ctx->nk2;
+  a.nth = ctx->nth;
+  a.rk = rk;
+  const double h = ctx->h_bar[rk - 1];
+  a.temp1 = 0.5 * ctx->nu * h;
+  a.temp2 = 0.5 * h;
+  a.temp3 = ZETA_BAR[rk - 1] * h;
+  a.temp4 = h;
+  a.temp5 = BETA_BAR[rk - 1] * h;
+  a.nu = ctx->nu;
+  a.beta = p.beta;
+  a.nu_v = p.nu_v_scale;
+  a.roinvd = ctx->ro_inv / p.delta;
+  a.grav_x = p.grav_x;
+  a.grav_y = p.grav_y;
+  a.grav_z = p.grav_z;
+  if (p.f_type == 1) a.px = a.temp4 * p.px0;
+  else if (p.f_type == 2) a.px = a.temp4 * (p.px0 + p.amp_omega0 * cos(p.omega0 * ctx->time));
+  a.jstart = ctx->jstart;
+  a.jend = ctx->jend;
+  a.ubc[0] = p.u_bc_ymin; a.ubc[1] = p.u_bc_ymax;
+  a.vbc[0] = p.v_bc_ymin; a.vbc[1] = p.v_bc_ymax;
+  a.wbc[0] = p.w_bc_ymin; a.wbc[1] = p.w_bc_ymax;
+  a.uc1[0] = p.u_bc_ymin_c1; a.uc1[1] = p.u_bc_ymax_c1;
+  a.vc1[0] = p.v_bc_ymin_c1; a.vc1[1] = p.v_bc_ymax_c1;
+  a.wc1[0] = p.w_bc_ymin_c1;
+  a.wc1[1] = p.w_bc_ymax == 0 ? p.w_bc_ymax_c1 : ctx->w_top_transient;
+  a.front = (p.flavor_front && ctx->ro_inv != 0.0) ? 1 : 0;
+  a.ly = p.ly;
+  a.front_coef = ctx->ro_inv != 0.0 ? p.delta / ctx->ro_inv : 0.0;
+  for (int n = 0; n < ctx->nth; ++n) {
+    a.jst[n] = ctx->jst[n];
+    a.jet[n] = ctx->jet[n];
+    a.thbc[n][0] = p.th_bc_ymin[n];
+    a.thbc[n][1] = p.th_bc_ymax[n];
+    a.thc1[n][0] = p.th_bc_ymin_c1[n];
+    a.thc1[n][1] = p.th_bc_ymax_c1[n];
+    a.pr[n] = p.pr[n];
+    a.dthdx[n] = p.dthdx[n];
+    a.dthdz[n] = p.dthdz[n];
+  }
+  a.dy = ctx->d_dy;
+  a.dyf = ctx->d_dyf;
+  a.gy = ctx->d_gy;
+  a.gyf = ctx->d_gyf;
+  a.kx = ctx->d_kx;
+  a.kz = ctx->d_kz;
+}
+
+// Update the time-dependent top value of u3 (apply_BC_3_upper, for/channel.f90:1775)
+static void update_transient(diablo_ctx* ctx) {
+  const diablo_params& p = ctx->p;
+  if (p.w_bc_ymax != 0 && p.f_type == 4)
+    ctx->w_top_transient = p.w_bc_ymax_c1 + p.amp_omega0 *
+        sin(p.omega0 * (ctx->ro_inv / p.delta * ctx->time - p.force_start));
+}
+
+template <typename T>
+static int substep_spectral(diablo_ctx* ctx) {
+  typedef typename CT<T>::C C;
+  const int nf = ctx->nf;
+  const int c = ctx->cur;
+  const C* tz = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tz64 : (const void*)ctx->tz32);
+  const C* tm = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tm64 : (const void*)ctx->tm32);
+  const C* tx = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tx64 : (const void*)ctx->tx32);
+  int rc;
+  // 1. z inverse of u1, u2, u3, th_n (all planes) -> x-spectral
+  {
+    ZInvArgs<C> a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < nf; ++f) {
+      a.src[f] = ctx->st[c][f < 3 ? f : f + 1];
+      a.dst[f] = (C*)ctx->xs[f];
+    }
+    a.q0 = 0;
+    a.nseq = ctx->nyp2 * ctx->nkx1;
+    a.g = ctx->g;
+    a.tw = tz;
+    if ((rc = launch_zinv<C>(a, ctx->nz, nf, ctx->stream))) return rc;
+    ctx->launches++;
+  }
+  // 2. x inverse -> physical
+  {
+    XInvArgs<C> a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < nf; ++f) {
+      a.src[f] = (const C*)ctx->xs[f];
+      a.dst[f] = (T*)ctx->phys[f];
+    }
+    a.j0 = 0;
+    a.g = ctx->g;
+    a.twM = tm;
+    a.twX = tx;
+    if ((rc = launch_xinv<C>(a, ctx->M, ctx->nyp2, nf, ctx->stream))) return rc;
+    ctx->launches++;
+  }
+  // 3. nonlinear products + x forward (planes 1..Ny)
+  {
+    XFwdArgs<T> a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < nf; ++f) {
+      a.in[f] = (const T*)ctx->phys[f];
+      a.outA[f] = (C*)ctx->xs[f];
+      a.outB[f] = (C*)ctx->xs[nf + f];
+    }
+    a.j0 = 1;
+    a.g = ctx->g;
+    a.twM = tm;
+    a.twX = tx;
+    a.kx = ctx->d_kx;
+    a.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
+    a.scale = 1.0 / ctx->nx;
+    if ((rc = launch_xfwd<T, true>(a, ctx->M, ctx->ny, nf, ctx->stream))) return rc;
+    ctx->launches++;
+  }
+  // 4. z forward + combine -> NL (planes 1..Ny)
+  {
+    ZFwdArgs<C, C> a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < nf; ++f) {
+      a.srcA[f] = (const C*)ctx->xs[f];
+      a.srcB[f] = (const C*)ctx->xs[nf + f];
+      a.dst[f] = (C*)ctx->nl[f];
+    }
+    a.q0 = ctx->nkx1;
+    a.nseq = ctx->ny * ctx->nkx1;
+    a.g = ctx->g;
+    a.tw = tz;
+    a.kz = ctx->d_kz;
+    a.scale = 1.0 / ctx->nz;
+    if ((rc = launch_zfwd<C, C, true>(a, ctx->nz, nf, ctx->stream))) return rc;
+    ctx->launches++;
+  }
+  return 0;
+}
+
+static int substep(diablo_ctx* ctx, int rk) {
+  if (ctx->p.use_les) return DIABLO_ERR_UNSUPPORTED;
+  int rc = ensure_scratch(ctx);
+  if (rc) return rc;
+  update_transient(ctx);
+  rc = ctx->precision == DIABLO_FP64 ? substep_spectral<double>(ctx) : substep_spectral<float>(ctx);
+  if (rc) return rc;
+  SolveArgs a;
+  fill_solve_args(ctx, a, rk);
+  const int c = ctx->cur, nx_ = 1 - c;
+  for (int q = 0; q < 3; ++q) {
+    a.cu_in[q] = ctx->st[c][q];
+    a.cu_out[q] = ctx->st[nx_][q];
+  }
+  a.cp_in = ctx->st[c][3];
+  a.cp_out = ctx->st[nx_][3];
+  for (int n = 0; n < ctx->nth; ++n) {
+    a.cth_in[n] = ctx->st[c][4 + n];
+    a.cth_out[n] = ctx->st[nx_][4 + n];
+  }
+  for (int f = 0; f < ctx->nf; ++f) {
+    a.cf_in[f] = ctx->cf[ctx->cf_cur][f];
+    a.cf_out[f] = ctx->cf[1 - ctx->cf_cur][f];
+    if (ctx->precision == DIABLO_FP64) a.nl64[f] = (const double2*)ctx->nl[f];
+    else a.nl32[f] = (const float2*)ctx->nl[f];
+  }
+  a.store_cf = rk < 3 ? 1 : 0;
+  if ((rc = launch_solve(a, false, ctx->stream))) return rc;
+  ctx->launches++;
+  CK(cudaGetLastError());
+  ctx->cur = nx_;
+  if (a.store_cf) ctx->cf_cur = 1 - ctx->cf_cur;
+  return 0;
+}
+
+// ==========================================================================
+// C ABI
+extern "C" {
+
+int diablo_abi_version(void) { return DIABLO_ABI_VERSION; }
+
+const char* diablo_status_string(int s) {
+  switch (s) {
+    case DIABLO_OK: return "ok";
+    case DIABLO_ERR_ARG: return "invalid argument";
+    case DIABLO_ERR_SIZE: return "unsupported grid size";
+    case DIABLO_ERR_CUDA: return "CUDA runtime error";
+    case DIABLO_ERR_NONFINITE: return "non-finite value in state";
+    case DIABLO_ERR_TIMEOUT: return "bounded device wait timed out";
+    case DIABLO_ERR_UNSUPPORTED: return "option not supported on the device";
+    case DIABLO_ERR_STATE: return "state violates the layout contract";
+    case DIABLO_ERR_NOMEM: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+
+static int validate(const diablo_params* p) {
+  if (!p || p->struct_size != (int)sizeof(diablo_params)) return DIABLO_ERR_ARG;
+  if (p->nx < 8 || (p->nx % 2) || p->ny < 4 || p->nz < 8) return DIABLO_ERR_SIZE;
+  if (p->n_th < 0 || p->n_th > DIABLO_MAX_TH) return DIABLO_ERR_ARG;
+  int a, b;
+  if (!factor(p->nz, &a, &b) || !factor(p->nx / 2, &a, &b)) return DIABLO_ERR_SIZE;
+  if ((p->ny + 2 + 31) / 32 > 17) return DIABLO_ERR_SIZE;
+  if (!(p->re > 0) || !(p->delta_t > 0) || !(p->lx > 0) || !(p->lz > 0)) return DIABLO_ERR_ARG;
+  if (p->precision != DIABLO_FP64 && p->precision != DIABLO_MIXED) return DIABLO_ERR_ARG;
+  for (int n = 0; n < p->n_th; ++n)
+    if (!(p->pr[n] > 0)) return DIABLO_ERR_ARG;
+  return 0;
+}
+
+diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status) {
+  int dummy;
+  if (!status) status = &dummy;
+  *status = validate(p);
+  if (*status) return nullptr;
+  if (!gy) { *status = DIABLO_ERR_ARG; return nullptr; }
+  diablo_ctx* ctx = new diablo_ctx();  // value-initialised: scalars and pointers are zero
+  ctx->p = *p;
+  ctx->scratch_prec = -1;
+  ctx->nx = p->nx; ctx->ny = p->ny; ctx->nz = p->nz; ctx->nth = p->n_th;
+  ctx->nf = 3 + p->n_th;
+  ctx->nxp = p->nx / 2;
+  ctx->M = p->nx / 2;
+  ctx->nkx = p->nx / 3;
+  ctx->nkz = p->nz / 3;
+  ctx->nkx1 = ctx->nkx + 1;
+  ctx->nk2 = 2 * ctx->nkz + 1;
+  ctx->kp = ctx->nk2;
+  ctx->nyp2 = p->ny + 2;
+  ctx->g = Geom{ctx->nx, ctx->nz, ctx->nyp2, ctx->nkx1, ctx->nkz, ctx->nk2, ctx->kp};
+  ctx->nu = 1.0 / p->re;
+  ctx->ro_inv = isinf(p->ro) ? 0.0 : 1.0 / p->ro;
+  ctx->jstart = p->u_bc_ymin == 1 ? 1 : 2;
+  ctx->jend = p->ny;
+  for (int n = 0; n < p->n_th; ++n) {
+    ctx->jst[n] = p->th_bc_ymin[n] == 1 ? 1 : 2;
+    ctx->jet[n] = p->ny;
+  }
+  ctx->delta_t = p->delta_t;
+  for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * p->delta_t;
+  ctx->w_top_transient = p->w_bc_ymax_c1;
+  ctx->precision = p->precision;
+  int rc = 0;
+#define FAIL(code) do { *status = (code); diablo_destroy(ctx); return nullptr; } while (0)
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    FAIL(DIABLO_ERR_CUDA);
+  }
+  ctx->stream = ctx->own_stream;
+  // grid metrics exactly as ReadGridHDF5 / create_grid_chan (for/domain.f90:230-248,501-527)
+  const int ny = p->ny;
+  std::vector<double> hgy(ny + 2, 0.0), hgyf(ny + 2, 0.0), hdy(ny + 2, 0.0), hdyf(ny + 2, 0.0);
+  for (int j = 1; j <= ny + 1; ++j) hgy[j] = gy[j - 1];
+  for (int j = 1; j <= ny; ++j) hgyf[j] = 0.5 * (hgy[j] + hgy[j + 1]);
+  hgyf[0] = 2.0 * hgyf[1] - hgyf[2];
+  hgyf[ny + 1] = 2.0 * hgyf[ny] - hgyf[ny - 1];
+  for (int j = 1; j <= ny + 1; ++j) hdy[j] = hgyf[j] - hgyf[j - 1];
+  for (int j = 1; j <= ny; ++j) hdyf[j] = hgy[j + 1] - hgy[j];
+  hdyf[0] = hdyf[1];
+  hdyf[ny + 1] = hdyf[ny];
+  for (int j = 1; j <= ny + 1; ++j)
+    if (!(hdy[j] > 0) || (j <= ny && !(hdyf[j] > 0))) FAIL(DIABLO_ERR_ARG);
+  ctx->h_gy = hgy; ctx->h_gyf = hgyf; ctx->h_dy = hdy; ctx->h_dyf = hdyf;
+  // wavenumbers (init_fft, for/fft.f90:213-230), with the reference's float32 pi
+  std::vector<double> hkx(ctx->nkx1), hkz(ctx->nk2);
+  for (int i = 0; i < ctx->nkx1; ++i) hkx[i] = i * (2. * PI_REF) / p->lx;
+  for (int k = 0; k <= ctx->nkz; ++k) hkz[k] = k * (2. * PI_REF) / p->lz;
+  for (int k = 1; k <= ctx->nkz; ++k) hkz[2 * ctx->nkz + 1 - k] = -k * (2. * PI_REF) / p->lz;
+  auto up = [&](double** d, const std::vector<double>& h) -> int {
+    int r = dev_alloc(ctx, (void**)d, h.size() * sizeof(double));
+    if (r) return r;
+    if (cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess) return DIABLO_ERR_CUDA;
+    return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? 0 : DIABLO_ERR_CUDA;
+  };
+  if ((rc = up(&ctx->d_gy, hgy)) || (rc = up(&ctx->d_gyf, hgyf)) || (rc = up(&ctx->d_dy, hdy)) ||
+      (rc = up(&ctx->d_dyf, hdyf)) || (rc = up(&ctx->d_kx, hkx)) || (rc = up(&ctx->d_kz, hkz)))
+    FAIL(rc);
+  if ((rc = upload_tw(ctx, ctx->nz, ctx->nz, &ctx->tz64, &ctx->tz32)) ||
+      (rc = upload_tw(ctx, ctx->M, ctx->M, &ctx->tm64, &ctx->tm32)) ||
+      (rc = upload_tw(ctx, ctx->nx, ctx->M + 1, &ctx->tx64, &ctx->tx32)))
+    FAIL(rc);
+  for (int b = 0; b < 2; ++b) {
+    for (int f = 0; f < 4 + ctx->nth; ++f)
+      if ((rc = dev_alloc(ctx, (void**)&ctx->st[b][f], four_elems(ctx) * sizeof(double2)))) FAIL(rc);
+    for (int f = 0; f < ctx->nf; ++f)
+      if ((rc = dev_alloc(ctx, (void**)&ctx->cf[b][f], four_elems(ctx) * sizeof(double2)))) FAIL(rc);
+  }
+  if ((rc = dev_alloc(ctx, (void**)&ctx->d_flag, sizeof(int)))) FAIL(rc);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) FAIL(DIABLO_ERR_CUDA);
+#undef FAIL
+  *status = 0;
+  return ctx;
+}
+
+int diablo_destroy(diablo_ctx* ctx) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  cudaGetLastError();
+  delete ctx;
+  return 0;
+}
+
+static int field_index(const diablo_ctx* ctx, int field) {
+  if (field >= DIABLO_U1 && field <= DIABLO_P) return field;
+  if (field >= DIABLO_TH && field < DIABLO_TH + ctx->nth) return field;
+  return -1;
+}
+
+// copy a reference-size buffer to device scratch (or use it in place)
+static int stage_in(diablo_ctx* ctx, const double* buf, const double** dev) {
+  if (is_device_ptr(buf)) { *dev = buf; return 0; }
+  CK(cudaMemcpyAsync(ctx->b_ref, buf, ref_doubles(ctx) * sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  *dev = ctx->b_ref;
+  return 0;
+}
+
+int diablo_upload_state(diablo_ctx* ctx, int field, const double* buf, int layout) {
+  if (!ctx || !buf) return DIABLO_ERR_ARG;
+  int fi = field_index(ctx, field);
+  if (fi < 0) return DIABLO_ERR_ARG;
+  int rc = ensure_bscratch(ctx);
+  if (rc) return rc;
+  const double* dref;
+  if ((rc = stage_in(ctx, buf, &dref))) return rc;
+  double2* dst = ctx->st[ctx->cur][fi];
+  if (layout == DIABLO_LAYOUT_FOURIER) {
+    CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+    size_t tot = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
+    k_ref_to_four<<<grid1d(tot), 256, 0, ctx->stream>>>((const double2*)dref, dst, ctx->g, ctx->nxp,
+                                                         ctx->d_flag);
+    ctx->launches++;
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (bad) return DIABLO_ERR_STATE;
+  } else if (layout == DIABLO_LAYOUT_PHYSICAL) {
+    k_ref_to_phys<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(dref, ctx->b_phys, ctx->nx,
+                                                                    ctx->nz, ctx->nyp2);
+    ctx->launches++;
+    if ((rc = fwd_phys_to_four(ctx, ctx->b_phys, ctx->b_xs, dst))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+  } else {
+    return DIABLO_ERR_ARG;
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout) {
+  if (!ctx || !buf) return DIABLO_ERR_ARG;
+  int fi = field_index(ctx, field);
+  if (fi < 0) return DIABLO_ERR_ARG;
+  int rc = ensure_bscratch(ctx);
+  if (rc) return rc;
+  const bool dev = is_device_ptr(buf);
+  double* dref = dev ? buf : ctx->b_ref;
+  const double2* src = ctx->st[ctx->cur][fi];
+  if (layout == DIABLO_LAYOUT_FOURIER) {
+    size_t tot = (size_t)ctx->nyp2 * (ctx->nz + 2) * (ctx->nxp + 1);
+    k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(src, (double2*)dref, ctx->g, ctx->nxp);
+    ctx->launches++;
+  } else if (layout == DIABLO_LAYOUT_PHYSICAL) {
+    if ((rc = inv_four_to_phys(ctx, src, ctx->b_xs, ctx->b_phys))) return rc;
+    k_phys_to_ref<<<grid1d(ref_doubles(ctx)), 256, 0, ctx->stream>>>(ctx->b_phys, dref, ctx->nx,
+                                                                     ctx->nz, ctx->nyp2);
+    ctx->launches++;
+  } else {
+    return DIABLO_ERR_ARG;
+  }
+  if (!dev)
+    CK(cudaMemcpyAsync(buf, dref, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_fft_xz_to_fourier(diablo_ctx* ctx, const double* v, double* vv) {
+  if (!ctx || !v || !vv) return DIABLO_ERR_ARG;
+  int rc = ensure_bscratch(ctx);
+  if (rc) return rc;
+  const double* dref;
+  if ((rc = stage_in(ctx, v, &dref))) return rc;
+  k_ref_to_phys<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(dref, ctx->b_phys, ctx->nx,
+                                                                  ctx->nz, ctx->nyp2);
+  ctx->launches++;
+  if ((rc = fwd_phys_to_four(ctx, ctx->b_phys, ctx->b_xs, ctx->b_four))) return rc;
+  const bool dev = is_device_ptr(vv);
+  double* out = dev ? vv : ctx->b_ref;
+  size_t tot = (size_t)ctx->nyp2 * (ctx->nz + 2) * (ctx->nxp + 1);
+  k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->b_four, (double2*)out, ctx->g, ctx->nxp);
+  ctx->launches++;
+  if (!dev)
+    CK(cudaMemcpyAsync(vv, out, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_fft_xz_to_physical(diablo_ctx* ctx, double* vv, double* v) {
+  if (!ctx || !v || !vv) return DIABLO_ERR_ARG;
+  int rc = ensure_bscratch(ctx);
+  if (rc) return rc;
+  const double* dref;
+  if ((rc = stage_in(ctx, vv, &dref))) return rc;
+  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  size_t tin = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
+  // modes above Nkx are zeroed by the reference before the x transform
+  // (for/fft.f90:372-378); the flag is ignored here
+  k_ref_to_four<<<grid1d(tin), 256, 0, ctx->stream>>>((const double2*)dref, ctx->b_four, ctx->g,
+                                                       ctx->nxp, ctx->d_flag);
+  ctx->launches++;
+  if ((rc = inv_four_to_phys(ctx, ctx->b_four, ctx->b_xs, ctx->b_phys))) return rc;
+  const bool dev = is_device_ptr(v);
+  double* out = dev ? v : ctx->b_ref;
+  k_phys_to_ref<<<grid1d(ref_doubles(ctx)), 256, 0, ctx->stream>>>(ctx->b_phys, out, ctx->nx,
+                                                                   ctx->nz, ctx->nyp2);
+  ctx->launches++;
+  if (!dev)
+    CK(cudaMemcpyAsync(v, out, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_rk_substep(diablo_ctx* ctx, int rk_step) {
+  if (!ctx || rk_step < 1 || rk_step > 3) return DIABLO_ERR_ARG;
+  return substep(ctx, rk_step);
+}
+
+int diablo_step(diablo_ctx* ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return DIABLO_ERR_ARG;
+  if (ctx->p.variable_dt) return DIABLO_ERR_UNSUPPORTED;
+  for (int s = 0; s < nsteps; ++s) {
+    ctx->time_step += 1;
+    for (int rk = 1; rk <= 3; ++rk) {
+      int rc = substep(ctx, rk);
+      if (rc) return rc;
+    }
+    ctx->time += ctx->delta_t;
+  }
+  return 0;
+}
+
+static int bc_post(diablo_ctx* ctx, int do_vel, int do_th) {
+  const diablo_params& p = ctx->p;
+  update_transient(ctx);
+  BcPostArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int q = 0; q < 3; ++q) a.cu[q] = ctx->st[ctx->cur][q];
+  for (int n = 0; n < ctx->nth; ++n) {
+    a.cth[n] = ctx->st[ctx->cur][4 + n];
+    a.thbc[n][0] = p.th_bc_ymin[n];
+    a.thbc[n][1] = p.th_bc_ymax[n];
+    a.thc1[n][0] = p.th_bc_ymin_c1[n];
+    a.thc1[n][1] = p.th_bc_ymax_c1[n];
+  }
+  a.nth = ctx->nth;
+  a.nyp = ctx->ny;
+  a.nkx1 = ctx->nkx1;
+  a.nk2 = ctx->nk2;
+  a.kp = ctx->kp;
+  a.ubc[0] = p.u_bc_ymin; a.ubc[1] = p.u_bc_ymax;
+  a.vbc[0] = p.v_bc_ymin; a.vbc[1] = p.v_bc_ymax;
+  a.wbc[0] = p.w_bc_ymin; a.wbc[1] = p.w_bc_ymax;
+  a.uc1[0] = p.u_bc_ymin_c1; a.uc1[1] = p.u_bc_ymax_c1;
+  a.vc1[0] = p.v_bc_ymin_c1; a.vc1[1] = p.v_bc_ymax_c1;
+  a.wc1[0] = p.w_bc_ymin_c1;
+  a.wc1[1] = p.w_bc_ymax == 0 ? p.w_bc_ymax_c1 : ctx->w_top_transient;
+  a.dy = ctx->d_dy;
+  a.dyf = ctx->d_dyf;
+  a.do_vel = do_vel;
+  a.do_th = do_th;
+  int tot = ctx->nkx1 * ctx->nk2;
+  k_bc_post<<<(tot + 127) / 128, 128, 0, ctx->stream>>>(a);
+  ctx->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_apply_bc_post(diablo_ctx* ctx) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  return bc_post(ctx, 1, 1);
+}
+
+int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  if (compute_pressure || ctx->p.variable_dt) return DIABLO_ERR_UNSUPPORTED;
+  // pre_first_step applies the velocity wall values only (for/advance.f90:25)
+  int rc = bc_post(ctx, 1, 0);
+  if (rc) return rc;
+  SolveArgs a;
+  fill_solve_args(ctx, a, 1);
+  for (int q = 0; q < 3; ++q) a.cu_out[q] = ctx->st[ctx->cur][q];
+  if ((rc = launch_solve(a, true, ctx->stream))) return rc;
+  ctx->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_set_precision(diablo_ctx* ctx, int precision) {
+  if (!ctx || (precision != DIABLO_FP64 && precision != DIABLO_MIXED)) return DIABLO_ERR_ARG;
+  if (ctx->scratch_prec >= 0 && ctx->scratch_prec != precision) {
+    // release step scratch sized for the other precision
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int f = 0; f < ctx->nf; ++f) {
+      for (void** pp : {&ctx->nl[f], &ctx->phys[f]}) {
+        for (size_t i = 0; i < ctx->allocs.size(); ++i)
+          if (ctx->allocs[i] == *pp) { ctx->allocs.erase(ctx->allocs.begin() + i); break; }
+        cudaFree(*pp);
+        *pp = nullptr;
+      }
+    }
+    for (int f = 0; f < 2 * ctx->nf; ++f) {
+      for (size_t i = 0; i < ctx->allocs.size(); ++i)
+        if (ctx->allocs[i] == ctx->xs[f]) { ctx->allocs.erase(ctx->allocs.begin() + i); break; }
+      cudaFree(ctx->xs[f]);
+      ctx->xs[f] = nullptr;
+    }
+    ctx->scratch_prec = -1;
+  }
+  ctx->precision = precision;
+  ctx->p.precision = precision;
+  return 0;
+}
+
+int diablo_get_time(diablo_ctx* ctx, double* time, int* time_step, double* delta_t) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  if (time) *time = ctx->time;
+  if (time_step) *time_step = ctx->time_step;
+  if (delta_t) *delta_t = ctx->delta_t;
+  return 0;
+}
+
+int diablo_set_time(diablo_ctx* ctx, double time, int time_step, double delta_t) {
+  if (!ctx || !(delta_t > 0)) return DIABLO_ERR_ARG;
+  ctx->time = time;
+  ctx->time_step = time_step;
+  ctx->delta_t = delta_t;
+  for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * delta_t;
+  return 0;
+}
+
+int diablo_set_stream(diablo_ctx* ctx, void* stream) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return 0;
+}
+
+int diablo_synchronize(diablo_ctx* ctx) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_check_finite(diablo_ctx* ctx) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  for (int f = 0; f < 4 + ctx->nth; ++f) {
+    k_check_finite<<<grid1d(four_elems(ctx)), 256, 0, ctx->stream>>>(ctx->st[ctx->cur][f], ctx->g,
+                                                                      ctx->d_flag);
+    ctx->launches++;
+  }
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return bad ? DIABLO_ERR_NONFINITE : 0;
+}
+
+long long diablo_kernel_launches(const diablo_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

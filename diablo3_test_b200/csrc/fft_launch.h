@@ -1,0 +1,16 @@
+// Declarations of the xz-FFT launchers (defined in fft_launch.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "kernels_fft.cuh"
+
+// supported transform lengths N = N1*N2 (N1, N2 register-DFT sizes)
+bool factor(int n, int* n1, int* n2);
+
+template <typename C>
+int launch_zinv(const ZInvArgs<C>& a, int nz, int nfield, cudaStream_t s);
+template <typename C, typename CO, bool COMB>
+int launch_zfwd(const ZFwdArgs<C, CO>& a, int nz, int nfield, cudaStream_t s);
+template <typename C>
+int launch_xinv(const XInvArgs<C>& a, int m, int nplanes, int nfield, cudaStream_t s);
+template <typename T, bool NL>
+int launch_xfwd(const XFwdArgs<T>& a, int m, int nplanes, int nfield, cudaStream_t s);

@@ -1,0 +1,372 @@
+// xz-FFT kernels of the channel step.
+//
+// Internal layouts (all contiguous, x or k fastest):
+//   physical  P[j][k][i]          (Ny+2) x Nz x Nx reals
+//   x-spectral X[j][m][k]          m in [0, Nkx], k in [0, Nz)      complex
+//   Fourier    F[j][m][kp]         m in [0, Nkx], kp in [0, 2Nkz]   complex, pitch KP
+// The x-spectral layout keeps z contiguous so the z transforms read and write
+// whole columns; the x transforms move tiles of KT z-rows through shared memory
+// so both sides stay coalesced.  Together the two kernels of a direction are
+// the reference's x-FFT + dealias + MPI_Alltoall repack + z-FFT + pack
+// (for/fft.f90:247-382): modes Nkx < m <= Nx/2 are never stored (they are the
+// zeroed ones, :264-266 and :372-378) and the dealiased z band is never stored
+// (the pack/unpack of :307-312 and :329-340 is the kp <-> k index map).
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+#define NF_MAX 12  // 3 velocities + up to DIABLO_MAX_TH scalars + spare
+
+struct Geom {
+  int nx, nz, nyp2;   // Nx, Nz, Ny+2
+  int nkx1;           // Nkx+1 stored x modes
+  int nkz, nk2, kp;   // Nkz, 2Nkz+1, Fourier pitch (>= nk2)
+};
+
+// packed Fourier index kp of the z-mode k in [0, Nz), or -1 in the dealiased band
+HDI int z_pack(int k, int nz, int nkz) {
+  return k <= nkz ? k : (k >= nz - nkz ? k - nz + 2 * nkz + 1 : -1);
+}
+
+// --------------------------------------------------------------------------
+// z inverse: Fourier (packed, double2) -> x-spectral (C), one column per N2 threads
+template <typename C> struct ZInvArgs {
+  const double2* src[NF_MAX];
+  C* dst[NF_MAX];
+  int q0, nseq;      // first (j, m) column and number of columns
+  Geom g;
+  const C* tw;       // exp(-2 pi i m / Nz)
+};
+
+template <typename C, int N1, int N2, int S>
+__global__ void __launch_bounds__(N2* S) k_zinv(ZInvArgs<C> a) {
+  __shared__ C sm[S][dfft::SmemSize<N1, N2>::v];
+  const int t = threadIdx.x, s = threadIdx.y;
+  const int q = blockIdx.x * S + s;
+  const int f = blockIdx.y;
+  const bool ok = q < a.nseq;
+  const double2* src = a.src[f] + (size_t)(a.q0 + q) * a.g.kp;
+  C v[N1];
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    int kp = z_pack(n1 * N2 + t, a.g.nz, a.g.nkz);
+    v[n1] = (ok && kp >= 0) ? cvt<C>(src[kp]) : czero<C>();
+  }
+  dfft::step1<N1, N2, +1>(v, t, a.tw, sm[s]);
+  __syncthreads();
+  if (!ok) return;
+  C* dst = a.dst[f] + (size_t)(a.q0 + q) * a.g.nz;
+  for (int k1 = t; k1 < N1; k1 += N2) {
+    C u[N2];
+    dfft::step2<N1, N2, +1>(u, k1, sm[s]);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) dst[k1 + N1 * k2] = u[k2];
+  }
+}
+
+// --------------------------------------------------------------------------
+// z forward: x-spectral -> Fourier (packed).
+//   plain:   out[kp] = X^[k] / Nz                        (for/fft.f90:298-313)
+//   combine: out[kp] = (i kz(kp) A^[k] + B^[k]) / Nz     (the sum of one
+//            momentum/scalar equation's nonlinear terms, for/channel.f90:299-459)
+template <typename C, typename CO> struct ZFwdArgs {
+  const C* srcA[NF_MAX];
+  const C* srcB[NF_MAX];   // null for the plain transform
+  CO* dst[NF_MAX];
+  int q0, nseq;
+  Geom g;
+  const C* tw;
+  const double* kz;        // wavenumbers kz(kp), length nk2
+  double scale;            // 1/Nz
+};
+
+template <typename C, typename CO, int N1, int N2, int S, bool COMBINE>
+__global__ void __launch_bounds__(N2* S) k_zfwd(ZFwdArgs<C, CO> a) {
+  typedef typename CReal<C>::R T;
+  __shared__ C sm[S][dfft::SmemSize<N1, N2>::v];
+  const int t = threadIdx.x, s = threadIdx.y;
+  const int q = blockIdx.x * S + s;
+  const int f = blockIdx.y;
+  const bool ok = q < a.nseq;
+  constexpr int NR = (N1 + N2 - 1) / N2;  // step-2 rows per thread
+  C ra[NR][N2];
+  const T sc = (T)a.scale;
+  // transform A
+  {
+    const C* src = a.srcA[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? src[n1 * N2 + t] : czero<C>();
+    dfft::step1<N1, N2, -1>(v, t, a.tw, sm[s]);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      int k1 = t + r * N2;
+      if (k1 < N1) dfft::step2<N1, N2, -1>(ra[r], k1, sm[s]);
+    }
+  }
+  if (COMBINE) {
+    __syncthreads();
+    const C* src = a.srcB[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? src[n1 * N2 + t] : czero<C>();
+    dfft::step1<N1, N2, -1>(v, t, a.tw, sm[s]);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      int k1 = t + r * N2;
+      if (k1 < N1) {
+        C u[N2];
+        dfft::step2<N1, N2, -1>(u, k1, sm[s]);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          int kp = z_pack(k1 + N1 * k2, a.g.nz, a.g.nkz);
+          T kzv = kp >= 0 ? (T)a.kz[kp] : (T)0;
+          ra[r][k2] = mul_ik(kzv, ra[r][k2]) + u[k2];
+        }
+      }
+    }
+  }
+  if (!ok) return;
+  CO* dst = a.dst[f] + (size_t)(a.q0 + q) * a.g.kp;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    int k1 = t + r * N2;
+    if (k1 < N1) {
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        int kp = z_pack(k1 + N1 * k2, a.g.nz, a.g.nkz);
+        if (kp >= 0) dst[kp] = cvt<CO>(sc * ra[r][k2]);
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// x inverse (c2r): x-spectral -> physical rows, KT z-rows per block.
+// Length-Nx real transform as a length-M=Nx/2 complex transform with the
+// standard even/odd split; only Re X[0] enters (FFTW c2r ignores Im of the
+// DC and Nyquist bins), and X[m] = 0 for Nkx < m <= M (for/fft.f90:372-378).
+template <typename C> struct XInvArgs {
+  const C* src[NF_MAX];
+  typename CReal<C>::R* dst[NF_MAX];
+  int j0;            // first plane
+  Geom g;
+  const C* twM;      // exp(-2 pi i m / M), m < M
+  const C* twX;      // exp(-2 pi i m / Nx), m <= M
+};
+
+template <typename C, int N1, int N2, int KT>
+__global__ void __launch_bounds__(N2* KT) k_xc2r(XInvArgs<C> a) {
+  typedef typename CReal<C>::R T;
+  constexpr int M = N1 * N2;
+  constexpr int SM = dfft::SmemSize<N1, N2>::v;
+  __shared__ C xs[KT][M + 1];
+  __shared__ C sm[KT][SM];
+  const int t = threadIdx.x, r = threadIdx.y;
+  const int tid = r * N2 + t;
+  const int k0 = blockIdx.x * KT;
+  const int j = a.j0 + blockIdx.y;
+  const int f = blockIdx.z;
+  const int nkx1 = a.g.nkx1, nz = a.g.nz;
+  const C* src = a.src[f] + (size_t)j * nkx1 * nz;
+  for (int idx = tid; idx < KT * (M + 1); idx += N2 * KT) {
+    int rr = idx % KT, m = idx / KT;
+    C val = czero<C>();
+    if (m < nkx1 && k0 + rr < nz) val = src[(size_t)m * nz + k0 + rr];
+    xs[rr][m] = val;
+  }
+  __syncthreads();
+  C v[N1];
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    int m = n1 * N2 + t;
+    C xm = xs[r][m];
+    C xc = conj(xs[r][M - m]);  // m == 0 reads X[M] = 0
+    if (m == 0) xm.y = 0;
+    C e = xm + xc;
+    C o = xm - xc;
+    C w = conj(a.twX[m]);           // exp(+2 pi i m / Nx)
+    v[n1] = e + mul_i(cmul(w, o));
+  }
+  dfft::step1<N1, N2, +1>(v, t, a.twM, sm[r]);
+  __syncthreads();
+  if (k0 + r >= nz) return;
+  T* dst = a.dst[f] + ((size_t)j * nz + k0 + r) * a.g.nx;
+  C* dstc = reinterpret_cast<C*>(dst);
+  for (int k1 = t; k1 < N1; k1 += N2) {
+    C u[N2];
+    dfft::step2<N1, N2, +1>(u, k1, sm[r]);
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) dstc[k1 + N1 * k2] = u[k2];
+  }
+}
+
+// --------------------------------------------------------------------------
+// x forward (r2c) of physical rows, KT z-rows per block, optionally of the
+// nonlinear products of the channel step.
+//   plain: out0 = X / Nx for m <= Nkx (for/fft.f90:258-266)
+//   NL:    for output equation f the products (A: needs d/dz, Bx: needs d/dx,
+//          B0: already a y-difference) give outA = Fx(A)/Nx and
+//          outB = (i kx Fx(Bx) + Fx(B0))/Nx.
+struct GridMetrics {
+  const double* dy;
+  const double* dyf;
+};
+
+template <typename T> struct XFwdArgs {
+  const T* in[NF_MAX];           // plain: field to transform; NL: u1,u2,u3,th_n
+  typename CT<T>::C* outA[NF_MAX];
+  typename CT<T>::C* outB[NF_MAX];
+  int j0;
+  Geom g;
+  const typename CT<T>::C* twM;
+  const typename CT<T>::C* twX;
+  const double* kx;              // kx(m)
+  GridMetrics gm;
+  double scale;                  // 1/Nx
+};
+
+// value pair of term q of equation f at (j, row, x = 2n, 2n+1)
+template <typename T> struct Pair { T a, b; };
+
+template <typename T>
+DI Pair<T> ld2(const T* p) {
+  typedef typename CT<T>::C C;
+  C v = *reinterpret_cast<const C*>(p);
+  return Pair<T>{v.x, v.y};
+}
+
+template <typename T>
+DI Pair<T> nl_term(const XFwdArgs<T>& a, int f, int q, int j, size_t off, size_t ps) {
+  // off = offset of (j, row, 2n) in a plane-major field; ps = plane stride
+  const T* u1 = a.in[0];
+  const T* u2 = a.in[1];
+  const T* u3 = a.in[2];
+  Pair<T> r;
+  if (f == 0 || f == 2) {
+    const T* uf = f == 0 ? u1 : u3;
+    if (q == 0) {  // f=0: u3*u1 (d/dz);  f=2: u3*u3 (d/dz)
+      Pair<T> x = ld2(u3 + off), y = ld2(uf + off);
+      r.a = x.a * y.a; r.b = x.b * y.b;
+    } else if (q == 1) {  // f=0: u1*u1 (d/dx);  f=2: u3*u1 (d/dx)
+      Pair<T> x = ld2(f == 0 ? u1 + off : u3 + off), y = ld2(u1 + off);
+      r.a = x.a * y.a; r.b = x.b * y.b;
+    } else {  // (uf(j+1)u2(j+1) + uf(j)u2(j+1) - uf(j)u2(j) - uf(j-1)u2(j)) / (2 dyf(j))
+      Pair<T> p = ld2(uf + off + ps), c = ld2(uf + off), m = ld2(uf + off - ps);
+      Pair<T> vp = ld2(u2 + off + ps), vc = ld2(u2 + off);
+      T den = (T)(2.0 * a.gm.dyf[j]);
+      r.a = (p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den;
+      r.b = (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den;
+    }
+  } else if (f == 1) {
+    if (q <= 1) {  // q=0: u3 interp * u2 (d/dz);  q=1: u1 interp * u2 (d/dx)
+      const T* uf = q == 0 ? u3 : u1;
+      Pair<T> c = ld2(uf + off), m = ld2(uf + off - ps), v = ld2(u2 + off);
+      T dyfj = (T)a.gm.dyf[j], dyfm = (T)a.gm.dyf[j - 1], den = (T)(2.0 * a.gm.dy[j]);
+      r.a = ((dyfj * c.a + dyfm * m.a) / den) * v.a;
+      r.b = ((dyfj * c.b + dyfm * m.b) / den) * v.b;
+    } else {  // (0.25(u2(j)+u2(j+1))^2 - 0.25(u2(j)+u2(j-1))^2) / dy(j)
+      Pair<T> p = ld2(u2 + off + ps), c = ld2(u2 + off), m = ld2(u2 + off - ps);
+      T dyj = (T)a.gm.dy[j];
+      T sa = c.a + p.a, sb = c.b + p.b, da = c.a + m.a, db = c.b + m.b;
+      r.a = ((T)0.25 * (sa * sa) - (T)0.25 * (da * da)) / dyj;
+      r.b = ((T)0.25 * (sb * sb) - (T)0.25 * (db * db)) / dyj;
+    }
+  } else {
+    const T* th = a.in[f];
+    if (q == 0) {  // th*u3 (d/dz)
+      Pair<T> x = ld2(th + off), y = ld2(u3 + off);
+      r.a = x.a * y.a; r.b = x.b * y.b;
+    } else if (q == 1) {  // th*u1 (d/dx)
+      Pair<T> x = ld2(th + off), y = ld2(u1 + off);
+      r.a = x.a * y.a; r.b = x.b * y.b;
+    } else {
+      Pair<T> p = ld2(th + off + ps), c = ld2(th + off), m = ld2(th + off - ps);
+      Pair<T> vp = ld2(u2 + off + ps), vc = ld2(u2 + off);
+      T den = (T)(2.0 * a.gm.dyf[j]);
+      r.a = (p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den;
+      r.b = (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den;
+    }
+  }
+  return r;
+}
+
+template <typename T, int N1, int N2, int KT, bool NL>
+__global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
+  typedef typename CT<T>::C C;
+  constexpr int M = N1 * N2;
+  constexpr int SM = dfft::SmemSize<N1, N2>::v;
+  constexpr int NS = N1;  // output slots per thread (m = t + s*N2 <= Nkx < M)
+  __shared__ C sm[KT][SM];
+  __shared__ C zs[KT][M + 1];
+  const int t = threadIdx.x, r = threadIdx.y;
+  const int k0 = blockIdx.x * KT;
+  const int j = a.j0 + blockIdx.y;
+  const int f = blockIdx.z;
+  const int nz = a.g.nz, nx = a.g.nx, nkx1 = a.g.nkx1;
+  const int row = min(k0 + r, nz - 1);
+  const size_t ps = (size_t)nz * nx;
+  const size_t rowoff = (size_t)j * ps + (size_t)row * nx;
+  const T sc = (T)a.scale;
+  C accA[NS], accB[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) { accA[s] = czero<C>(); accB[s] = czero<C>(); }
+  constexpr int NQ = NL ? 3 : 1;
+  for (int q = 0; q < NQ; ++q) {
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      int n = n1 * N2 + t;
+      if (NL) {
+        Pair<T> pr = nl_term<T>(a, f, q, j, rowoff + 2 * n, ps);
+        v[n1] = CT<T>::mk(pr.a, pr.b);
+      } else {
+        v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * n);
+      }
+    }
+    dfft::step1<N1, N2, -1>(v, t, a.twM, sm[r]);
+    __syncthreads();
+    for (int k1 = t; k1 < N1; k1 += N2) {
+      C u[N2];
+      dfft::step2<N1, N2, -1>(u, k1, sm[r]);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) zs[r][k1 + N1 * k2] = u[k2];
+    }
+    if (t == 0) zs[r][M] = zs[r][0];
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      int m = t + s * N2;
+      if (m < nkx1) {
+        C zm = zs[r][m], zc = conj(zs[r][M - m]);
+        C e = (T)0.5 * (zm + zc);
+        C o = (T)0.5 * (zm - zc);
+        C x = e - mul_i(cmul(a.twX[m], o));
+        x = sc * x;
+        if (!NL || q == 0) accA[s] = x;
+        else if (q == 1) accB[s] = mul_ik((T)a.kx[m], x);
+        else accB[s] = accB[s] + x;
+      }
+    }
+    __syncthreads();
+  }
+  // transpose through shared memory so that stores run along k
+  C* os = &sm[0][0];  // reuse: [m][KT+1]
+  const int OP = KT + 1;
+  for (int pass = 0; pass < (NL ? 2 : 1); ++pass) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      int m = t + s * N2;
+      if (m < nkx1) os[m * OP + r] = pass == 0 ? accA[s] : accB[s];
+    }
+    __syncthreads();
+    C* dst = (pass == 0 ? a.outA[f] : a.outB[f]) + (size_t)j * nkx1 * nz;
+    for (int idx = r * N2 + t; idx < nkx1 * KT; idx += N2 * KT) {
+      int rr = idx % KT, m = idx / KT;
+      if (k0 + rr < nz) dst[(size_t)m * nz + k0 + rr] = os[m * OP + rr];
+    }
+    __syncthreads();
+  }
+}

@@ -1,0 +1,100 @@
+"""Seeded synthetic initial conditions for the benchmark configurations.
+
+The reference builds its initial fields in physical space (``for/ics.f90``)
+and reads/writes them through ``start.h5``; neither is part of the step.  The
+configurations here are the synthetic stand-ins the step is measured on.  Every
+function returns physical fields in the reference layout (numpy shape
+``(Ny+2, Nz+2, Nx+2)``, index ``[j, k, i]``) that a caller uploads with
+``LAYOUT_PHYSICAL`` and then projects with ``pre_first_step``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .config import ChannelParams
+from .grid import create_grid, metrics, TANH_ENDS_SYMMETRIC
+
+
+def _empty(p: ChannelParams):
+    return np.zeros((p.ny + 2, p.nz + 2, p.nx + 2))
+
+
+def _noise(rng, p: ChannelParams, amp, damp):
+    """Gaussian noise with its plane mean removed, scaled by amp*damp(y)."""
+    f = _empty(p)
+    n = rng.standard_normal((p.ny + 2, p.nz, p.nx))
+    n -= n.mean(axis=(1, 2), keepdims=True)
+    f[:, :p.nz, :p.nx] = amp * damp[:, None, None] * n
+    return f
+
+
+def laminar_dns(p: ChannelParams, gy, seed: int = 1, amp: float = 0.01):
+    """Laminar parabola u1 = 1.5(1 - y^2) plus seeded Gaussian noise of
+    amplitude ``amp`` (plane mean removed) and scalar th_n = y."""
+    _, gyf, _, _ = metrics(gy)
+    rng = np.random.default_rng(seed)
+    y = gyf
+    fields = {}
+    ones = np.ones_like(y)
+    u1 = _noise(rng, p, amp, ones)
+    u1[:, :p.nz, :p.nx] += (1.5 * (1.0 - y ** 2))[:, None, None]
+    fields["u1"] = u1
+    fields["u2"] = _noise(rng, p, amp, ones)
+    fields["u3"] = _noise(rng, p, amp, ones)
+    for n in range(p.n_th):
+        t = _empty(p)
+        t[:, :p.nz, :p.nx] = y[:, None, None]
+        fields[f"th{n}"] = t
+    return fields
+
+
+def log_law_turbulent(p: ChannelParams, gy, seed: int = 2, amp: float = 0.1, re_tau: float = 180.0):
+    """Log-law mean (u+ = y+ below y+ = 11, (1/0.41) ln y+ + 5.2 above) in
+    wall units with u_tau = 1, plus seeded random perturbations of ``amp``
+    times the centreline velocity, damped to zero at the walls; the projection
+    in ``pre_first_step`` makes them divergence-free.  Scalars: th_0 = y,
+    th_n = y^2 (n >= 1), each with 1% noise."""
+    _, gyf, _, _ = metrics(gy)
+    rng = np.random.default_rng(seed)
+    y = gyf
+    yp = np.clip((1.0 - np.abs(y)) * re_tau, 0.0, None)
+    with np.errstate(divide="ignore"):
+        ulog = np.where(yp < 11.0, yp, np.log(np.maximum(yp, 1e-30)) / 0.41 + 5.2)
+    ucl = float(ulog.max())
+    damp = np.clip(1.0 - y ** 2, 0.0, None)
+    fields = {}
+    u1 = _noise(rng, p, amp * ucl, damp)
+    u1[:, :p.nz, :p.nx] += ulog[:, None, None]
+    fields["u1"] = u1
+    fields["u2"] = _noise(rng, p, amp * ucl, damp)
+    fields["u3"] = _noise(rng, p, amp * ucl, damp)
+    for n in range(p.n_th):
+        t = _noise(rng, p, 0.01, damp)
+        t[:, :p.nz, :p.nx] += (y if n == 0 else y ** 2)[:, None, None]
+        fields[f"th{n}"] = t
+    return fields
+
+
+def config_c1(n_th: int = 1):
+    """Plain FP64 DNS: 64 x 193 x 32, Lx = 2pi, Lz = pi, tanh 1.8, Re = 1000,
+    Pr = 1, no-slip walls, zero-flux scalar, dt = 1e-3."""
+    p = ChannelParams.with_scalars(
+        n_th, nx=64, ny=193, nz=32, lx=2 * math.pi, lz=math.pi, ly=2.0, re=1000.0,
+        delta_t=1e-3, grav_y=1.0, pr=[1.0] * n_th)
+    gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 1.8)
+    return p, gy
+
+
+def config_c2(precision: int = 0):
+    """Turbulent channel at Re_tau = 180: 256 x 257 x 256, Lx = 4pi, Lz = 2pi,
+    tanh 2.0, two passive scalars (Pr = 0.71, 1.0), constant pressure gradient
+    px0 = -1 (f_type 1), dt = 5e-4."""
+    p = ChannelParams.with_scalars(
+        2, nx=256, ny=257, nz=256, lx=4 * math.pi, lz=2 * math.pi, ly=2.0, re=180.0,
+        delta_t=5e-4, f_type=1, px0=-1.0, pr=[0.71, 1.0],
+        th_bc_ymin=[0, 1], th_bc_ymax=[0, 1], th_bc_ymin_c1=[-1.0, 0.0], th_bc_ymax_c1=[1.0, 0.0],
+        precision=precision)
+    gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.0)
+    return p, gy

@@ -1,0 +1,146 @@
+/*
+ * libdiablo_gpu -- B200 (sm_100a) implementation of DIABLO 3's RK3 /
+ * Crank-Nicolson channel-flow step behind the reference's plugin surface.
+ *
+ * The reference surface this replaces:
+ *   fft_xz_to_fourier(v, vv)   for/fft.f90:247   -> diablo_fft_xz_to_fourier
+ *   fft_xz_to_physical(vv, v)  for/fft.f90:319   -> diablo_fft_xz_to_physical
+ *   rk_chan_1                  for/channel.f90:10 (called 3x per step from
+ *                              for/diablo.f90:104-107) -> diablo_rk_substep,
+ *                              diablo_step
+ *   pre_first_step             for/advance.f90:17 -> diablo_pre_first_step
+ *   apply_BC_vel_mpi_post,
+ *   apply_BC_th_mpi_post       for/boundary.f90:824,841 -> diablo_apply_bc_post
+ *   module state (flow.f90:20-51, init_flow :58-88, read_inputs/
+ *   set_parameters parameters.f90:88-281, create_grid_chan domain.f90:209)
+ *                              -> diablo_create, diablo_upload_state,
+ *                                 diablo_download_state
+ *
+ * Array layouts at the boundary are the reference's own, Fortran order, one
+ * y-rank and one z-rank (Nxp = Nx/2, Nzp = Nz, Nyp = Ny):
+ *   physical  real    v(0:Nx+1, 0:Nz+1, 0:Ny+1)      (x fastest)
+ *   Fourier   complex vv(0:Nx/2, 0:Nz+1, 0:Ny+1)     (same bytes; kx fastest)
+ * Only the significant entries are defined: physical i < Nx, k < Nz; Fourier
+ * i < Nxp, k <= 2*Nkz (Nkx = Nx/3, Nkz = Nz/3, for/domain.f90:18-23).  Entries
+ * outside that region are written as 0.  Fourier modes Nkx < i < Nxp are zero
+ * in every state the reference produces (for/fft.f90:264-266); uploads that
+ * carry nonzero values there are rejected with DIABLO_ERR_STATE.
+ *
+ * Every entry point returns an int status (0 = DIABLO_OK, negative = error);
+ * nothing aborts the process.  One context per host thread; all device work
+ * of a context is ordered on its CUDA stream.
+ */
+#ifndef DIABLO_GPU_H
+#define DIABLO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIABLO_ABI_VERSION 1
+#define DIABLO_MAX_TH 8
+
+enum diablo_status {
+  DIABLO_OK = 0,
+  DIABLO_ERR_ARG = -1,          /* null pointer, bad enum or bad value */
+  DIABLO_ERR_SIZE = -2,         /* grid size the kernels do not support */
+  DIABLO_ERR_CUDA = -3,         /* a CUDA runtime call failed */
+  DIABLO_ERR_NONFINITE = -4,    /* NaN/Inf found in the state */
+  DIABLO_ERR_TIMEOUT = -5,      /* a bounded device wait gave up */
+  DIABLO_ERR_UNSUPPORTED = -6,  /* option not implemented on the device */
+  DIABLO_ERR_STATE = -7,        /* uploaded state violates the layout contract */
+  DIABLO_ERR_NOMEM = -8         /* device allocation failed */
+};
+
+enum diablo_precision { DIABLO_FP64 = 0, DIABLO_MIXED = 1 };
+
+/* field ids for upload/download: u1, u2, u3, p, then scalar n at DIABLO_TH+n */
+enum diablo_field { DIABLO_U1 = 0, DIABLO_U2 = 1, DIABLO_U3 = 2, DIABLO_P = 3, DIABLO_TH = 4 };
+
+enum diablo_layout {
+  DIABLO_LAYOUT_FOURIER = 0,   /* complex vv(0:Nx/2, 0:Nz+1, 0:Ny+1) */
+  DIABLO_LAYOUT_PHYSICAL = 1   /* real v(0:Nx+1, 0:Nz+1, 0:Ny+1); transformed on the device */
+};
+
+/*
+ * Run parameters: the fields of the reference's `parameters` module that the
+ * step reads (for/parameters.f90:22-82) plus the compile-time grid
+ * (grid_def: Nx, Ny, Nz, N_th).  Velocity BC names follow the reference's
+ * internal variables: u_* -> u1, v_* -> u2 (wall-normal), w_* -> u3.
+ * BC type 0 = Dirichlet, 1 = Neumann.  `ro` = +inf means no rotation.
+ * `struct_size` must be sizeof(diablo_params) (ABI check).
+ */
+typedef struct diablo_params {
+  int struct_size;
+  int nx, ny, nz, n_th;
+  double lx, ly, lz;
+  double re, nu_v_scale, beta, ro, delta;
+  double grav_x, grav_y, grav_z;
+  double delta_t;
+  int f_type;
+  double ubulk0, px0, omega0, amp_omega0, force_start;
+  int u_bc_ymin, v_bc_ymin, w_bc_ymin, u_bc_ymax, v_bc_ymax, w_bc_ymax;
+  double u_bc_ymin_c1, v_bc_ymin_c1, w_bc_ymin_c1;
+  double u_bc_ymax_c1, v_bc_ymax_c1, w_bc_ymax_c1;
+  double pr[DIABLO_MAX_TH], ri[DIABLO_MAX_TH];
+  int th_bc_ymin[DIABLO_MAX_TH], th_bc_ymax[DIABLO_MAX_TH];
+  double th_bc_ymin_c1[DIABLO_MAX_TH], th_bc_ymax_c1[DIABLO_MAX_TH];
+  double dthdx[DIABLO_MAX_TH], dthdz[DIABLO_MAX_TH];
+  int use_les, les_model_type, create_new_flow;
+  int variable_dt;
+  double cfl;
+  int update_dt;
+  double max_dt;
+  int precision;      /* DIABLO_FP64 or DIABLO_MIXED */
+  int flavor_front;   /* 1 = flavor 'Front' (thermal-wind forcing) */
+} diablo_params;
+
+typedef struct diablo_ctx diablo_ctx;
+
+/* Create a context on the current CUDA device.  `gy` holds the Ny+1 wall-normal
+ * base-grid points gy(1..Ny+1), i.e. grid.h5:/grids/y (for/domain.f90:383-527).
+ * Replaces read_inputs + init_mpi + create_grid_chan + init_flow + init_fft. */
+diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status);
+int diablo_destroy(diablo_ctx* ctx);
+
+/* Copy one field between a buffer in the reference layout and the device
+ * state.  `buf` may be host or device memory.  PHYSICAL uploads are
+ * transformed with fft_xz_to_fourier semantics; PHYSICAL downloads with
+ * fft_xz_to_physical semantics (the state itself stays in Fourier space). */
+int diablo_upload_state(diablo_ctx* ctx, int field, const double* buf, int layout);
+int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
+
+/* for/fft.f90:247-315.  v: physical array, vv: Fourier array, both full
+ * reference-size buffers (host or device); v == vv is allowed, as in the
+ * reference, and the input is consumed.  Computes in FP64. */
+int diablo_fft_xz_to_fourier(diablo_ctx* ctx, const double* v, double* vv);
+/* for/fft.f90:319-382; vv == v allowed. */
+int diablo_fft_xz_to_physical(diablo_ctx* ctx, double* vv, double* v);
+
+/* One RK substep, rk_step in {1,2,3} (for/channel.f90:10-917). */
+int diablo_rk_substep(diablo_ctx* ctx, int rk_step);
+/* nsteps full steps: 3 substeps each, time += delta_t (for/diablo.f90:98-108). */
+int diablo_step(diablo_ctx* ctx, int nsteps);
+/* Wall values, projection, optional initial pressure (for/advance.f90:17-44). */
+int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure);
+/* Fourier-space wall/ghost values of u and theta (for/boundary.f90:824-855). */
+int diablo_apply_bc_post(diablo_ctx* ctx);
+
+int diablo_set_precision(diablo_ctx* ctx, int precision);
+int diablo_get_time(diablo_ctx* ctx, double* time, int* time_step, double* delta_t);
+int diablo_set_time(diablo_ctx* ctx, double time, int time_step, double delta_t);
+/* Bind the context to an existing cudaStream_t (NULL = the context's own stream). */
+int diablo_set_stream(diablo_ctx* ctx, void* stream);
+int diablo_synchronize(diablo_ctx* ctx);
+/* DIABLO_ERR_NONFINITE if any significant Fourier entry of the state is NaN
+ * or Inf, 0 otherwise. */
+int diablo_check_finite(diablo_ctx* ctx);
+/* number of kernels this context has launched since creation */
+long long diablo_kernel_launches(const diablo_ctx* ctx);
+const char* diablo_status_string(int status);
+int diablo_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DIABLO_GPU_H */
