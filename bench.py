@@ -1,0 +1,374 @@
+"""Benchmark of the channel step on the Re_tau = 180 workload (256 x 257 x 256,
+three velocities + two scalars), Mpoint-steps/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm runs the mixed-precision and FP64 steps through the C ABI with the
+state resident in HBM (the state, ~1 GB, is larger than L2), times K steps
+with CUDA events on the context's stream between barriers, and reports
+mixed precision as `value` with FP64 beside it, the mixed-vs-FP64 error, the
+dominant kernel's live roofline, an end-to-end figure through the C ABI with
+host buffers, the CPU-oracle baseline and the SM clocks seen.  Under torchrun
+every rank runs an independent replica (the step does not shard).
+
+The reference arm (`--impl reference`) times the CPU restatement of the
+reference's step (the Fortran cannot be built on this image) on all host
+cores, one RK substep of the same workload restricted to 33 wall-normal
+planes per timed step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpoint-steps/s on 1 B200: FP64 vs mixed at ≤1e-6 rel err; adjoint/forward cost"
+UNIT = "Mpoint-steps/s"
+WORKLOAD = "Re_tau=180 channel 256x257x256, 3 velocities + 2 scalars (Pr 0.71, 1.0), dt=5e-4"
+SAMPLE_NY = 33
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            pk = json.load(fh)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+def kernel_bytes(p, nf, mixed):
+    """Algorithmic HBM bytes per launch of each step kernel: every input read
+    once and every output written once (state FP64; step scratch FP32 in mixed
+    precision).  Fourier fields hold (Nkx+1)(2Nkz+1) modes per plane, x-spectral
+    fields (Nkx+1)Nz, physical fields NxNz."""
+    cs = 8 if mixed else 16
+    rs = cs // 2
+    nyp2, ny = p.ny + 2, p.ny
+    four = (p.nx // 3 + 1) * (2 * (p.nz // 3) + 1)
+    xsp = (p.nx // 3 + 1) * p.nz
+    phys = p.nx * p.nz
+    nth = p.n_th
+    return {
+        "z_inverse": nf * nyp2 * (four * 16 + xsp * cs),
+        "x_inverse_c2r": nf * nyp2 * (xsp * cs + phys * rs),
+        "products_x_forward_r2c": nf * nyp2 * phys * rs + 2 * nf * ny * xsp * cs,
+        "z_forward_combine": 2 * nf * ny * xsp * cs + nf * ny * four * cs,
+        # state (3 u + p + scalars) in and out, NL in, cf in on 2 of 3 substeps
+        # and out on 2 of 3 substeps
+        "column_solve": nyp2 * four * (2 * (4 + nth) * 16 + nf * cs + 2 * (2.0 / 3.0) * nf * 16),
+    }
+
+
+def setup_channel(p, gy, fields, precision):
+    from diablo3_test_b200 import _lib
+    from diablo3_test_b200.channel import Channel
+    ch = Channel(p, gy)
+    ch.set_precision(precision)
+    ids = [("u1", _lib.U1), ("u2", _lib.U2), ("u3", _lib.U3)] + \
+        [(f"th{n}", _lib.TH + n) for n in range(p.n_th)]
+    for name, fid in ids:
+        ch.upload(fid, np.ascontiguousarray(fields[name]), _lib.LAYOUT_PHYSICAL)
+    ch.pre_first_step()
+    ch.synchronize()
+    return ch
+
+
+def state_sig(ch):
+    from diablo3_test_b200 import _lib
+    p = ch.params
+    out = {}
+    for name, fid in [("u1", _lib.U1), ("u2", _lib.U2), ("u3", _lib.U3)]:
+        c = ch.download(fid).view(np.complex128)
+        out[name] = c[:, :2 * (p.nz // 3) + 1, :p.nx // 2].copy()
+    return out
+
+
+def timed_steps(ch, torch, stream, k, dist=None):
+    """K steps between barriers, CUDA events on the context's stream."""
+    ch.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ch.step(k)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    return e0.elapsed_time(e1)
+
+
+def cpu_baseline(steps=3, warmup=1):
+    """The CPU oracle on all host cores: RK substeps of the benchmark workload
+    restricted to SAMPLE_NY wall-normal planes."""
+    import dataclasses
+    from diablo3_test_b200 import ics
+    from diablo3_test_b200.grid import create_grid, TANH_ENDS_SYMMETRIC
+    from tests.helpers import setup_oracle
+    p, _ = ics.config_c2()
+    p = dataclasses.replace(p, ny=SAMPLE_NY)
+    gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.0)
+    fields = ics.log_law_turbulent(p, gy)
+    cores = os.cpu_count() or 1
+    o = setup_oracle(p, gy, fields, workers=cores)
+    times = []
+    for s in range(warmup + steps):
+        o.rk_step = 1 + s % 3
+        t = time.perf_counter()
+        o.rk_chan_1()
+        dt = time.perf_counter() - t
+        if s >= warmup:
+            times.append(dt)
+    t_sub = sum(times) / len(times)
+    value = p.nx * p.ny * p.nz / 3.0 / t_sub / 1e6
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"oracle RK substeps of the workload on {SAMPLE_NY} of 257 planes "
+                      f"(256x{SAMPLE_NY}x256), mean of {steps} after {warmup} warm-up; "
+                      f"one substep = 1/3 step", "s_per_substep": t_sub}
+
+
+def read_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/*.md lines 'traffic_per_launch <kernel> <bytes>')."""
+    out = {}
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return out
+    for fn in os.listdir(pdir):
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            m = re.match(r"\s*traffic_per_launch\s+(\S+)\s+(\d+)", line)
+            if m:
+                out[m.group(1)] = int(m.group(2))
+    return out
+
+
+def e2e_round_trip(ch, torch, k):
+    """End to end through the C ABI with pinned host buffers: each step
+    uploads the state (u1, u2, u3, p, scalars) from the host in the reference
+    layout, advances one step and downloads the state again."""
+    from diablo3_test_b200 import _lib
+    p = ch.params
+    ids = [_lib.U1, _lib.U2, _lib.U3, _lib.P] + [_lib.TH + n for n in range(p.n_th)]
+    shape = (p.ny + 2, p.nz + 2, p.nx + 2)
+    bufs = [torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() for _ in ids]
+    for b, fid in zip(bufs, ids):
+        ch.download(fid, out=b)
+    ch.synchronize()
+    box = (p.ny + 2) * (2 * (p.nz // 3) + 1) * (p.nx // 2) * 16
+    t0 = time.perf_counter()
+    for _ in range(k):
+        for b, fid in zip(bufs, ids):
+            ch.upload(fid, b)
+        ch.step(1)
+        for b, fid in zip(bufs, ids):
+            ch.download(fid, out=b)
+    ch.synchronize()
+    dt = time.perf_counter() - t0
+    pts = p.nx * p.ny * p.nz
+    return {"value": pts * k / dt / 1e6, "unit": UNIT, "h2d_bytes_per_step": box * len(ids),
+            "d2h_bytes_per_step": box * len(ids), "ms_per_step": dt / k * 1e3,
+            "path": "diablo_upload_state x6 (host, pinned) + diablo_step + diablo_download_state x6"}
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    from diablo3_test_b200 import ics, _lib
+    from diablo3_test_b200.config import FP64, MIXED
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    torch.cuda.init()
+    p, gy = ics.config_c2()
+    fields = ics.log_law_turbulent(p, gy)
+    nf = 3 + p.n_th
+    pts = p.nx * p.ny * p.nz
+    stream = torch.cuda.Stream()
+    chm = setup_channel(p, gy, fields, MIXED)
+    chd = setup_channel(p, gy, fields, FP64)
+    for ch in (chm, chd):
+        ch.set_stream(stream.cuda_stream)
+    # warm-up
+    chm.step(args.warmup)
+    chd.step(args.warmup)
+    sampler = ClockSampler(local)
+    sampler.start()
+    chm.set_profiling(True)
+    l0 = chm.kernel_launches()
+    ms_mixed = timed_steps(chm, torch, stream, args.steps, dist)
+    launches = chm.kernel_launches() - l0
+    ktimes = chm.kernel_times()
+    chm.set_profiling(False)
+    ms_fp64 = timed_steps(chd, torch, stream, args.steps, dist)
+    clocks = sampler.stop()
+    if dist is not None:
+        t = torch.tensor([ms_mixed, ms_fp64], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_mixed, ms_fp64 = float(t[0]), float(t[1])
+    # mixed vs FP64 after the same W+K steps from the same state
+    sm, sd = state_sig(chm), state_sig(chd)
+    err = {k: float(np.linalg.norm(sm[k] - sd[k]) / np.linalg.norm(sd[k])) for k in sm}
+    if rank != 0:
+        chm.close()
+        chd.close()
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = _peaks()
+    kb = kernel_bytes(p, nf, mixed=True)
+    per_kernel = {}
+    for name, (ms, n) in ktimes.items():
+        if n and name in kb:
+            avg = ms / n
+            per_kernel[name] = {"launches": n, "avg_ms": avg, "share": ms / max(ms_mixed, 1e-9),
+                                "alg_bytes": kb[name], "achieved_gbs": kb[name] / (avg * 1e-3) / 1e9}
+    dom = max(per_kernel, key=lambda k: per_kernel[k]["avg_ms"] * per_kernel[k]["launches"])
+    traffic = read_traffic().get(dom)
+    achieved = per_kernel[dom]["achieved_gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs"}
+    # whole-step roofline against the 3*(8NF+9)*s bytes-per-point-step model
+    alg64 = 3 * (8 * nf + 9) * 8
+    value = pts * world * args.steps / (ms_mixed * 1e-3) / 1e6
+    v64 = pts * world * args.steps / (ms_fp64 * 1e-3) / 1e6
+    step_roof = {"model_bytes_per_point_step_fp64": alg64,
+                 "fp64_frac": alg64 * pts / (ms_fp64 / args.steps * 1e-3) / 1e9 / peak}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 FFT/nonlinear + f64 solves/state (mixed)",
+        "data": "synthetic (seeded log-law mean + 10% perturbations, projected)",
+        "config": {"workload": WORKLOAD, "grid": [p.nx, p.ny, p.nz], "n_th": p.n_th,
+                   "precision": "mixed", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "state (~1 GB FP64 Fourier + scratch) larger than the 126 MB L2; no flush"},
+        "fp64": {"value": v64, "unit": UNIT, "ms_per_step": ms_fp64 / args.steps,
+                 "dtype": "f64"},
+        "mixed_speedup_vs_fp64": ms_fp64 / ms_mixed,
+        "mixed_vs_fp64_rel_err": err,
+        "rel_err_steps": args.warmup + args.steps,
+        "roofline": roofline,
+        "step_roofline": step_roof,
+        "kernels": per_kernel,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if not args.no_e2e:
+        out["e2e"] = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)))
+    chm.close()
+    chd.close()
+    if world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    print(json.dumps(out))
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline(steps=args.steps, warmup=args.warmup)
+    out = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": cb["s_per_substep"] * 3e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+           "data": "synthetic (seeded log-law mean + 10% perturbations, projected)",
+           "config": {"workload": WORKLOAD, "precision": "fp64",
+                      "sample": f"256x{SAMPLE_NY}x256 slice of the workload, one RK substep per timed step"},
+           "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "note": "reference Fortran (gfortran+MPI+FFTW+HDF5+toml-f) cannot be built on this image; "
+                   "the CPU restatement of its step (oracle/) is timed instead"}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -50,6 +50,10 @@ SIGNATURES = {
     "diablo_synchronize": (_i, [_vp]),
     "diablo_check_finite": (_i, [_vp]),
     "diablo_kernel_launches": (ctypes.c_longlong, [_vp]),
+    "diablo_set_profiling": (_i, [_vp, _i]),
+    "diablo_kernel_times": (_i, [_vp, _i, ctypes.POINTER(_d), ctypes.POINTER(ctypes.c_longlong)]),
+    "diablo_kernel_slots": (_i, []),
+    "diablo_kernel_name": (ctypes.c_char_p, [_i]),
     "diablo_status_string": (ctypes.c_char_p, [_i]),
     "diablo_abi_version": (_i, []),
 }

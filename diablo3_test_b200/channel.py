@@ -134,3 +134,22 @@ class Channel:
 
     def kernel_launches(self) -> int:
         return int(self.lib.diablo_kernel_launches(self.ctx))
+
+    def set_profiling(self, enable: bool):
+        _lib.check(self.lib.diablo_set_profiling(self.ctx, int(enable)), "set_profiling")
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total device ms, launches)} since profiling was enabled."""
+        out = {}
+        for s in range(self.lib.diablo_kernel_slots()):
+            ms = ctypes.c_double(0)
+            n = ctypes.c_longlong(0)
+            _lib.check(self.lib.diablo_kernel_times(self.ctx, s, ctypes.byref(ms), ctypes.byref(n)),
+                       "kernel_times")
+            out[self.lib.diablo_kernel_name(s).decode()] = (ms.value, n.value)
+        return out
+
+    def set_stream(self, stream_handle: int):
+        """Order the context's work on an existing cudaStream_t (0 = own stream)."""
+        _lib.check(self.lib.diablo_set_stream(self.ctx, ctypes.c_void_p(stream_handle or None)),
+                   "set_stream")

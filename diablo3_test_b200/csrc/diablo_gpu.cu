@@ -73,7 +73,51 @@ struct diablo_ctx {
   double* b_ref;
   int* d_flag;
   std::vector<void*> allocs;
+  // opt-in per-kernel timing: events recorded around each step kernel
+  int profiling;
+  struct Timed { int slot; cudaEvent_t a, b; };
+  std::vector<Timed> timed;        // pending (recorded, not yet read)
+  std::vector<cudaEvent_t> pool;   // free events
+  double slot_ms[8];
+  long long slot_n[8];
 };
+
+enum { K_ZINV = 0, K_XINV = 1, K_XFWD_NL = 2, K_ZFWD_NL = 3, K_SOLVE = 4, K_OTHER = 5, K_NSLOTS = 6 };
+static const char* K_NAMES[K_NSLOTS] = {"z_inverse", "x_inverse_c2r", "products_x_forward_r2c",
+                                        "z_forward_combine", "column_solve", "other"};
+
+static cudaEvent_t ev_get(diablo_ctx* ctx) {
+  if (!ctx->pool.empty()) { cudaEvent_t e = ctx->pool.back(); ctx->pool.pop_back(); return e; }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+// Bracket one kernel launch with events when profiling is on.
+struct Prof {
+  diablo_ctx* ctx; int slot; cudaEvent_t a = nullptr;
+  Prof(diablo_ctx* c, int s) : ctx(c), slot(s) {
+    ctx->launches++;
+    if (ctx->profiling) { a = ev_get(ctx); cudaEventRecord(a, ctx->stream); }
+  }
+  ~Prof() {
+    if (!a) return;
+    cudaEvent_t b = ev_get(ctx);
+    cudaEventRecord(b, ctx->stream);
+    ctx->timed.push_back({slot, a, b});
+  }
+};
+static void prof_collect(diablo_ctx* ctx) {
+  for (auto& t : ctx->timed) {
+    float ms = 0.f;
+    cudaEventSynchronize(t.b);
+    cudaEventElapsedTime(&ms, t.a, t.b);
+    ctx->slot_ms[t.slot] += ms;
+    ctx->slot_n[t.slot] += 1;
+    ctx->pool.push_back(t.a);
+    ctx->pool.push_back(t.b);
+  }
+  ctx->timed.clear();
+}
 
 #include "fft_launch.h"
 
@@ -327,8 +371,8 @@ static int substep_spectral(diablo_ctx* ctx) {
     a.nseq = ctx->nyp2 * ctx->nkx1;
     a.g = ctx->g;
     a.tw = tz;
+    Prof pr(ctx, K_ZINV);
     if ((rc = launch_zinv<C>(a, ctx->nz, nf, ctx->stream))) return rc;
-    ctx->launches++;
   }
   // 2. x inverse -> physical
   {
@@ -342,8 +386,8 @@ static int substep_spectral(diablo_ctx* ctx) {
     a.g = ctx->g;
     a.twM = tm;
     a.twX = tx;
+    Prof pr(ctx, K_XINV);
     if ((rc = launch_xinv<C>(a, ctx->M, ctx->nyp2, nf, ctx->stream))) return rc;
-    ctx->launches++;
   }
   // 3. nonlinear products + x forward (planes 1..Ny)
   {
@@ -361,8 +405,8 @@ static int substep_spectral(diablo_ctx* ctx) {
     a.kx = ctx->d_kx;
     a.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
     a.scale = 1.0 / ctx->nx;
+    Prof pr(ctx, K_XFWD_NL);
     if ((rc = launch_xfwd<T, true>(a, ctx->M, ctx->ny, nf, ctx->stream))) return rc;
-    ctx->launches++;
   }
   // 4. z forward + combine -> NL (planes 1..Ny)
   {
@@ -379,8 +423,8 @@ static int substep_spectral(diablo_ctx* ctx) {
     a.tw = tz;
     a.kz = ctx->d_kz;
     a.scale = 1.0 / ctx->nz;
+    Prof pr(ctx, K_ZFWD_NL);
     if ((rc = launch_zfwd<C, C, true>(a, ctx->nz, nf, ctx->stream))) return rc;
-    ctx->launches++;
   }
   return 0;
 }
@@ -412,8 +456,10 @@ static int substep(diablo_ctx* ctx, int rk) {
     else a.nl32[f] = (const float2*)ctx->nl[f];
   }
   a.store_cf = rk < 3 ? 1 : 0;
-  if ((rc = launch_solve(a, false, ctx->stream))) return rc;
-  ctx->launches++;
+  {
+    Prof pr(ctx, K_SOLVE);
+    if ((rc = launch_solve(a, false, ctx->stream))) return rc;
+  }
   CK(cudaGetLastError());
   ctx->cur = nx_;
   if (a.store_cf) ctx->cf_cur = 1 - ctx->cf_cur;
@@ -544,6 +590,8 @@ int diablo_destroy(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
+  for (auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+  for (auto e : ctx->pool) cudaEventDestroy(e);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   cudaGetLastError();
   delete ctx;
@@ -556,12 +604,102 @@ static int field_index(const diablo_ctx* ctx, int field) {
   return -1;
 }
 
-// copy a reference-size buffer to device scratch (or use it in place)
-static int stage_in(diablo_ctx* ctx, const double* buf, const double** dev) {
-  if (is_device_ptr(buf)) { *dev = buf; return 0; }
-  CK(cudaMemcpyAsync(ctx->b_ref, buf, ref_doubles(ctx) * sizeof(double), cudaMemcpyHostToDevice,
-                     ctx->stream));
-  *dev = ctx->b_ref;
+// ---- boundary copies --------------------------------------------------------
+// Host buffers move only their significant box, one cudaMemcpy3DAsync per
+// field: Fourier i < Nxp, k <= 2Nkz; physical i < Nx, k < Nz.
+static cudaMemcpy3DParms box_parms(void* dst, size_t dpitch, size_t dheight, const void* src,
+                                   size_t spitch, size_t sheight, size_t wbytes, size_t rows,
+                                   size_t planes, cudaMemcpyKind kind) {
+  cudaMemcpy3DParms m;
+  memset(&m, 0, sizeof(m));
+  m.srcPtr = make_cudaPitchedPtr(const_cast<void*>(src), spitch, wbytes, sheight);
+  m.dstPtr = make_cudaPitchedPtr(dst, dpitch, wbytes, dheight);
+  m.extent = make_cudaExtent(wbytes, rows, planes);
+  m.kind = kind;
+  return m;
+}
+
+// significant Fourier box of `buf` -> internal layout `dst`
+static int four_in(diablo_ctx* ctx, const double* buf, double2* dst, bool check) {
+  const double2* src;
+  int rp, rows;
+  if (is_device_ptr(buf)) {
+    src = (const double2*)buf;
+    rp = ctx->nxp + 1;
+    rows = ctx->nz + 2;
+  } else {
+    cudaMemcpy3DParms m = box_parms(ctx->b_ref, ctx->nxp * sizeof(double2), ctx->nk2, buf,
+                                    (ctx->nxp + 1) * sizeof(double2), ctx->nz + 2,
+                                    ctx->nxp * sizeof(double2), ctx->nk2, ctx->nyp2,
+                                    cudaMemcpyHostToDevice);
+    CK(cudaMemcpy3DAsync(&m, ctx->stream));
+    src = (const double2*)ctx->b_ref;
+    rp = ctx->nxp;
+    rows = ctx->nk2;
+  }
+  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  size_t tot = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
+  {
+    Prof pr(ctx, K_OTHER);
+    k_ref_to_four<<<grid1d(tot), 256, 0, ctx->stream>>>(src, dst, ctx->g, ctx->nxp, rp, rows,
+                                                         ctx->d_flag);
+  }
+  if (check) {
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (bad) return DIABLO_ERR_STATE;
+  }
+  return 0;
+}
+
+// internal Fourier `src` -> significant box of `buf`
+static int four_out(diablo_ctx* ctx, const double2* src, double* buf) {
+  const bool dev = is_device_ptr(buf);
+  double2* dst = dev ? (double2*)buf : (double2*)ctx->b_ref;
+  int rp = dev ? ctx->nxp + 1 : ctx->nxp, rows = dev ? ctx->nz + 2 : ctx->nk2;
+  size_t tot = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
+  {
+    Prof pr(ctx, K_OTHER);
+    k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(src, dst, ctx->g, ctx->nxp, rp, rows);
+  }
+  if (!dev) {
+    cudaMemcpy3DParms m = box_parms(buf, (ctx->nxp + 1) * sizeof(double2), ctx->nz + 2, ctx->b_ref,
+                                    ctx->nxp * sizeof(double2), ctx->nk2, ctx->nxp * sizeof(double2),
+                                    ctx->nk2, ctx->nyp2, cudaMemcpyDeviceToHost);
+    CK(cudaMemcpy3DAsync(&m, ctx->stream));
+  }
+  return 0;
+}
+
+// significant physical box of `buf` -> internal physical `dst`
+static int phys_in(diablo_ctx* ctx, const double* buf, double* dst) {
+  if (is_device_ptr(buf)) {
+    Prof pr(ctx, K_OTHER);
+    k_ref_to_phys<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(buf, dst, ctx->nx, ctx->nz,
+                                                                    ctx->nyp2);
+  } else {
+    cudaMemcpy3DParms m = box_parms(dst, ctx->nx * sizeof(double), ctx->nz, buf,
+                                    (ctx->nx + 2) * sizeof(double), ctx->nz + 2,
+                                    ctx->nx * sizeof(double), ctx->nz, ctx->nyp2,
+                                    cudaMemcpyHostToDevice);
+    CK(cudaMemcpy3DAsync(&m, ctx->stream));
+  }
+  return 0;
+}
+
+// internal physical `src` -> significant box of `buf`
+static int phys_out(diablo_ctx* ctx, const double* src, double* buf) {
+  if (is_device_ptr(buf)) {
+    Prof pr(ctx, K_OTHER);
+    k_phys_to_ref<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(src, buf, ctx->nx, ctx->nz,
+                                                                    ctx->nyp2);
+  } else {
+    cudaMemcpy3DParms m = box_parms(buf, (ctx->nx + 2) * sizeof(double), ctx->nz + 2, src,
+                                    ctx->nx * sizeof(double), ctx->nz, ctx->nx * sizeof(double),
+                                    ctx->nz, ctx->nyp2, cudaMemcpyDeviceToHost);
+    CK(cudaMemcpy3DAsync(&m, ctx->stream));
+  }
   return 0;
 }
 
@@ -571,23 +709,11 @@ int diablo_upload_state(diablo_ctx* ctx, int field, const double* buf, int layou
   if (fi < 0) return DIABLO_ERR_ARG;
   int rc = ensure_bscratch(ctx);
   if (rc) return rc;
-  const double* dref;
-  if ((rc = stage_in(ctx, buf, &dref))) return rc;
   double2* dst = ctx->st[ctx->cur][fi];
   if (layout == DIABLO_LAYOUT_FOURIER) {
-    CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
-    size_t tot = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
-    k_ref_to_four<<<grid1d(tot), 256, 0, ctx->stream>>>((const double2*)dref, dst, ctx->g, ctx->nxp,
-                                                         ctx->d_flag);
-    ctx->launches++;
-    int bad = 0;
-    CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    if (bad) return DIABLO_ERR_STATE;
+    if ((rc = four_in(ctx, buf, dst, true))) return rc;
   } else if (layout == DIABLO_LAYOUT_PHYSICAL) {
-    k_ref_to_phys<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(dref, ctx->b_phys, ctx->nx,
-                                                                    ctx->nz, ctx->nyp2);
-    ctx->launches++;
+    if ((rc = phys_in(ctx, buf, ctx->b_phys))) return rc;
     if ((rc = fwd_phys_to_four(ctx, ctx->b_phys, ctx->b_xs, dst))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
   } else {
@@ -603,24 +729,15 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout) {
   if (fi < 0) return DIABLO_ERR_ARG;
   int rc = ensure_bscratch(ctx);
   if (rc) return rc;
-  const bool dev = is_device_ptr(buf);
-  double* dref = dev ? buf : ctx->b_ref;
   const double2* src = ctx->st[ctx->cur][fi];
   if (layout == DIABLO_LAYOUT_FOURIER) {
-    size_t tot = (size_t)ctx->nyp2 * (ctx->nz + 2) * (ctx->nxp + 1);
-    k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(src, (double2*)dref, ctx->g, ctx->nxp);
-    ctx->launches++;
+    if ((rc = four_out(ctx, src, buf))) return rc;
   } else if (layout == DIABLO_LAYOUT_PHYSICAL) {
     if ((rc = inv_four_to_phys(ctx, src, ctx->b_xs, ctx->b_phys))) return rc;
-    k_phys_to_ref<<<grid1d(ref_doubles(ctx)), 256, 0, ctx->stream>>>(ctx->b_phys, dref, ctx->nx,
-                                                                     ctx->nz, ctx->nyp2);
-    ctx->launches++;
+    if ((rc = phys_out(ctx, ctx->b_phys, buf))) return rc;
   } else {
     return DIABLO_ERR_ARG;
   }
-  if (!dev)
-    CK(cudaMemcpyAsync(buf, dref, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
-                       ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;
@@ -630,20 +747,9 @@ int diablo_fft_xz_to_fourier(diablo_ctx* ctx, const double* v, double* vv) {
   if (!ctx || !v || !vv) return DIABLO_ERR_ARG;
   int rc = ensure_bscratch(ctx);
   if (rc) return rc;
-  const double* dref;
-  if ((rc = stage_in(ctx, v, &dref))) return rc;
-  k_ref_to_phys<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(dref, ctx->b_phys, ctx->nx,
-                                                                  ctx->nz, ctx->nyp2);
-  ctx->launches++;
+  if ((rc = phys_in(ctx, v, ctx->b_phys))) return rc;
   if ((rc = fwd_phys_to_four(ctx, ctx->b_phys, ctx->b_xs, ctx->b_four))) return rc;
-  const bool dev = is_device_ptr(vv);
-  double* out = dev ? vv : ctx->b_ref;
-  size_t tot = (size_t)ctx->nyp2 * (ctx->nz + 2) * (ctx->nxp + 1);
-  k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->b_four, (double2*)out, ctx->g, ctx->nxp);
-  ctx->launches++;
-  if (!dev)
-    CK(cudaMemcpyAsync(vv, out, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+  if ((rc = four_out(ctx, ctx->b_four, vv))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;
@@ -653,24 +759,11 @@ int diablo_fft_xz_to_physical(diablo_ctx* ctx, double* vv, double* v) {
   if (!ctx || !v || !vv) return DIABLO_ERR_ARG;
   int rc = ensure_bscratch(ctx);
   if (rc) return rc;
-  const double* dref;
-  if ((rc = stage_in(ctx, vv, &dref))) return rc;
-  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
-  size_t tin = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
   // modes above Nkx are zeroed by the reference before the x transform
-  // (for/fft.f90:372-378); the flag is ignored here
-  k_ref_to_four<<<grid1d(tin), 256, 0, ctx->stream>>>((const double2*)dref, ctx->b_four, ctx->g,
-                                                       ctx->nxp, ctx->d_flag);
-  ctx->launches++;
+  // (for/fft.f90:372-378), so they are not checked here
+  if ((rc = four_in(ctx, vv, ctx->b_four, false))) return rc;
   if ((rc = inv_four_to_phys(ctx, ctx->b_four, ctx->b_xs, ctx->b_phys))) return rc;
-  const bool dev = is_device_ptr(v);
-  double* out = dev ? v : ctx->b_ref;
-  k_phys_to_ref<<<grid1d(ref_doubles(ctx)), 256, 0, ctx->stream>>>(ctx->b_phys, out, ctx->nx,
-                                                                   ctx->nz, ctx->nyp2);
-  ctx->launches++;
-  if (!dev)
-    CK(cudaMemcpyAsync(v, out, ref_doubles(ctx) * sizeof(double), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+  if ((rc = phys_out(ctx, ctx->b_phys, v))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;
@@ -823,5 +916,28 @@ int diablo_check_finite(diablo_ctx* ctx) {
 }
 
 long long diablo_kernel_launches(const diablo_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int diablo_set_profiling(diablo_ctx* ctx, int enable) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  prof_collect(ctx);
+  ctx->profiling = enable ? 1 : 0;
+  for (int i = 0; i < K_NSLOTS; ++i) { ctx->slot_ms[i] = 0.0; ctx->slot_n[i] = 0; }
+  return 0;
+}
+
+int diablo_kernel_times(diablo_ctx* ctx, int slot, double* total_ms, long long* launches) {
+  if (!ctx || slot < 0 || slot >= K_NSLOTS) return DIABLO_ERR_ARG;
+  prof_collect(ctx);
+  if (total_ms) *total_ms = ctx->slot_ms[slot];
+  if (launches) *launches = ctx->slot_n[slot];
+  return 0;
+}
+
+int diablo_kernel_slots(void) { return K_NSLOTS; }
+
+const char* diablo_kernel_name(int slot) {
+  return (slot >= 0 && slot < K_NSLOTS) ? K_NAMES[slot] : "";
+}
 
 }  // extern "C"

@@ -17,23 +17,25 @@ __global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict
   out[idx] = ref[((size_t)j * (nz + 2) + k) * (nx + 2) + i];
 }
 
-// internal P -> reference physical, padding written as 0
+// internal P -> the significant box (i < Nx, k < Nz) of a reference physical array
 __global__ void k_phys_to_ref(const double* __restrict__ in, double* __restrict__ ref,
                               int nx, int nz, int nyp2) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  size_t tot = (size_t)nyp2 * (nz + 2) * (nx + 2);
+  size_t tot = (size_t)nyp2 * nz * nx;
   if (idx >= tot) return;
-  int i = idx % (nx + 2);
-  size_t r = idx / (nx + 2);
-  int k = r % (nz + 2);
-  int j = r / (nz + 2);
-  ref[idx] = (i < nx && k < nz) ? in[((size_t)j * nz + k) * nx + i] : 0.0;
+  int i = idx % nx;
+  size_t r = idx / nx;
+  int k = r % nz;
+  int j = r / nz;
+  ref[((size_t)j * (nz + 2) + k) * (nx + 2) + i] = in[idx];
 }
 
 // reference Fourier vv(0:Nxp, 0:Nz+1, 0:Ny+1) -> internal F[j][m][kp]; sets
-// *bad if a significant mode above Nkx is nonzero
+// *bad if a significant mode above Nkx is nonzero.  The source has row pitch
+// `rp` complex elements and `rows` rows per plane (Nxp+1 and Nz+2 for a full
+// reference array, Nxp and 2Nkz+1 for a packed copy of its significant box).
 __global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restrict__ out,
-                              Geom g, int nxp, int* bad) {
+                              Geom g, int nxp, int rp, int rows, int* bad) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)g.nyp2 * g.nk2 * nxp;
   if (idx >= tot) return;
@@ -41,7 +43,7 @@ __global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restri
   size_t r = idx / nxp;
   int kp = r % g.nk2;
   int j = r / g.nk2;
-  double2 v = ref[((size_t)j * (g.nz + 2) + kp) * (nxp + 1) + i];
+  double2 v = ref[((size_t)j * rows + kp) * rp + i];
   if (i < g.nkx1) {
     out[((size_t)j * g.nkx1 + i) * g.kp + kp] = v;
   } else if (v.x != 0.0 || v.y != 0.0) {
@@ -49,19 +51,20 @@ __global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restri
   }
 }
 
-// internal F -> reference Fourier, non-significant entries written as 0
+// internal F -> the significant box (i < Nxp, k <= 2Nkz) of a Fourier array
+// with row pitch `rp` and `rows` rows per plane; modes above Nkx written as 0
 __global__ void k_four_to_ref(const double2* __restrict__ in, double2* __restrict__ ref,
-                              Geom g, int nxp) {
+                              Geom g, int nxp, int rp, int rows) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  size_t tot = (size_t)g.nyp2 * (g.nz + 2) * (nxp + 1);
+  size_t tot = (size_t)g.nyp2 * g.nk2 * nxp;
   if (idx >= tot) return;
-  int i = idx % (nxp + 1);
-  size_t r = idx / (nxp + 1);
-  int k = r % (g.nz + 2);
-  int j = r / (g.nz + 2);
+  int i = idx % nxp;
+  size_t r = idx / nxp;
+  int k = r % g.nk2;
+  int j = r / g.nk2;
   double2 v = make_double2(0.0, 0.0);
-  if (i < g.nkx1 && k < g.nk2) v = in[((size_t)j * g.nkx1 + i) * g.kp + k];
-  ref[idx] = v;
+  if (i < g.nkx1) v = in[((size_t)j * g.nkx1 + i) * g.kp + k];
+  ref[((size_t)j * rows + k) * rp + i] = v;
 }
 
 // any non-finite significant entry -> *bad

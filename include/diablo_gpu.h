@@ -20,11 +20,13 @@
  * y-rank and one z-rank (Nxp = Nx/2, Nzp = Nz, Nyp = Ny):
  *   physical  real    v(0:Nx+1, 0:Nz+1, 0:Ny+1)      (x fastest)
  *   Fourier   complex vv(0:Nx/2, 0:Nz+1, 0:Ny+1)     (same bytes; kx fastest)
- * Only the significant entries are defined: physical i < Nx, k < Nz; Fourier
- * i < Nxp, k <= 2*Nkz (Nkx = Nx/3, Nkz = Nz/3, for/domain.f90:18-23).  Entries
- * outside that region are written as 0.  Fourier modes Nkx < i < Nxp are zero
- * in every state the reference produces (for/fft.f90:264-266); uploads that
- * carry nonzero values there are rejected with DIABLO_ERR_STATE.
+ * Only the significant entries are read or written: physical i < Nx, k < Nz;
+ * Fourier i < Nxp, k <= 2*Nkz (Nkx = Nx/3, Nkz = Nz/3, for/domain.f90:18-23).
+ * Every other entry of a destination buffer is left as it was (the reference
+ * leaves stale values there too, for/fft.f90:301-313).  Fourier modes
+ * Nkx < i < Nxp are zero in every state the reference produces
+ * (for/fft.f90:264-266): they are written as 0, and uploads that carry nonzero
+ * values there are rejected with DIABLO_ERR_STATE.
  *
  * Every entry point returns an int status (0 = DIABLO_OK, negative = error);
  * nothing aborts the process.  One context per host thread; all device work
@@ -137,6 +139,16 @@ int diablo_synchronize(diablo_ctx* ctx);
 int diablo_check_finite(diablo_ctx* ctx);
 /* number of kernels this context has launched since creation */
 long long diablo_kernel_launches(const diablo_ctx* ctx);
+
+/* Per-kernel timing (tracing; no reference counterpart beyond the wall-clock
+ * "Wall Seconds per Iteration" print, for/control.f90:104-109).  When on, every
+ * step kernel is bracketed by CUDA events on the context's stream;
+ * diablo_kernel_times returns the accumulated device time and launch count of
+ * one kernel class since profiling was (re)enabled. */
+int diablo_set_profiling(diablo_ctx* ctx, int enable);
+int diablo_kernel_times(diablo_ctx* ctx, int slot, double* total_ms, long long* launches);
+int diablo_kernel_slots(void);
+const char* diablo_kernel_name(int slot);
 const char* diablo_status_string(int status);
 int diablo_abi_version(void);
 

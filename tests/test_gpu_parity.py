@@ -45,10 +45,14 @@ def test_fft_xz_pair_matches_oracle(cuda_device, nx, ny, nz):
         o.fft_xz_to_physical(o.u1)
         ref = o.u1.buf[:, :nz, :nx]
         assert rel_err(back[:, :nz, :nx], ref) < TOL_FFT
-        # padding and the non-significant Fourier entries are written as zero
-        assert np.all(back[:, :, nx:] == 0) and np.all(back[:, nz:, :] == 0)
+        # modes above Nkx are written as zero; entries outside the significant
+        # box are left as they were
         c = w.view(np.complex128)
-        assert np.all(c[:, 2 * (nz // 3) + 1:, :] == 0) and np.all(c[:, :, nx // 3 + 1:] == 0)
+        c0 = v.view(np.complex128)
+        nk2 = 2 * (nz // 3) + 1
+        assert np.all(c[:, :nk2, nx // 3 + 1:nx // 2] == 0)
+        assert np.array_equal(c[:, nk2:, :], c0[:, nk2:, :]) and np.array_equal(c[:, :, nx // 2], c0[:, :, nx // 2])
+        assert np.all(back[:, :, nx:] == 0) and np.all(back[:, nz:, :] == 0)
 
 
 def test_upload_rejects_modes_above_nkx(cuda_device):
