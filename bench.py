@@ -249,10 +249,24 @@ def run_ours(args):
         torch.cuda.set_device(local)
     torch.cuda.init()
     p, gy = ics.config_c2()
+    if args.grid:
+        import dataclasses
+        from diablo3_test_b200.grid import create_grid, TANH_ENDS_SYMMETRIC
+        p = dataclasses.replace(p, nx=args.grid[0], ny=args.grid[1], nz=args.grid[2])
+        gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.0)
     fields = ics.log_law_turbulent(p, gy)
     nf = 3 + p.n_th
     pts = p.nx * p.ny * p.nz
     stream = torch.cuda.Stream()
+    if args.grid or args.precision != "both":
+        # profiling run: one precision, no JSON line
+        ch = setup_channel(p, gy, fields, MIXED if args.precision != "fp64" else FP64)
+        ch.set_stream(stream.cuda_stream)
+        ch.step(args.warmup)
+        ms = timed_steps(ch, torch, stream, args.steps)
+        print(f"profiling run {p.nx}x{p.ny}x{p.nz} {args.precision}: {ms / max(args.steps, 1):.3f} ms/step")
+        ch.close()
+        return
     chm = setup_channel(p, gy, fields, MIXED)
     chd = setup_channel(p, gy, fields, FP64)
     for ch in (chm, chd):
@@ -361,6 +375,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"), default=None,
+                    help="profiling: run a smaller grid of the same workload (no JSON contract)")
+    ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
+                    help="profiling: run one precision only")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -30,6 +30,18 @@ def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+def _includes(path, seen=None):
+    """Headers a source file pulls in (quoted #includes, followed recursively)."""
+    import re
+    seen = set() if seen is None else seen
+    for inc in re.findall(r'^\s*#\s*include\s+"([^"]+)"', open(path).read(), re.M):
+        full = os.path.normpath(os.path.join(os.path.dirname(path), inc))
+        if os.path.exists(full) and full not in seen:
+            seen.add(full)
+            _includes(full, seen)
+    return seen
+
+
 def _stale(target: str, deps) -> bool:
     if not os.path.exists(target):
         return True
@@ -49,8 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
-        hdr_deps = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
-        if not force and not _stale(obj, [src] + hdr_deps):
+        if not force and not _stale(obj, [src] + sorted(_includes(src))):
             continue
         cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
         if verbose:

@@ -13,6 +13,7 @@
 #include "fft.cuh"
 #include "kernels_layout.cuh"
 #include "kernels_solve.cuh"
+#include "kernels_solve2.cuh"
 
 static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
 static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
@@ -75,6 +76,10 @@ struct diablo_ctx {
   std::vector<void*> allocs;
   // opt-in per-kernel timing: events recorded around each step kernel
   int profiling;
+  int use_general_solver;   // 1: per-lane-load column kernel instead of the tiled one
+  Solve2Args solve2;        // tile schedule of the current substep
+  double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
+  double* d_met;            // Poisson and metric rows [MET_N][n]
   struct Timed { int slot; cudaEvent_t a, b; };
   std::vector<Timed> timed;        // pending (recorded, not yet read)
   std::vector<cudaEvent_t> pool;   // free events
@@ -129,6 +134,24 @@ static void launch_solve_t(const SolveArgs& a, bool project_only, cudaStream_t s
   if (project_only) k_rem_div<R><<<grd, blk, 0, s>>>(a);
   else k_column_solve<R><<<grd, blk, 0, s>>>(a);
 }
+template <int R>
+static void launch_tiles_t(const Solve2Args& A, cudaStream_t s) {
+  const int smem = ((1 + T2_STAGES) * A.s.n * T2_PITCH + T2_COLS * 32 * R) * (int)sizeof(double2);
+  cudaFuncSetAttribute(k_column_tiles<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int ngroups = (A.s.nk2 + T2_COLS - 1) / T2_COLS;
+  k_column_tiles<R><<<A.s.nkx1 * ngroups, 32 * T2_COLS, smem, s>>>(A);
+}
+static int launch_tiles(const Solve2Args& A, cudaStream_t s) {
+  int R = (A.s.n + 31) / 32;
+  if (R < 3) R = 3;
+  switch (R) {
+#define X(r) case r: launch_tiles_t<r>(A, s); return 0;
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return DIABLO_ERR_SIZE;
+  }
+}
+
 static int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s) {
   int R = (a.n + 31) / 32;
   if (R < 3) R = 3;
@@ -285,6 +308,73 @@ static bool is_device_ptr(const void* p) {
 }
 
 // --------------------------------------------------------------------------
+// Row coefficients of the implicit solves, evaluated with the reference's
+// expressions (for/channel.f90:664-670 scalars, :726-733 u2, :782-788 and
+// :838-845 u1/u3, :969-976 rem_div), for each RK substep.
+static int upload_coefficients(diablo_ctx* ctx) {
+  const int n = ctx->nyp2, ny = ctx->ny, nk = 2 + ctx->nth;
+  const std::vector<double>& dy = ctx->h_dy;
+  const std::vector<double>& dyf = ctx->h_dyf;
+  const double nuv = ctx->p.nu_v_scale;
+  for (int rk = 0; rk < 3; ++rk) {
+    std::vector<double> kc((size_t)nk * 3 * n, 0.0);
+    const double temp1 = 0.5 * ctx->nu * ctx->h_bar[rk];
+    for (int kind = 0; kind < nk; ++kind) {
+      double* A = &kc[(size_t)kind * 3 * n];
+      double* B = A + n;
+      double* C = B + n;
+      for (int j = 0; j < n; ++j) B[j] = 1.0;
+      if (kind == 0) {
+        for (int j = 1; j <= ny; ++j) {
+          A[j] = -temp1 * nuv / (dy[j] * dyf[j]);
+          B[j] = 1. - temp1 * nuv * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
+          C[j] = -temp1 * nuv / (dy[j + 1] * dyf[j]);
+        }
+      } else if (kind == 1) {
+        for (int j = 2; j <= ny; ++j) {
+          A[j] = -temp1 * nuv / (dyf[j - 1] * dy[j]);
+          B[j] = 1. + temp1 * nuv / (dyf[j] * dy[j]) + temp1 * nuv / (dyf[j - 1] * dy[j]);
+          C[j] = -temp1 * nuv / (dyf[j] * dy[j]);
+        }
+      } else {
+        const double tm = temp1 / ctx->p.pr[kind - 2] * nuv;
+        for (int j = 1; j <= ny; ++j) {
+          A[j] = -tm / (dy[j] * dyf[j]);
+          B[j] = 1. + tm / (dy[j + 1] * dyf[j]) + tm / (dy[j] * dyf[j]);
+          C[j] = -tm / (dy[j + 1] * dyf[j]);
+        }
+      }
+    }
+    if (!ctx->d_kc[rk]) {
+      int rc = dev_alloc(ctx, (void**)&ctx->d_kc[rk], kc.size() * sizeof(double));
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->d_kc[rk], kc.data(), kc.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  std::vector<double> met((size_t)MET_N * n, 0.0);
+  for (int j = 1; j <= ny; ++j) {
+    met[MET_PA * n + j] = 1. / (dy[j] * dyf[j]);
+    met[MET_PC * n + j] = 1. / (dy[j + 1] * dyf[j]);
+    met[MET_PB0 * n + j] = -1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]);
+    met[MET_IDYF * n + j] = 1.0 / dyf[j];
+  }
+  for (int j = 1; j <= ny + 1; ++j) met[MET_IDY * n + j] = 1.0 / dy[j];
+  for (int j = 2; j <= ny; ++j) {
+    met[MET_WB1 * n + j] = dyf[j - 1] / (2.0 * dy[j]);
+    met[MET_WB2 * n + j] = dyf[j] / (2.0 * dy[j]);
+  }
+  if (!ctx->d_met) {
+    int rc = dev_alloc(ctx, (void**)&ctx->d_met, met.size() * sizeof(double));
+    if (rc) return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->d_met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
 static void fill_solve_args(diablo_ctx* ctx, SolveArgs& a, int rk) {
   memset(&a, 0, sizeof(a));
   const diablo_params& p = ctx->p;
@@ -456,9 +546,54 @@ static int substep(diablo_ctx* ctx, int rk) {
     else a.nl32[f] = (const float2*)ctx->nl[f];
   }
   a.store_cf = rk < 3 ? 1 : 0;
+  // tiled kernel: the schedule of tiles this substep needs
+  Solve2Args& A = ctx->solve2;
+  A.s = a;
+  A.kc = ctx->d_kc[rk - 1];
+  A.met = ctx->d_met;
+  A.nstep = 0;
+  bool fits = true;
+  auto add = [&](int op, int arg, double coef, const void* src, void* dst, const void* src2) {
+    if (A.nstep >= T2_MAXSTEPS) { fits = false; return; }
+    A.steps[A.nstep++] = TileStep{op, arg, coef, src, dst, src2};
+  };
+  const diablo_params& p = ctx->p;
+  const int f32 = ctx->precision == DIABLO_FP64 ? 0 : 1;
+  for (int comp = 0; comp < 3; comp += 2) {
+    add(OP_OWN_U13, comp, 0, a.cu_in[comp], nullptr, nullptr);
+    if (a.roinvd != 0.0) add(OP_ADD_CF, 0, comp == 0 ? a.roinvd : -a.roinvd, a.cu_in[2 - comp], nullptr, nullptr);
+    const double g = comp == 0 ? p.grav_x : p.grav_z;
+    if (g != 0.0)
+      for (int n = 0; n < ctx->nth; ++n) add(OP_ADD_CF, 0, g, a.cth_in[n], nullptr, nullptr);
+    add(OP_NL, f32, 0, ctx->nl[comp], a.store_cf ? a.cf_out[comp] : nullptr, nullptr);
+    if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[comp], nullptr, nullptr);
+    add(OP_SOLVE, comp, 0, nullptr, a.cu_out[comp], a.cu_in[comp]);
+  }
+  add(OP_OWN_U2, 1, 0, a.cu_in[1], nullptr, nullptr);
+  if (p.grav_y != 0.0)
+    for (int n = 0; n < ctx->nth; ++n) add(OP_BUOY, 0, p.grav_y, a.cth_in[n], nullptr, nullptr);
+  add(OP_NL, f32, 0, ctx->nl[1], a.store_cf ? a.cf_out[1] : nullptr, nullptr);
+  if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[1], nullptr, nullptr);
+  add(OP_SOLVE, 1, 0, nullptr, a.cu_out[1], a.cu_in[1]);
+  for (int n = 0; n < ctx->nth; ++n) {
+    add(OP_OWN_TH, n, 0, a.cth_in[n], nullptr, nullptr);
+    if (p.dthdx[n] != 0.0) add(OP_ADD_CF, 0, -p.dthdx[n], a.cu_in[0], nullptr, nullptr);
+    if (p.dthdz[n] != 0.0) add(OP_ADD_CF, 0, -p.dthdz[n], a.cu_in[2], nullptr, nullptr);
+    add(OP_NL, f32, 0, ctx->nl[3 + n], a.store_cf ? a.cf_out[3 + n] : nullptr, nullptr);
+    if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[3 + n], nullptr, nullptr);
+    add(OP_SOLVE, 3 + n, 0, nullptr, a.cth_out[n], a.cth_in[n]);
+  }
+  add(OP_POISSON, 0, 0, nullptr, nullptr, nullptr);
+  add(OP_PROJ, 0, 0, a.cu_out[0], a.cu_out[0], nullptr);
+  add(OP_PROJ, 2, 0, a.cu_out[2], a.cu_out[2], nullptr);
+  add(OP_PROJ, 1, 0, a.cu_out[1], a.cu_out[1], nullptr);
+  add(OP_CP, 0, 0, nullptr, a.cp_out, nullptr);
   {
     Prof pr(ctx, K_SOLVE);
-    if ((rc = launch_solve(a, false, ctx->stream))) return rc;
+    // thermal-wind forcing (flavor 'Front') keeps the general kernel
+    if (fits && !a.front && !ctx->use_general_solver) rc = launch_tiles(A, ctx->stream);
+    else rc = launch_solve(a, false, ctx->stream);
+    if (rc) return rc;
   }
   CK(cudaGetLastError());
   ctx->cur = nx_;
@@ -533,6 +668,10 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
   for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * p->delta_t;
   ctx->w_top_transient = p->w_bc_ymax_c1;
   ctx->precision = p->precision;
+  {
+    const char* e = getenv("DIABLO_GENERAL_SOLVER");
+    ctx->use_general_solver = (e && e[0] == '1') ? 1 : 0;
+  }
   int rc = 0;
 #define FAIL(code) do { *status = (code); diablo_destroy(ctx); return nullptr; } while (0)
   if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -580,6 +719,7 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
       if ((rc = dev_alloc(ctx, (void**)&ctx->cf[b][f], four_elems(ctx) * sizeof(double2)))) FAIL(rc);
   }
   if ((rc = dev_alloc(ctx, (void**)&ctx->d_flag, sizeof(int)))) FAIL(rc);
+  if ((rc = upload_coefficients(ctx))) FAIL(rc);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) FAIL(DIABLO_ERR_CUDA);
 #undef FAIL
   *status = 0;
@@ -882,9 +1022,10 @@ int diablo_set_time(diablo_ctx* ctx, double time, int time_step, double delta_t)
   if (!ctx || !(delta_t > 0)) return DIABLO_ERR_ARG;
   ctx->time = time;
   ctx->time_step = time_step;
+  const bool changed = delta_t != ctx->delta_t;
   ctx->delta_t = delta_t;
   for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * delta_t;
-  return 0;
+  return changed ? upload_coefficients(ctx) : 0;
 }
 
 int diablo_set_stream(diablo_ctx* ctx, void* stream) {

@@ -165,8 +165,12 @@ DI void step2(C (&u)[N2], int k1, const C* sm) {
   RegDFT<N2, DIR, C>::run(u);
 }
 
+// Complex elements of one sequence's tile, padded so that consecutive tiles
+// start 64 bytes apart modulo 128: two sequences in one warp then use
+// disjoint shared-memory banks.
 template <int N1, int N2> struct SmemSize {
-  static constexpr int v = N1 * Pitch<N2>::v;  // complex elements per sequence
+  static constexpr int raw = N1 * Pitch<N2>::v;
+  static constexpr int v = raw + ((((raw * 8) % 128) == 64) ? 0 : ((128 + 64 - (raw * 8) % 128) % 128) / 8);
 };
 
 }  // namespace dfft

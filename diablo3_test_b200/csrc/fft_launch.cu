@@ -82,13 +82,13 @@ int launch_xinv(const XInvArgs<C>& a, int m, int nplanes, int nfield, cudaStream
 // ---- x forward ----
 template <typename T, int N1, int N2, bool NL>
 static void launch_xfwd_t(const XFwdArgs<T>& a, int nplanes, int nfield, cudaStream_t s) {
-  typedef typename CT<T>::C C;
-  constexpr int M = N1 * N2;
-  constexpr int ROW = (M + 1 + dfft::SmemSize<N1, N2>::v) * (int)sizeof(C);
-  constexpr int KT0 = (40 * 1024) / ROW;
-  constexpr int KT = KT0 >= 16 ? 16 : (KT0 >= 8 ? 8 : (KT0 >= 4 ? 4 : 2));
-  dim3 blk(N2, KT), grd((a.g.nz + KT - 1) / KT, nplanes, nfield);
-  k_xr2c<T, N1, N2, KT, NL><<<grd, blk, 0, s>>>(a);
+  // rows per block: as many as fit ~56 KB of shared memory, at most 16
+  constexpr int KT = XFwdSmem<T, N1, N2, 16>::bytes <= 57344 ? 16
+                   : (XFwdSmem<T, N1, N2, 8>::bytes <= 57344 ? 8 : 4);
+  constexpr int SMB = XFwdSmem<T, N1, N2, KT>::bytes;
+  cudaFuncSetAttribute(k_xr2c<T, N1, N2, KT, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMB);
+  dim3 blk(N2, KT), grd(nfield, (a.g.nz + KT - 1) / KT, nplanes);
+  k_xr2c<T, N1, N2, KT, NL><<<grd, blk, SMB, s>>>(a);
 }
 template <typename T, bool NL>
 int launch_xfwd(const XFwdArgs<T>& a, int m, int nplanes, int nfield, cudaStream_t s) {

@@ -293,26 +293,40 @@ DI Pair<T> nl_term(const XFwdArgs<T>& a, int f, int q, int j, size_t off, size_t
   return r;
 }
 
+// Shared-memory bytes of k_xr2c for a given configuration.
+template <typename T, int N1, int N2, int KT>
+struct XFwdSmem {
+  typedef typename CT<T>::C C;
+  static constexpr int M = N1 * N2;
+  static constexpr int NKX1 = (2 * M) / 3 + 1;   // upper bound of Nkx+1
+  static constexpr int bytes =
+      (KT * dfft::SmemSize<N1, N2>::v + KT * (M + 1) + 2 * NKX1 * (KT + 1)) * (int)sizeof(C);
+};
+
 template <typename T, int N1, int N2, int KT, bool NL>
 __global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   constexpr int M = N1 * N2;
   constexpr int SM = dfft::SmemSize<N1, N2>::v;
-  constexpr int NS = N1;  // output slots per thread (m = t + s*N2 <= Nkx < M)
-  __shared__ C sm[KT][SM];
-  __shared__ C zs[KT][M + 1];
+  constexpr int NKX1 = XFwdSmem<T, N1, N2, KT>::NKX1;
+  constexpr int NS = (NKX1 + N2 - 1) / N2;  // output slots per thread
+  constexpr int OP = KT + 1;
+  extern __shared__ __align__(16) unsigned char xr2c_smem[];
+  C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][SM]  four-step tile
+  C* zsb = smb + KT * SM;                              // [KT][M+1] natural order
+  C* acc = zsb + KT * (M + 1);                         // [2][NKX1][OP] outputs A, B
   const int t = threadIdx.x, r = threadIdx.y;
-  const int k0 = blockIdx.x * KT;
-  const int j = a.j0 + blockIdx.y;
-  const int f = blockIdx.z;
+  // field fastest: the blocks that read the same input rows run together
+  const int f = blockIdx.x;
+  const int k0 = blockIdx.y * KT;
+  const int j = a.j0 + blockIdx.z;
   const int nz = a.g.nz, nx = a.g.nx, nkx1 = a.g.nkx1;
   const int row = min(k0 + r, nz - 1);
   const size_t ps = (size_t)nz * nx;
   const size_t rowoff = (size_t)j * ps + (size_t)row * nx;
   const T sc = (T)a.scale;
-  C accA[NS], accB[NS];
-#pragma unroll
-  for (int s = 0; s < NS; ++s) { accA[s] = czero<C>(); accB[s] = czero<C>(); }
+  C* sm = smb + r * SM;
+  C* zs = zsb + r * (M + 1);
   constexpr int NQ = NL ? 3 : 1;
   for (int q = 0; q < NQ; ++q) {
     C v[N1];
@@ -326,47 +340,39 @@ __global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
         v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * n);
       }
     }
-    dfft::step1<N1, N2, -1>(v, t, a.twM, sm[r]);
+    dfft::step1<N1, N2, -1>(v, t, a.twM, sm);
     __syncthreads();
     for (int k1 = t; k1 < N1; k1 += N2) {
       C u[N2];
-      dfft::step2<N1, N2, -1>(u, k1, sm[r]);
+      dfft::step2<N1, N2, -1>(u, k1, sm);
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) zs[r][k1 + N1 * k2] = u[k2];
+      for (int k2 = 0; k2 < N2; ++k2) zs[k1 + N1 * k2] = u[k2];
     }
-    if (t == 0) zs[r][M] = zs[r][0];
+    if (t == 0) zs[M] = zs[0];
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       int m = t + s * N2;
       if (m < nkx1) {
-        C zm = zs[r][m], zc = conj(zs[r][M - m]);
+        C zm = zs[m], zc = conj(zs[M - m]);
         C e = (T)0.5 * (zm + zc);
         C o = (T)0.5 * (zm - zc);
-        C x = e - mul_i(cmul(a.twX[m], o));
-        x = sc * x;
-        if (!NL || q == 0) accA[s] = x;
-        else if (q == 1) accB[s] = mul_ik((T)a.kx[m], x);
-        else accB[s] = accB[s] + x;
+        C x = sc * (e - mul_i(cmul(a.twX[m], o)));
+        // each thread owns its (m, r) entries: no synchronisation needed
+        if (!NL || q == 0) acc[m * OP + r] = x;
+        else if (q == 1) acc[(NKX1 + m) * OP + r] = mul_ik((T)a.kx[m], x);
+        else acc[(NKX1 + m) * OP + r] = acc[(NKX1 + m) * OP + r] + x;
       }
     }
     __syncthreads();
   }
-  // transpose through shared memory so that stores run along k
-  C* os = &sm[0][0];  // reuse: [m][KT+1]
-  const int OP = KT + 1;
+  // stores run along k (KT consecutive rows per mode)
   for (int pass = 0; pass < (NL ? 2 : 1); ++pass) {
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      int m = t + s * N2;
-      if (m < nkx1) os[m * OP + r] = pass == 0 ? accA[s] : accB[s];
-    }
-    __syncthreads();
     C* dst = (pass == 0 ? a.outA[f] : a.outB[f]) + (size_t)j * nkx1 * nz;
+    const C* src = acc + pass * NKX1 * OP;
     for (int idx = r * N2 + t; idx < nkx1 * KT; idx += N2 * KT) {
       int rr = idx % KT, m = idx / KT;
-      if (k0 + rr < nz) dst[(size_t)m * nz + k0 + rr] = os[m * OP + rr];
+      if (k0 + rr < nz) dst[(size_t)m * nz + k0 + rr] = src[m * OP + rr];
     }
-    __syncthreads();
   }
 }

@@ -1,0 +1,452 @@
+// Tiled Fourier-space column kernel (the default path of the column solve).
+//
+// Same mathematics as k_column_solve (kernels_solve.cuh): explicit RK terms,
+// explicit Crank-Nicolson half, implicit y solves with wall rows, projection
+// and pressure update (for/channel.f90:29-249, :468-514, :553-877, :901-911,
+// rem_div_chan :946-1023), one warp per (kx, kz) column.  The difference is
+// the data path: a block owns 4 adjacent kz columns of one kx, and every
+// field it needs moves through shared memory as an (Ny+2) x 4 tile copied with
+// cp.async (16-byte pieces, 64-byte rows), double buffered so the next tile is
+// in flight while the current one is consumed.  Lanes then read their own
+// rows (and y-neighbours) from shared memory.  The host builds the list of
+// tiles (`steps`) once per substep; terms whose coefficient is zero are not
+// loaded at all.
+#pragma once
+#include "common.cuh"
+#include "kernels_solve.cuh"
+
+#define T2_COLS 4
+#define T2_PITCH 5      // complex elements per tile row (4 + 1 pad)
+#define T2_MAXSTEPS 96
+
+enum TileOp {
+  OP_OWN_U13 = 1,  // u1/u3 own field: cf = -nu kk u ; cr = u + t1v*lap(u)      arg: comp
+  OP_OWN_U2,       // u2 own field (staggered metric)
+  OP_OWN_TH,       // scalar own field                                        arg: scalar
+  OP_ADD_CF,       // cf += coef * tile
+  OP_BUOY,         // cf += grav_y * interp_y(tile), rows 2..Nyp, not the (0,0) mode
+  OP_NL,           // cf -= tile ; store cf ; cr += temp5*cf                  arg: fp32 flag
+  OP_CFOLD,        // cr += temp3 * tile
+  OP_SOLVE,        // pressure gradient, matrix + wall rows, solve, store     arg: field kind
+  OP_POISSON,      // phi from the accumulated divergence
+  OP_PROJ,         // tile = new velocity; subtract grad phi; store           arg: comp
+  OP_CP            // cp_out = cp_in + phi/temp4
+};
+
+struct TileStep {
+  int op, arg;
+  double coef;
+  const void* src;   // tile source (nullptr: no tile)
+  void* dst;         // store target (cf_out, cu_out, ...)
+  const void* src2;  // rows outside the write range are copied from here (OP_SOLVE)
+};
+
+// Row coefficients precomputed on the host (the reference's expressions,
+// for/channel.f90:664-670, :726-733, :782-788, :969-976):
+//   kc[kind][3][n]  implicit rows A, B, C of this substep; kind 0 = u1/u3,
+//                   1 = u2, 2+n = scalar n.  The explicit Crank-Nicolson half is
+//                   u - C (u(j+1) - u(j)) + A (u(j) - u(j-1)).
+//   met[7][n]       Poisson A, C, B without k^2; 1/dy; 1/dyf; buoyancy weights
+//                   dyf(j-1)/(2dy(j)), dyf(j)/(2dy(j)).
+enum { MET_PA = 0, MET_PC, MET_PB0, MET_IDY, MET_IDYF, MET_WB1, MET_WB2, MET_N };
+
+struct Solve2Args {
+  SolveArgs s;
+  const double* kc;
+  const double* met;
+  int nstep;
+  TileStep steps[T2_MAXSTEPS];
+};
+
+namespace csolve2 {
+
+DI void cp_async16(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+DI void cp_async8(void* smem, const void* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+DI void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> DI void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// issue the copies of one (n x 4) tile; element bytes 16 (double2) or 8 (float2)
+DI void load_tile(void* tile, const void* g, bool fp32, size_t ps, size_t cbase, int nvalid,
+                  int n, int tid, int nthr) {
+  if (g) {
+    for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
+      const int j = idx >> 2, c = idx & 3;
+      if (c < nvalid) {
+        if (fp32)
+          cp_async8((float2*)tile + j * T2_PITCH + c, (const float2*)g + j * ps + cbase + c);
+        else
+          cp_async16((double2*)tile + j * T2_PITCH + c, (const double2*)g + j * ps + cbase + c);
+      } else {
+        if (fp32) ((float2*)tile)[j * T2_PITCH + c] = make_float2(0.f, 0.f);
+        else ((double2*)tile)[j * T2_PITCH + c] = make_double2(0.0, 0.0);
+      }
+    }
+  }
+  cp_commit();
+}
+
+}  // namespace csolve2
+
+namespace csolve2 {
+// warp_tridiag with b supplied row by row (it is only read by the forward sweep)
+template <int R, typename BF>
+DI void warp_tridiag_b(double (&a)[R], BF bf, double (&c)[R], double2 (&d)[R], int lane) {
+  using namespace csolve;
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    double ib = 1.0 / bf(r);
+    a[r] *= ib; c[r] *= ib; d[r] = ib * d[r];
+  }
+#pragma unroll
+  for (int r = 2; r < R; ++r) {
+    double ib = 1.0 / (bf(r) - a[r] * c[r - 1]);
+    d[r] = ib * (d[r] - a[r] * d[r - 1]);
+    a[r] = -ib * a[r] * a[r - 1];
+    c[r] = ib * c[r];
+  }
+#pragma unroll
+  for (int r = R - 3; r >= 1; --r) {
+    d[r] = d[r] - c[r] * d[r + 1];
+    a[r] = a[r] - c[r] * a[r + 1];
+    c[r] = -c[r] * c[r + 1];
+  }
+  {
+    double ib = 1.0 / (1.0 - c[0] * a[1]);
+    d[0] = ib * (d[0] - c[0] * d[1]);
+    a[0] = ib * a[0];
+    c[0] = -ib * c[0] * c[1];
+  }
+  const double as = a[0], gs = c[0];
+  const double2 ds = d[0];
+  const double ae = a[R - 1], ge = c[R - 1];
+  const double2 de = d[R - 1];
+  double ae_m = __shfl_up_sync(0xffffffffu, ae, 1);
+  double ge_m = __shfl_up_sync(0xffffffffu, ge, 1);
+  double2 de_m = shfl_up2(de, 1);
+  if (lane == 0) { ae_m = 0.0; ge_m = 0.0; de_m = make_double2(0.0, 0.0); }
+  double L = -as * ae_m;
+  double D = 1.0 - as * ge_m - gs * ae;
+  double U = -gs * ge;
+  double2 Q = ds - as * de_m - gs * de;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    double Lm = __shfl_up_sync(0xffffffffu, L, s);
+    double Dm = __shfl_up_sync(0xffffffffu, D, s);
+    double Um = __shfl_up_sync(0xffffffffu, U, s);
+    double2 Qm = shfl_up2(Q, s);
+    double Lp = __shfl_down_sync(0xffffffffu, L, s);
+    double Dp = __shfl_down_sync(0xffffffffu, D, s);
+    double Up = __shfl_down_sync(0xffffffffu, U, s);
+    double2 Qp = shfl_down2(Q, s);
+    if (lane < s) { Lm = 0.0; Dm = 1.0; Um = 0.0; Qm = make_double2(0.0, 0.0); }
+    if (lane + s >= 32) { Lp = 0.0; Dp = 1.0; Up = 0.0; Qp = make_double2(0.0, 0.0); }
+    double k1 = L / Dm, k2 = U / Dp;
+    L = -k1 * Lm;
+    U = -k2 * Up;
+    D = D - k1 * Um - k2 * Lp;
+    Q = Q - k1 * Qm - k2 * Qp;
+  }
+  double2 S = (1.0 / D) * Q;
+  double2 Sn = shfl_down2(S, 1);
+  if (lane == 31) Sn = make_double2(0.0, 0.0);
+  double2 E = de - ae * S - ge * Sn;
+  d[0] = S;
+  d[R - 1] = E;
+#pragma unroll
+  for (int r = 1; r < R - 1; ++r) d[r] = d[r] - a[r] * S - c[r] * E;
+}
+}  // namespace csolve2
+
+#define T2_STAGES 3
+
+template <int R>
+__global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ Solve2Args A) {
+  using namespace csolve;
+  using namespace csolve2;
+  const SolveArgs& a = A.s;
+  extern __shared__ __align__(16) unsigned char t2_smem[];
+  const int n = a.n, nyp = a.nyp;
+  const int tsz = n * T2_PITCH;
+  double2* Tcp = reinterpret_cast<double2*>(t2_smem);
+  double2* Tbase = Tcp + tsz;                         // T2_STAGES streamed tiles
+  double2* dvs = Tbase + T2_STAGES * tsz;             // lane-private divergence rows
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int lane = tid & 31, c = tid >> 5;
+  const int ngroups = (a.nk2 + T2_COLS - 1) / T2_COLS;
+  const int m = blockIdx.x / ngroups;
+  const int kq0 = (blockIdx.x % ngroups) * T2_COLS;
+  const int nvalid = min(T2_COLS, a.nk2 - kq0);
+  const bool valid = c < nvalid;
+  const int kq = min(kq0 + c, a.nk2 - 1);
+  const size_t ps = (size_t)a.nkx1 * a.kp;
+  const size_t cbase = (size_t)m * a.kp + kq0;
+  const bool m00 = (m == 0 && kq == 0 && valid);
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double k2s = kxm * kxm + kzq * kzq;
+  const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+  const double2 z2 = make_double2(0.0, 0.0);
+  const int j0 = lane * R;
+  const double v00 = m00 ? 1.0 : 0.0;
+  const double* met = A.met;
+  double2* dv = dvs + c * (32 * R) + j0;              // this lane's R rows
+
+  double2 cr[R], cf[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) { cr[r] = z2; cf[r] = z2; dv[r] = z2; }
+  int lo = 0, hi = -1;           // explicit row range of the current field
+  const double* K = A.kc;        // implicit rows of the current field
+
+  load_tile(Tcp, a.cp_in, false, ps, cbase, nvalid, n, tid, nthr);
+  for (int q = 0; q < T2_STAGES - 1; ++q) {
+    const TileStep* st = q < A.nstep ? &A.steps[q] : nullptr;
+    load_tile(Tbase + q * tsz, st ? st->src : nullptr, st && st->op == OP_NL && st->arg, ps, cbase,
+              nvalid, n, tid, nthr);
+  }
+  for (int k = 0; k < A.nstep; ++k) {
+    const TileStep st = A.steps[k];
+    {
+      const int kn = k + T2_STAGES - 1;
+      const TileStep* nx = kn < A.nstep ? &A.steps[kn] : nullptr;
+      load_tile(Tbase + (kn % T2_STAGES) * tsz, nx ? nx->src : nullptr,
+                nx && nx->op == OP_NL && nx->arg, ps, cbase, nvalid, n, tid, nthr);
+      cp_wait<T2_STAGES - 1>();
+    }
+    __syncthreads();
+    double2* T = Tbase + (k % T2_STAGES) * tsz;
+    const float2* T32 = reinterpret_cast<const float2*>(T);
+    auto TV = [&](int j) -> double2 { return T[j * T2_PITCH + c]; };
+
+    switch (st.op) {
+      case OP_OWN_U13:
+      case OP_OWN_U2:
+      case OP_OWN_TH: {
+        int kind;
+        if (st.op == OP_OWN_U13) { lo = a.jstart; hi = a.jend; kind = 0; }
+        else if (st.op == OP_OWN_U2) { lo = 2; hi = nyp; kind = 1; }
+        else { lo = a.jst[st.arg]; hi = a.jet[st.arg]; kind = 2 + st.arg; }
+        K = A.kc + (size_t)kind * 3 * n;
+        const double cfc = st.op == OP_OWN_TH ? (a.nu / a.pr[st.arg]) * kk : a.nu * kk;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          cr[r] = z2; cf[r] = z2;
+          if (j >= lo && j <= hi) {
+            const double2 u = TV(j), um = TV(j - 1), up = TV(j + 1);
+            cf[r] = -cfc * u;
+            cr[r] = u - K[2 * n + j] * (up - u) + K[j] * (u - um);
+          }
+        }
+        break;
+      }
+      case OP_ADD_CF: {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= lo && j <= hi) cf[r] = cf[r] + st.coef * TV(j);
+        }
+        break;
+      }
+      case OP_BUOY: {
+        if (!m00) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi)
+              cf[r] = cf[r] + st.coef * (met[MET_WB1 * n + j] * TV(j) + met[MET_WB2 * n + j] * TV(j - 1));
+          }
+        }
+        break;
+      }
+      case OP_NL: {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= lo && j <= hi) {
+            double2 nl;
+            if (st.arg) { float2 v = T32[j * T2_PITCH + c]; nl = make_double2(v.x, v.y); }
+            else nl = TV(j);
+            cf[r] = cf[r] - nl;
+            cr[r] = cr[r] + a.temp5 * cf[r];
+          }
+        }
+        if (st.dst) {  // cf for the next substep, stored through the tile
+          __syncthreads();
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j < n) T[j * T2_PITCH + c] = cf[r];
+          }
+          __syncthreads();
+          for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
+            const int j = idx >> 2, cc = idx & 3;
+            if (cc < nvalid && j >= lo && j <= hi)
+              ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+          }
+        }
+        break;
+      }
+      case OP_CFOLD: {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= lo && j <= hi) cr[r] = cr[r] + a.temp3 * TV(j);
+        }
+        break;
+      }
+      case OP_SOLVE: {
+        // st.arg: 0 = u1, 1 = u2, 2 = u3, 3+n = scalar n
+        const int kind = st.arg;
+        int b0, b1;
+        double c0, c1;
+        if (kind == 0) { b0 = a.ubc[0]; b1 = a.ubc[1]; c0 = a.uc1[0]; c1 = a.uc1[1]; }
+        else if (kind == 2) { b0 = a.wbc[0]; b1 = a.wbc[1]; c0 = a.wc1[0]; c1 = a.wc1[1]; }
+        else if (kind == 1) { b0 = a.vbc[0]; b1 = a.vbc[1]; c0 = a.vc1[0]; c1 = a.vc1[1]; }
+        else { b0 = a.thbc[kind - 3][0]; b1 = a.thbc[kind - 3][1]; c0 = a.thc1[kind - 3][0]; c1 = a.thc1[kind - 3][1]; }
+        double Am[R], Cm[R];
+        // wall rows overwrite these entries (for/channel.f90:1545-1876); 0 = interior
+        int wall[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          Am[r] = 0.0; Cm[r] = 0.0; wall[r] = 1;
+          double2 d = z2;
+          if (j >= lo && j <= hi) {
+            d = cr[r];
+            if (kind == 1) {
+              d = d - a.temp4 * met[MET_IDY * n + j] * (Tcp[j * T2_PITCH + c] - Tcp[(j - 1) * T2_PITCH + c]);
+            } else if (kind == 0 || kind == 2) {
+              d = d - a.temp4 * mul_ik(kind == 0 ? kxm : kzq, Tcp[j * T2_PITCH + c]);
+              if (kind == 0 && m00) d.x -= a.px;
+            }
+            Am[r] = K[j]; Cm[r] = K[2 * n + j]; wall[r] = 0;
+          }
+          if (kind == 1) {
+            if (b0 == 0 && (j == 1 || j == 2)) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c0 * v00, 0); }
+            if (b0 == 1 && j == 1) { Am[r] = 0; Cm[r] = 1; wall[r] = -1; d = make_double2(a.dyf[1] * c0 * v00, 0); }
+            if (j == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
+            if (b1 == 0 && (j == nyp || j == nyp + 1)) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c1 * v00, 0); }
+            if (b1 == 1 && j == nyp + 1) { Am[r] = -1; Cm[r] = 0; wall[r] = 1; d = make_double2(a.dyf[nyp] * c1 * v00, 0); }
+          } else {
+            if (j == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
+            if (j == 1) {
+              if (b0 == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c0 * v00, 0); }
+              else { Am[r] = 0; Cm[r] = 1; wall[r] = -1; d = make_double2(a.dy[2] * c0 * v00, 0); }
+            }
+            if (j == nyp) {
+              if (b1 == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c1 * v00, 0); }
+              else { Am[r] = -1; Cm[r] = 0; wall[r] = 1; d = make_double2(a.dy[nyp] * c1 * v00, 0); }
+            }
+            if (j == nyp + 1) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
+          }
+          cr[r] = d;
+        }
+        warp_tridiag_b<R>(Am, [&](int r) -> double {
+          return wall[r] == 0 ? K[n + j0 + r] : (double)wall[r];
+        }, Cm, cr, lane);
+        // divergence of the new velocity (rem_div_chan RHS, for/channel.f90:980-986)
+        if (kind == 0 || kind == 2) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= 1 && j <= nyp) dv[r] = dv[r] + mul_ik(kind == 0 ? kxm : kzq, cr[r]);
+          }
+        } else if (kind == 1) {
+          const double2 xn = shfl_down2(cr[0], 1);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            const double2 xp = r == R - 1 ? xn : cr[r + 1];
+            if (j >= 1 && j <= nyp) dv[r] = dv[r] + met[MET_IDYF * n + j] * (xp - cr[r]);
+          }
+        }
+        const int w0 = (kind == 1) ? 1 : lo - 1;
+        const int w1 = nyp + 1;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j < n) T[j * T2_PITCH + c] = cr[r];
+        }
+        __syncthreads();
+        for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
+          const int j = idx >> 2, cc = idx & 3;
+          if (cc >= nvalid) continue;
+          const size_t o = j * ps + cbase + cc;
+          ((double2*)st.dst)[o] = (j >= w0 && j <= w1) ? T[j * T2_PITCH + cc] : ((const double2*)st.src2)[o];
+        }
+        break;
+      }
+      case OP_POISSON: {
+        double Am[R], Cm[R];
+        const double k2n = -kxm * kxm - kzq * kzq;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          Am[r] = 0.0; Cm[r] = 0.0;
+          double2 d = z2;
+          if (j >= 1 && j <= nyp) {
+            Am[r] = met[MET_PA * n + j];
+            Cm[r] = met[MET_PC * n + j];
+            d = dv[r];
+          }
+          if (j == 1) { Am[r] = 0; Cm[r] = m00 ? 0.0 : -1.0; d = z2; }
+          if (j == nyp) { Am[r] = 1; Cm[r] = 0; d = z2; }
+          cr[r] = d;
+        }
+        warp_tridiag_b<R>(Am, [&](int r) -> double {
+          const int j = j0 + r;
+          return (j == 1) ? 1.0 : (j == nyp ? -1.0 : ((j > 1 && j < nyp) ? k2n + met[MET_PB0 * n + j] : 1.0));
+        }, Cm, cr, lane);  // cr = phi from here on
+        break;
+      }
+      case OP_PROJ: {
+        const int comp = st.arg;
+        const double2 phm = shfl_up2(cr[R - 1], 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= n) continue;
+          double2 u = TV(j);
+          if (comp != 1 && j >= 1 && j <= nyp) u = u - mul_ik(comp == 0 ? kxm : kzq, cr[r]);
+          if (comp == 1 && j >= 2 && j <= nyp) {
+            const double2 pm = r == 0 ? phm : cr[r - 1];
+            u = u - met[MET_IDY * n + j] * (cr[r] - pm);
+          }
+          T[j * T2_PITCH + c] = u;
+        }
+        __syncthreads();
+        const int w0 = comp == 1 ? 2 : 1;
+        for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
+          const int j = idx >> 2, cc = idx & 3;
+          if (cc < nvalid && j >= w0 && j <= nyp) ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+        }
+        break;
+      }
+      case OP_CP: {
+        const double ih = 1.0 / a.temp4;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= n) continue;
+          double2 p = Tcp[j * T2_PITCH + c];
+          if (j >= a.jstart && j <= a.jend) p = p + ih * cr[r];
+          T[j * T2_PITCH + c] = p;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
+          const int j = idx >> 2, cc = idx & 3;
+          if (cc < nvalid) ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+        }
+        break;
+      }
+      default:
+        break;
+    }
+    __syncthreads();
+  }
+}
