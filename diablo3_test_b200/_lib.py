@@ -55,6 +55,7 @@ SIGNATURES = {
     "diablo_kernel_slots": (_i, []),
     "diablo_kernel_name": (ctypes.c_char_p, [_i]),
     "diablo_status_string": (ctypes.c_char_p, [_i]),
+    "diablo_fft_xz_to_fourier_noalloc": (_i, [_i, _i, _i, _vp, _vp, _vp]),
     "diablo_abi_version": (_i, []),
 }
 

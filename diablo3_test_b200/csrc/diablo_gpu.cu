@@ -125,6 +125,7 @@ static void prof_collect(diablo_ctx* ctx) {
 }
 
 #include "fft_launch.h"
+#include "layout_launch.h"
 
 // ---- column solve ----
 template <int R>
@@ -161,6 +162,16 @@ static int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s) {
 #undef X
     default: return DIABLO_ERR_SIZE;
   }
+}
+
+// launchers shared with other translation units (layout_launch.h)
+void launch_ref_to_phys(const double* ref, double* out, int nx, int nz, int nyp2, cudaStream_t s) {
+  size_t tot = (size_t)nyp2 * nz * nx;
+  k_ref_to_phys<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(ref, out, nx, nz, nyp2);
+}
+void launch_four_to_ref(const double2* in, double2* ref, const Geom& g, int nxp, cudaStream_t s) {
+  size_t tot = (size_t)g.nyp2 * g.nk2 * nxp;
+  k_four_to_ref<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(in, ref, g, nxp, nxp + 1, g.nz + 2);
 }
 
 // --------------------------------------------------------------------------
