@@ -80,6 +80,7 @@ struct diablo_ctx {
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
+  double* d_fac[3];         // factored field systems per RK substep (k_factor)
   struct Timed { int slot; cudaEvent_t a, b; };
   std::vector<Timed> timed;        // pending (recorded, not yet read)
   std::vector<cudaEvent_t> pool;   // free events
@@ -147,6 +148,30 @@ static int launch_tiles(const Solve2Args& A, cudaStream_t s) {
   if (R < 3) R = 3;
   switch (R) {
 #define X(r) case r: launch_tiles_t<r>(A, s); return 0;
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return DIABLO_ERR_SIZE;
+  }
+}
+
+template <int R>
+static size_t factor_doubles_t(int nf) { return (size_t)nf * Fac<R>::N * 32; }
+template <int R>
+static void launch_factor_t(const SolveArgs& a, const double* kc, double* out, int nf, cudaStream_t s) {
+  k_factor<R><<<nf, 32, 0, s>>>(a, kc, out);
+}
+static int rows_per_lane(int n) { int R = (n + 31) / 32; return R < 3 ? 3 : R; }
+static size_t factor_doubles(int n, int nf) {
+  switch (rows_per_lane(n)) {
+#define X(r) case r: return factor_doubles_t<r>(nf);
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return 0;
+  }
+}
+static int launch_factor(const SolveArgs& a, const double* kc, double* out, int nf, cudaStream_t s) {
+  switch (rows_per_lane(a.n)) {
+#define X(r) case r: launch_factor_t<r>(a, kc, out, nf, s); return 0;
     X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
 #undef X
     default: return DIABLO_ERR_SIZE;
@@ -318,6 +343,8 @@ static bool is_device_ptr(const void* p) {
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+static void fill_solve_args(diablo_ctx* ctx, SolveArgs& a, int rk);
+
 // --------------------------------------------------------------------------
 // Row coefficients of the implicit solves, evaluated with the reference's
 // expressions (for/channel.f90:664-670 scalars, :726-733 u2, :782-788 and
@@ -363,6 +390,19 @@ static int upload_coefficients(diablo_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->d_kc[rk], kc.data(), kc.size() * sizeof(double), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+  }
+  // the met rows (below) are not used by the factorisation, the kc rows are
+  for (int rk = 0; rk < 3; ++rk) {
+    if (!ctx->d_fac[rk]) {
+      int rc = dev_alloc(ctx, (void**)&ctx->d_fac[rk], factor_doubles(n, ctx->nf) * sizeof(double));
+      if (rc) return rc;
+    }
+    SolveArgs a;
+    fill_solve_args(ctx, a, rk + 1);
+    int rc = launch_factor(a, ctx->d_kc[rk], ctx->d_fac[rk], ctx->nf, ctx->stream);
+    if (rc) return rc;
+    ctx->launches++;
+    CK(cudaGetLastError());
   }
   std::vector<double> met((size_t)MET_N * n, 0.0);
   for (int j = 1; j <= ny; ++j) {
@@ -562,6 +602,7 @@ static int substep(diablo_ctx* ctx, int rk) {
   A.s = a;
   A.kc = ctx->d_kc[rk - 1];
   A.met = ctx->d_met;
+  A.fac = ctx->d_fac[rk - 1];
   A.nstep = 0;
   bool fits = true;
   auto add = [&](int op, int arg, double coef, const void* src, void* dst, const void* src2) {

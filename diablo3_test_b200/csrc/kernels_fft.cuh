@@ -228,7 +228,10 @@ template <typename T> struct XFwdArgs {
   double scale;                  // 1/Nx
 };
 
-// value pair of term q of equation f at (j, row, x = 2n, 2n+1)
+// The four kinds of nonlinear product of for/channel.f90:299-459,553-608 at
+// the x pair (2n, 2n+1) of one row.  Each `fill_*` evaluates all N1 pairs of a
+// thread with straight-line code, so every load of the term is in flight
+// before the first product is formed.
 template <typename T> struct Pair { T a, b; };
 
 template <typename T>
@@ -238,59 +241,85 @@ DI Pair<T> ld2(const T* p) {
   return Pair<T>{v.x, v.y};
 }
 
-template <typename T>
-DI Pair<T> nl_term(const XFwdArgs<T>& a, int f, int q, int j, size_t off, size_t ps) {
-  // off = offset of (j, row, 2n) in a plane-major field; ps = plane stride
+// x(j) * y(j)
+template <typename T, int N1, int N2>
+DI void fill_prod(typename CT<T>::C (&v)[N1], const T* x, const T* y, size_t off, int t) {
+  Pair<T> px[N1], py[N1];
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    const size_t o = off + 2 * (n1 * N2 + t);
+    px[n1] = ld2(x + o); py[n1] = ld2(y + o);
+  }
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) v[n1] = CT<T>::mk(px[n1].a * py[n1].a, px[n1].b * py[n1].b);
+}
+
+// (uf(j+1)u2(j+1) + uf(j)u2(j+1) - uf(j)u2(j) - uf(j-1)u2(j)) / (2 dyf(j))
+template <typename T, int N1, int N2>
+DI void fill_flux(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t off, size_t ps,
+                  T den, int t) {
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    const size_t o = off + 2 * (n1 * N2 + t);
+    Pair<T> p = ld2(uf + o + ps), c = ld2(uf + o), m = ld2(uf + o - ps);
+    Pair<T> vp = ld2(u2 + o + ps), vc = ld2(u2 + o);
+    v[n1] = CT<T>::mk((p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den,
+                      (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den);
+  }
+}
+
+// ((dyf(j) uf(j) + dyf(j-1) uf(j-1)) / (2 dy(j))) * u2(j)
+template <typename T, int N1, int N2>
+DI void fill_interp(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t off, size_t ps,
+                    T dyfj, T dyfm, T den, int t) {
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    const size_t o = off + 2 * (n1 * N2 + t);
+    Pair<T> c = ld2(uf + o), m = ld2(uf + o - ps), w = ld2(u2 + o);
+    v[n1] = CT<T>::mk(((dyfj * c.a + dyfm * m.a) / den) * w.a, ((dyfj * c.b + dyfm * m.b) / den) * w.b);
+  }
+}
+
+// (0.25 (u2(j) + u2(j+1))^2 - 0.25 (u2(j) + u2(j-1))^2) / dy(j)
+template <typename T, int N1, int N2>
+DI void fill_v2(typename CT<T>::C (&v)[N1], const T* u2, size_t off, size_t ps, T dyj, int t) {
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) {
+    const size_t o = off + 2 * (n1 * N2 + t);
+    Pair<T> p = ld2(u2 + o + ps), c = ld2(u2 + o), m = ld2(u2 + o - ps);
+    T sa = c.a + p.a, sb = c.b + p.b, da = c.a + m.a, db = c.b + m.b;
+    v[n1] = CT<T>::mk(((T)0.25 * (sa * sa) - (T)0.25 * (da * da)) / dyj,
+                      ((T)0.25 * (sb * sb) - (T)0.25 * (db * db)) / dyj);
+  }
+}
+
+// term q (0: needs d/dz, 1: needs d/dx, 2: y-flux) of output equation f
+// (0 = u1, 1 = u2, 2 = u3, 3+n = scalar n)
+template <typename T, int N1, int N2>
+DI void nl_fill(typename CT<T>::C (&v)[N1], const XFwdArgs<T>& a, int f, int q, int j, size_t off,
+                size_t ps, int t) {
   const T* u1 = a.in[0];
   const T* u2 = a.in[1];
   const T* u3 = a.in[2];
-  Pair<T> r;
-  if (f == 0 || f == 2) {
-    const T* uf = f == 0 ? u1 : u3;
-    if (q == 0) {  // f=0: u3*u1 (d/dz);  f=2: u3*u3 (d/dz)
-      Pair<T> x = ld2(u3 + off), y = ld2(uf + off);
-      r.a = x.a * y.a; r.b = x.b * y.b;
-    } else if (q == 1) {  // f=0: u1*u1 (d/dx);  f=2: u3*u1 (d/dx)
-      Pair<T> x = ld2(f == 0 ? u1 + off : u3 + off), y = ld2(u1 + off);
-      r.a = x.a * y.a; r.b = x.b * y.b;
-    } else {  // (uf(j+1)u2(j+1) + uf(j)u2(j+1) - uf(j)u2(j) - uf(j-1)u2(j)) / (2 dyf(j))
-      Pair<T> p = ld2(uf + off + ps), c = ld2(uf + off), m = ld2(uf + off - ps);
-      Pair<T> vp = ld2(u2 + off + ps), vc = ld2(u2 + off);
-      T den = (T)(2.0 * a.gm.dyf[j]);
-      r.a = (p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den;
-      r.b = (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den;
-    }
-  } else if (f == 1) {
-    if (q <= 1) {  // q=0: u3 interp * u2 (d/dz);  q=1: u1 interp * u2 (d/dx)
-      const T* uf = q == 0 ? u3 : u1;
-      Pair<T> c = ld2(uf + off), m = ld2(uf + off - ps), v = ld2(u2 + off);
-      T dyfj = (T)a.gm.dyf[j], dyfm = (T)a.gm.dyf[j - 1], den = (T)(2.0 * a.gm.dy[j]);
-      r.a = ((dyfj * c.a + dyfm * m.a) / den) * v.a;
-      r.b = ((dyfj * c.b + dyfm * m.b) / den) * v.b;
-    } else {  // (0.25(u2(j)+u2(j+1))^2 - 0.25(u2(j)+u2(j-1))^2) / dy(j)
-      Pair<T> p = ld2(u2 + off + ps), c = ld2(u2 + off), m = ld2(u2 + off - ps);
-      T dyj = (T)a.gm.dy[j];
-      T sa = c.a + p.a, sb = c.b + p.b, da = c.a + m.a, db = c.b + m.b;
-      r.a = ((T)0.25 * (sa * sa) - (T)0.25 * (da * da)) / dyj;
-      r.b = ((T)0.25 * (sb * sb) - (T)0.25 * (db * db)) / dyj;
-    }
-  } else {
-    const T* th = a.in[f];
-    if (q == 0) {  // th*u3 (d/dz)
-      Pair<T> x = ld2(th + off), y = ld2(u3 + off);
-      r.a = x.a * y.a; r.b = x.b * y.b;
-    } else if (q == 1) {  // th*u1 (d/dx)
-      Pair<T> x = ld2(th + off), y = ld2(u1 + off);
-      r.a = x.a * y.a; r.b = x.b * y.b;
+  if (f == 1) {
+    if (q == 2) {
+      fill_v2<T, N1, N2>(v, u2, off, ps, (T)a.gm.dy[j], t);
     } else {
-      Pair<T> p = ld2(th + off + ps), c = ld2(th + off), m = ld2(th + off - ps);
-      Pair<T> vp = ld2(u2 + off + ps), vc = ld2(u2 + off);
-      T den = (T)(2.0 * a.gm.dyf[j]);
-      r.a = (p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den;
-      r.b = (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den;
+      fill_interp<T, N1, N2>(v, q == 0 ? u3 : u1, u2, off, ps, (T)a.gm.dyf[j], (T)a.gm.dyf[j - 1],
+                             (T)(2.0 * a.gm.dy[j]), t);
     }
+    return;
   }
-  return r;
+  const T* own = f == 0 ? u1 : (f == 2 ? u3 : a.in[f]);
+  if (q == 2) {
+    fill_flux<T, N1, N2>(v, own, u2, off, ps, (T)(2.0 * a.gm.dyf[j]), t);
+  } else if (q == 0) {
+    // f=0: u3*u1; f=2: u3*u3; scalar: th*u3
+    fill_prod<T, N1, N2>(v, f == 0 ? u3 : own, f == 0 ? u1 : u3, off, t);
+  } else {
+    // f=0: u1*u1; f=2: u3*u1; scalar: th*u1
+    fill_prod<T, N1, N2>(v, own, u1, off, t);
+  }
 }
 
 // Shared-memory bytes of k_xr2c for a given configuration.
@@ -299,22 +328,24 @@ struct XFwdSmem {
   typedef typename CT<T>::C C;
   static constexpr int M = N1 * N2;
   static constexpr int NKX1 = (2 * M) / 3 + 1;   // upper bound of Nkx+1
-  static constexpr int bytes =
-      (KT * dfft::SmemSize<N1, N2>::v + KT * (M + 1) + 2 * NKX1 * (KT + 1)) * (int)sizeof(C);
+  // per row one four-step tile (also used for the natural-order spectrum,
+  // which needs M+1 entries) + the two output tiles
+  static constexpr int ROWC = dfft::SmemSize<N1, N2>::v > M + 1 ? dfft::SmemSize<N1, N2>::v : M + 1;
+  static constexpr int bytes = (KT * ROWC + 2 * NKX1 * (KT + 1)) * (int)sizeof(C);
 };
 
 template <typename T, int N1, int N2, int KT, bool NL>
 __global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   constexpr int M = N1 * N2;
-  constexpr int SM = dfft::SmemSize<N1, N2>::v;
+  constexpr int ROWC = XFwdSmem<T, N1, N2, KT>::ROWC;
   constexpr int NKX1 = XFwdSmem<T, N1, N2, KT>::NKX1;
   constexpr int NS = (NKX1 + N2 - 1) / N2;  // output slots per thread
+  constexpr int NR = (N1 + N2 - 1) / N2;    // step-2 rows per thread
   constexpr int OP = KT + 1;
   extern __shared__ __align__(16) unsigned char xr2c_smem[];
-  C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][SM]  four-step tile
-  C* zsb = smb + KT * SM;                              // [KT][M+1] natural order
-  C* acc = zsb + KT * (M + 1);                         // [2][NKX1][OP] outputs A, B
+  C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][ROWC] four-step tile / spectrum
+  C* acc = smb + KT * ROWC;                            // [2][NKX1][OP] outputs A, B
   const int t = threadIdx.x, r = threadIdx.y;
   // field fastest: the blocks that read the same input rows run together
   const int f = blockIdx.x;
@@ -325,30 +356,35 @@ __global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
   const size_t ps = (size_t)nz * nx;
   const size_t rowoff = (size_t)j * ps + (size_t)row * nx;
   const T sc = (T)a.scale;
-  C* sm = smb + r * SM;
-  C* zs = zsb + r * (M + 1);
+  C* sm = smb + r * ROWC;
+  C* zs = sm;  // the natural-order spectrum replaces the tile after step 2
   constexpr int NQ = NL ? 3 : 1;
+#pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
     C v[N1];
+    if (NL) {
+      nl_fill<T, N1, N2>(v, a, f, q, j, rowoff, ps, t);
+    } else {
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      int n = n1 * N2 + t;
-      if (NL) {
-        Pair<T> pr = nl_term<T>(a, f, q, j, rowoff + 2 * n, ps);
-        v[n1] = CT<T>::mk(pr.a, pr.b);
-      } else {
-        v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * n);
-      }
+      for (int n1 = 0; n1 < N1; ++n1)
+        v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * (n1 * N2 + t));
     }
     dfft::step1<N1, N2, -1>(v, t, a.twM, sm);
     __syncthreads();
-    for (int k1 = t; k1 < N1; k1 += N2) {
-      C u[N2];
-      dfft::step2<N1, N2, -1>(u, k1, sm);
+    C u[NR][N2];
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) zs[k1 + N1 * k2] = u[k2];
+    for (int rr = 0; rr < NR; ++rr)
+      if (t + rr * N2 < N1) dfft::step2<N1, N2, -1>(u[rr], t + rr * N2, sm);
+    __syncthreads();
+#pragma unroll
+    for (int rr = 0; rr < NR; ++rr) {
+      const int k1 = t + rr * N2;
+      if (k1 < N1) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) zs[k1 + N1 * k2] = u[rr][k2];
+      }
     }
-    if (t == 0) zs[M] = zs[0];
+    if (t == 0) zs[M] = u[0][0];
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < NS; ++s) {

@@ -54,6 +54,7 @@ struct Solve2Args {
   SolveArgs s;
   const double* kc;
   const double* met;
+  const double* fac;   // factored u1, u2, u3, scalar systems of this substep (see k_factor)
   int nstep;
   TileStep steps[T2_MAXSTEPS];
 };
@@ -162,6 +163,177 @@ DI void warp_tridiag_b(double (&a)[R], BF bf, double (&c)[R], double2 (&d)[R], i
   for (int r = 1; r < R - 1; ++r) d[r] = d[r] - a[r] * S - c[r] * E;
 }
 }  // namespace csolve2
+
+
+// ---- factored solves ----------------------------------------------------------
+// The u1, u2, u3 and scalar systems have the same matrix in every (kx, kz)
+// column (their rows depend on y only; the wall rows on the BC type only), so
+// warp_tridiag's elimination multipliers are computed once per substep by
+// k_factor and each column only replays them on its right-hand side.  The
+// replay performs the same operations on d as warp_tridiag_b.
+// Per-lane item layout (stored [item][lane]):
+template <int R> struct Fac {
+  static constexpr int IB = 0;            // r = 0..R-1
+  static constexpr int ARAW = R;          // r = 2..R-1 (input a of the row)
+  static constexpr int CF = 2 * R;        // r = 1..R-3 (c after the forward sweep)
+  static constexpr int AFIN = 3 * R;      // r = 1..R-2
+  static constexpr int CFIN = 4 * R;      // r = 1..R-2
+  static constexpr int IB0B = 5 * R, C0F = 5 * R + 1, AS = 5 * R + 2, GS = 5 * R + 3;
+  static constexpr int AE = 5 * R + 4, GE = 5 * R + 5, INVD = 5 * R + 6;
+  static constexpr int K1 = 5 * R + 7, K2 = 5 * R + 12;
+  static constexpr int N = 5 * R + 17;
+};
+
+// rows of field kind (0 = u1, 1 = u2, 2 = u3, 3+n = scalar n): interior rows
+// from kc, wall rows of for/channel.f90:1545-1876, identity elsewhere
+template <int R>
+DI void system_rows(const SolveArgs& a, const double* kc, int kind, int lane, double (&Am)[R],
+                    double (&Bm)[R], double (&Cm)[R]) {
+  const int n = a.n, nyp = a.nyp;
+  int lo, hi, b0, b1;
+  const double* K;
+  if (kind == 1) { lo = 2; hi = nyp; K = kc + (size_t)1 * 3 * n; b0 = a.vbc[0]; b1 = a.vbc[1]; }
+  else if (kind == 0 || kind == 2) {
+    lo = a.jstart; hi = a.jend; K = kc;
+    b0 = kind == 0 ? a.ubc[0] : a.wbc[0];
+    b1 = kind == 0 ? a.ubc[1] : a.wbc[1];
+  } else {
+    lo = a.jst[kind - 3]; hi = a.jet[kind - 3]; K = kc + (size_t)(kind - 1) * 3 * n;
+    b0 = a.thbc[kind - 3][0]; b1 = a.thbc[kind - 3][1];
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = lane * R + r;
+    Am[r] = 0.0; Bm[r] = 1.0; Cm[r] = 0.0;
+    if (j >= lo && j <= hi) { Am[r] = K[j]; Bm[r] = K[n + j]; Cm[r] = K[2 * n + j]; }
+    if (kind == 1) {
+      if (b0 == 0 && (j == 1 || j == 2)) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+      if (b0 == 1 && j == 1) { Am[r] = 0; Bm[r] = -1; Cm[r] = 1; }
+      if (j == 0) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+      if (b1 == 0 && (j == nyp || j == nyp + 1)) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+      if (b1 == 1 && j == nyp + 1) { Am[r] = -1; Bm[r] = 1; Cm[r] = 0; }
+    } else {
+      if (j == 0 || j == nyp + 1) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+      if (j == 1) {
+        if (b0 == 0) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+        else { Am[r] = 0; Bm[r] = -1; Cm[r] = 1; }
+      }
+      if (j == nyp) {
+        if (b1 == 0) { Am[r] = 0; Bm[r] = 1; Cm[r] = 0; }
+        else { Am[r] = -1; Bm[r] = 1; Cm[r] = 0; }
+      }
+    }
+  }
+}
+
+// warp_tridiag_b's elimination on the matrix alone, recording its multipliers
+template <int R>
+DI void factor_rows(double (&a)[R], double (&b)[R], double (&c)[R], int lane, double* out) {
+  using F = Fac<R>;
+  auto W = [&](int item, double v) { out[item * 32 + lane] = v; };
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    double ib = 1.0 / b[r];
+    W(F::IB + r, ib);
+    a[r] *= ib; c[r] *= ib;
+  }
+#pragma unroll
+  for (int r = 2; r < R; ++r) {
+    double ib = 1.0 / (b[r] - a[r] * c[r - 1]);
+    W(F::IB + r, ib);
+    W(F::ARAW + r, a[r]);
+    a[r] = -ib * a[r] * a[r - 1];
+    c[r] = ib * c[r];
+  }
+#pragma unroll
+  for (int r = R - 3; r >= 1; --r) {
+    W(F::CF + r, c[r]);
+    a[r] = a[r] - c[r] * a[r + 1];
+    c[r] = -c[r] * c[r + 1];
+  }
+  {
+    double ib = 1.0 / (1.0 - c[0] * a[1]);
+    W(F::IB0B, ib);
+    W(F::C0F, c[0]);
+    a[0] = ib * a[0];
+    c[0] = -ib * c[0] * c[1];
+  }
+#pragma unroll
+  for (int r = 1; r < R - 1; ++r) { W(F::AFIN + r, a[r]); W(F::CFIN + r, c[r]); }
+  const double as = a[0], gs = c[0], ae = a[R - 1], ge = c[R - 1];
+  W(F::AS, as); W(F::GS, gs); W(F::AE, ae); W(F::GE, ge);
+  double ae_m = __shfl_up_sync(0xffffffffu, ae, 1);
+  double ge_m = __shfl_up_sync(0xffffffffu, ge, 1);
+  if (lane == 0) { ae_m = 0.0; ge_m = 0.0; }
+  double L = -as * ae_m;
+  double D = 1.0 - as * ge_m - gs * ae;
+  double U = -gs * ge;
+  int lev = 0;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1, ++lev) {
+    double Lm = __shfl_up_sync(0xffffffffu, L, s);
+    double Dm = __shfl_up_sync(0xffffffffu, D, s);
+    double Um = __shfl_up_sync(0xffffffffu, U, s);
+    double Lp = __shfl_down_sync(0xffffffffu, L, s);
+    double Dp = __shfl_down_sync(0xffffffffu, D, s);
+    double Up = __shfl_down_sync(0xffffffffu, U, s);
+    if (lane < s) { Lm = 0.0; Dm = 1.0; Um = 0.0; }
+    if (lane + s >= 32) { Lp = 0.0; Dp = 1.0; Up = 0.0; }
+    double k1 = L / Dm, k2 = U / Dp;
+    W(F::K1 + lev, k1);
+    W(F::K2 + lev, k2);
+    L = -k1 * Lm;
+    U = -k2 * Up;
+    D = D - k1 * Um - k2 * Lp;
+  }
+  W(F::INVD, 1.0 / D);
+}
+
+// replay of the recorded elimination on one right-hand side (d <- x)
+template <int R>
+DI void apply_factored(const double* __restrict__ fac, double2 (&d)[R], int lane) {
+  using namespace csolve;
+  using F = Fac<R>;
+  auto G = [&](int item) -> double { return __ldg(fac + item * 32 + lane); };
+#pragma unroll
+  for (int r = 0; r < 2; ++r) d[r] = G(F::IB + r) * d[r];
+#pragma unroll
+  for (int r = 2; r < R; ++r) d[r] = G(F::IB + r) * (d[r] - G(F::ARAW + r) * d[r - 1]);
+#pragma unroll
+  for (int r = R - 3; r >= 1; --r) d[r] = d[r] - G(F::CF + r) * d[r + 1];
+  d[0] = G(F::IB0B) * (d[0] - G(F::C0F) * d[1]);
+  const double2 ds = d[0], de = d[R - 1];
+  double2 de_m = shfl_up2(de, 1);
+  if (lane == 0) de_m = make_double2(0.0, 0.0);
+  double2 Q = ds - G(F::AS) * de_m - G(F::GS) * de;
+  int lev = 0;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1, ++lev) {
+    double2 Qm = shfl_up2(Q, s);
+    double2 Qp = shfl_down2(Q, s);
+    if (lane < s) Qm = make_double2(0.0, 0.0);
+    if (lane + s >= 32) Qp = make_double2(0.0, 0.0);
+    Q = Q - G(F::K1 + lev) * Qm - G(F::K2 + lev) * Qp;
+  }
+  const double2 S = G(F::INVD) * Q;
+  double2 Sn = shfl_down2(S, 1);
+  if (lane == 31) Sn = make_double2(0.0, 0.0);
+  const double2 E = de - G(F::AE) * S - G(F::GE) * Sn;
+  d[0] = S;
+  d[R - 1] = E;
+#pragma unroll
+  for (int r = 1; r < R - 1; ++r) d[r] = d[r] - G(F::AFIN + r) * S - G(F::CFIN + r) * E;
+}
+
+// one warp per field kind: factor its system for the substep coefficients kc
+template <int R>
+__global__ void __launch_bounds__(32) k_factor(const __grid_constant__ SolveArgs a, const double* kc,
+                                               double* out) {
+  const int kind = blockIdx.x, lane = threadIdx.x;
+  double Am[R], Bm[R], Cm[R];
+  system_rows<R>(a, kc, kind, lane, Am, Bm, Cm);
+  factor_rows<R>(Am, Bm, Cm, lane, out + (size_t)kind * Fac<R>::N * 32);
+}
 
 #define T2_STAGES 3
 
@@ -308,13 +480,11 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
         else if (kind == 2) { b0 = a.wbc[0]; b1 = a.wbc[1]; c0 = a.wc1[0]; c1 = a.wc1[1]; }
         else if (kind == 1) { b0 = a.vbc[0]; b1 = a.vbc[1]; c0 = a.vc1[0]; c1 = a.vc1[1]; }
         else { b0 = a.thbc[kind - 3][0]; b1 = a.thbc[kind - 3][1]; c0 = a.thc1[kind - 3][0]; c1 = a.thc1[kind - 3][1]; }
-        double Am[R], Cm[R];
-        // wall rows overwrite these entries (for/channel.f90:1545-1876); 0 = interior
-        int wall[R];
+        // right-hand side: explicit terms on the interior rows, wall values
+        // on the wall rows (the matrix itself is in the factor table)
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int j = j0 + r;
-          Am[r] = 0.0; Cm[r] = 0.0; wall[r] = 1;
           double2 d = z2;
           if (j >= lo && j <= hi) {
             d = cr[r];
@@ -324,31 +494,21 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
               d = d - a.temp4 * mul_ik(kind == 0 ? kxm : kzq, Tcp[j * T2_PITCH + c]);
               if (kind == 0 && m00) d.x -= a.px;
             }
-            Am[r] = K[j]; Cm[r] = K[2 * n + j]; wall[r] = 0;
           }
           if (kind == 1) {
-            if (b0 == 0 && (j == 1 || j == 2)) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c0 * v00, 0); }
-            if (b0 == 1 && j == 1) { Am[r] = 0; Cm[r] = 1; wall[r] = -1; d = make_double2(a.dyf[1] * c0 * v00, 0); }
-            if (j == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
-            if (b1 == 0 && (j == nyp || j == nyp + 1)) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c1 * v00, 0); }
-            if (b1 == 1 && j == nyp + 1) { Am[r] = -1; Cm[r] = 0; wall[r] = 1; d = make_double2(a.dyf[nyp] * c1 * v00, 0); }
+            if (b0 == 0 && (j == 1 || j == 2)) d = make_double2(c0 * v00, 0);
+            if (b0 == 1 && j == 1) d = make_double2(a.dyf[1] * c0 * v00, 0);
+            if (j == 0) d = z2;
+            if (b1 == 0 && (j == nyp || j == nyp + 1)) d = make_double2(c1 * v00, 0);
+            if (b1 == 1 && j == nyp + 1) d = make_double2(a.dyf[nyp] * c1 * v00, 0);
           } else {
-            if (j == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
-            if (j == 1) {
-              if (b0 == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c0 * v00, 0); }
-              else { Am[r] = 0; Cm[r] = 1; wall[r] = -1; d = make_double2(a.dy[2] * c0 * v00, 0); }
-            }
-            if (j == nyp) {
-              if (b1 == 0) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = make_double2(c1 * v00, 0); }
-              else { Am[r] = -1; Cm[r] = 0; wall[r] = 1; d = make_double2(a.dy[nyp] * c1 * v00, 0); }
-            }
-            if (j == nyp + 1) { Am[r] = 0; Cm[r] = 0; wall[r] = 1; d = z2; }
+            if (j == 0 || j == nyp + 1) d = z2;
+            if (j == 1) d = make_double2((b0 == 0 ? c0 : a.dy[2] * c0) * v00, 0);
+            if (j == nyp) d = make_double2((b1 == 0 ? c1 : a.dy[nyp] * c1) * v00, 0);
           }
           cr[r] = d;
         }
-        warp_tridiag_b<R>(Am, [&](int r) -> double {
-          return wall[r] == 0 ? K[n + j0 + r] : (double)wall[r];
-        }, Cm, cr, lane);
+        apply_factored<R>(A.fac + (size_t)kind * Fac<R>::N * 32, cr, lane);
         // divergence of the new velocity (rem_div_chan RHS, for/channel.f90:980-986)
         if (kind == 0 || kind == 2) {
 #pragma unroll
