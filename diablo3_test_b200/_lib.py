@@ -37,6 +37,7 @@ SIGNATURES = {
     "diablo_destroy": (_i, [_vp]),
     "diablo_upload_state": (_i, [_vp, _i, _vp, _i]),
     "diablo_download_state": (_i, [_vp, _i, _vp, _i]),
+    "diablo_download_nu_t": (_i, [_vp, _vp]),
     "diablo_fft_xz_to_fourier": (_i, [_vp, _vp, _vp]),
     "diablo_fft_xz_to_physical": (_i, [_vp, _vp, _vp]),
     "diablo_rk_substep": (_i, [_vp, _i]),

@@ -88,6 +88,13 @@ class Channel:
         _lib.check(self.lib.diablo_download_state(self.ctx, field, _ptr(out), layout), "download_state")
         return out
 
+    def download_nu_t(self, out=None) -> np.ndarray:
+        """Eddy viscosity of the last LES substep, reference physical layout."""
+        if out is None:
+            out = self.new_field()
+        _lib.check(self.lib.diablo_download_nu_t(self.ctx, _ptr(out)), "download_nu_t")
+        return out
+
     # -- reference surface ---------------------------------------------
     def fft_xz_to_fourier(self, v, vv):
         _lib.check(self.lib.diablo_fft_xz_to_fourier(self.ctx, _ptr(v), _ptr(vv)), "fft_xz_to_fourier")

@@ -14,6 +14,7 @@
 #include "kernels_layout.cuh"
 #include "kernels_solve.cuh"
 #include "kernels_solve2.cuh"
+#include "kernels_les.cuh"
 
 static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
 static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
@@ -81,6 +82,25 @@ struct diablo_ctx {
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
+  // LES substep buffers (FP64), allocated on first use
+  struct Les {
+    int ready;
+    double2* S[6];            // Fourier strain tensor
+    double2* T[7];            // Fourier stresses and nu_t dU/dy, nu_t dW/dy
+    double2* cr[3 + DIABLO_MAX_TH];
+    double2* thg[2 * DIABLO_MAX_TH];
+    double* Sp[6];            // physical strain / stresses
+    double* tmp[2];
+    double* thp[2 * DIABLO_MAX_TH];
+    double* r[3 + DIABLO_MAX_TH];
+    double *nu_t, *sf, *sg, *c2, *d2;
+    double2* xs[NF_MAX];      // x-spectral scratch of the batched transforms
+    double *d_cf, *d_cg, *d_d2f, *d_d2g, *d_sclf, *d_sclg;
+    int dyn_ready;            // dynamic model: test-filter inputs and plane sums
+    double* dp[DYN_NF];
+    double2* df[DYN_NF];
+    double* dsums;
+  } les;
   struct Timed { int slot; cudaEvent_t a, b; };
   std::vector<Timed> timed;        // pending (recorded, not yet read)
   std::vector<cudaEvent_t> pool;   // free events
@@ -492,7 +512,7 @@ static void update_transient(diablo_ctx* ctx) {
 }
 
 template <typename T>
-static int substep_spectral(diablo_ctx* ctx) {
+static int spectral_inverse(diablo_ctx* ctx) {
   typedef typename CT<T>::C C;
   const int nf = ctx->nf;
   const int c = ctx->cur;
@@ -530,6 +550,18 @@ static int substep_spectral(diablo_ctx* ctx) {
     Prof pr(ctx, K_XINV);
     if ((rc = launch_xinv<C>(a, ctx->M, ctx->nyp2, nf, ctx->stream))) return rc;
   }
+  return 0;
+}
+
+template <typename T>
+static int spectral_nl(diablo_ctx* ctx) {
+  typedef typename CT<T>::C C;
+  const int nf = ctx->nf;
+  const int c = ctx->cur;
+  const C* tz = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tz64 : (const void*)ctx->tz32);
+  const C* tm = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tm64 : (const void*)ctx->tm32);
+  const C* tx = (const C*)(sizeof(T) == 8 ? (const void*)ctx->tx64 : (const void*)ctx->tx32);
+  int rc;
   // 3. nonlinear products + x forward (planes 1..Ny)
   {
     XFwdArgs<T> a;
@@ -570,8 +602,382 @@ static int substep_spectral(diablo_ctx* ctx) {
   return 0;
 }
 
+template <typename T>
+static int substep_spectral(diablo_ctx* ctx) {
+  int rc = spectral_inverse<T>(ctx);
+  return rc ? rc : spectral_nl<T>(ctx);
+}
+
+// ==========================================================================
+// LES substep (FP64): the reference's physical-space path, for/channel.f90
+// :29-911 with les_chan/les_chan_th (for/les.f90:20-1200)
+
+static const double LES_C_SMAG = 0.17;   // for/les.f90:38
+static const double LES_BETA = 3.0;      // for/les.f90:58
+
+static int ensure_les(diablo_ctx* ctx) {
+  diablo_ctx::Les& L = ctx->les;
+  if (L.ready) return 0;
+  const size_t fe = four_elems(ctx) * sizeof(double2), pe = phys_elems(ctx) * sizeof(double);
+  int rc;
+#define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
+  for (int i = 0; i < 6; ++i) { AL(L.S[i], fe); AL(L.Sp[i], pe); }
+  for (int i = 0; i < 7; ++i) AL(L.T[i], fe);
+  for (int f = 0; f < ctx->nf; ++f) { AL(L.cr[f], fe); AL(L.r[f], pe); }
+  for (int i = 0; i < 2 * ctx->nth; ++i) { AL(L.thg[i], fe); AL(L.thp[i], pe); }
+  AL(L.tmp[0], pe); AL(L.tmp[1], pe);
+  AL(L.nu_t, pe); AL(L.sf, pe); AL(L.sg, pe);
+  AL(L.c2, pe * ctx->nf); AL(L.d2, pe * ctx->nf);
+  for (int i = 0; i < NF_MAX; ++i) AL(L.xs[i], xs_elems(ctx) * sizeof(double2));
+  const int n = ctx->nyp2;
+  AL(L.d_cf, n * sizeof(double)); AL(L.d_cg, n * sizeof(double));
+  AL(L.d_d2f, n * sizeof(double)); AL(L.d_d2g, n * sizeof(double));
+  AL(L.d_sclf, n * sizeof(double)); AL(L.d_sclg, n * sizeof(double));
+#undef AL
+  // filter widths Delta^2 and the constant-model scalings (for/les.f90:224-245)
+  std::vector<double> d2f(n, 0.0), d2g(n, 0.0), cf(n, 0.0), cg(n, 0.0), sclf(n, 1.0), sclg(n, 1.0);
+  const double dx1 = ctx->p.lx / ctx->nx, dz1 = ctx->p.lz / ctx->nz;
+  const double c2 = pow(LES_C_SMAG, 2.0);
+  for (int j = 1; j <= ctx->ny; ++j)
+    d2f[j] = pow(dx1 * LES_BETA * ctx->h_dyf[j] * 1.0 * dz1 * LES_BETA, 2.0 / 3.0);
+  for (int j = 1; j <= ctx->ny + 1; ++j)
+    d2g[j] = pow(dx1 * LES_BETA * ctx->h_dy[j] * 2.0 * dz1 * LES_BETA, 2.0 / 3.0);
+  if (ctx->p.les_model_type == 1) {
+    for (int j = 0; j < n; ++j) {
+      cf[j] = c2; cg[j] = c2;
+      sclf[j] = -2.0 * c2 * d2f[j];
+      sclg[j] = -2.0 * c2 * d2g[j];
+    }
+  }
+  CK(cudaMemcpyAsync(L.d_d2f, d2f.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_d2g, d2g.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_cf, cf.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_cg, cg.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_sclf, sclf.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_sclg, sclg.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  L.ready = 1;
+  return 0;
+}
+
+// batched FP64 transforms between the internal Fourier and physical layouts
+static int ifft_batch(diablo_ctx* ctx, const double2* const* four, double* const* phys, int nf) {
+  for (int b = 0; b < nf; b += NF_MAX) {
+    const int m = nf - b < NF_MAX ? nf - b : NF_MAX;
+    ZInvArgs<double2> za;
+    memset(&za, 0, sizeof(za));
+    XInvArgs<double2> xa;
+    memset(&xa, 0, sizeof(xa));
+    for (int f = 0; f < m; ++f) {
+      za.src[f] = four[b + f];
+      za.dst[f] = ctx->les.xs[f];
+      xa.src[f] = ctx->les.xs[f];
+      xa.dst[f] = phys[b + f];
+    }
+    za.nseq = ctx->nyp2 * ctx->nkx1;
+    za.g = ctx->g;
+    za.tw = ctx->tz64;
+    xa.g = ctx->g;
+    xa.twM = ctx->tm64;
+    xa.twX = ctx->tx64;
+    int rc;
+    { Prof pr(ctx, K_ZINV); if ((rc = launch_zinv<double2>(za, ctx->nz, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_XINV); if ((rc = launch_xinv<double2>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
+  }
+  return 0;
+}
+
+static int fft_batch(diablo_ctx* ctx, const double* const* phys, double2* const* four, int nf) {
+  for (int b = 0; b < nf; b += NF_MAX) {
+    const int m = nf - b < NF_MAX ? nf - b : NF_MAX;
+    XFwdArgs<double> xa;
+    memset(&xa, 0, sizeof(xa));
+    ZFwdArgs<double2, double2> za;
+    memset(&za, 0, sizeof(za));
+    for (int f = 0; f < m; ++f) {
+      xa.in[f] = phys[b + f];
+      xa.outA[f] = ctx->les.xs[f];
+      za.srcA[f] = ctx->les.xs[f];
+      za.dst[f] = four[b + f];
+    }
+    xa.g = ctx->g;
+    xa.twM = ctx->tm64;
+    xa.twX = ctx->tx64;
+    xa.kx = ctx->d_kx;
+    xa.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
+    xa.scale = 1.0 / ctx->nx;
+    za.nseq = ctx->nyp2 * ctx->nkx1;
+    za.g = ctx->g;
+    za.tw = ctx->tz64;
+    za.kz = ctx->d_kz;
+    za.scale = 1.0 / ctx->nz;
+    int rc;
+    { Prof pr(ctx, K_OTHER); if ((rc = launch_xfwd<double, false>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_OTHER); if ((rc = launch_zfwd<double2, double2, false>(za, ctx->nz, m, ctx->stream))) return rc; }
+  }
+  return 0;
+}
+
+static int les_active(const diablo_ctx* ctx) {
+  // for/channel.f90:259: LES only after 100 steps of a newly created flow
+  return ctx->p.use_les && (!ctx->p.create_new_flow || ctx->time_step > 100);
+}
+
+static int dynamic_coefficient(diablo_ctx* ctx);
+extern "C" {
+static int bc_post(diablo_ctx* ctx, int do_vel, int do_th);
+}
+
+static int substep_les(diablo_ctx* ctx, int rk) {
+  diablo_ctx::Les& L = ctx->les;
+  const int nf = ctx->nf, nth = ctx->nth;
+  const int c = ctx->cur, nx_ = 1 - c;
+  int rc;
+  if ((rc = ensure_scratch(ctx)) || (rc = ensure_les(ctx))) return rc;
+  update_transient(ctx);
+  const FGeom fg{ctx->ny, ctx->nyp2, ctx->nkx1, ctx->nk2, ctx->kp, (size_t)ctx->nkx1 * ctx->kp};
+  const size_t ftot = four_elems(ctx), ptot = phys_elems(ctx);
+  SolveArgs a;
+  fill_solve_args(ctx, a, rk);
+  for (int q = 0; q < 3; ++q) { a.cu_in[q] = ctx->st[c][q]; a.cu_out[q] = ctx->st[nx_][q]; }
+  a.cp_in = ctx->st[c][3];
+  a.cp_out = ctx->st[nx_][3];
+  for (int n = 0; n < nth; ++n) { a.cth_in[n] = ctx->st[c][4 + n]; a.cth_out[n] = ctx->st[nx_][4 + n]; }
+  double2* cf_out[3 + DIABLO_MAX_TH];
+  for (int f = 0; f < nf; ++f) {
+    a.cf_in[f] = ctx->cf[ctx->cf_cur][f];
+    a.cf_out[f] = cf_out[f] = ctx->cf[1 - ctx->cf_cur][f];
+  }
+  // 1. explicit RK terms from the state before the LES wall/ghost updates
+  {
+    ExplicitArgs2 E;
+    memset(&E, 0, sizeof(E));
+    E.s = a;
+    for (int f = 0; f < nf; ++f) E.cr[f] = L.cr[f];
+    Prof pr(ctx, K_OTHER);
+    k_explicit2<<<grid1d(ftot), 256, 0, ctx->stream>>>(E);
+  }
+  // 2. apply_BC_vel/th_mpi_post and apply_BC_les/th_les on the state (for/les.f90:80-90)
+  if ((rc = bc_post(ctx, 1, 1))) return rc;
+  {
+    LesBcArgs b;
+    memset(&b, 0, sizeof(b));
+    for (int q = 0; q < 3; ++q) b.cu[q] = ctx->st[c][q];
+    for (int n = 0; n < nth; ++n) {
+      b.cth[n] = ctx->st[c][4 + n];
+      b.thbc[n][0] = ctx->p.th_bc_ymin[n];
+      b.thbc[n][1] = ctx->p.th_bc_ymax[n];
+    }
+    b.nth = nth; b.nyp = ctx->ny; b.nkx1 = ctx->nkx1; b.nk2 = ctx->nk2; b.kp = ctx->kp;
+    b.ubc[0] = ctx->p.u_bc_ymin; b.ubc[1] = ctx->p.u_bc_ymax;
+    b.wbc[0] = ctx->p.w_bc_ymin; b.wbc[1] = ctx->p.w_bc_ymax;
+    Prof pr(ctx, K_OTHER);
+    k_les_bc<<<(ctx->nkx1 * ctx->nk2 + 127) / 128, 128, 0, ctx->stream>>>(b);
+  }
+  // 3. strain tensor, 4. strain and u, th to physical space
+  {
+    StrainArgs sa;
+    for (int q = 0; q < 3; ++q) sa.cu[q] = ctx->st[c][q];
+    for (int i = 0; i < 6; ++i) sa.S[i] = L.S[i];
+    sa.kx = ctx->d_kx; sa.kz = ctx->d_kz; sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf; sa.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_strain<<<grid1d(ftot), 256, 0, ctx->stream>>>(sa);
+  }
+  if ((rc = ifft_batch(ctx, L.S, L.Sp, 6))) return rc;
+  if ((rc = spectral_inverse<double>(ctx))) return rc;       // u, th -> ctx->phys
+  double* const* up = (double* const*)ctx->phys;
+  // 5. |S|, the coefficient (dynamic model), eddy viscosity and stresses
+  {
+    LesPointArgs pa;
+    memset(&pa, 0, sizeof(pa));
+    for (int i = 0; i < 6; ++i) pa.S[i] = L.Sp[i];
+    pa.u1 = up[0]; pa.u3 = up[2];
+    pa.nu_t = L.nu_t;
+    pa.tmp[0] = L.tmp[0]; pa.tmp[1] = L.tmp[1];
+    pa.dy = ctx->d_dy; pa.dyf = ctx->d_dyf;
+    pa.cf = L.d_cf; pa.cg = L.d_cg; pa.d2f = L.d_d2f; pa.d2g = L.d_d2g;
+    pa.nx = ctx->nx; pa.nz = ctx->nz; pa.nyp = ctx->ny;
+    pa.dynamic = ctx->p.les_model_type == 2;
+    { Prof pr(ctx, K_OTHER); k_les_norms<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg); }
+    if (ctx->p.les_model_type == 2 && (rc = dynamic_coefficient(ctx))) return rc;
+    { Prof pr(ctx, K_OTHER); k_les_point<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg); }
+  }
+  // 6. stresses to Fourier space, divergence into cf (for/les.f90:245-274, 850-880)
+  {
+    const double* src[7] = {L.Sp[0], L.Sp[2], L.Sp[3], L.Sp[4], L.Sp[5], L.tmp[0], L.tmp[1]};
+    if ((rc = fft_batch(ctx, src, L.T, 7))) return rc;
+    LesDivArgs da;
+    for (int i = 0; i < 7; ++i) da.T[i] = L.T[i];
+    for (int q = 0; q < 3; ++q) da.cf[q] = cf_out[q];
+    da.kx = ctx->d_kx; da.kz = ctx->d_kz; da.dyf = ctx->d_dyf;
+    da.sf = L.d_sclf; da.sg = L.d_sclg; da.g = fg;
+    da.j1 = ctx->jstart; da.j2 = ctx->ny - 1;
+    Prof pr(ctx, K_OTHER);
+    k_les_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(da);
+  }
+  // 7. scalar SGS flux with kappa_t = nu_t (for/les.f90:1130-1200)
+  if (nth > 0) {
+    ThGradArgs ga;
+    memset(&ga, 0, sizeof(ga));
+    for (int n = 0; n < nth; ++n) { ga.cth[n] = ctx->st[c][4 + n]; ga.gx[n] = L.thg[2 * n]; ga.gz[n] = L.thg[2 * n + 1]; }
+    ga.kx = ctx->d_kx; ga.kz = ctx->d_kz; ga.g = fg; ga.nth = nth;
+    { Prof pr(ctx, K_OTHER); k_th_grad<<<grid1d(ftot), 256, 0, ctx->stream>>>(ga); }
+    if ((rc = ifft_batch(ctx, L.thg, L.thp, 2 * nth))) return rc;
+    {
+      ScaleArgs sa;
+      memset(&sa, 0, sizeof(sa));
+      for (int q = 0; q < 2 * nth; ++q) sa.f[q] = L.thp[q];
+      sa.nfield = 2 * nth;
+      sa.w = L.nu_t;                                   // kappa_t = nu_t (:1130-1140)
+      sa.ps = (size_t)ctx->nz * ctx->nx;
+      sa.nyp = ctx->ny;
+      Prof pr(ctx, K_OTHER);
+      k_scale_by<<<grid1d(ptot), 256, 0, ctx->stream>>>(sa);
+    }
+    if ((rc = fft_batch(ctx, L.thp, L.thg, 2 * nth))) return rc;
+    ThDivArgs ta;
+    memset(&ta, 0, sizeof(ta));
+    for (int n = 0; n < nth; ++n) {
+      ta.fx[n] = L.thg[2 * n]; ta.fz[n] = L.thg[2 * n + 1]; ta.cfth[n] = cf_out[3 + n];
+      ta.jst[n] = ctx->jst[n]; ta.jet[n] = ctx->jet[n];
+    }
+    ta.kx = ctx->d_kx; ta.kz = ctx->d_kz; ta.g = fg; ta.nth = nth;
+    Prof pr(ctx, K_OTHER);
+    k_th_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(ta);
+  }
+  // 8. nonlinear terms (as the DNS step), cf -= NL, cr += beta h cf
+  if ((rc = spectral_nl<double>(ctx))) return rc;
+  {
+    CfFinishArgs fa;
+    memset(&fa, 0, sizeof(fa));
+    for (int f = 0; f < nf; ++f) { fa.cf[f] = cf_out[f]; fa.cr[f] = L.cr[f]; fa.nl[f] = ctx->nl[f]; }
+    fa.lo[0] = fa.lo[2] = ctx->jstart; fa.hi[0] = fa.hi[2] = ctx->jend;
+    fa.lo[1] = 2; fa.hi[1] = ctx->ny;
+    for (int n = 0; n < nth; ++n) { fa.lo[3 + n] = ctx->jst[n]; fa.hi[3 + n] = ctx->jet[n]; }
+    fa.nf = nf; fa.temp5 = a.temp5; fa.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_cf_finish<<<grid1d(ftot), 256, 0, ctx->stream>>>(fa);
+  }
+  // 9. r = IFFT(cr); CN in y per physical column; 10. u, th back to Fourier
+  if ((rc = ifft_batch(ctx, L.cr, L.r, nf))) return rc;
+  {
+    PhysSolveArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = up[f]; }
+    sa.nu_t = L.nu_t;
+    for (int n = 0; n < nth; ++n) sa.kap[n] = L.nu_t;
+    sa.c2 = L.c2; sa.d2 = L.d2;
+    sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf;
+    sa.nf = nf; sa.nth = nth; sa.n = ctx->nyp2; sa.nyp = ctx->ny; sa.cols = ctx->nz * ctx->nx;
+    sa.temp1 = a.temp1; sa.temp2 = a.temp2; sa.nu_v = a.nu_v;
+    sa.jstart = ctx->jstart; sa.jend = ctx->jend;
+    for (int n = 0; n < nth; ++n) {
+      sa.jst[n] = ctx->jst[n]; sa.jet[n] = ctx->jet[n]; sa.pr[n] = ctx->p.pr[n];
+      sa.thbc[n][0] = a.thbc[n][0]; sa.thbc[n][1] = a.thbc[n][1];
+      sa.thc1[n][0] = a.thc1[n][0]; sa.thc1[n][1] = a.thc1[n][1];
+    }
+    for (int i = 0; i < 2; ++i) {
+      sa.ubc[i] = a.ubc[i]; sa.vbc[i] = a.vbc[i]; sa.wbc[i] = a.wbc[i];
+      sa.uc1[i] = a.uc1[i]; sa.vc1[i] = a.vc1[i]; sa.wc1[i] = a.wc1[i];
+    }
+    const size_t threads = (size_t)nf * sa.cols;
+    Prof pr(ctx, K_SOLVE);
+    k_phys_solve<<<(unsigned)((threads + 127) / 128), 128, 0, ctx->stream>>>(sa);
+  }
+  {
+    double2* dst[3 + DIABLO_MAX_TH];
+    for (int f = 0; f < nf; ++f) dst[f] = ctx->st[nx_][f < 3 ? f : f + 1];
+    if ((rc = fft_batch(ctx, (const double* const*)up, dst, nf))) return rc;
+  }
+  // 11. projection and pressure update on the new state (for/channel.f90:901-911)
+  {
+    const int R = rows_per_lane(ctx->nyp2);
+    const int warps = 4;
+    dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
+    Prof pr(ctx, K_OTHER);
+    switch (R) {
+#define X(r) case r: k_project<r><<<grd, blk, 0, ctx->stream>>>(a); break;
+      X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+      default: return DIABLO_ERR_SIZE;
+    }
+  }
+  CK(cudaGetLastError());
+  ctx->cur = nx_;
+  if (rk < 3) ctx->cf_cur = 1 - ctx->cf_cur;
+  return 0;
+}
+
+// Dynamic Smagorinsky coefficient C(y) into les.d_cf (GYF) and les.d_cg (GY):
+// build the 21 Germano/Lilly inputs, test-filter them in Fourier space,
+// contract and average over x-z planes.  Needs les.Sp (raw strain), les.sf
+// and the physical velocities in ctx->phys.
+static int dynamic_coefficient(diablo_ctx* ctx) {
+  diablo_ctx::Les& L = ctx->les;
+  int rc;
+  const size_t ptot = phys_elems(ctx), ftot = four_elems(ctx);
+  if (!L.dyn_ready) {
+    for (int q = 0; q < DYN_NF; ++q) {
+      if ((rc = dev_alloc(ctx, (void**)&L.dp[q], ptot * sizeof(double)))) return rc;
+      if ((rc = dev_alloc(ctx, (void**)&L.df[q], ftot * sizeof(double2)))) return rc;
+    }
+    if ((rc = dev_alloc(ctx, (void**)&L.dsums, (size_t)ctx->nyp2 * 12 * sizeof(double)))) return rc;
+    L.dyn_ready = 1;
+  }
+  const size_t ps = (size_t)ctx->nz * ctx->nx;
+  {
+    DynPrepArgs pa;
+    for (int q = 0; q < 3; ++q) pa.u[q] = (const double*)ctx->phys[q];
+    for (int q = 0; q < 6; ++q) pa.S[q] = L.Sp[q];
+    pa.sf = L.sf;
+    for (int q = 0; q < DYN_NF; ++q) pa.out[q] = L.dp[q];
+    pa.nyp = ctx->ny;
+    pa.ps = ps;
+    Prof pr(ctx, K_OTHER);
+    k_dyn_prep<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa);
+  }
+  if ((rc = fft_batch(ctx, L.dp, L.df, DYN_NF))) return rc;
+  const FGeom fg{ctx->ny, ctx->nyp2, ctx->nkx1, ctx->nk2, ctx->kp, (size_t)ctx->nkx1 * ctx->kp};
+  for (int b = 0; b < DYN_NF; b += NF_MAX) {
+    MaskArgs ma;
+    memset(&ma, 0, sizeof(ma));
+    ma.nfield = DYN_NF - b < NF_MAX ? DYN_NF - b : NF_MAX;
+    for (int q = 0; q < ma.nfield; ++q) ma.f[q] = L.df[b + q];
+    ma.mx = ctx->nkx / 2;
+    ma.mz = ctx->nkz / 2;
+    ma.nkz = ctx->nkz;
+    ma.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_test_mask<<<grid1d(ftot), 256, 0, ctx->stream>>>(ma);
+  }
+  if ((rc = ifft_batch(ctx, L.df, L.dp, DYN_NF))) return rc;
+  {
+    DynContractArgs ca;
+    for (int q = 0; q < DYN_NF; ++q) ca.F[q] = L.dp[q];
+    for (int q = 0; q < 3; ++q) ca.u[q] = (const double*)ctx->phys[q];
+    ca.d2f = L.d_d2f;
+    ca.sums = L.dsums;
+    ca.nyp = ctx->ny;
+    ca.ps = ps;
+    ca.ratio2 = 4.0;   // (2 Delta / Delta)^2
+    Prof pr(ctx, K_OTHER);
+    k_dyn_contract<<<ctx->ny, 256, 0, ctx->stream>>>(ca);
+  }
+  {
+    Prof pr(ctx, K_OTHER);
+    k_dyn_coef<<<(ctx->nyp2 + 127) / 128, 128, 0, ctx->stream>>>(L.dsums, ctx->d_dy, ctx->d_dyf, L.d_cf, L.d_cg,
+                                                                  ctx->ny, (double)ps);
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
 static int substep(diablo_ctx* ctx, int rk) {
-  if (ctx->p.use_les) return DIABLO_ERR_UNSUPPORTED;
+  if (les_active(ctx)) {
+    if (ctx->precision != DIABLO_FP64) return DIABLO_ERR_UNSUPPORTED;
+    if (ctx->p.les_model_type != 1 && ctx->p.les_model_type != 2) return DIABLO_ERR_UNSUPPORTED;
+    return substep_les(ctx, rk);
+  }
   int rc = ensure_scratch(ctx);
   if (rc) return rc;
   update_transient(ctx);
@@ -930,6 +1336,21 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout) {
   } else {
     return DIABLO_ERR_ARG;
   }
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_download_nu_t(diablo_ctx* ctx, double* buf) {
+  if (!ctx || !buf) return DIABLO_ERR_ARG;
+  int rc = ensure_bscratch(ctx);
+  if (rc) return rc;
+  const double* src = ctx->les.nu_t;
+  if (!ctx->les.ready) {
+    CK(cudaMemsetAsync(ctx->b_phys, 0, phys_elems(ctx) * sizeof(double), ctx->stream));
+    src = ctx->b_phys;
+  }
+  if ((rc = phys_out(ctx, src, buf))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;

@@ -1,0 +1,699 @@
+// Kernels of the LES substep (eddy viscosity varies in x and z, so the
+// implicit y solves run per physical column as in the reference).
+//
+// Substep order (for/channel.f90:29-911 with les_chan / les_chan_th,
+// for/les.f90:20-1200):
+//   k_explicit      Fourier explicit RK terms from the state before the LES
+//                   wall/ghost updates (:29-249)
+//   (BC post + apply_BC_les on the state)
+//   k_strain        Fourier strain-rate tensor (compute_strain_chan)
+//   inverse FFTs    S1..S6 and u, th to physical space
+//   k_les_point     |S|, eddy viscosity nu_t, SGS stress components and
+//                   nu_t dU/dy, nu_t dW/dy
+//   forward FFTs    stresses
+//   k_les_div       cf -= div(tau) (:850-880)
+//   k_les_th_*      scalar SGS flux with kappa_t = nu_t (:1130-1200)
+//   (nonlinear terms as in the DNS step)
+//   k_cf_finish     cf -= NL, cr += beta h cf
+//   inverse FFT     cr -> r
+//   k_phys_solve    CN explicit half + implicit solve per physical column
+//                   with the eddy-viscosity rows (:494-877)
+//   forward FFT     u, th -> state; projection + pressure (:901-911)
+#pragma once
+#include "common.cuh"
+#include "kernels_fft.cuh"
+#include "kernels_solve.cuh"
+
+#define LES_MAXF 11
+
+// Fourier index helpers: F[j][m][kp], pitch kp
+struct FGeom {
+  int nyp, n;          // Nyp, Ny+2
+  int nkx1, nk2, kp;
+  size_t ps;           // plane stride (elements)
+};
+
+// ---------------------------------------------------------------------------
+// explicit RK terms in Fourier space; one thread per (j, m, kq)
+struct ExplicitArgs2 {
+  SolveArgs s;
+  double2* cr[SOLVE_NF];
+};
+
+__global__ void k_explicit2(const __grid_constant__ ExplicitArgs2 E) {
+  const SolveArgs& a = E.s;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t ps = (size_t)a.nkx1 * a.kp;
+  const size_t tot = (size_t)a.n * ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.kp;
+  if (kq >= a.nk2) return;
+  const int m = (idx / a.kp) % a.nkx1;
+  const int j = idx / ps;
+  const size_t o = idx;
+  const bool m00 = (m == 0 && kq == 0);
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double k2s = kxm * kxm + kzq * kzq;
+  const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+  const int nyp = a.nyp;
+  // u1 / u3 rows jstart..jend (:40-92, :128-153, :184-198)
+  for (int comp = 0; comp < 3; comp += 2) {
+    if (j < a.jstart || j > a.jend) continue;
+    const double2 u = a.cu_in[comp][o];
+    double2 cr = u;
+    if (a.rk > 1) cr = cr + a.temp3 * a.cf_in[comp][o];
+    cr = cr - a.temp4 * mul_ik(comp == 0 ? kxm : kzq, a.cp_in[o]);
+    if (comp == 0 && m00) cr.x -= a.px;
+    double2 cf = -(a.nu * kk) * u;
+    const double2 oth = a.cu_in[2 - comp][o];
+    cf = comp == 0 ? cf + a.roinvd * oth : cf - a.roinvd * oth;
+    for (int th = 0; th < a.nth; ++th) cf = cf + (comp == 0 ? a.grav_x : a.grav_z) * a.cth_in[th][o];
+    E.cr[comp][o] = cr;
+    a.cf_out[comp][o] = cf;
+  }
+  // u2 rows 2..Nyp (:48-100, :136-182)
+  if (j >= 2 && j <= nyp) {
+    const double2 u = a.cu_in[1][o];
+    double2 cr = u;
+    if (a.rk > 1) cr = cr + a.temp3 * a.cf_in[1][o];
+    const double2 pc = a.cp_in[o], pm = a.cp_in[o - ps];
+    cr = cr - a.temp4 * make_double2((pc.x - pm.x) / a.dy[j], (pc.y - pm.y) / a.dy[j]);
+    double2 cf = -(a.nu * kk) * u;
+    if (!m00) {
+      for (int th = 0; th < a.nth; ++th) {
+        const double2 tc = a.cth_in[th][o], tm = a.cth_in[th][o - ps];
+        cf = cf + a.grav_y * make_double2((tc.x * a.dyf[j - 1] + tm.x * a.dyf[j]) / (2.0 * a.dy[j]),
+                                          (tc.y * a.dyf[j - 1] + tm.y * a.dyf[j]) / (2.0 * a.dy[j]));
+      }
+    }
+    E.cr[1][o] = cr;
+    a.cf_out[1][o] = cf;
+  }
+  // scalars rows jstart_th..jend_th (:209-246)
+  for (int th = 0; th < a.nth; ++th) {
+    if (j < a.jst[th] || j > a.jet[th]) continue;
+    const double2 t = a.cth_in[th][o];
+    double2 cr = t;
+    if (a.rk > 1) cr = cr + a.temp3 * a.cf_in[3 + th][o];
+    double2 cf = -((a.nu / a.pr[th]) * kk) * t;
+    cf = cf - a.dthdx[th] * a.cu_in[0][o] - a.dthdz[th] * a.cu_in[2][o];
+    E.cr[3 + th][o] = cr;
+    a.cf_out[3 + th][o] = cf;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Neumann ghost planes for the LES gradients (apply_BC_les / apply_BC_th_les,
+// for/les.f90:2001-2105), one thread per stored mode
+struct LesBcArgs {
+  double2* cu[3];
+  double2* cth[8];
+  int nth, nyp, nkx1, nk2, kp;
+  int ubc[2], wbc[2];
+  int thbc[8][2];
+};
+
+__global__ void k_les_bc(LesBcArgs a) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.nkx1 * a.nk2) return;
+  const int m = idx / a.nk2, kq = idx % a.nk2;
+  const size_t ps = (size_t)a.nkx1 * a.kp, c = (size_t)m * a.kp + kq;
+  const int nyp = a.nyp;
+  auto P = [&](double2* f, int j) -> double2& { return f[(size_t)j * ps + c]; };
+  for (int q = 0; q < 2; ++q) {
+    double2* cu = a.cu[q == 0 ? 0 : 2];
+    const int* b = q == 0 ? a.ubc : a.wbc;
+    if (b[1] == 1) { P(cu, nyp) = P(cu, nyp - 1); P(cu, nyp + 1) = P(cu, nyp); }
+    if (b[0] == 1) { P(cu, 1) = P(cu, 2); P(cu, 0) = P(cu, 1); }
+  }
+  for (int n = 0; n < a.nth; ++n) {
+    double2* ct = a.cth[n];
+    if (a.thbc[n][1] == 1) { P(ct, nyp) = P(ct, nyp - 1); P(ct, nyp + 1) = P(ct, nyp); }
+    if (a.thbc[n][0] == 1) { P(ct, 1) = P(ct, 2); P(ct, 0) = P(ct, 1); }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// strain-rate tensor in Fourier space (compute_strain_chan, :1463-1510 and the
+// ghost_CS2_mpi sentinel of :2521-2527); one thread per (j, m, kq)
+struct StrainArgs {
+  const double2* cu[3];
+  double2* S[6];
+  const double* kx;
+  const double* kz;
+  const double* dy;
+  const double* dyf;
+  FGeom g;
+};
+
+__global__ void k_strain(StrainArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double2 u1 = a.cu[0][idx], u2 = a.cu[1][idx], u3 = a.cu[2][idx];
+  a.S[0][idx] = mul_ik(kxm, u1);
+  a.S[2][idx] = mul_ik(kzq, u3);
+  a.S[4][idx] = 0.5 * (mul_ik(kzq, u1) + mul_ik(kxm, u3));
+  if (j <= a.g.nyp) {
+    const double2 u2p = a.cu[1][idx + a.g.ps];
+    a.S[1][idx] = make_double2((u2p.x - u2.x) / a.dyf[j], (u2p.y - u2.y) / a.dyf[j]);
+  } else {
+    a.S[1][idx] = make_double2(-10000.0, 0.0);
+  }
+  if (j >= 1) {
+    const double2 u1m = a.cu[0][idx - a.g.ps], u3m = a.cu[2][idx - a.g.ps];
+    a.S[3][idx] = 0.5 * (make_double2((u1.x - u1m.x) / a.dy[j], (u1.y - u1m.y) / a.dy[j]) + mul_ik(kxm, u2));
+    a.S[5][idx] = 0.5 * (mul_ik(kzq, u2) + make_double2((u3.x - u3m.x) / a.dy[j], (u3.y - u3m.y) / a.dy[j]));
+  } else {
+    a.S[3][idx] = make_double2(0.0, 0.0);
+    a.S[5][idx] = make_double2(0.0, 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pointwise eddy viscosity and stresses in physical space (:123-241, Smagorinsky)
+// S[0..5] in: strain components (S2 is zeroed on output, as the reference
+// does); out: |S| S_ij at GYF (S1, S3, S5), |S|_GY (S_ij - implicit part) at GY
+// (S4, S6); tmp[0] = nu_t dU1/dy, tmp[1] = nu_t dU3/dy at GY; nu_t at GY.
+struct LesPointArgs {
+  double* S[6];
+  const double* u1;
+  const double* u3;
+  double* nu_t;
+  double* nu_f;          // dynamic model only: clipped nu_t at GYF (may be null)
+  double* tmp[2];
+  const double* dy;
+  const double* dyf;
+  const double* cf;      // C(y) at GYF (constant model: c_s^2 for all j)
+  const double* cg;      // C(y) at GY
+  const double* d2f;     // Delta^2 at GYF
+  const double* d2g;     // Delta^2 at GY
+  int nx, nz, nyp;
+  int dynamic;
+};
+
+// |S| at GYF point j (needs S4, S6 at j and j+1)
+DI double snorm_f(const LesPointArgs& a, size_t o, size_t ps) {
+  const double s4 = 0.5 * (a.S[3][o + ps] + a.S[3][o]);
+  const double s6 = 0.5 * (a.S[5][o + ps] + a.S[5][o]);
+  const double s1 = a.S[0][o], s2 = a.S[1][o], s3 = a.S[2][o], s5 = a.S[4][o];
+  return sqrt(2.0 * (s1 * s1) + 4.0 * (s4 * s4) + 4.0 * (s5 * s5) + 2.0 * (s2 * s2) + 4.0 * (s6 * s6) +
+              2.0 * (s3 * s3));
+}
+// |S| at GY point j (GYF components interpolated)
+DI double snorm_g(const LesPointArgs& a, size_t o, size_t ps, int j) {
+  const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
+  auto I = [&](const double* f) { return (f[o] * w1 + f[o - ps] * w0) / den; };
+  const double s1 = I(a.S[0]), s2 = I(a.S[1]), s3 = I(a.S[2]), s5 = I(a.S[4]);
+  const double s4 = a.S[3][o], s6 = a.S[5][o];
+  return sqrt(2.0 * (s1 * s1) + 4.0 * (s4 * s4) + 4.0 * (s5 * s5) + 2.0 * (s2 * s2) + 4.0 * (s6 * s6) +
+              2.0 * (s3 * s3));
+}
+
+// pass 1: |S| at GYF and GY into scratch (two planes are read per point)
+__global__ void k_les_norms(LesPointArgs a, double* sf, double* sg) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t ps = (size_t)a.nz * a.nx;
+  const size_t tot = (size_t)(a.nyp + 2) * ps;
+  if (idx >= tot) return;
+  const int j = idx / ps;
+  sf[idx] = (j >= 1 && j <= a.nyp) ? snorm_f(a, idx, ps) : 0.0;
+  sg[idx] = (j >= 1 && j <= a.nyp + 1) ? snorm_g(a, idx, ps, j) : 0.0;
+}
+
+// pass 2: stresses, nu_t and the implicit-part fluxes
+__global__ void k_les_point(LesPointArgs a, const double* sf, const double* sg) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t ps = (size_t)a.nz * a.nx;
+  const size_t tot = (size_t)(a.nyp + 2) * ps;
+  if (idx >= tot) return;
+  const int j = idx / ps;
+  const int nyp = a.nyp;
+  // eddy viscosity at GY: nu_t = -0.5 delta_y |S| = C Delta^2 |S| (:235-241)
+  double nt = 0.0;
+  if (j >= 2 && j <= nyp) {
+    nt = a.cg[j] * a.d2g[j] * sg[idx];
+    if (a.dynamic) nt = fmax(nt, 0.0);
+  }
+  if (j >= 1 && j <= nyp) {
+    const double s = sf[idx];
+    if (a.dynamic) {
+      const double nf = fmax(a.cf[j] * a.d2f[j] * s, 0.0);
+      a.S[0][idx] = -2.0 * nf * a.S[0][idx];
+      a.S[2][idx] = -2.0 * nf * a.S[2][idx];
+      a.S[4][idx] = -2.0 * nf * a.S[4][idx];
+    } else {
+      a.S[0][idx] = s * a.S[0][idx];
+      a.S[2][idx] = s * a.S[2][idx];
+      a.S[4][idx] = s * a.S[4][idx];
+    }
+    a.S[1][idx] = 0.0;
+  }
+  if (j >= 1 && j <= nyp + 1) {
+    const double g = sg[idx];
+    const double d1 = 0.5 * (a.u1[idx] - a.u1[idx - ps]) / a.dy[j];
+    const double d3 = 0.5 * (a.u3[idx] - a.u3[idx - ps]) / a.dy[j];
+    if (a.dynamic) {
+      a.S[3][idx] = -2.0 * nt * (a.S[3][idx] - d1);
+      a.S[5][idx] = -2.0 * nt * (a.S[5][idx] - d3);
+    } else {
+      a.S[3][idx] = g * (a.S[3][idx] - d1);
+      a.S[5][idx] = g * (a.S[5][idx] - d3);
+    }
+  }
+  // ghost_les_mpi at one rank: nu_t = 0 on planes 1, 2, Nyp, Nyp+1 (:2241-2262)
+  if (j <= 2 || j >= nyp) nt = 0.0;
+  a.nu_t[idx] = nt;
+  if (j >= 2 && j <= nyp) {
+    a.tmp[0][idx] = nt * (a.u1[idx] - a.u1[idx - ps]) / a.dy[j];
+    a.tmp[1][idx] = nt * (a.u3[idx] - a.u3[idx - ps]) / a.dy[j];
+  } else {
+    a.tmp[0][idx] = 0.0;
+    a.tmp[1][idx] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cf -= div(tau) in Fourier space (:253-274 scaling, :850-880 divergence);
+// T[0..4] = tau11, tau33, tau12, tau13, tau23 (Fourier), T[5..6] = the
+// transformed nu_t dU/dy, nu_t dW/dy; scale arrays are delta_yf (GYF) and
+// delta_y (GY) (all ones for the dynamic model, whose stresses carry -2 nu_t)
+struct LesDivArgs {
+  const double2* T[7];
+  double2* cf[3];
+  const double* kx;
+  const double* kz;
+  const double* dyf;
+  const double* sf;   // delta_yf
+  const double* sg;   // delta_y
+  FGeom g;
+  int j1, j2;
+};
+
+__global__ void k_les_div(LesDivArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  const size_t ps = a.g.ps;
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  if (j >= a.j1 && j <= a.j2) {
+    const double2 c1 = a.sf[j] * a.T[0][idx], c3 = a.sf[j] * a.T[1][idx], c5 = a.sf[j] * a.T[3][idx];
+    const double2 c4 = a.sg[j] * a.T[2][idx], c4p = a.sg[j + 1] * a.T[2][idx + ps];
+    const double2 c6 = a.sg[j] * a.T[4][idx], c6p = a.sg[j + 1] * a.T[4][idx + ps];
+    const double idf = a.dyf[j];
+    a.cf[0][idx] = a.cf[0][idx] - mul_ik(kxm, c1) - make_double2((c4p.x - c4.x) / idf, (c4p.y - c4.y) / idf) -
+                   mul_ik(kzq, c5);
+    a.cf[2][idx] = a.cf[2][idx] - mul_ik(kxm, c5) - make_double2((c6p.x - c6.x) / idf, (c6p.y - c6.y) / idf) -
+                   mul_ik(kzq, c3);
+  }
+  if (j >= 2 && j <= a.g.nyp) {
+    const double2 c4 = a.sg[j] * a.T[2][idx], c6 = a.sg[j] * a.T[4][idx];
+    a.cf[1][idx] = a.cf[1][idx] - mul_ik(kxm, c4) - mul_ik(kzq, c6) + mul_ik(kxm, a.T[5][idx]) +
+                   mul_ik(kzq, a.T[6][idx]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// scalar SGS flux (:1144-1200): out_x = ikx cth, out_z = ikz cth on planes 1..Nyp+1
+struct ThGradArgs {
+  const double2* cth[8];
+  double2* gx[8];
+  double2* gz[8];
+  const double* kx;
+  const double* kz;
+  FGeom g;
+  int nth;
+};
+
+__global__ void k_th_grad(ThGradArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  for (int n = 0; n < a.nth; ++n) {
+    double2 t = j >= 1 ? a.cth[n][idx] : make_double2(0.0, 0.0);
+    a.gx[n][idx] = mul_ik(a.kx[m], t);
+    a.gz[n][idx] = mul_ik(a.kz[kq], t);
+  }
+}
+
+// physical: f *= nu_t on planes 1..Nyp+1
+struct ScaleArgs {
+  double* f[2 * 8];
+  int nfield;
+  const double* w;
+  size_t ps;
+  int nyp;
+};
+
+__global__ void k_scale_by(ScaleArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)(a.nyp + 2) * a.ps;
+  if (idx >= tot) return;
+  const int j = idx / a.ps;
+  const double w = (j >= 1) ? a.w[idx] : 0.0;
+  for (int q = 0; q < a.nfield; ++q) a.f[q][idx] = w * a.f[q][idx];
+}
+
+struct ThDivArgs {
+  const double2* fx[8];
+  const double2* fz[8];
+  double2* cfth[8];
+  const double* kx;
+  const double* kz;
+  FGeom g;
+  int nth;
+  int jst[8], jet[8];
+};
+
+__global__ void k_th_div(ThDivArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  for (int n = 0; n < a.nth; ++n) {
+    if (j < a.jst[n] || j > a.jet[n]) continue;
+    a.cfth[n][idx] = a.cfth[n][idx] + mul_ik(a.kx[m], a.fx[n][idx]) + mul_ik(a.kz[kq], a.fz[n][idx]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cf -= NL ; cr += temp5*cf on each field's rows (:299-459 accumulation, :468-482, :610-617)
+struct CfFinishArgs {
+  double2* cf[SOLVE_NF];
+  double2* cr[SOLVE_NF];
+  const void* nl[SOLVE_NF];
+  int nl_fp32;
+  int lo[SOLVE_NF], hi[SOLVE_NF];
+  int nf;
+  double temp5;
+  FGeom g;
+};
+
+__global__ void k_cf_finish(CfFinishArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int j = idx / a.g.ps;
+  for (int f = 0; f < a.nf; ++f) {
+    if (j < a.lo[f] || j > a.hi[f]) continue;
+    double2 nl;
+    if (a.nl_fp32) { float2 v = ((const float2*)a.nl[f])[idx]; nl = make_double2(v.x, v.y); }
+    else nl = ((const double2*)a.nl[f])[idx];
+    const double2 cf = a.cf[f][idx] - nl;
+    a.cf[f][idx] = cf;
+    a.cr[f][idx] = a.cr[f][idx] + a.temp5 * cf;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Crank-Nicolson in y per physical column with the eddy viscosity
+// (:494-547 explicit half, :625-646 scalars, :657-877 implicit rows, Thomas
+// :1335-1496).  One thread per (field, x-z column); the forward sweep keeps
+// the modified upper diagonal and right-hand side in scratch (c2, d2).
+struct PhysSolveArgs {
+  const double* r[SOLVE_NF];    // inverse-transformed cr
+  double* u[SOLVE_NF];          // in: physical field at the start; out: solution on the write rows
+  const double* nu_t;
+  const double* kap[8];
+  double* c2;                   // scratch [nf][n][cols]
+  double* d2;
+  const double* dy;
+  const double* dyf;
+  int nf, nth, n, nyp, cols;
+  double temp1, temp2, nu_v;
+  int jstart, jend;
+  int jst[8], jet[8];
+  double pr[8];
+  int ubc[2], vbc[2], wbc[2];
+  double uc1[2], vc1[2], wc1[2];
+  int thbc[8][2];
+  double thc1[8][2];
+};
+
+__global__ void k_phys_solve(PhysSolveArgs a) {
+  const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (size_t)a.nf * a.cols) return;
+  const int f = gid / a.cols;
+  const size_t col = gid % a.cols;
+  const size_t ps = a.cols;
+  const int n = a.n, nyp = a.nyp;
+  const double* r = a.r[f];
+  double* u = a.u[f];
+  const double* nt = f < 3 ? a.nu_t : a.kap[f - 3];
+  double* c2 = a.c2 + (size_t)f * n * ps + col;
+  double* d2 = a.d2 + (size_t)f * n * ps + col;
+  int lo, hi, w0, b0, b1;
+  double c0v, c1v, tc;
+  if (f == 1) { lo = 2; hi = nyp; w0 = 1; b0 = a.vbc[0]; b1 = a.vbc[1]; c0v = a.vc1[0]; c1v = a.vc1[1]; tc = a.temp1 * a.nu_v; }
+  else if (f == 0 || f == 2) {
+    lo = a.jstart; hi = a.jend; w0 = lo - 1;
+    b0 = f == 0 ? a.ubc[0] : a.wbc[0]; b1 = f == 0 ? a.ubc[1] : a.wbc[1];
+    c0v = f == 0 ? a.uc1[0] : a.wc1[0]; c1v = f == 0 ? a.uc1[1] : a.wc1[1];
+    tc = a.temp1 * a.nu_v;
+  } else {
+    const int t = f - 3;
+    lo = a.jst[t]; hi = a.jet[t]; w0 = lo - 1;
+    b0 = a.thbc[t][0]; b1 = a.thbc[t][1]; c0v = a.thc1[t][0]; c1v = a.thc1[t][1];
+    tc = a.temp1 / a.pr[t] * a.nu_v;
+  }
+  // row j of the system
+  auto row = [&](int j, double& A, double& B, double& C, double& D) {
+    A = 0.0; B = 1.0; C = 0.0; D = 0.0;
+    if (j >= lo && j <= hi) {
+      const size_t o = (size_t)j * ps + col;
+      const double uc = u[o], um = u[o - ps], up = u[o + ps];
+      double rhs = r[o];
+      if (f == 1) {
+        const double dyj = a.dy[j], dyfj = a.dyf[j], dyfm = a.dyf[j - 1];
+        rhs += tc * (((up - uc) / dyfj - (uc - um) / dyfm) / dyj);
+        const double ntp = 0.5 * (nt[o] + nt[o + ps]), ntm = 0.5 * (nt[o] + nt[o - ps]);
+        rhs += a.temp2 * ((ntp * (up - uc) / dyfj - ntm * (uc - um) / dyfm) / dyj);
+        A = -tc / (dyfm * dyj) - a.temp2 * ntm / (dyfm * dyj);
+        B = 1. + tc / (dyfj * dyj) + tc / (dyfm * dyj) + a.temp2 * ntp / (dyfj * dyj) + a.temp2 * ntm / (dyfm * dyj);
+        C = -tc / (dyfj * dyj) - a.temp2 * ntp / (dyfj * dyj);
+      } else {
+        const double dyj = a.dy[j], dyj1 = a.dy[j + 1], dyfj = a.dyf[j];
+        rhs += tc * (((up - uc) / dyj1 - (uc - um) / dyj) / dyfj);
+        const double ntp = nt[o + ps], ntc = nt[o];
+        rhs += a.temp2 * ((ntp * (up - uc) / dyj1 - ntc * (uc - um) / dyj) / dyfj);
+        A = -tc / (dyj * dyfj) - a.temp2 * ntc / (dyj * dyfj);
+        // u1/u3 keep the reference's form of the diagonal (:785), the scalars theirs (:668)
+        B = f < 3 ? 1. - tc * (-1. / (dyj1 * dyfj) - 1. / (dyj * dyfj))
+                  : 1. + tc / (dyj1 * dyfj) + tc / (dyj * dyfj);
+        B = B + a.temp2 * ntp / (dyj1 * dyfj) + a.temp2 * ntc / (dyj * dyfj);
+        C = -tc / (dyj1 * dyfj) - a.temp2 * ntp / (dyj1 * dyfj);
+      }
+      D = rhs;
+    }
+    if (f == 1) {
+      if (b0 == 0 && (j == 1 || j == 2)) { A = 0; B = 1; C = 0; D = c0v; }
+      if (b0 == 1 && j == 1) { A = 0; B = -1; C = 1; D = a.dyf[1] * c0v; }
+      if (j == 0) { A = 0; B = 1; C = 0; D = 0; }
+      if (b1 == 0 && (j == nyp || j == nyp + 1)) { A = 0; B = 1; C = 0; D = c1v; }
+      if (b1 == 1 && j == nyp + 1) { A = -1; B = 1; C = 0; D = a.dyf[nyp] * c1v; }
+    } else {
+      if (j == 0 || j == nyp + 1) { A = 0; B = 1; C = 0; D = 0; }
+      if (j == 1) {
+        if (b0 == 0) { A = 0; B = 1; C = 0; D = c0v; }
+        else { A = 0; B = -1; C = 1; D = a.dy[2] * c0v; }
+      }
+      if (j == nyp) {
+        if (b1 == 0) { A = 0; B = 1; C = 0; D = c1v; }
+        else { A = -1; B = 1; C = 0; D = a.dy[nyp] * c1v; }
+      }
+    }
+  };
+  // Thomas (thomas_forward_real_mpi + thomas_backward_real_mpi at one rank),
+  // kept as x(j) = f(j) - e(j) x(j+1) with e = c/b', f = g'/b' in scratch
+  double A, B, C, D;
+  row(0, A, B, C, D);
+  double bprev = B, cprev = C, gprev = D;
+  c2[0] = C / B;
+  d2[0] = D / B;
+  for (int j = 1; j < n; ++j) {
+    row(j, A, B, C, D);
+    const double aj = -A / bprev;
+    B = B + aj * cprev;
+    D = D + aj * gprev;
+    c2[(size_t)j * ps] = C / B;
+    d2[(size_t)j * ps] = D / B;
+    bprev = B; cprev = C; gprev = D;
+  }
+  // every read of u is done: write the solution on the rows the reference writes
+  const int w1 = nyp + 1;
+  double x = d2[(size_t)(n - 1) * ps];
+  if (n - 1 >= w0 && n - 1 <= w1) u[(size_t)(n - 1) * ps + col] = x;
+  for (int j = n - 2; j >= 0; --j) {
+    x = d2[(size_t)j * ps] - c2[(size_t)j * ps] * x;
+    if (j >= w0 && j <= w1) u[(size_t)j * ps + col] = x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dynamic Smagorinsky coefficient (Germano identity with Lilly's least-squares
+// contraction, sharp spectral test filter of width 2 Delta in x and z).  The
+// reference stops on this model (for/les.f90:272-277); its commented-out test
+// filters are at :1773-1990.
+//
+// Field order of the 21 test-filtered inputs, all at GYF points j = 1..Nyp:
+//   0..2   U_a      (u1, (u2(j) + u2(j+1)) / 2, u3)
+//   3..8   S_ab     (11, 22, 33, 12, 13, 23; S12, S23 averaged from GY)
+//   9..14  U_a U_b  (same pair order)
+//   15..20 |S| S_ab
+#define DYN_NF 21
+struct DynPrepArgs {
+  const double* u[3];
+  const double* S[6];     // raw strain components S1..S6 (physical)
+  const double* sf;       // |S| at GYF
+  double* out[DYN_NF];
+  int nyp;
+  size_t ps;              // Nx * Nz
+};
+
+__device__ __constant__ int c_pair_a[6] = {0, 1, 2, 0, 0, 1};
+__device__ __constant__ int c_pair_b[6] = {0, 1, 2, 1, 2, 2};
+
+__global__ void k_dyn_prep(DynPrepArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)(a.nyp + 2) * a.ps;
+  if (idx >= tot) return;
+  const int j = idx / a.ps;
+  if (j < 1 || j > a.nyp) {
+    for (int q = 0; q < DYN_NF; ++q) a.out[q][idx] = 0.0;
+    return;
+  }
+  double U[3], S[6];
+  U[0] = a.u[0][idx];
+  U[1] = 0.5 * (a.u[1][idx] + a.u[1][idx + a.ps]);
+  U[2] = a.u[2][idx];
+  S[0] = a.S[0][idx];
+  S[1] = a.S[1][idx];
+  S[2] = a.S[2][idx];
+  S[3] = 0.5 * (a.S[3][idx] + a.S[3][idx + a.ps]);
+  S[4] = a.S[4][idx];
+  S[5] = 0.5 * (a.S[5][idx] + a.S[5][idx + a.ps]);
+  const double s = a.sf[idx];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) a.out[q][idx] = U[q];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    a.out[3 + q][idx] = S[q];
+    a.out[9 + q][idx] = U[c_pair_a[q]] * U[c_pair_b[q]];
+    a.out[15 + q][idx] = s * S[q];
+  }
+}
+
+// Sharp spectral test filter: zero the stored modes with kx index > mx or
+// |kz index| > mz (packed z index kq: kz = kq for kq <= Nkz, else kq - nk2).
+struct MaskArgs {
+  double2* f[NF_MAX];
+  int nfield, mx, mz, nkz;
+  FGeom g;
+};
+
+__global__ void k_test_mask(MaskArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int kz = kq <= a.nkz ? kq : a.g.nk2 - kq;
+  if (m > a.mx || kz > a.mz) {
+    for (int q = 0; q < a.nfield; ++q) a.f[q][idx] = make_double2(0.0, 0.0);
+  }
+}
+
+// Per-plane Germano/Lilly sums: one block per GYF plane j (blockIdx.x + 1).
+// sums[j][0..5] = sum over the plane of L_ab M_ab per pair, [6..11] of M_ab^2.
+struct DynContractArgs {
+  const double* F[DYN_NF];    // test-filtered fields (physical)
+  const double* u[3];         // unfiltered u1, u2 (GY), u3
+  const double* d2f;          // Delta^2 at GYF
+  double* sums;               // [(Ny+2) * 12]
+  int nyp;
+  size_t ps;
+  double ratio2;              // (test / grid width)^2
+};
+
+__global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs a) {
+  const int j = blockIdx.x + 1;
+  const size_t base = (size_t)j * a.ps;
+  double acc[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) acc[q] = 0.0;
+  const double w2[6] = {1.0, 1.0, 1.0, 2.0, 2.0, 2.0};
+  const double d2 = a.d2f[j];
+  for (size_t p = threadIdx.x; p < a.ps; p += blockDim.x) {
+    const size_t o = base + p;
+    double Uh[3], Sh[6];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) Uh[q] = a.F[q][o];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) Sh[q] = a.F[3 + q][o];
+    double sum = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sum = sum + w2[q] * 2.0 * (Sh[q] * Sh[q]);
+    const double sh = sqrt(sum);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const double L = a.F[9 + q][o] - Uh[c_pair_a[q]] * Uh[c_pair_b[q]];
+      const double M = 2.0 * d2 * (a.F[15 + q][o] - a.ratio2 * sh * Sh[q]);
+      acc[q] += L * M;
+      acc[6 + q] += M * M;
+    }
+  }
+  __shared__ double red[8][12];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 12; ++q) {
+    double v = acc[q];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) red[warp][q] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 12) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
+    a.sums[(size_t)j * 12 + threadIdx.x] = v;
+  }
+}
+
+// C(y) at GYF from the plane sums, and interpolated to GY (for/les.f90's
+// GYF-to-GY weights); one thread per plane, planes 0..Ny+1.
+__global__ void k_dyn_coef(const double* sums, const double* dy, const double* dyf, double* cf, double* cg,
+                           int nyp, double nps) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j > nyp + 1) return;
+  const double w2[6] = {1.0, 1.0, 1.0, 2.0, 2.0, 2.0};
+  auto C = [&](int jj) -> double {
+    if (jj < 1 || jj > nyp) return 0.0;
+    double num = 0.0, den = 0.0;
+    for (int q = 0; q < 6; ++q) {
+      num += w2[q] * (sums[(size_t)jj * 12 + q] / nps);
+      den += w2[q] * (sums[(size_t)jj * 12 + 6 + q] / nps);
+    }
+    return den > 0.0 ? num / den : 0.0;
+  };
+  const double cj = C(j);
+  cf[j] = cj;
+  cg[j] = (j >= 2 && j <= nyp) ? (cj * dyf[j - 1] + C(j - 1) * dyf[j]) / (2.0 * dy[j]) : 0.0;
+}

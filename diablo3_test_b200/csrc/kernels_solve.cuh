@@ -452,3 +452,17 @@ __global__ void __launch_bounds__(128) k_rem_div(SolveArgs a) {
   project_column<R>(a, a.cu_out, nullptr, nullptr, false, lane, ps, cidx, a.kx[m], a.kz[kq],
                     m == 0 && kq == 0);
 }
+
+// Projection with the pressure update, in place on cu_out (the LES substep,
+// for/channel.f90:901-911).
+template <int R>
+__global__ void __launch_bounds__(128) k_project(SolveArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (col >= a.ncol) return;
+  const int m = col / a.nk2, kq = col % a.nk2;
+  const size_t ps = (size_t)a.nkx1 * a.kp;
+  const size_t cidx = (size_t)m * a.kp + kq;
+  project_column<R>(a, a.cu_out, a.cp_in, a.cp_out, true, lane, ps, cidx, a.kx[m], a.kz[kq],
+                    m == 0 && kq == 0);
+}

@@ -111,6 +111,11 @@ int diablo_destroy(diablo_ctx* ctx);
  * fft_xz_to_physical semantics (the state itself stays in Fourier space). */
 int diablo_upload_state(diablo_ctx* ctx, int field, const double* buf, int layout);
 int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
+/* The eddy viscosity nu_t(0:Nx+1, 0:Nzp+1, 0:Nyp+1) of the last LES substep
+ * (module array of for/flow.f90:50, set by les_chan, for/les.f90:235-241 and
+ * :2241-2262) in the reference's physical layout; host or device `buf`.
+ * All zero before the first LES substep, as the reference's array is. */
+int diablo_download_nu_t(diablo_ctx* ctx, double* buf);
 
 /* for/fft.f90:247-315.  v: physical array, vv: Fourier array, both full
  * reference-size buffers (host or device); v == vv is allowed, as in the

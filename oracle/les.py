@@ -1,0 +1,277 @@
+"""numpy restatement of the reference's LES closures (test infrastructure only).
+
+* Type 1, constant Smagorinsky: ``les_chan`` (for/les.f90:20-270, 850-925)
+  and ``les_chan_th`` (for/les.f90:1091-1200), with ``compute_strain_chan``
+  (:1463-1510), ``apply_BC_les``/``apply_BC_th_les`` (:2001-2105),
+  ``ghost_les_mpi`` and ``ghost_CS2_mpi`` at one y-rank (:2107-2270, :2444-2530).
+* Type 2, dynamic Smagorinsky: the reference stops on it
+  (for/les.f90:272-277, :1214-1218), so this is a restatement of the published
+  model (Germano et al. 1991 with Lilly's 1992 least-squares contraction):
+  sharp spectral test filter of width 2 Delta in x and z, coefficient averaged
+  over x-z planes, negative eddy viscosity clipped to zero.  It reuses the
+  type-1 stress layout (the S2 and dU1/dy, dU3/dy parts stay implicit) and
+  replaces the constant -2 c_s^2 Delta^2 by -2 C(y) Delta^2.  Parity for it is
+  unpinned against the reference, which has no such model.
+
+Arrays follow oracle/channel.py (numpy index [j, k, i]).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle.channel import Field
+
+C_SMAG = 0.17          # for/les.f90:38
+BETA_SGS = 3.0         # for/les.f90:58
+TEST_RATIO = 2.0       # test / grid filter width of the dynamic model
+
+
+def _fields(o):
+    if not hasattr(o, "_les"):
+        mk = lambda: Field(o.Ny, o.Nz, o.Nx)
+        o._les = {name: mk() for name in ("S1", "S2", "S3", "S4", "S5", "S6", "temp")}
+    return o._les
+
+
+def apply_bc_les(o):
+    """Neumann walls: copy the first interior plane into the ghosts (:2001-2058)."""
+    p, Nyp, K, I = o.p, o.Nyp, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    for cu, bmax, bmin in ((o.u1.c, p.u_bc_ymax, p.u_bc_ymin), (o.u3.c, p.w_bc_ymax, p.w_bc_ymin)):
+        if bmax == 1:
+            cu[Nyp, K, I] = cu[Nyp - 1, K, I]
+            cu[Nyp + 1, K, I] = cu[Nyp, K, I]
+        if bmin == 1:
+            cu[1, K, I] = cu[2, K, I]
+            cu[0, K, I] = cu[1, K, I]
+
+
+def apply_bc_th_les(o):
+    """:2062-2105"""
+    p, Nyp, K, I = o.p, o.Nyp, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    for n in range(o.Nth):
+        cth = o.th[n].c
+        if p.th_bc_ymax[n] == 1:
+            cth[Nyp, K, I] = cth[Nyp - 1, K, I]
+            cth[Nyp + 1, K, I] = cth[Nyp, K, I]
+        if p.th_bc_ymin[n] == 1:
+            cth[1, K, I] = cth[2, K, I]
+            cth[0, K, I] = cth[1, K, I]
+
+
+def compute_strain(o, F):
+    """compute_strain_chan (:1463-1510) + ghost_CS2_mpi at one rank."""
+    Nyp, K, I = o.Nyp, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    cikx, cikz = o.cikx[None, None, :o.Nxp], o.cikz[None, :, None]
+    cu1, cu2, cu3 = o.u1.c, o.u2.c, o.u3.c
+    dy, dyf = o.dy[:, None, None], o.dyf[:, None, None]
+    A = slice(0, Nyp + 2)
+    F["S1"].c[A, K, I] = cikx * cu1[A, K, I]
+    F["S3"].c[A, K, I] = cikz * cu3[A, K, I]
+    F["S5"].c[A, K, I] = 0.5 * (cikz * cu1[A, K, I] + cikx * cu3[A, K, I])
+    B = slice(0, Nyp + 1)
+    F["S2"].c[B, K, I] = (cu2[1:Nyp + 2, K, I] - cu2[B, K, I]) / dyf[B]
+    G = slice(1, Nyp + 2)
+    F["S4"].c[G, K, I] = 0.5 * ((cu1[G, K, I] - cu1[0:Nyp + 1, K, I]) / dy[G] + cikx * cu2[G, K, I])
+    F["S6"].c[G, K, I] = 0.5 * (cikz * cu2[G, K, I] + (cu3[G, K, I] - cu3[0:Nyp + 1, K, I]) / dy[G])
+    F["S2"].c[Nyp + 1, K, I] = -10000.0          # ghost_CS2_mpi sentinel (:2521-2527)
+    for nm in ("S1", "S2", "S3", "S4", "S5", "S6"):
+        o.fft_xz_to_physical(F[nm])
+
+
+def _interp_gy(o, a, j):
+    """(a(j) dyf(j-1) + a(j-1) dyf(j)) / (2 dy(j)): a GYF field at GY point j."""
+    return (a[j] * o.dyf[j - 1] + a[j - 1] * o.dyf[j]) / (2.0 * o.dy[j])
+
+
+def _strain_norms(o, S):
+    """|S| at GYF points (j = 1..Nyp) and at GY points (j = 1..Nyp+1) (:123-166)."""
+    Nyp = o.Nyp
+    s_f = np.zeros_like(S["S1"])
+    s_g = np.zeros_like(S["S1"])
+    for j in range(1, Nyp + 1):
+        s_f[j] = np.sqrt(2.0 * S["S1"][j] ** 2.0
+                         + 4.0 * (0.5 * (S["S4"][j + 1] + S["S4"][j])) ** 2.0
+                         + 4.0 * S["S5"][j] ** 2.0
+                         + 2.0 * S["S2"][j] ** 2.0
+                         + 4.0 * (0.5 * (S["S6"][j + 1] + S["S6"][j])) ** 2.0
+                         + 2.0 * S["S3"][j] ** 2.0)
+    for j in range(1, Nyp + 2):
+        s_g[j] = np.sqrt(2.0 * _interp_gy(o, S["S1"], j) ** 2.0
+                         + 4.0 * S["S4"][j] ** 2.0
+                         + 4.0 * _interp_gy(o, S["S5"], j) ** 2.0
+                         + 2.0 * _interp_gy(o, S["S2"], j) ** 2.0
+                         + 4.0 * S["S6"][j] ** 2.0
+                         + 2.0 * _interp_gy(o, S["S3"], j) ** 2.0)
+    return s_f, s_g
+
+
+def _filter_widths(o):
+    """delta_yf (GYF) and delta_y (GY): -2 c^2 Delta^2 without the constant (:224-245)."""
+    dx1 = o.p.lx / o.Nx
+    dz1 = o.p.lz / o.Nz
+    d2f = np.zeros(o.Ny + 2)
+    d2g = np.zeros(o.Ny + 2)
+    for j in range(1, o.Nyp + 1):
+        d2f[j] = (dx1 * BETA_SGS * o.dyf[j] * 1.0 * dz1 * BETA_SGS) ** (2.0 / 3.0)
+    for j in range(1, o.Nyp + 2):
+        d2g[j] = (dx1 * BETA_SGS * o.dy[j] * 2.0 * dz1 * BETA_SGS) ** (2.0 / 3.0)
+    return d2f, d2g
+
+
+def _test_filter(o, phys):
+    """Sharp spectral test filter of width 2 Delta on physical planes [j, k, i]:
+    keep |kx| <= Nkx/2 and |kz| <= Nkz/2 of the resolved band."""
+    Nx, Nz = o.Nx, o.Nz
+    f = np.fft.rfft2(phys[:, :Nz, :Nx], axes=(1, 2))
+    kxi = np.arange(f.shape[2])
+    kzi = np.abs(np.fft.fftfreq(Nz, 1.0 / Nz))
+    mask = (kxi[None, :] <= o.Nkx // 2) & (kzi[:, None] <= o.Nkz // 2)
+    f *= mask[None]
+    out = np.zeros_like(phys)
+    out[:, :Nz, :Nx] = np.fft.irfft2(f, s=(Nz, Nx), axes=(1, 2))
+    return out
+
+
+def _dynamic_coefficient(o, S, s_f, d2f):
+    """C(y) at GYF points from the Germano identity with Lilly's contraction.
+    Velocities, strain and |S| are taken at GYF points (u2, S4, S6 averaged
+    from the neighbouring GY points); <.> is the x-z plane mean."""
+    Nyp, Nx, Nz = o.Nyp, o.Nx, o.Nz
+    R = slice(1, Nyp + 1)
+    u1, u2, u3 = o.u1.r, o.u2.r, o.u3.r
+    U = [np.zeros_like(u1) for _ in range(3)]
+    U[0][R] = u1[R]
+    U[1][R] = 0.5 * (u2[R] + u2[2:Nyp + 2])
+    U[2][R] = u3[R]
+    Sf = {"11": S["S1"], "22": S["S2"], "33": S["S3"], "13": S["S5"]}
+    S12 = np.zeros_like(u1)
+    S23 = np.zeros_like(u1)
+    S12[R] = 0.5 * (S["S4"][R] + S["S4"][2:Nyp + 2])
+    S23[R] = 0.5 * (S["S6"][R] + S["S6"][2:Nyp + 2])
+    Sf["12"] = S12
+    Sf["23"] = S23
+    pairs = (("11", 0, 0), ("22", 1, 1), ("33", 2, 2), ("12", 0, 1), ("13", 0, 2), ("23", 1, 2))
+    weight = {"11": 1.0, "22": 1.0, "33": 1.0, "12": 2.0, "13": 2.0, "23": 2.0}
+    Uh = [_test_filter(o, u) for u in U]
+    Sh = {nm: _test_filter(o, Sf[nm]) for nm, _, _ in pairs}
+    sh = np.zeros_like(u1)
+    sh[R] = np.sqrt(sum(weight[nm] * 2.0 * Sh[nm][R] ** 2 for nm, _, _ in pairs))
+    num = np.zeros(o.Ny + 2)
+    den = np.zeros(o.Ny + 2)
+    d2 = d2f[:, None, None]
+    for nm, a, b in pairs:
+        L = _test_filter(o, U[a] * U[b]) - Uh[a] * Uh[b]
+        M = 2.0 * d2 * (_test_filter(o, s_f * Sf[nm]) - TEST_RATIO ** 2 * sh * Sh[nm])
+        num[R] += weight[nm] * np.mean((L * M)[R, :Nz, :Nx], axis=(1, 2))
+        den[R] += weight[nm] * np.mean((M * M)[R, :Nz, :Nx], axis=(1, 2))
+    C = np.zeros(o.Ny + 2)
+    ok = den[R] > 0
+    C[R] = np.where(ok, num[R] / np.where(ok, den[R], 1.0), 0.0)
+    return C
+
+
+def les_chan(o):
+    """Eddy viscosity and SGS stress divergence for the momentum equations."""
+    p = o.p
+    Nyp, Nx, Nz, K, I = o.Nyp, o.Nx, o.Nz, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    j1, j2 = o.jstart, Nyp - 1                       # rankY == NprocY-1 branch (:62-66)
+    o.apply_bc_vel_post()                             # :80
+    o.apply_bc_th_post()                              # :81
+    apply_bc_les(o)                                   # :89
+    apply_bc_th_les(o)                                # :90
+    F = _fields(o)
+    if p.les_model_type not in (1, 2):
+        raise NotImplementedError(f"LES model {p.les_model_type}")
+    compute_strain(o, F)
+    for f in (o.u1, o.u2, o.u3):                      # :118-120
+        o.fft_xz_to_physical(f)
+    S = {nm: F[nm].r for nm in ("S1", "S2", "S3", "S4", "S5", "S6")}
+    s_f, s_g = _strain_norms(o, S)
+    d2f, d2g = _filter_widths(o)
+    if p.les_model_type == 1:
+        cf_ = np.full(o.Ny + 2, C_SMAG ** 2.0)
+        cg_ = cf_
+    else:
+        Cf = _dynamic_coefficient(o, S, s_f, d2f)
+        cf_ = Cf
+        cg_ = np.zeros(o.Ny + 2)
+        for j in range(2, Nyp + 1):                   # C at GY points
+            cg_[j] = (Cf[j] * o.dyf[j - 1] + Cf[j - 1] * o.dyf[j]) / (2.0 * o.dy[j])
+    delta_yf = -2.0 * cf_ * d2f
+    delta_y = -2.0 * cg_ * d2g
+    R = slice(1, Nyp + 1)
+    G = slice(1, Nyp + 2)
+    u1, u3 = o.u1.r, o.u3.r
+    dyg = o.dy[G, None, None]
+    nt = o.nu_t
+    nt[:] = 0.0
+    if p.les_model_type == 1:
+        S["S1"][R] = s_f[R] * S["S1"][R]              # :169-178
+        S["S5"][R] = s_f[R] * S["S5"][R]
+        S["S2"][R] = 0.0
+        S["S3"][R] = s_f[R] * S["S3"][R]
+        S["S4"][G] = s_g[G] * (S["S4"][G] - 0.5 * (u1[G] - u1[0:Nyp + 1]) / dyg)   # :181-193
+        S["S6"][G] = s_g[G] * (S["S6"][G] - 0.5 * (u3[G] - u3[0:Nyp + 1]) / dyg)
+        for j in range(2, Nyp + 1):                   # :235-241
+            nt[j, :Nz, :Nx] = -0.5 * delta_y[j] * s_g[j, :Nz, :Nx]
+    else:
+        # clipped viscosities at GY (nu_t) and GYF (nuf); the stresses carry
+        # -2 nu S themselves, so the delta scalings below become ones
+        for j in range(2, Nyp + 1):
+            nt[j, :Nz, :Nx] = np.maximum(-0.5 * delta_y[j] * s_g[j, :Nz, :Nx], 0.0)
+        nuf = np.zeros_like(nt)
+        for j in range(1, Nyp + 1):
+            nuf[j] = np.maximum(-0.5 * delta_yf[j] * s_f[j], 0.0)
+        for nm in ("S1", "S3", "S5"):
+            S[nm][R] = -2.0 * nuf[R] * S[nm][R]
+        S["S2"][R] = 0.0
+        S["S4"][G] = -2.0 * nt[G] * (S["S4"][G] - 0.5 * (u1[G] - u1[0:Nyp + 1]) / dyg)
+        S["S6"][G] = -2.0 * nt[G] * (S["S6"][G] - 0.5 * (u3[G] - u3[0:Nyp + 1]) / dyg)
+        delta_yf = np.ones(o.Ny + 2)
+        delta_y = np.ones(o.Ny + 2)
+    nt[1] = 0.0; nt[2] = 0.0; nt[Nyp] = 0.0; nt[Nyp + 1] = 0.0   # ghost_les_mpi (:2241-2262)
+    for nm in ("S1", "S3", "S4", "S5", "S6"):          # :245-253
+        o.fft_xz_to_fourier(F[nm])
+    C1, C3, C4, C5, C6 = (F[nm].c for nm in ("S1", "S3", "S4", "S5", "S6"))
+    C1[R, K, I] *= delta_yf[R, None, None]            # :256-274
+    C5[R, K, I] *= delta_yf[R, None, None]
+    C3[R, K, I] *= delta_yf[R, None, None]
+    C4[G, K, I] *= delta_y[G, None, None]
+    C6[G, K, I] *= delta_y[G, None, None]
+    cikx, cikz = o.cikx[None, None, :o.Nxp], o.cikz[None, :, None]
+    cf1, cf2, cf3 = o.f1.c, o.f2.c, o.f3.c
+    J = slice(j1, j2 + 1)
+    JP = slice(j1 + 1, j2 + 2)
+    dyf = o.dyf[J, None, None]
+    cf1[J, K, I] = cf1[J, K, I] - cikx * C1[J, K, I] - (C4[JP, K, I] - C4[J, K, I]) / dyf - cikz * C5[J, K, I]
+    cf3[J, K, I] = cf3[J, K, I] - cikx * C5[J, K, I] - (C6[JP, K, I] - C6[J, K, I]) / dyf - cikz * C3[J, K, I]
+    J2 = slice(2, Nyp + 1)
+    cf2[J2, K, I] = cf2[J2, K, I] - cikx * C4[J2, K, I] - cikz * C6[J2, K, I]
+    temp = F["temp"]
+    for u, ck in ((u1, cikx), (u3, cikz)):           # :862-880
+        temp.r[J2, :Nz, :Nx] = nt[J2, :Nz, :Nx] * (u[J2, :Nz, :Nx] - u[1:Nyp, :Nz, :Nx]) / o.dy[J2, None, None]
+        o.fft_xz_to_fourier(temp)
+        cf2[J2, K, I] = cf2[J2, K, I] + ck * temp.c[J2, K, I]
+
+
+def les_chan_th(o):
+    """kappa_t = nu_t and the horizontal SGS scalar flux (:1130-1200)."""
+    p = o.p
+    Nyp, Nx, Nz, K, I = o.Nyp, o.Nx, o.Nz, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    if p.les_model_type not in (1, 2):
+        raise NotImplementedError(f"LES model {p.les_model_type}")
+    G = slice(1, Nyp + 2)
+    for n in range(o.Nth):
+        o.kappa_t[n][G] = 1.0 * o.nu_t[G]
+    cs1 = o.s1
+    for n in range(o.Nth):
+        cth, cfth = o.th[n].c, o.fth[n].c
+        Jt = slice(o.jstart_th[n], o.jend_th[n] + 1)
+        for ck in (o.cikx[None, None, :o.Nxp], o.cikz[None, :, None]):
+            cs1.c[G, K, I] = ck * cth[G, K, I]
+            o.fft_xz_to_physical(cs1)
+            cs1.r[G, :Nz, :Nx] = o.kappa_t[n][G, :Nz, :Nx] * cs1.r[G, :Nz, :Nx]
+            o.fft_xz_to_fourier(cs1)
+            cfth[Jt, K, I] = cfth[Jt, K, I] + ck * cs1.c[Jt, K, I]
+    for n in range(o.Nth):
+        o.fft_xz_to_physical(o.th[n])
