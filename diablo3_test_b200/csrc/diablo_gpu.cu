@@ -96,6 +96,11 @@ struct diablo_ctx {
     double *nu_t, *sf, *sg, *c2, *d2;
     double2* xs[NF_MAX];      // x-spectral scratch of the batched transforms
     double *d_cf, *d_cg, *d_d2f, *d_d2g, *d_sclf, *d_sclg;
+    int amd_ready;            // AMD models: rotation, invariant strain, gradients
+    double2 *Of[3], *SIf[6], *Gf[9], *Tf[3 * DIABLO_MAX_TH];
+    double *Op[3], *SIp[6], *Gp[9], *Tp[3 * DIABLO_MAX_TH];
+    double *fxp[DIABLO_MAX_TH], *fzp[DIABLO_MAX_TH], *kap[DIABLO_MAX_TH];
+    double2 *fxf[DIABLO_MAX_TH], *fzf[DIABLO_MAX_TH];
     int dyn_ready;            // dynamic model: test-filter inputs and plane sums
     double* dp[DYN_NF];
     double2* df[DYN_NF];
@@ -614,6 +619,7 @@ static int substep_spectral(diablo_ctx* ctx) {
 
 static const double LES_C_SMAG = 0.17;   // for/les.f90:38
 static const double LES_BETA = 3.0;      // for/les.f90:58
+static const double LES_C_AMD = 0.2887;  // for/les.f90:42
 
 static int ensure_les(diablo_ctx* ctx) {
   diablo_ctx::Les& L = ctx->les;
@@ -642,12 +648,28 @@ static int ensure_les(diablo_ctx* ctx) {
     d2f[j] = pow(dx1 * LES_BETA * ctx->h_dyf[j] * 1.0 * dz1 * LES_BETA, 2.0 / 3.0);
   for (int j = 1; j <= ctx->ny + 1; ++j)
     d2g[j] = pow(dx1 * LES_BETA * ctx->h_dy[j] * 2.0 * dz1 * LES_BETA, 2.0 / 3.0);
-  if (ctx->p.les_model_type == 1) {
+  const int model = ctx->p.les_model_type;
+  if (model == 1) {
     for (int j = 0; j < n; ++j) {
       cf[j] = c2; cg[j] = c2;
       sclf[j] = -2.0 * c2 * d2f[j];
       sclg[j] = -2.0 * c2 * d2g[j];
     }
+  } else if (model == 4 || model == 5) {
+    // AMD: delta_yf, delta_y of for/les.f90:500-516 (4) and :776-797 (5);
+    // nu_t = -0.5 delta_y temp, carried as cg with unit Delta^2
+    for (int j = 1; j <= ctx->ny + 1; ++j) {
+      if (model == 4) {
+        sclf[j] = -2.0 * pow(LES_C_AMD, 2.0);
+        sclg[j] = -2.0 * pow(LES_C_AMD, 2.0);
+      } else {
+        const double ix = 1.0 / pow(dx1 * LES_BETA, 2.0), iz = 1.0 / pow(dz1 * LES_BETA, 2.0);
+        sclf[j] = -2.0 * pow(LES_C_AMD, 2.0) * 3.0 / (ix + 1.0 / pow(ctx->h_dyf[j] * 2.0, 2.0) + iz);
+        sclg[j] = -2.0 * pow(LES_C_AMD, 2.0) * 3.0 / (ix + 1.0 / pow(ctx->h_dy[j] * 2.0, 2.0) + iz);
+      }
+      cg[j] = -0.5 * sclg[j];
+    }
+    for (int j = 0; j < n; ++j) d2g[j] = 1.0;
   }
   CK(cudaMemcpyAsync(L.d_d2f, d2f.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(L.d_d2g, d2g.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -728,6 +750,27 @@ extern "C" {
 static int bc_post(diablo_ctx* ctx, int do_vel, int do_th);
 }
 
+static int ensure_amd(diablo_ctx* ctx) {
+  diablo_ctx::Les& L = ctx->les;
+  if (L.amd_ready) return 0;
+  const size_t fe = four_elems(ctx) * sizeof(double2), pe = phys_elems(ctx) * sizeof(double);
+  const bool m5 = ctx->p.les_model_type == 5;
+  int rc;
+#define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
+  for (int q = 0; q < 3; ++q) { AL(L.Of[q], fe); AL(L.Op[q], pe); }
+  if (m5) {
+    for (int q = 0; q < 6; ++q) { AL(L.SIf[q], fe); AL(L.SIp[q], pe); }
+    for (int q = 0; q < 9; ++q) { AL(L.Gf[q], fe); AL(L.Gp[q], pe); }
+    for (int q = 0; q < 3 * ctx->nth; ++q) { AL(L.Tf[q], fe); AL(L.Tp[q], pe); }
+    for (int n = 0; n < ctx->nth; ++n) {
+      AL(L.fxp[n], pe); AL(L.fzp[n], pe); AL(L.fxf[n], fe); AL(L.fzf[n], fe); AL(L.kap[n], pe);
+    }
+  }
+#undef AL
+  L.amd_ready = 1;
+  return 0;
+}
+
 static int substep_les(diablo_ctx* ctx, int rk) {
   diablo_ctx::Les& L = ctx->les;
   const int nf = ctx->nf, nth = ctx->nth;
@@ -784,6 +827,32 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     k_strain<<<grid1d(ftot), 256, 0, ctx->stream>>>(sa);
   }
   if ((rc = ifft_batch(ctx, L.S, L.Sp, 6))) return rc;
+  const int model = ctx->p.les_model_type;
+  const bool amd = model == 4 || model == 5;
+  const double dxb = ctx->p.lx / ctx->nx * LES_BETA, dzb = ctx->p.lz / ctx->nz * LES_BETA;
+  if (amd) {
+    // rotation (and for model 5 the invariant strain and all gradients), to physical
+    if ((rc = ensure_amd(ctx))) return rc;
+    AmdFourierArgs af;
+    memset(&af, 0, sizeof(af));
+    for (int q = 0; q < 3; ++q) { af.cu[q] = ctx->st[c][q]; af.O[q] = L.Of[q]; }
+    for (int n = 0; n < nth; ++n) af.cth[n] = ctx->st[c][4 + n];
+    if (model == 5) {
+      for (int q = 0; q < 6; ++q) af.SI[q] = L.SIf[q];
+      for (int q = 0; q < 9; ++q) af.G[q] = L.Gf[q];
+      for (int q = 0; q < 3 * nth; ++q) af.T[q] = L.Tf[q];
+    }
+    af.kx = ctx->d_kx; af.kz = ctx->d_kz; af.dy = ctx->d_dy; af.dyf = ctx->d_dyf;
+    af.deltax = dxb; af.deltaz = dzb;
+    af.model = model; af.nth = nth; af.g = fg;
+    { Prof pr(ctx, K_OTHER); k_amd_fourier<<<grid1d(ftot), 256, 0, ctx->stream>>>(af); }
+    if ((rc = ifft_batch(ctx, L.Of, L.Op, 3))) return rc;
+    if (model == 5) {
+      if ((rc = ifft_batch(ctx, L.SIf, L.SIp, 6))) return rc;
+      if ((rc = ifft_batch(ctx, L.Gf, L.Gp, 9))) return rc;
+      if (nth > 0 && (rc = ifft_batch(ctx, L.Tf, L.Tp, 3 * nth))) return rc;
+    }
+  }
   if ((rc = spectral_inverse<double>(ctx))) return rc;       // u, th -> ctx->phys
   double* const* up = (double* const*)ctx->phys;
   // 5. |S|, the coefficient (dynamic model), eddy viscosity and stresses
@@ -797,9 +866,24 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     pa.dy = ctx->d_dy; pa.dyf = ctx->d_dyf;
     pa.cf = L.d_cf; pa.cg = L.d_cg; pa.d2f = L.d_d2f; pa.d2g = L.d_d2g;
     pa.nx = ctx->nx; pa.nz = ctx->nz; pa.nyp = ctx->ny;
-    pa.dynamic = ctx->p.les_model_type == 2;
-    { Prof pr(ctx, K_OTHER); k_les_norms<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg); }
-    if (ctx->p.les_model_type == 2 && (rc = dynamic_coefficient(ctx))) return rc;
+    pa.dynamic = model == 2;
+    pa.amd = amd;
+    if (amd) {
+      AmdCoefArgs ca;
+      for (int q = 0; q < 6; ++q) ca.S[q] = model == 5 ? L.SIp[q] : L.Sp[q];
+      for (int q = 0; q < 3; ++q) ca.O[q] = L.Op[q];
+      ca.dy = ctx->d_dy; ca.dyf = ctx->d_dyf;
+      ca.sf = L.sf; ca.sg = L.sg;
+      ca.wx = pow(dxb, 2.0); ca.wz = pow(dzb, 2.0);
+      ca.model = model; ca.nyp = ctx->ny; ca.jstart = ctx->jstart; ca.jend = ctx->jend;
+      ca.ps = (size_t)ctx->nz * ctx->nx;
+      Prof pr(ctx, K_OTHER);
+      k_amd_coef<<<grid1d(ptot), 256, 0, ctx->stream>>>(ca);
+    } else {
+      Prof pr(ctx, K_OTHER);
+      k_les_norms<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg);
+    }
+    if (model == 2 && (rc = dynamic_coefficient(ctx))) return rc;
     { Prof pr(ctx, K_OTHER); k_les_point<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg); }
   }
   // 6. stresses to Fourier space, divergence into cf (for/les.f90:245-274, 850-880)
@@ -815,8 +899,38 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     Prof pr(ctx, K_OTHER);
     k_les_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(da);
   }
-  // 7. scalar SGS flux with kappa_t = nu_t (for/les.f90:1130-1200)
-  if (nth > 0) {
+  // 7. scalar SGS flux: the AMD scalar model (model 5, for/les.f90:1219-1412)
+  // or kappa_t = nu_t (for/les.f90:1130-1200)
+  if (nth > 0 && model == 5) {
+    AmdThArgs ta;
+    memset(&ta, 0, sizeof(ta));
+    for (int q = 0; q < 9; ++q) ta.G[q] = L.Gp[q];
+    for (int q = 0; q < 3 * nth; ++q) ta.T[q] = L.Tp[q];
+    for (int n = 0; n < nth; ++n) {
+      ta.fx[n] = L.fxp[n]; ta.fz[n] = L.fzp[n]; ta.kap[n] = L.kap[n];
+      ta.jst[n] = ctx->jst[n]; ta.jet[n] = ctx->jet[n];
+    }
+    ta.dy = ctx->d_dy; ta.dyf = ctx->d_dyf; ta.hdy = L.d_cg;
+    ta.deltax = dxb; ta.deltaz = dzb;
+    ta.nth = nth; ta.nyp = ctx->ny; ta.ps = (size_t)ctx->nz * ctx->nx;
+    { Prof pr(ctx, K_OTHER); k_amd_th<<<grid1d(ptot), 256, 0, ctx->stream>>>(ta); }
+    double* srcp[2 * DIABLO_MAX_TH];
+    double2* dstf[2 * DIABLO_MAX_TH];
+    for (int n = 0; n < nth; ++n) {
+      srcp[2 * n] = L.fxp[n]; srcp[2 * n + 1] = L.fzp[n];
+      dstf[2 * n] = L.fxf[n]; dstf[2 * n + 1] = L.fzf[n];
+    }
+    if ((rc = fft_batch(ctx, srcp, dstf, 2 * nth))) return rc;
+    AmdThDivArgs da;
+    memset(&da, 0, sizeof(da));
+    for (int n = 0; n < nth; ++n) {
+      da.fx[n] = L.fxf[n]; da.fz[n] = L.fzf[n]; da.cfth[n] = cf_out[3 + n];
+      da.jst[n] = ctx->jst[n]; da.jet[n] = ctx->jet[n];
+    }
+    da.kx = ctx->d_kx; da.kz = ctx->d_kz; da.dlyf = L.d_sclf; da.g = fg; da.nth = nth;
+    Prof pr(ctx, K_OTHER);
+    k_amd_th_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(da);
+  } else if (nth > 0) {
     ThGradArgs ga;
     memset(&ga, 0, sizeof(ga));
     for (int n = 0; n < nth; ++n) { ga.cth[n] = ctx->st[c][4 + n]; ga.gx[n] = L.thg[2 * n]; ga.gz[n] = L.thg[2 * n + 1]; }
@@ -865,7 +979,7 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     memset(&sa, 0, sizeof(sa));
     for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = up[f]; }
     sa.nu_t = L.nu_t;
-    for (int n = 0; n < nth; ++n) sa.kap[n] = L.nu_t;
+    for (int n = 0; n < nth; ++n) sa.kap[n] = model == 5 ? L.kap[n] : L.nu_t;
     sa.c2 = L.c2; sa.d2 = L.d2;
     sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf;
     sa.nf = nf; sa.nth = nth; sa.n = ctx->nyp2; sa.nyp = ctx->ny; sa.cols = ctx->nz * ctx->nx;
@@ -975,7 +1089,8 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
 static int substep(diablo_ctx* ctx, int rk) {
   if (les_active(ctx)) {
     if (ctx->precision != DIABLO_FP64) return DIABLO_ERR_UNSUPPORTED;
-    if (ctx->p.les_model_type != 1 && ctx->p.les_model_type != 2) return DIABLO_ERR_UNSUPPORTED;
+    const int m = ctx->p.les_model_type;
+    if (m != 1 && m != 2 && m != 4 && m != 5) return DIABLO_ERR_UNSUPPORTED;
     return substep_les(ctx, rk);
   }
   int rc = ensure_scratch(ctx);

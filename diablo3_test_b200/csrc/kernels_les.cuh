@@ -195,6 +195,7 @@ struct LesPointArgs {
   const double* d2g;     // Delta^2 at GY
   int nx, nz, nyp;
   int dynamic;
+  int amd;               // AMD models: the GY stresses start at j = 2 (row 1 keeps the strain)
 };
 
 // |S| at GYF point j (needs S4, S6 at j and j+1)
@@ -254,7 +255,7 @@ __global__ void k_les_point(LesPointArgs a, const double* sf, const double* sg) 
     }
     a.S[1][idx] = 0.0;
   }
-  if (j >= 1 && j <= nyp + 1) {
+  if (j >= (a.amd ? 2 : 1) && j <= nyp + 1) {
     const double g = sg[idx];
     const double d1 = 0.5 * (a.u1[idx] - a.u1[idx - ps]) / a.dy[j];
     const double d3 = 0.5 * (a.u3[idx] - a.u3[idx - ps]) / a.dy[j];
@@ -696,4 +697,263 @@ __global__ void k_dyn_coef(const double* sums, const double* dy, const double* d
   const double cj = C(j);
   cf[j] = cj;
   cg[j] = (j >= 2 && j <= nyp) ? (cj * dyf[j - 1] + C(j - 1) * dyf[j]) / (2.0 * dy[j]) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Anisotropic minimum dissipation models (for/les.f90:279-850): Rozema (4)
+// with the plain rotation tensor, Verstappen (5) with the scaled-invariant
+// strain and rotation tensors and, for the scalar, all velocity and scalar
+// gradients.  Fourier inputs, one thread per (j, m, kq).
+struct AmdFourierArgs {
+  const double2* cu[3];
+  const double2* cth[8];
+  double2* O[3];          // O4, O5, O6
+  double2* SI[6];         // model 5: SI1..SI6
+  double2* G[9];          // model 5: du1dx du2dy du3dz du2dx du3dx du1dz du2dz du1dy du3dy
+  double2* T[3 * 8];      // model 5: dth/dx, dth/dy, dth/dz per scalar
+  const double* kx;
+  const double* kz;
+  const double* dy;
+  const double* dyf;
+  double deltax, deltaz;  // dx(1) beta, dz(1) beta
+  int model, nth;
+  FGeom g;
+};
+
+DI double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+DI double2 cdiff_over(double2 a, double2 b, double d) { return make_double2((a.x - b.x) / d, (a.y - b.y) / d); }
+
+__global__ void k_amd_fourier(const __grid_constant__ AmdFourierArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  const size_t ps = a.g.ps;
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double2 u1 = a.cu[0][idx], u2 = a.cu[1][idx], u3 = a.cu[2][idx];
+  const double2 z = make_double2(0.0, 0.0);
+  const bool inv = a.model == 5;
+  const double rzx = a.deltaz / a.deltax, rxz = a.deltax / a.deltaz;
+  // omega_13 (:1595, :1641): all planes
+  a.O[1][idx] = inv ? 0.5 * (cscale(mul_ik(kzq, u1), rzx) - cscale(mul_ik(kxm, u3), rxz))
+                    : 0.5 * (mul_ik(kzq, u1) - mul_ik(kxm, u3));
+  if (j >= 1) {
+    const double2 d1 = cdiff_over(u1, a.cu[0][idx - ps], a.dy[j]);
+    const double2 d3 = cdiff_over(u3, a.cu[2][idx - ps], a.dy[j]);
+    if (inv) {
+      const double dly = a.dy[j] * 2.0;
+      const double ryx = dly / a.deltax, rxy = a.deltax / dly, rzy = a.deltaz / dly, ryz = dly / a.deltaz;
+      a.O[0][idx] = 0.5 * (cscale(d1, ryx) - cscale(mul_ik(kxm, u2), rxy));
+      a.O[2][idx] = 0.5 * (cscale(mul_ik(kzq, u2), rzy) - cscale(d3, ryz));
+      a.SI[3][idx] = 0.5 * (cscale(d1, ryx) + cscale(mul_ik(kxm, u2), rxy));
+      a.SI[5][idx] = 0.5 * (cscale(mul_ik(kzq, u2), rzy) + cscale(d3, ryz));
+    } else {
+      a.O[0][idx] = 0.5 * (d1 - mul_ik(kxm, u2));
+      a.O[2][idx] = 0.5 * (mul_ik(kzq, u2) - d3);
+    }
+  } else {
+    a.O[0][idx] = z;
+    a.O[2][idx] = z;
+    if (inv) { a.SI[3][idx] = z; a.SI[5][idx] = z; }
+  }
+  if (!inv) return;
+  // scaled-invariant strain (:1514-1577)
+  a.SI[0][idx] = mul_ik(kxm, u1);
+  a.SI[2][idx] = mul_ik(kzq, u3);
+  a.SI[4][idx] = 0.5 * (cscale(mul_ik(kzq, u1), rzx) + cscale(mul_ik(kxm, u3), rxz));
+  a.SI[1][idx] = j <= a.g.nyp ? cdiff_over(a.cu[1][idx + ps], u2, a.dyf[j]) : make_double2(-10000.0, 0.0);
+  // all gradients (:1681-1767)
+  a.G[0][idx] = mul_ik(kxm, u1);
+  a.G[2][idx] = mul_ik(kzq, u3);
+  a.G[3][idx] = mul_ik(kxm, u2);
+  a.G[4][idx] = mul_ik(kxm, u3);
+  a.G[5][idx] = mul_ik(kzq, u1);
+  a.G[6][idx] = mul_ik(kzq, u2);
+  if (j >= 1) {
+    a.G[7][idx] = cdiff_over(u1, a.cu[0][idx - ps], a.dy[j]);
+    a.G[1][idx] = cdiff_over(u2, a.cu[1][idx - ps], a.dyf[j - 1]);   // dyf(j-1), as the reference
+    a.G[8][idx] = cdiff_over(u3, a.cu[2][idx - ps], a.dy[j]);
+  } else {
+    a.G[7][idx] = z;
+    a.G[1][idx] = z;
+    a.G[8][idx] = z;
+  }
+  for (int n = 0; n < a.nth; ++n) {
+    if (j >= 1) {
+      const double2 t = a.cth[n][idx];
+      a.T[3 * n][idx] = mul_ik(kxm, t);
+      a.T[3 * n + 1][idx] = cdiff_over(t, a.cth[n][idx - ps], a.dy[j]);
+      a.T[3 * n + 2][idx] = mul_ik(kzq, t);
+    } else {
+      a.T[3 * n][idx] = z;
+      a.T[3 * n + 1][idx] = z;
+      a.T[3 * n + 2][idx] = z;
+    }
+  }
+}
+
+// max(0, -(I3 - I4)) / (I1 - I2) from the six strain and three rotation
+// components at one point, with direction weights (wx, wy, wz)
+// (for/les.f90:300-350 form; unit weights give the :591-650 form)
+DI double amd_ratio(double a1, double a2, double a3, double a4, double a5, double a6, double o4, double o5,
+                    double o6, double dx, double dy, double dz) {
+  const double i3 = dx * (a1 * a1 * a1) + dy * (a2 * a2 * a2) + dz * (a3 * a3 * a3) +
+                    (2.0 * dx + dy) * a1 * (a4 * a4) + (2.0 * dx + dz) * a1 * (a5 * a5) +
+                    (2.0 * dy + dx) * a2 * (a4 * a4) + (2.0 * dy + dz) * a2 * (a6 * a6) +
+                    (2.0 * dz + dx) * a3 * (a5 * a5) + (2.0 * dz + dy) * a3 * (a6 * a6) +
+                    2.0 * (dx + dy + dz) * a4 * a5 * a6;
+  const double num = -i3 - dy * a1 * (o4 * o4) - dz * a1 * (o5 * o5) - dx * a2 * (o4 * o4) -
+                     dz * a2 * (o6 * o6) - dx * a3 * (o5 * o5) - dy * a3 * (o6 * o6) -
+                     2.0 * dz * a4 * o5 * o6 + 2.0 * dy * a5 * o4 * o6 - 2.0 * dx * a6 * o4 * o5;
+  if (num <= 0.0) return 0.0;
+  const double den = a1 * a1 + a2 * a2 + a3 * a3 + 2.0 * (a4 * a4) + 2.0 * (o4 * o4) + 2.0 * (a5 * a5) +
+                     2.0 * (o5 * o5) + 2.0 * (a6 * a6) + 2.0 * (o6 * o6);
+  return num / den;
+}
+
+// AMD coefficient at GYF (sf) and GY (sg) points, physical, one thread per point.
+// Model 4: strain S, weights delta_i^2 with (2 dy(j))^2 in y, GYF rows 1..Nyp,
+// GY rows 2..Nyp+1.  Model 5: invariant strain, unit weights, GYF rows
+// jstart..jend, GY rows 2..Nyp.
+struct AmdCoefArgs {
+  const double* S[6];
+  const double* O[3];
+  const double* dy;
+  const double* dyf;
+  double* sf;
+  double* sg;
+  double wx, wz;          // (dx beta)^2, (dz beta)^2 (model 4)
+  int model, nyp, jstart, jend;
+  size_t ps;
+};
+
+__global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)(a.nyp + 2) * a.ps;
+  if (idx >= tot) return;
+  const int j = idx / a.ps;
+  const size_t ps = a.ps;
+  const bool m4 = a.model == 4;
+  const int f0 = m4 ? 1 : a.jstart, f1 = m4 ? a.nyp : a.jend;
+  const int g1 = m4 ? a.nyp + 1 : a.nyp;
+  double sfv = 0.0, sgv = 0.0;
+  if (j >= f0 && j <= f1) {
+    const double wy = m4 ? (a.dy[j] * 2.0) * (a.dy[j] * 2.0) : 1.0;
+    const double wx = m4 ? a.wx : 1.0, wz = m4 ? a.wz : 1.0;
+    auto av = [&](const double* f) { return 0.5 * (f[idx + ps] + f[idx]); };
+    sfv = amd_ratio(a.S[0][idx], a.S[1][idx], a.S[2][idx], av(a.S[3]), a.S[4][idx], av(a.S[5]), av(a.O[0]),
+                    a.O[1][idx], av(a.O[2]), wx, wy, wz);
+  }
+  if (j >= 2 && j <= g1) {
+    const double wy = m4 ? (a.dy[j] * 2.0) * (a.dy[j] * 2.0) : 1.0;
+    const double wx = m4 ? a.wx : 1.0, wz = m4 ? a.wz : 1.0;
+    const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
+    auto ip = [&](const double* f) { return (f[idx] * w1 + f[idx - ps] * w0) / den; };
+    sgv = amd_ratio(ip(a.S[0]), ip(a.S[1]), ip(a.S[2]), a.S[3][idx], ip(a.S[4]), a.S[5][idx], a.O[0][idx],
+                    ip(a.O[1]), a.O[2][idx], wx, wy, wz);
+  }
+  a.sf[idx] = sfv;
+  a.sg[idx] = sgv;
+}
+
+// Type-5 scalar model (for/les.f90:1239-1380) for every scalar: the horizontal
+// fluxes s1_th dth/dx, s1_th dth/dz at GYF rows jstart_th..jend_th into fx, fz
+// (zero elsewhere) and kappa_t = -0.5 delta_y temp_th at GY rows 2..Nyp, zero
+// on planes 0, 1, 2, Nyp, Nyp+1 (ghost_les_th_mpi at one rank).
+struct AmdThArgs {
+  const double* G[9];
+  const double* T[3 * 8];
+  double* fx[8];
+  double* fz[8];
+  double* kap[8];
+  const double* dy;
+  const double* dyf;
+  const double* hdy;      // -0.5 delta_y(j)
+  double deltax, deltaz;
+  int nth, nyp;
+  int jst[8], jet[8];
+  size_t ps;
+};
+
+__global__ void k_amd_th(const __grid_constant__ AmdThArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)(a.nyp + 2) * a.ps;
+  if (idx >= tot) return;
+  const int j = idx / a.ps;
+  const size_t ps = a.ps;
+  const double dx2 = a.deltax * a.deltax, dz2 = a.deltaz * a.deltaz;
+  for (int n = 0; n < a.nth; ++n) {
+    const double* tx = a.T[3 * n];
+    const double* ty = a.T[3 * n + 1];
+    const double* tz = a.T[3 * n + 2];
+    double s1 = 0.0;
+    if (j >= a.jst[n] && j <= a.jet[n]) {
+      const double dly = a.dyf[j] * 2.0, dy2 = dly * dly;
+      const double tyf = 0.5 * (ty[idx + ps] + ty[idx]);
+      const double txj = tx[idx], tzj = tz[idx];
+      auto av = [&](const double* f) { return 0.5 * (f[idx + ps] + f[idx]); };
+      const double num = -(dx2 * a.G[0][idx] * (txj * txj) + dy2 * a.G[1][idx] * (tyf * tyf) +
+                           dz2 * a.G[2][idx] * (tzj * tzj) +
+                           (dy2 * av(a.G[7]) + dx2 * av(a.G[3])) * txj * tyf +
+                           (dz2 * a.G[5][idx] + dx2 * a.G[4][idx]) * txj * tzj +
+                           (dz2 * av(a.G[6]) + dy2 * av(a.G[8])) * tyf * tzj);
+      if (num > 0.0) {
+        const double ex = a.deltax * txj, ey = dly * tyf, ez = a.deltaz * tzj;
+        s1 = num / (ex * ex + ey * ey + ez * ez);
+      }
+      a.fx[n][idx] = s1 * txj;
+      a.fz[n][idx] = s1 * tzj;
+    } else {
+      a.fx[n][idx] = 0.0;
+      a.fz[n][idx] = 0.0;
+    }
+    double kt = 0.0;
+    if (j >= 3 && j <= a.nyp - 1) {
+      const double dly = a.dy[j] * 2.0, dy2 = dly * dly;
+      const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
+      auto ip = [&](const double* f) { return (f[idx] * w1 + f[idx - ps] * w0) / den; };
+      const double txg = ip(tx), tzg = ip(tz), tyg = ty[idx];
+      const double num = -(dx2 * ip(a.G[0]) * (txg * txg) + dy2 * ip(a.G[1]) * (tyg * tyg) +
+                           dz2 * ip(a.G[2]) * (tzg * tzg) +
+                           (dy2 * a.G[7][idx] + dx2 * a.G[3][idx]) * txg * tyg +
+                           (dz2 * ip(a.G[5]) + dx2 * ip(a.G[4])) * txg * tzg +
+                           (dz2 * a.G[6][idx] + dy2 * a.G[8][idx]) * tyg * tzg);
+      if (num > 0.0) {
+        const double ex = a.deltax * txg, ey = dly * tyg, ez = a.deltaz * tzg;
+        kt = a.hdy[j] * (num / (ex * ex + ey * ey + ez * ez));
+      }
+    }
+    a.kap[n][idx] = kt;
+  }
+}
+
+// cfth -= ikx (delta_yf/2) F(fx) + ikz (delta_yf/2) F(fz) on rows jstart_th..jend_th (:1391-1412)
+struct AmdThDivArgs {
+  const double2* fx[8];
+  const double2* fz[8];
+  double2* cfth[8];
+  const double* kx;
+  const double* kz;
+  const double* dlyf;     // delta_yf(j)
+  FGeom g;
+  int nth;
+  int jst[8], jet[8];
+};
+
+__global__ void k_amd_th_div(const __grid_constant__ AmdThDivArgs a) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tot = (size_t)a.g.n * a.g.ps;
+  if (idx >= tot) return;
+  const int kq = idx % a.g.kp;
+  if (kq >= a.g.nk2) return;
+  const int m = (idx / a.g.kp) % a.g.nkx1;
+  const int j = idx / a.g.ps;
+  const double h = 0.5 * a.dlyf[j];
+  for (int n = 0; n < a.nth; ++n) {
+    if (j < a.jst[n] || j > a.jet[n]) continue;
+    a.cfth[n][idx] = a.cfth[n][idx] - mul_ik(a.kx[m], h * a.fx[n][idx]) - mul_ik(a.kz[kq], h * a.fz[n][idx]);
+  }
 }

@@ -1,9 +1,10 @@
 """Parity of the CUDA LES substep with the CPU oracle (oracle/les.py), through
 the C ABI.
 
-Constant Smagorinsky (model 1) follows les_chan / les_chan_th of the
-reference (for/les.f90:20-270, 850-925, 1091-1200) with the eddy-viscosity
-terms of the Crank-Nicolson rows (for/channel.f90:519-547, 657-877).  The
+Constant Smagorinsky (model 1) and the anisotropic minimum dissipation
+models of Rozema (4) and Verstappen (5) follow les_chan / les_chan_th of the
+reference (for/les.f90:20-925, 1091-1412) with the eddy-viscosity terms of
+the Crank-Nicolson rows (for/channel.f90:519-547, 657-877).  The
 dynamic model (2) has no reference implementation (the reference stops on
 it, for/les.f90:272-277); both sides restate Germano/Lilly with a sharp
 spectral test filter.  Tolerance: relative L2 error <= 1e-10 per field and
@@ -13,7 +14,8 @@ import numpy as np
 import pytest
 
 from diablo3_test_b200 import _lib
-from diablo3_test_b200.config import LES_SMAGORINSKY, LES_DYNAMIC_SMAGORINSKY, MIXED
+from diablo3_test_b200.config import (LES_SMAGORINSKY, LES_DYNAMIC_SMAGORINSKY, LES_AMD_ROZEMA,
+                                      LES_AMD_VERSTAPPEN, MIXED)
 from tests.helpers import (small_params, grid_for, initial_fields, setup_oracle, setup_gpu,
                            oracle_state, gpu_state, rel_err)
 
@@ -30,6 +32,14 @@ LES_CASES = {
                                     th_bc_ymin_c1=[-1.0, 0.0], th_bc_ymax_c1=[1.0, 0.0]),
     "smagorinsky_rotation_forcing": dict(les_model_type=LES_SMAGORINSKY, f_type=1, px0=-0.5, ro=5.0,
                                          grav_x=0.1, dthdx=[0.3]),
+    "amd_rozema": dict(les_model_type=LES_AMD_ROZEMA),
+    "amd_rozema_neumann_walls": dict(les_model_type=LES_AMD_ROZEMA, u_bc_ymin=1, w_bc_ymin=1,
+                                     u_bc_ymax=1, w_bc_ymax=1),
+    "amd_verstappen": dict(les_model_type=LES_AMD_VERSTAPPEN),
+    "amd_verstappen_two_scalars": dict(les_model_type=LES_AMD_VERSTAPPEN, n_th=2, pr=[0.71, 1.0],
+                                       th_bc_ymin=[0, 1], th_bc_ymax=[0, 1],
+                                       th_bc_ymin_c1=[-1.0, 0.0], th_bc_ymax_c1=[1.0, 0.0],
+                                       u_bc_ymin=1, w_bc_ymin=1),
     "dynamic": dict(les_model_type=LES_DYNAMIC_SMAGORINSKY),
     "dynamic_neumann_top": dict(les_model_type=LES_DYNAMIC_SMAGORINSKY, u_bc_ymax=1, w_bc_ymax=1),
 }

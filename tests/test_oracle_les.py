@@ -8,12 +8,17 @@ restated formulas have by construction:
   the implicit Crank-Nicolson rows, so les_chan leaves cf unchanged;
 * dynamic Smagorinsky (Germano/Lilly): the plane-averaged coefficient is
   invariant under scaling of the velocity, and vanishes for a flow without
-  x-z variation (the resolved Leonard stress is then zero).
+  x-z variation (the resolved Leonard stress is then zero);
+* anisotropic minimum dissipation (for/les.f90:279-850, 1219-1412): no eddy
+  viscosity in a plane shear flow (-(I3 - I4) vanishes identically there),
+  and nu_t and the type-5 kappa_t are homogeneous of degree one in the
+  velocity.
 """
 import numpy as np
 import pytest
 
-from diablo3_test_b200.config import LES_SMAGORINSKY, LES_DYNAMIC_SMAGORINSKY
+from diablo3_test_b200.config import (LES_SMAGORINSKY, LES_DYNAMIC_SMAGORINSKY, LES_AMD_ROZEMA,
+                                      LES_AMD_VERSTAPPEN)
 from tests.helpers import small_params, grid_for, initial_fields, setup_oracle
 
 
@@ -99,3 +104,30 @@ def test_dynamic_coefficient_vanishes_without_xz_variation():
     _shear(o)
     les.les_chan(o)
     assert np.abs(o.nu_t).max() < 1e-20
+
+
+@pytest.mark.parametrize("model", [LES_AMD_ROZEMA, LES_AMD_VERSTAPPEN])
+def test_amd_no_viscosity_in_plane_shear(model):
+    from oracle import les
+    o = _oracle(model)
+    _shear(o)
+    les.les_chan(o)
+    assert np.all(o.nu_t == 0)
+
+
+@pytest.mark.parametrize("model", [LES_AMD_ROZEMA, LES_AMD_VERSTAPPEN])
+def test_amd_viscosity_is_linear_in_velocity(model):
+    from oracle import les
+    out = []
+    for amp in (1.0, 2.0):
+        p = small_params(nx=32, ny=33, nz=24, n_th=1, use_les=True, create_new_flow=False,
+                         les_model_type=model)
+        gy = grid_for(p)
+        f = initial_fields(p, gy, kind="turbulent", seed=13)
+        o = setup_oracle(p, gy, {k: amp * v for k, v in f.items()})
+        les.les_chan(o)
+        les.les_chan_th(o)
+        out.append((o.nu_t.copy(), o.kappa_t[0].copy()))
+    assert np.abs(out[0][0]).max() > 0 and np.abs(out[0][1]).max() > 0
+    np.testing.assert_allclose(out[1][0], 2.0 * out[0][0], rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(out[1][1], 2.0 * out[0][1], rtol=1e-9, atol=1e-14)
