@@ -107,10 +107,14 @@ def kernel_bytes(p, nf, mixed):
         "z_inverse": nf * nyp2 * (four * 16 + xsp * cs),
         "x_inverse_c2r": nf * nyp2 * (xsp * cs + phys * rs),
         "products_x_forward_r2c": nf * nyp2 * phys * rs + 2 * nf * ny * xsp * cs,
-        "z_forward_combine": 2 * nf * ny * xsp * cs + nf * ny * four * cs,
+        # mixed: the u1 equation's NL is FP64 and takes the mean epilogue
+        # (state u1, u3, u2 on two planes read; 8 more bytes written per mode)
+        "z_forward_combine": 2 * nf * ny * xsp * cs + nf * ny * four * cs
+                             + (ny * four * (4 * 16 + 8) if mixed else 0),
         # state (3 u + p + scalars) in and out, NL in, cf in on 2 of 3 substeps
         # and out on 2 of 3 substeps
-        "column_solve": nyp2 * four * (2 * (4 + nth) * 16 + nf * cs + 2 * (2.0 / 3.0) * nf * 16),
+        "column_solve": nyp2 * four * (2 * (4 + nth) * 16 + nf * cs + (16 - cs if mixed else 0)
+                                       + 2 * (2.0 / 3.0) * nf * 16),
     }
 
 
@@ -128,13 +132,46 @@ def setup_channel(p, gy, fields, precision):
     return ch
 
 
-def state_sig(ch):
+def state_sig(ch, scalars=False):
     from diablo3_test_b200 import _lib
     p = ch.params
     out = {}
-    for name, fid in [("u1", _lib.U1), ("u2", _lib.U2), ("u3", _lib.U3)]:
+    ids = [("u1", _lib.U1), ("u2", _lib.U2), ("u3", _lib.U3)]
+    if scalars:
+        ids += [(f"th{n}", _lib.TH + n) for n in range(p.n_th)]
+    for name, fid in ids:
         c = ch.download(fid).view(np.complex128)
         out[name] = c[:, :2 * (p.nz // 3) + 1, :p.nx // 2].copy()
+    return out
+
+
+def accuracy_report(sm, sd, p, gy):
+    """Mixed (sm) against FP64 (sd) states: per-field relative L2 error of the
+    significant Fourier modes, relative error of the mean wall shear dU1/dy at
+    both walls, and relative L2 error of the streamwise energy spectrum
+    E(kx) = sum over y and kz of |u_hat|^2 per velocity component."""
+    from diablo3_test_b200.grid import metrics
+    _, _, dy, _ = metrics(gy)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out = {"field_rel_l2": {k: rel(sm[k], sd[k]) for k in sm}}
+    ny = p.ny
+    shear = {}
+    for tag, (ja, jb, jd) in {"lower": (1, 2, 2), "upper": (ny - 1, ny, ny)}.items():
+        tm = (sm["u1"][jb, 0, 0].real - sm["u1"][ja, 0, 0].real) / dy[jd]
+        td = (sd["u1"][jb, 0, 0].real - sd["u1"][ja, 0, 0].real) / dy[jd]
+        shear[tag] = float(abs(tm - td) / abs(td))
+    out["wall_shear_rel"] = shear
+    spec = {}
+    for k in ("u1", "u2", "u3"):
+        w = np.full(sm[k].shape[2], 2.0)
+        w[0] = 1.0
+        em = (np.abs(sm[k][1:ny + 1]) ** 2).sum(axis=(0, 1)) * w
+        ed = (np.abs(sd[k][1:ny + 1]) ** 2).sum(axis=(0, 1)) * w
+        spec[k] = rel(em, ed)
+    out["spectrum_kx_rel_l2"] = spec
+    vel = max(out["field_rel_l2"][k] for k in ("u1", "u2", "u3"))
+    out["max_velocity_rel_l2"] = vel
+    out["within_1e-6"] = bool(vel <= 1e-6)
     return out
 
 
@@ -291,6 +328,14 @@ def run_ours(args):
     # mixed vs FP64 after the same W+K steps from the same state
     sm, sd = state_sig(chm), state_sig(chd)
     err = {k: float(np.linalg.norm(sm[k] - sd[k]) / np.linalg.norm(sd[k])) for k in sm}
+    # both continued (untimed) to the workload's 100 steps
+    acc = None
+    done = args.warmup + args.steps
+    if args.acc_steps > done:
+        chm.step(args.acc_steps - done)
+        chd.step(args.acc_steps - done)
+        acc = accuracy_report(state_sig(chm, True), state_sig(chd, True), p, gy)
+        acc["steps"] = args.acc_steps
     if rank != 0:
         chm.close()
         chd.close()
@@ -330,6 +375,7 @@ def run_ours(args):
         "mixed_speedup_vs_fp64": ms_fp64 / ms_mixed,
         "mixed_vs_fp64_rel_err": err,
         "rel_err_steps": args.warmup + args.steps,
+        "mixed_accuracy": acc,
         "roofline": roofline,
         "step_roofline": step_roof,
         "kernels": per_kernel,
@@ -374,6 +420,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--acc-steps", type=int, default=100,
+                    help="steps after which mixed and FP64 states are compared (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"), default=None,
                     help="profiling: run a smaller grid of the same workload (no JSON contract)")

@@ -81,6 +81,7 @@ struct diablo_ctx {
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
+  double* d_prof;           // U1(y), I(U1)(y) of the mixed-precision mean split [2][n]
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
   struct Les {
@@ -163,7 +164,8 @@ static void launch_solve_t(const SolveArgs& a, bool project_only, cudaStream_t s
 }
 template <int R>
 static void launch_tiles_t(const Solve2Args& A, cudaStream_t s) {
-  const int smem = ((1 + T2_STAGES) * A.s.n * T2_PITCH + T2_COLS * 32 * R) * (int)sizeof(double2);
+  const int smem = ((1 + T2_STAGES) * A.s.n * T2_PITCH + T2_COLS * 32 * R) * (int)sizeof(double2) +
+                   (A.mean_split ? 2 * A.s.n * (int)sizeof(double) : 0);
   cudaFuncSetAttribute(k_column_tiles<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int ngroups = (A.s.nk2 + T2_COLS - 1) / T2_COLS;
   k_column_tiles<R><<<A.s.nkx1 * ngroups, 32 * T2_COLS, smem, s>>>(A);
@@ -275,7 +277,8 @@ static int ensure_scratch(diablo_ctx* ctx) {
   const size_t cs = ctx->precision == DIABLO_FP64 ? sizeof(double2) : sizeof(float2);
   const size_t rs = cs / 2;
   for (int f = 0; f < ctx->nf; ++f) {
-    int rc = dev_alloc(ctx, &ctx->nl[f], four_elems(ctx) * cs);
+    // nl[0] is FP64 in both precisions (the mean-split u1 equation, mixed)
+    int rc = dev_alloc(ctx, &ctx->nl[f], four_elems(ctx) * (f == 0 ? sizeof(double2) : cs));
     if (rc) return rc;
     rc = dev_alloc(ctx, &ctx->phys[f], phys_elems(ctx) * rs);
     if (rc) return rc;
@@ -445,6 +448,10 @@ static int upload_coefficients(diablo_ctx* ctx) {
     int rc = dev_alloc(ctx, (void**)&ctx->d_met, met.size() * sizeof(double));
     if (rc) return rc;
   }
+  if (!ctx->d_prof) {
+    int rc = dev_alloc(ctx, (void**)&ctx->d_prof, 2 * (size_t)n * sizeof(double));
+    if (rc) return rc;
+  }
   CK(cudaMemcpyAsync(ctx->d_met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice,
                      ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -516,8 +523,10 @@ static void update_transient(diablo_ctx* ctx) {
         sin(p.omega0 * (ctx->ro_inv / p.delta * ctx->time - p.force_start));
 }
 
+// mean_mask: fields whose (0,0) mode (the mean profile) stays out of the
+// physical fields; its products are added in FP64 further on.
 template <typename T>
-static int spectral_inverse(diablo_ctx* ctx) {
+static int spectral_inverse(diablo_ctx* ctx, unsigned mean_mask = 0) {
   typedef typename CT<T>::C C;
   const int nf = ctx->nf;
   const int c = ctx->cur;
@@ -537,6 +546,7 @@ static int spectral_inverse(diablo_ctx* ctx) {
     a.nseq = ctx->nyp2 * ctx->nkx1;
     a.g = ctx->g;
     a.tw = tz;
+    a.mean_mask = mean_mask;
     Prof pr(ctx, K_ZINV);
     if ((rc = launch_zinv<C>(a, ctx->nz, nf, ctx->stream))) return rc;
   }
@@ -559,7 +569,7 @@ static int spectral_inverse(diablo_ctx* ctx) {
 }
 
 template <typename T>
-static int spectral_nl(diablo_ctx* ctx) {
+static int spectral_nl(diablo_ctx* ctx, bool mean_free_u1 = false) {
   typedef typename CT<T>::C C;
   const int nf = ctx->nf;
   const int c = ctx->cur;
@@ -601,6 +611,15 @@ static int spectral_nl(diablo_ctx* ctx) {
     a.tw = tz;
     a.kz = ctx->d_kz;
     a.scale = 1.0 / ctx->nz;
+    if (mean_free_u1) {
+      // the u1 equation takes the FP64 mean epilogue into its FP64 NL array
+      for (int q = 0; q < 3; ++q) a.cu[q] = ctx->st[c][q];
+      a.kx = ctx->d_kx;
+      a.dy = ctx->d_dy;
+      a.dyf = ctx->d_dyf;
+      a.prof = ctx->d_prof;
+      a.fps = (size_t)ctx->nkx1 * ctx->kp;
+    }
     Prof pr(ctx, K_ZFWD_NL);
     if ((rc = launch_zfwd<C, C, true>(a, ctx->nz, nf, ctx->stream))) return rc;
   }
@@ -608,9 +627,9 @@ static int spectral_nl(diablo_ctx* ctx) {
 }
 
 template <typename T>
-static int substep_spectral(diablo_ctx* ctx) {
-  int rc = spectral_inverse<T>(ctx);
-  return rc ? rc : spectral_nl<T>(ctx);
+static int substep_spectral(diablo_ctx* ctx, unsigned mean_mask) {
+  int rc = spectral_inverse<T>(ctx, mean_mask);
+  return rc ? rc : spectral_nl<T>(ctx, (mean_mask & 1u) != 0);
 }
 
 // ==========================================================================
@@ -1096,10 +1115,18 @@ static int substep(diablo_ctx* ctx, int rk) {
   int rc = ensure_scratch(ctx);
   if (rc) return rc;
   update_transient(ctx);
-  rc = ctx->precision == DIABLO_FP64 ? substep_spectral<double>(ctx) : substep_spectral<float>(ctx);
-  if (rc) return rc;
   SolveArgs a;
   fill_solve_args(ctx, a, rk);
+  // Mixed precision with the tiled kernel: the physical u1 of the FP32
+  // products is u1 minus its mean profile U1(y).  The products with U1 are
+  // linear in the state and are added in FP64: by the z-forward epilogue for
+  // the u1 equation (whose NL is then FP64), by the column kernel for the
+  // others.  This keeps the large mean-flow products out of FP32.
+  const bool tiled = !a.front && !ctx->use_general_solver;
+  const bool mean_split = ctx->precision == DIABLO_MIXED && tiled;
+  rc = ctx->precision == DIABLO_FP64 ? substep_spectral<double>(ctx, 0u)
+                                     : substep_spectral<float>(ctx, mean_split ? 0x1u : 0u);
+  if (rc) return rc;
   const int c = ctx->cur, nx_ = 1 - c;
   for (int q = 0; q < 3; ++q) {
     a.cu_in[q] = ctx->st[c][q];
@@ -1124,6 +1151,8 @@ static int substep(diablo_ctx* ctx, int rk) {
   A.kc = ctx->d_kc[rk - 1];
   A.met = ctx->d_met;
   A.fac = ctx->d_fac[rk - 1];
+  A.mean_split = mean_split ? 1 : 0;
+  A.prof = ctx->d_prof;
   A.nstep = 0;
   bool fits = true;
   auto add = [&](int op, int arg, double coef, const void* src, void* dst, const void* src2) {
@@ -1138,7 +1167,8 @@ static int substep(diablo_ctx* ctx, int rk) {
     const double g = comp == 0 ? p.grav_x : p.grav_z;
     if (g != 0.0)
       for (int n = 0; n < ctx->nth; ++n) add(OP_ADD_CF, 0, g, a.cth_in[n], nullptr, nullptr);
-    add(OP_NL, f32, 0, ctx->nl[comp], a.store_cf ? a.cf_out[comp] : nullptr, nullptr);
+    add(OP_NL, (comp == 0 && mean_split) ? 0 : f32, 0, ctx->nl[comp], a.store_cf ? a.cf_out[comp] : nullptr,
+        nullptr);
     if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[comp], nullptr, nullptr);
     add(OP_SOLVE, comp, 0, nullptr, a.cu_out[comp], a.cu_in[comp]);
   }
@@ -1164,7 +1194,8 @@ static int substep(diablo_ctx* ctx, int rk) {
   {
     Prof pr(ctx, K_SOLVE);
     // thermal-wind forcing (flavor 'Front') keeps the general kernel
-    if (fits && !a.front && !ctx->use_general_solver) rc = launch_tiles(A, ctx->stream);
+    if (fits && tiled) rc = launch_tiles(A, ctx->stream);
+    else if (mean_split) rc = DIABLO_ERR_UNSUPPORTED;
     else rc = launch_solve(a, false, ctx->stream);
     if (rc) return rc;
   }

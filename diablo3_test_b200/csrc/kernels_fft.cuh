@@ -36,6 +36,7 @@ template <typename C> struct ZInvArgs {
   int q0, nseq;      // first (j, m) column and number of columns
   Geom g;
   const C* tw;       // exp(-2 pi i m / Nz)
+  unsigned mean_mask;  // fields transformed without their (kx, kz) = (0, 0) mode
 };
 
 template <typename C, int N1, int N2, int S>
@@ -46,11 +47,13 @@ __global__ void __launch_bounds__(N2* S) k_zinv(ZInvArgs<C> a) {
   const int f = blockIdx.y;
   const bool ok = q < a.nseq;
   const double2* src = a.src[f] + (size_t)(a.q0 + q) * a.g.kp;
+  // the mean-free transform leaves out kp = 0 of the m = 0 sequences
+  const int kmin = (((a.mean_mask >> f) & 1u) && (a.q0 + q) % a.g.nkx1 == 0) ? 1 : 0;
   C v[N1];
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     int kp = z_pack(n1 * N2 + t, a.g.nz, a.g.nkz);
-    v[n1] = (ok && kp >= 0) ? cvt<C>(src[kp]) : czero<C>();
+    v[n1] = (ok && kp >= kmin) ? cvt<C>(src[kp]) : czero<C>();
   }
   dfft::step1<N1, N2, +1>(v, t, a.tw, sm[s]);
   __syncthreads();
@@ -78,6 +81,20 @@ template <typename C, typename CO> struct ZFwdArgs {
   const C* tw;
   const double* kz;        // wavenumbers kz(kp), length nk2
   double scale;            // 1/Nz
+  // Mean epilogue of field 0 (the u1 equation, COMBINE, when cu[0] is set):
+  // its products were taken with u1 minus its mean profile U1(y), and the
+  // products with U1, linear in the state, are added here in FP64
+  //   ikz U1 u3 + 2 ikx U1 u1 + (U1(j+1)u2(j+1) + U1(j)u2(j+1) - U1(j)u2(j) - U1(j-1)u2(j)) / (2 dyf(j))
+  // (for/channel.f90:299-335, :398-417); dst[0] is then a double2 array.
+  // cu = state u1, u2, u3, fps = its plane stride.  prof[j] = U1(j) and
+  // prof[Ny+2+j] = (dyf(j) U1(j) + dyf(j-1) U1(j-1)) / (2 dy(j)) are written
+  // for the column kernel's own corrections.
+  const double2* cu[3];
+  const double* kx;
+  const double* dy;
+  const double* dyf;
+  double* prof;
+  size_t fps;
 };
 
 template <typename C, typename CO, int N1, int N2, int S, bool COMBINE>
@@ -130,6 +147,38 @@ __global__ void __launch_bounds__(N2* S) k_zfwd(ZFwdArgs<C, CO> a) {
   }
   if (!ok) return;
   CO* dst = a.dst[f] + (size_t)(a.q0 + q) * a.g.kp;
+  if (COMBINE && f == 0 && a.cu[0]) {
+    double2* dst64 = reinterpret_cast<double2*>(a.dst[0]) + (size_t)(a.q0 + q) * a.g.kp;
+    const int j = (a.q0 + q) / a.g.nkx1, m = (a.q0 + q) % a.g.nkx1;
+    const size_t ps = a.fps, o = (size_t)(a.q0 + q) * a.g.kp;
+    const double U0 = a.cu[0][(size_t)j * ps].x, Um = a.cu[0][(size_t)(j - 1) * ps].x,
+                 Up = a.cu[0][(size_t)(j + 1) * ps].x;
+    const double kxm = a.kx[m], id = 1.0 / (2.0 * a.dyf[j]);
+    if (m == 0 && t == 0) {
+      a.prof[j] = U0;
+      a.prof[a.g.nyp2 + j] = (a.dyf[j] * U0 + a.dyf[j - 1] * Um) / (2.0 * a.dy[j]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      int k1 = t + r * N2;
+      if (k1 < N1) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          int kp = z_pack(k1 + N1 * k2, a.g.nz, a.g.nkz);
+          if (kp >= 0) {
+            const double2 u1 = a.cu[0][o + kp], u3 = a.cu[2][o + kp];
+            const double2 vc = a.cu[1][o + kp], vp = a.cu[1][o + ps + kp];
+            double2 v = cvt<double2>(sc * ra[r][k2]);
+            v = v + mul_ik(a.kz[kp] * U0, u3) + mul_ik(2.0 * kxm * U0, u1);
+            v.x += ((Up + U0) * vp.x - (U0 + Um) * vc.x) * id;
+            v.y += ((Up + U0) * vp.y - (U0 + Um) * vc.y) * id;
+            dst64[kp] = v;
+          }
+        }
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     int k1 = t + r * N2;

@@ -55,6 +55,14 @@ struct Solve2Args {
   const double* kc;
   const double* met;
   const double* fac;   // factored u1, u2, u3, scalar systems of this substep (see k_factor)
+  // 1: the nonlinear tiles (FP32) of the u2, u3 and scalar equations were
+  // computed with u1 minus its mean profile U1(y) (the (0,0) mode); the
+  // products with U1 are linear in the state and are added here in FP64:
+  //   u3: ikx U1 u3,   u2: ikx I(U1) u2,   scalar: ikx U1 th
+  // with I the GYF-to-GY interpolation of for/channel.f90:356-375.  (The u1
+  // equation's FP64 NL carries its own mean terms, see ZFwdArgs.)
+  int mean_split;
+  const double* prof;  // [2][n]: U1(j), I(U1)(j) (written by the z-forward epilogue)
   int nstep;
   TileStep steps[T2_MAXSTEPS];
 };
@@ -348,6 +356,7 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
   double2* Tcp = reinterpret_cast<double2*>(t2_smem);
   double2* Tbase = Tcp + tsz;                         // T2_STAGES streamed tiles
   double2* dvs = Tbase + T2_STAGES * tsz;             // lane-private divergence rows
+  double* Um = reinterpret_cast<double*>(dvs + T2_COLS * 32 * R);   // U1, I(U1) (mean_split)
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, c = tid >> 5;
   const int ngroups = (a.nk2 + T2_COLS - 1) / T2_COLS;
@@ -374,6 +383,8 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
   int lo = 0, hi = -1;           // explicit row range of the current field
   const double* K = A.kc;        // implicit rows of the current field
 
+  if (A.mean_split)
+    for (int j = tid; j < 2 * n; j += nthr) Um[j] = A.prof[j];
   load_tile(Tcp, a.cp_in, false, ps, cbase, nvalid, n, tid, nthr);
   for (int q = 0; q < T2_STAGES - 1; ++q) {
     const TileStep* st = q < A.nstep ? &A.steps[q] : nullptr;
@@ -412,6 +423,8 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
             const double2 u = TV(j), um = TV(j - 1), up = TV(j + 1);
             cf[r] = -cfc * u;
             cr[r] = u - K[2 * n + j] * (up - u) + K[j] * (u - um);
+            if (A.mean_split && !(kind == 0 && st.arg == 0))
+              cf[r] = cf[r] - mul_ik(kxm * Um[kind == 1 ? n + j : j], u);
           }
         }
         break;

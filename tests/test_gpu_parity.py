@@ -153,3 +153,25 @@ def test_mixed_precision_close_to_fp64(cuda_device):
     finally:
         a.close()
         b.close()
+
+
+def test_mixed_precision_100_steps_within_1e6(cuda_device):
+    # the workload's accuracy bar: <= 1e-6 relative velocity error over 100
+    # steps (turbulent log-law state, 96 x 97 x 64, pressure-gradient forcing)
+    from diablo3_test_b200.config import MIXED
+    p = small_params(nx=96, ny=97, nz=64, n_th=2, re=180.0, delta_t=5e-4, f_type=1, px0=-1.0,
+                     grav_y=0.0, pr=[0.71, 1.0])
+    gy = grid_for(p, cs=2.0)
+    fields = initial_fields(p, gy, kind="turbulent", seed=8)
+    a = setup_gpu(p, gy, fields)
+    b = setup_gpu(p, gy, fields)
+    try:
+        b.set_precision(MIXED)
+        a.step(100)
+        b.step(100)
+        sa, sb = gpu_state(a), gpu_state(b)
+        for k in ("u1", "u2", "u3", "th0", "th1"):
+            assert rel_err(sb[k], sa[k]) < 1e-6, (k, rel_err(sb[k], sa[k]))
+    finally:
+        a.close()
+        b.close()
