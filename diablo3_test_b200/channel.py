@@ -160,3 +160,35 @@ class Channel:
         """Order the context's work on an existing cudaStream_t (0 = own stream)."""
         _lib.check(self.lib.diablo_set_stream(self.ctx, ctypes.c_void_p(stream_handle or None)),
                    "set_stream")
+
+
+class Ensemble:
+    """Independent channels (any mix of grids, parameters and precisions)
+    stepped together: one CUDA graph launch per step for all members, each
+    member's kernels on a parallel branch (``diablo_ensemble_*`` of the C ABI).
+    The members stay usable on their own and must outlive the ensemble."""
+
+    def __init__(self, members):
+        self.lib = _lib.load()
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.ctx for m in self.members])
+        st = ctypes.c_int(0)
+        self.e = self.lib.diablo_ensemble_create(arr, len(self.members), ctypes.byref(st))
+        _lib.check(st.value, "ensemble_create")
+
+    def step(self, nsteps: int = 1):
+        _lib.check(self.lib.diablo_ensemble_step(self.e, nsteps), "ensemble_step")
+
+    def synchronize(self):
+        _lib.check(self.lib.diablo_ensemble_synchronize(self.e), "ensemble_synchronize")
+
+    def close(self):
+        if self.e:
+            self.lib.diablo_ensemble_destroy(self.e)
+            self.e = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -77,6 +77,7 @@ struct diablo_ctx {
   std::vector<void*> allocs;
   // opt-in per-kernel timing: events recorded around each step kernel
   int profiling;
+  int generation;           // bumped whenever captured kernel arguments go stale (dt, precision)
   int use_general_solver;   // 1: per-lane-load column kernel instead of the tiled one
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
@@ -1041,6 +1042,20 @@ static int substep_les(diablo_ctx* ctx, int rk) {
   return 0;
 }
 
+static int ensure_dyn(diablo_ctx* ctx) {
+  diablo_ctx::Les& L = ctx->les;
+  if (L.dyn_ready) return 0;
+  const size_t ptot = phys_elems(ctx), ftot = four_elems(ctx);
+  int rc;
+  for (int q = 0; q < DYN_NF; ++q) {
+    if ((rc = dev_alloc(ctx, (void**)&L.dp[q], ptot * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(ctx, (void**)&L.df[q], ftot * sizeof(double2)))) return rc;
+  }
+  if ((rc = dev_alloc(ctx, (void**)&L.dsums, (size_t)ctx->nyp2 * 12 * sizeof(double)))) return rc;
+  L.dyn_ready = 1;
+  return 0;
+}
+
 // Dynamic Smagorinsky coefficient C(y) into les.d_cf (GYF) and les.d_cg (GY):
 // build the 21 Germano/Lilly inputs, test-filter them in Fourier space,
 // contract and average over x-z planes.  Needs les.Sp (raw strain), les.sf
@@ -1049,14 +1064,7 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
   diablo_ctx::Les& L = ctx->les;
   int rc;
   const size_t ptot = phys_elems(ctx), ftot = four_elems(ctx);
-  if (!L.dyn_ready) {
-    for (int q = 0; q < DYN_NF; ++q) {
-      if ((rc = dev_alloc(ctx, (void**)&L.dp[q], ptot * sizeof(double)))) return rc;
-      if ((rc = dev_alloc(ctx, (void**)&L.df[q], ftot * sizeof(double2)))) return rc;
-    }
-    if ((rc = dev_alloc(ctx, (void**)&L.dsums, (size_t)ctx->nyp2 * 12 * sizeof(double)))) return rc;
-    L.dyn_ready = 1;
-  }
+  if ((rc = ensure_dyn(ctx))) return rc;
   const size_t ps = (size_t)ctx->nz * ctx->nx;
   {
     DynPrepArgs pa;
@@ -1626,6 +1634,7 @@ int diablo_set_precision(diablo_ctx* ctx, int precision) {
   }
   ctx->precision = precision;
   ctx->p.precision = precision;
+  ctx->generation++;
   return 0;
 }
 
@@ -1644,6 +1653,7 @@ int diablo_set_time(diablo_ctx* ctx, double time, int time_step, double delta_t)
   const bool changed = delta_t != ctx->delta_t;
   ctx->delta_t = delta_t;
   for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * delta_t;
+  if (changed) ctx->generation++;
   return changed ? upload_coefficients(ctx) : 0;
 }
 
@@ -1698,6 +1708,231 @@ int diablo_kernel_slots(void) { return K_NSLOTS; }
 
 const char* diablo_kernel_name(int slot) {
   return (slot >= 0 && slot < K_NSLOTS) ? K_NAMES[slot] : "";
+}
+
+}  // extern "C"
+
+// ==========================================================================
+// Ensembles: independent members stepped by one CUDA graph launch per step.
+// Each member's kernel chain is one branch of the graph (its own stream
+// during capture), so small members run concurrently.  Kernel arguments hold
+// the double-buffer pointers, so two graphs are kept, one per buffer parity.
+
+struct MemberKey {
+  int cur, cf_cur, les, generation;
+  bool operator==(const MemberKey& o) const {
+    return cur == o.cur && cf_cur == o.cf_cur && les == o.les && generation == o.generation;
+  }
+};
+
+struct diablo_ensemble {
+  std::vector<diablo_ctx*> m;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> joins;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  std::vector<MemberKey> key[2];
+  std::vector<long long> nlaunch[2];
+  int last_cuda = 0;
+};
+
+static MemberKey member_key(const diablo_ctx* c) {
+  return MemberKey{c->cur, c->cf_cur, les_active(c), c->generation};
+}
+
+// Everything a step allocates on first use, so that capture allocates nothing.
+static int prepare_member(diablo_ctx* ctx) {
+  int rc;
+  if ((rc = ensure_scratch(ctx))) return rc;
+  if (les_active(ctx) && ctx->precision == DIABLO_FP64) {
+    if ((rc = ensure_les(ctx))) return rc;
+    const int m = ctx->p.les_model_type;
+    if ((m == 4 || m == 5) && (rc = ensure_amd(ctx))) return rc;
+    if (m == 2 && (rc = ensure_dyn(ctx))) return rc;
+  }
+  return 0;
+}
+
+static int one_step(diablo_ctx* ctx) {
+  ctx->time_step += 1;
+  for (int rk = 1; rk <= 3; ++rk) {
+    int rc = substep(ctx, rk);
+    if (rc) return rc;
+  }
+  ctx->time += ctx->delta_t;
+  return 0;
+}
+
+#define ECK(call)                                 \
+  do {                                            \
+    cudaError_t e__ = (call);                     \
+    if (e__ != cudaSuccess) {                     \
+      e->last_cuda = (int)e__;                    \
+      return DIABLO_ERR_CUDA;                     \
+    }                                             \
+  } while (0)
+
+// Capture one step of every member into exec[w], from the members' current
+// host state; the host state is advanced as the step would advance it.
+static int capture(diablo_ensemble* e, int w) {
+  const int n = (int)e->m.size();
+  std::vector<cudaStream_t> saved(n);
+  std::vector<int> prof(n);
+  e->key[w].resize(n);
+  e->nlaunch[w].resize(n);
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    saved[i] = c->stream;
+    prof[i] = c->profiling;
+    c->profiling = 0;
+    c->stream = e->streams[i];
+    e->key[w][i] = member_key(c);
+  }
+  cudaGraph_t graph = nullptr;
+  int rc = 0;
+  cudaError_t ce = cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    cudaEventRecord(e->fork, e->origin);
+    for (int i = 0; i < n && !rc; ++i) {
+      diablo_ctx* c = e->m[i];
+      cudaStreamWaitEvent(e->streams[i], e->fork, 0);
+      const long long l0 = c->launches;
+      rc = one_step(c);
+      e->nlaunch[w][i] = c->launches - l0;
+      cudaEventRecord(e->joins[i], e->streams[i]);
+      cudaStreamWaitEvent(e->origin, e->joins[i], 0);
+    }
+    ce = cudaStreamEndCapture(e->origin, &graph);
+  }
+  for (int i = 0; i < n; ++i) {
+    e->m[i]->stream = saved[i];
+    e->m[i]->profiling = prof[i];
+  }
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc;
+  }
+  ECK(ce);
+  if (e->exec[w]) { cudaGraphExecDestroy(e->exec[w]); e->exec[w] = nullptr; }
+  ce = cudaGraphInstantiate(&e->exec[w], graph, 0);
+  cudaGraphDestroy(graph);
+  ECK(ce);
+  return 0;
+}
+
+// (Re)capture both graphs from the members' current state, leaving the
+// members' host state as it was.
+static int capture_both(diablo_ensemble* e) {
+  const int n = (int)e->m.size();
+  struct Saved { double time; int time_step, cur, cf_cur; double wtt; };
+  std::vector<Saved> sv(n);
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    int rc = prepare_member(c);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return DIABLO_ERR_CUDA;
+    sv[i] = Saved{c->time, c->time_step, c->cur, c->cf_cur, c->w_top_transient};
+  }
+  int rc = capture(e, 0);
+  if (!rc) rc = capture(e, 1);
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    c->time = sv[i].time; c->time_step = sv[i].time_step;
+    c->cur = sv[i].cur; c->cf_cur = sv[i].cf_cur; c->w_top_transient = sv[i].wtt;
+  }
+  return rc;
+}
+
+extern "C" {
+
+diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* status) {
+  int st = 0;
+  diablo_ensemble* e = nullptr;
+  if (!members || n <= 0) st = DIABLO_ERR_ARG;
+  for (int i = 0; i < n && !st; ++i) {
+    const diablo_ctx* c = members[i];
+    if (!c) { st = DIABLO_ERR_ARG; break; }
+    for (int k = 0; k < i; ++k)
+      if (members[k] == c) st = DIABLO_ERR_ARG;
+    // kernel arguments that change every step cannot be replayed from a graph
+    if (c->p.variable_dt || c->p.f_type == 2 || (c->p.f_type == 4 && c->p.w_bc_ymax != 0))
+      st = DIABLO_ERR_UNSUPPORTED;
+  }
+  if (!st) {
+    e = new diablo_ensemble();
+    e->m.assign(members, members + n);
+    bool ok = cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+    e->streams.assign(n, nullptr);
+    e->joins.assign(n, nullptr);
+    for (int i = 0; i < n && ok; ++i)
+      ok = cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking) == cudaSuccess &&
+           cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) { st = DIABLO_ERR_CUDA; diablo_ensemble_destroy(e); e = nullptr; }
+  }
+  if (status) *status = st;
+  return e;
+}
+
+int diablo_ensemble_step(diablo_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return DIABLO_ERR_ARG;
+  const int n = (int)e->m.size();
+  for (int s = 0; s < nsteps; ++s) {
+    // the graph captured for this parity must match every member's state
+    int w = -1;
+    for (int k = 0; k < 2 && w < 0; ++k) {
+      if (!e->exec[k] || (int)e->key[k].size() != n) continue;
+      bool ok = true;
+      for (int i = 0; i < n && ok; ++i) ok = member_key(e->m[i]) == e->key[k][i];
+      if (ok) w = k;
+    }
+    if (w < 0) {
+      int rc = capture_both(e);
+      if (rc) return rc;
+      w = 0;
+    }
+    // order the graph after each member's earlier work on its own stream
+    for (int i = 0; i < n; ++i) {
+      ECK(cudaEventRecord(e->joins[i], e->m[i]->stream));
+      ECK(cudaStreamWaitEvent(e->origin, e->joins[i], 0));
+    }
+    ECK(cudaGraphLaunch(e->exec[w], e->origin));
+    ECK(cudaEventRecord(e->fork, e->origin));
+    for (int i = 0; i < n; ++i) {
+      diablo_ctx* c = e->m[i];
+      ECK(cudaStreamWaitEvent(c->stream, e->fork, 0));
+      c->time_step += 1;
+      c->time += c->delta_t;
+      c->cur ^= 1;                 // three substeps flip the state buffer
+      c->launches += e->nlaunch[w][i];
+    }
+  }
+  return 0;
+}
+
+int diablo_ensemble_synchronize(diablo_ensemble* e) {
+  if (!e) return DIABLO_ERR_ARG;
+  ECK(cudaStreamSynchronize(e->origin));
+  for (diablo_ctx* c : e->m) ECK(cudaStreamSynchronize(c->stream));
+  ECK(cudaGetLastError());
+  return 0;
+}
+
+int diablo_ensemble_destroy(diablo_ensemble* e) {
+  if (!e) return DIABLO_ERR_ARG;
+  if (e->origin) cudaStreamSynchronize(e->origin);
+  for (int k = 0; k < 2; ++k)
+    if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
+  for (cudaStream_t s : e->streams)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t v : e->joins)
+    if (v) cudaEventDestroy(v);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+  return 0;
 }
 
 }  // extern "C"

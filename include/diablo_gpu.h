@@ -179,6 +179,28 @@ int diablo_abi_version(void);
 int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, double* vv,
                                      void* stream);
 
+/*
+ * Ensembles of independent channels, stepped together.  No reference
+ * counterpart: the reference runs one channel per MPI job.  Members are
+ * contexts from diablo_create with any mix of grid sizes, parameters and
+ * precisions; they stay owned by the caller and must outlive the ensemble.
+ * diablo_ensemble_step advances every member by nsteps steps with one CUDA
+ * graph launch per step, the members' kernel chains on parallel branches of
+ * the graph.  The graphs are captured on first use and again whenever a
+ * member's state no longer matches them (a member stepped on its own, a
+ * changed delta_t or precision, the LES gate opening).  Members whose kernel
+ * arguments change every step are rejected with DIABLO_ERR_UNSUPPORTED:
+ * variable_dt, the oscillating pressure gradient (f_type 2) and the
+ * time-dependent top-wall u3 (f_type 4 with a Neumann top).  A member's own
+ * entry points (upload, download, step) stay usable and are ordered with the
+ * ensemble's work through the member's stream.
+ */
+typedef struct diablo_ensemble diablo_ensemble;
+diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* status);
+int diablo_ensemble_step(diablo_ensemble* e, int nsteps);
+int diablo_ensemble_synchronize(diablo_ensemble* e);
+int diablo_ensemble_destroy(diablo_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif
