@@ -239,6 +239,108 @@ def read_traffic():
     return out
 
 
+def ensemble_bench(torch, k, warmup=3):
+    """The uneven-grid ensemble (48 mixed-precision members cycling four grid
+    sizes, 23.5 M points per ensemble step): one graph launch per step for all
+    members against the same members run one at a time on one stream.  Both
+    are timed with CUDA events; their final states are compared."""
+    from diablo3_test_b200 import ics
+    from diablo3_test_b200.channel import Ensemble
+    from diablo3_test_b200.config import MIXED
+    cfg = ics.config_c5()
+    pts = sum(p.nx * p.ny * p.nz for p, _, _ in cfg)
+    ens_m = [setup_channel(p, gy, f, MIXED) for p, gy, f in cfg]
+    one_m = [setup_channel(p, gy, f, MIXED) for p, gy, f in cfg]
+    s1 = torch.cuda.Stream()
+    for ch in one_m:
+        ch.set_stream(s1.cuda_stream)
+    ens = Ensemble(ens_m)
+    ens.step(warmup)
+    for ch in one_m:
+        ch.step(warmup)
+    ens.synchronize()
+    torch.cuda.synchronize()
+    es = torch.cuda.ExternalStream(ens.stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(es)
+    ens.step(k)
+    e1.record(es)
+    ens.synchronize()
+    ms_graph = e0.elapsed_time(e1)
+    e0.record(s1)
+    for ch in one_m:
+        ch.step(k)
+    e1.record(s1)
+    torch.cuda.synchronize()
+    ms_one = e0.elapsed_time(e1)
+    diff = 0.0
+    for a, b in zip(ens_m, one_m):
+        sa, sb = state_sig(a), state_sig(b)
+        for key in sa:
+            nb = np.linalg.norm(sb[key])
+            diff = max(diff, float(np.linalg.norm(sa[key] - sb[key]) / (nb if nb > 0 else 1.0)))
+    launches = sum(ch.kernel_launches() for ch in ens_m)
+    ens.close()
+    for ch in ens_m + one_m:
+        ch.close()
+    return {"workload": "48 independent channels, (Nx,Ny,Nz) cycling (32,33,32), (64,65,64), (96,97,64), "
+                        "(128,65,128); Re ~ U[500,3000] (seed 5); mixed precision; dt=1e-3",
+            "points_per_step": pts, "steps": k, "warmup": warmup,
+            "value": pts * k / (ms_graph * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_graph / k,
+            "singly": {"value": pts * k / (ms_one * 1e-3) / 1e6, "ms_per_step": ms_one / k},
+            "speedup_vs_singly": ms_one / ms_graph,
+            "max_rel_diff_vs_singly": diff,
+            "graph": "one CUDA graph launch per ensemble step, one branch per member",
+            "kernel_launches_total": launches}
+
+
+def adjoint_bench(torch, nsteps=50, every=10):
+    """Cost of the hand-written discrete adjoint on the 64 x 97 x 64,
+    Re = 2000 velocity-only case: 50 FP64 steps forward (diablo_step) against
+    the checkpointed forward (diablo_adjoint_record, a checkpoint every 10
+    steps) and the backward sweep (diablo_adjoint_run: segment recompute +
+    adjoint substeps), all timed with CUDA events on the context's stream."""
+    from diablo3_test_b200 import ics, _lib
+    from diablo3_test_b200.config import FP64
+    p, gy, fields = ics.config_c4()
+    ch = setup_channel(p, gy, fields, FP64)
+    s = torch.cuda.Stream()
+    ch.set_stream(s.cuda_stream)
+    ids = (_lib.U1, _lib.U2, _lib.U3, _lib.P)
+    x0 = [torch.tensor(ch.download(f), device="cuda") for f in ids]
+    lam = [torch.zeros_like(x0[0]) for _ in ids]
+
+    def timed(fn):
+        for f, x in zip(ids, x0):
+            ch.upload(f, x, _lib.LAYOUT_FOURIER)
+        ch.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    timed(lambda: ch.step(nsteps))                     # warm-up
+    t_fwd = min(timed(lambda: ch.step(nsteps)) for _ in range(3))
+    timed(lambda: ch.adjoint_record(nsteps, every))    # first call allocates the checkpoints
+    t_rec = timed(lambda: ch.adjoint_record(nsteps, every))
+    for l in lam:
+        l.normal_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    ch.adjoint_run(lam)
+    e1.record(s)
+    e1.synchronize()
+    t_run = e0.elapsed_time(e1)
+    ch.close()
+    return {"workload": "64x97x64, Re=2000, velocities only, FP64, 50 steps, dt=1e-3, checkpoints every 10",
+            "forward_ms": t_fwd, "record_ms": t_rec, "adjoint_run_ms": t_run,
+            "adjoint_over_forward": t_run / t_fwd,
+            "record_plus_adjoint_over_forward": (t_rec + t_run) / t_fwd,
+            "note": "adjoint_run includes recomputing every segment from its checkpoint"}
+
+
 def e2e_round_trip(ch, torch, k):
     """End to end through the C ABI with pinned host buffers: each step
     uploads the state (u1, u2, u3, p, scalars) from the host in the reference
@@ -386,6 +488,10 @@ def run_ours(args):
         out["e2e"] = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)))
     chm.close()
     chd.close()
+    if world == 1 and not args.no_adjoint:
+        out["adjoint"] = adjoint_bench(torch)
+    if world == 1 and args.ensemble_steps > 0:
+        out["ensemble"] = ensemble_bench(torch, args.ensemble_steps)
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     if dist is not None:
@@ -420,6 +526,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost section")
+    ap.add_argument("--ensemble-steps", type=int, default=20,
+                    help="timed steps of the 48-member ensemble section (0: skip)")
     ap.add_argument("--acc-steps", type=int, default=100,
                     help="steps after which mixed and FP64 states are compared (untimed)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

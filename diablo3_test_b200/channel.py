@@ -88,6 +88,20 @@ class Channel:
         _lib.check(self.lib.diablo_download_state(self.ctx, field, _ptr(out), layout), "download_state")
         return out
 
+    def adjoint_record(self, nsteps: int, every: int):
+        """Advance nsteps steps, keeping checkpoints every `every` steps for
+        adjoint_run (velocity-only DNS in FP64)."""
+        _lib.check(self.lib.diablo_adjoint_record(self.ctx, nsteps, every), "adjoint_record")
+
+    def adjoint_run(self, lam):
+        """lam: four reference-layout Fourier arrays (numpy or torch) holding
+        dJ/d(u1, u2, u3, p) of the recorded final state; overwritten with
+        dJ/d of the recorded initial state."""
+        if len(lam) != 4:
+            raise ValueError("four arrays: u1, u2, u3, p")
+        arr = (ctypes.c_void_p * 4)(*[_ptr(a) for a in lam])
+        _lib.check(self.lib.diablo_adjoint_run(self.ctx, arr), "adjoint_run")
+
     def download_nu_t(self, out=None) -> np.ndarray:
         """Eddy viscosity of the last LES substep, reference physical layout."""
         if out is None:
@@ -181,6 +195,11 @@ class Ensemble:
 
     def synchronize(self):
         _lib.check(self.lib.diablo_ensemble_synchronize(self.e), "ensemble_synchronize")
+
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t the ensemble's graphs run on (for device timing)."""
+        return int(self.lib.diablo_ensemble_stream(self.e) or 0)
 
     def close(self):
         if self.e:

@@ -98,3 +98,35 @@ def config_c2(precision: int = 0):
         precision=precision)
     gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.0)
     return p, gy
+
+
+ENSEMBLE_SIZES = [(32, 33, 32), (64, 65, 64), (96, 97, 64), (128, 65, 128)]
+
+
+def config_c5(n_members: int = 48, precision: int = 1, seed: int = 5):
+    """Ensemble of independent channels with uneven grids: (Nx, Ny, Nz) cycles
+    through ENSEMBLE_SIZES; Lx = 2pi, Lz = pi, tanh 1.8; one scalar (Pr 1,
+    grav_y 0); Re drawn uniformly from [500, 3000]; dt = 1e-3, mixed precision
+    by default.  Returns [(params, gy, physical fields)] with each member's
+    own seeded perturbation on the laminar parabola."""
+    rng = np.random.default_rng(seed)
+    res = rng.uniform(500.0, 3000.0, n_members)
+    out = []
+    for i in range(n_members):
+        nx, ny, nz = ENSEMBLE_SIZES[i % len(ENSEMBLE_SIZES)]
+        p = ChannelParams.with_scalars(1, nx=nx, ny=ny, nz=nz, lx=2 * math.pi, lz=math.pi, ly=2.0,
+                                       re=float(res[i]), delta_t=1e-3, grav_y=0.0, precision=precision)
+        gy, _ = create_grid(ny, 2.0, TANH_ENDS_SYMMETRIC, 1.8)
+        out.append((p, gy, laminar_dns(p, gy, seed=seed * 1000 + i, amp=0.05)))
+    return out
+
+
+def config_c4():
+    """Adjoint sensitivity case: 64 x 97 x 64, Lx = 2pi, Lz = pi, tanh 1.8,
+    Re = 2000, velocities only, dt = 1e-3, laminar parabola driven by the
+    matching pressure gradient (f_type 1, px0 = -2/Re) plus seeded noise
+    (seed 4)."""
+    p = ChannelParams.with_scalars(0, nx=64, ny=97, nz=64, lx=2 * math.pi, lz=math.pi, ly=2.0, re=2000.0,
+                                   delta_t=1e-3, f_type=1, px0=-2.0 / 2000.0, grav_y=0.0)
+    gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 1.8)
+    return p, gy, laminar_dns(p, gy, seed=4, amp=0.05)

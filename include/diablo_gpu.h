@@ -180,6 +180,27 @@ int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, do
                                      void* stream);
 
 /*
+ * Discrete adjoint of diablo_step.  No reference counterpart: the reference
+ * has no adjoint.  For velocity-only DNS contexts in FP64 (n_th = 0, no LES,
+ * fixed delta_t); other contexts get DIABLO_ERR_UNSUPPORTED.
+ * diablo_adjoint_record advances nsteps steps exactly as diablo_step does and
+ * keeps the state (u1, u2, u3, p) every `every` steps on the device.
+ * diablo_adjoint_run takes lam[0..3] = dJ/d(u1, u2, u3, p) of the recorded
+ * final state for any objective J and overwrites them with dJ/d of the state
+ * the recording started from.  It recomputes each segment of `every` steps
+ * from its checkpoint and runs the hand-written adjoint of every RK substep
+ * backwards through it (transposed tridiagonal solves, adjoint transforms,
+ * adjoint nonlinear products), and leaves the context at the recorded final
+ * state.  lam arrays use the reference Fourier layout (host or device); each
+ * complex entry holds (dJ/dRe, dJ/dIm) of the matching coefficient; only the
+ * significant entries are read, and modes Nkx < i < Nxp are written as zero.
+ * Stepping the context between the two calls makes the run fail with
+ * DIABLO_ERR_STATE.
+ */
+int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every);
+int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam);
+
+/*
  * Ensembles of independent channels, stepped together.  No reference
  * counterpart: the reference runs one channel per MPI job.  Members are
  * contexts from diablo_create with any mix of grid sizes, parameters and
@@ -199,6 +220,10 @@ typedef struct diablo_ensemble diablo_ensemble;
 diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* status);
 int diablo_ensemble_step(diablo_ensemble* e, int nsteps);
 int diablo_ensemble_synchronize(diablo_ensemble* e);
+/* The stream each ensemble step's graph is launched on (cudaStream_t); its
+ * completion follows the whole step of every member, so events recorded on
+ * it time the ensemble on the device. */
+void* diablo_ensemble_stream(diablo_ensemble* e);
 int diablo_ensemble_destroy(diablo_ensemble* e);
 
 #ifdef __cplusplus
