@@ -294,6 +294,34 @@ def ensemble_bench(torch, k, warmup=3):
             "kernel_launches_total": launches}
 
 
+def les_bench(torch, k=5, warmup=2):
+    """LES workload (config 3: dynamic Smagorinsky, 128 x 129 x 128, Re_tau =
+    1000, k^-5/3 random-phase start, LES active from step 1), FP64, and the
+    reference's constant-Smagorinsky model on the same state for comparison.
+    CUDA events on the context's stream; nu_t summarised after the timed steps."""
+    from diablo3_test_b200 import ics
+    from diablo3_test_b200.config import FP64
+    out = {}
+    for name, model in (("dynamic_smagorinsky", 2), ("constant_smagorinsky", 1)):
+        p, gy, fields = ics.config_c3(model)
+        ch = setup_channel(p, gy, fields, FP64)
+        s = torch.cuda.Stream()
+        ch.set_stream(s.cuda_stream)
+        ch.step(warmup)
+        ms = timed_steps(ch, torch, s, k)
+        nt = ch.download_nu_t()[:, :p.nz, :p.nx]
+        pts = p.nx * p.ny * p.nz
+        out[name] = {"value": pts * k / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / k,
+                     "steps": k, "warmup": warmup, "dtype": "f64",
+                     "nu_t_max": float(nt.max()), "nu_t_mean": float(nt.mean()),
+                     "nu_t_positive_fraction": float((nt > 0).mean()), "finite": bool(ch.check_finite())}
+        ch.close()
+    out["workload"] = ("Re_tau=1000 channel LES 128x129x128, tanh 2.2, dt=2e-4, log-law mean + "
+                       "k^-5/3 random-phase fluctuations (seed 3), LES active from step 1")
+    out["mixed"] = "not built: an LES context in mixed precision returns DIABLO_ERR_UNSUPPORTED"
+    return out
+
+
 def adjoint_bench(torch, nsteps=50, every=10):
     """Cost of the hand-written discrete adjoint on the 64 x 97 x 64,
     Re = 2000 velocity-only case: 50 FP64 steps forward (diablo_step) against
@@ -488,6 +516,8 @@ def run_ours(args):
         out["e2e"] = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)))
     chm.close()
     chd.close()
+    if world == 1 and not args.no_les:
+        out["les"] = les_bench(torch)
     if world == 1 and not args.no_adjoint:
         out["adjoint"] = adjoint_bench(torch)
     if world == 1 and args.ensemble_steps > 0:
@@ -527,6 +557,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost section")
+    ap.add_argument("--no-les", action="store_true", help="skip the LES section")
     ap.add_argument("--ensemble-steps", type=int, default=20,
                     help="timed steps of the 48-member ensemble section (0: skip)")
     ap.add_argument("--acc-steps", type=int, default=100,

@@ -17,6 +17,7 @@
 #include "kernels_solve2.cuh"
 #include "kernels_les.cuh"
 #include "kernels_adjoint.cuh"
+#include "kernels_init.cuh"
 
 static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
 static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
@@ -85,6 +86,11 @@ struct diablo_ctx {
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
   double* d_prof;           // U1(y), I(U1)(y) of the mixed-precision mean split [2][n]
+  // variable dt (courant): solved velocities before the projection, their
+  // physical FP64 copies and the per-plane maxima
+  double2* ustar[3];
+  double* cfl_phys[3];
+  double* d_cfl;
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
   struct Les {
@@ -818,6 +824,10 @@ static int ensure_amd(diablo_ctx* ctx) {
   return 0;
 }
 
+static int ensure_cfl(diablo_ctx* ctx);
+static int courant_phys(diablo_ctx* ctx, const double* const* u);
+static bool courant_due(const diablo_ctx* ctx, int rk);
+
 static int substep_les(diablo_ctx* ctx, int rk) {
   diablo_ctx::Les& L = ctx->les;
   const int nf = ctx->nf, nth = ctx->nth;
@@ -1045,6 +1055,10 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     Prof pr(ctx, K_SOLVE);
     k_phys_solve<<<(unsigned)((threads + 127) / 128), 128, 0, ctx->stream>>>(sa);
   }
+  // variable dt: courant on the solved physical velocities (for/channel.f90:885-888)
+  if (courant_due(ctx, rk)) {
+    if ((rc = ensure_cfl(ctx)) || (rc = courant_phys(ctx, up))) return rc;
+  }
   {
     double2* dst[3 + DIABLO_MAX_TH];
     for (int f = 0; f < nf; ++f) dst[f] = ctx->st[nx_][f < 3 ? f : f + 1];
@@ -1140,6 +1154,143 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
   return 0;
 }
 
+// courant (for/advance.f90:47-158) from the velocities u (physical FP64,
+// planes 1..Ny): the new delta_t and RK coefficients for the steps that follow.
+static int ensure_cfl(diablo_ctx* ctx) {
+  if (ctx->d_cfl) return 0;
+  int rc;
+  for (int q = 0; q < 3; ++q) {
+    if ((rc = dev_alloc(ctx, (void**)&ctx->ustar[q], four_elems(ctx) * sizeof(double2)))) return rc;
+    if ((rc = dev_alloc(ctx, (void**)&ctx->cfl_phys[q], phys_elems(ctx) * sizeof(double)))) return rc;
+  }
+  return dev_alloc(ctx, (void**)&ctx->d_cfl, (size_t)3 * ctx->nyp2 * sizeof(double));
+}
+
+static int courant_phys(diablo_ctx* ctx, const double* const* u) {
+  const diablo_params& p = ctx->p;
+  const size_t ps = (size_t)ctx->nz * ctx->nx;
+  {
+    Prof pr(ctx, K_OTHER);
+    k_plane_absmax<<<ctx->ny, 256, 0, ctx->stream>>>(u[0], u[1], u[2], ctx->d_cfl, ps);
+  }
+  std::vector<double> mx((size_t)3 * ctx->nyp2);
+  CK(cudaMemcpyAsync(mx.data(), ctx->d_cfl, mx.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double dt = p.max_dt;
+  if (ctx->ro_inv != 0.0) dt = fmin(dt, 2.0 * PI_REF / fabs(ctx->ro_inv / p.delta) / 20.0);
+  for (int n = 0; n < ctx->nth; ++n) {
+    const double nmax = sqrt(fabs(p.th_bc_ymin_c1[n]));
+    // the literal 0.1 is default (single-precision) REAL in the reference
+    if (nmax > 0) dt = fmin(dt, (double)0.1f * 2.0 * PI_REF / nmax);
+  }
+  const double cx = p.cfl * (p.lx / ctx->nx), cz = p.cfl * (p.lz / ctx->nz);
+  double m1 = 0.0, m3 = 0.0, dty = INFINITY;
+  for (int j = 1; j <= ctx->ny; ++j) {
+    m1 = fmax(m1, mx[(size_t)j * 3]);
+    m3 = fmax(m3, mx[(size_t)j * 3 + 2]);
+    const double m2 = mx[(size_t)j * 3 + 1];
+    if (m2 > 0) dty = fmin(dty, p.cfl * ctx->h_dy[j] / m2);
+  }
+  const double dtx = m1 > 0 ? cx / m1 : INFINITY, dtz = m3 > 0 ? cz / m3 : INFINITY;
+  dt = fmin(fmin(dt, dtx), fmin(dty, dtz));
+  double nd;
+  if (dt <= 0) nd = 0.00001;
+  else if (dt >= 1000.) nd = 1000.;
+  else nd = dt;
+  if (nd != ctx->delta_t) {
+    ctx->delta_t = nd;
+    for (int r = 0; r < 3; ++r) ctx->h_bar[r] = H_FRAC[r] * nd;
+    ctx->generation++;
+    int rc = upload_coefficients(ctx);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+static int courant_four(diablo_ctx* ctx, double2* const* cu) {
+  int rc;
+  if ((rc = ensure_xs64(ctx)) || (rc = ensure_cfl(ctx))) return rc;
+  if ((rc = ifft_batch(ctx, cu, ctx->cfl_phys, 3))) return rc;
+  return courant_phys(ctx, ctx->cfl_phys);
+}
+
+static bool courant_due(const diablo_ctx* ctx, int rk) {
+  return ctx->p.variable_dt && rk == 3 && ctx->p.update_dt > 0 && ctx->time_step % ctx->p.update_dt == 0;
+}
+
+// poisson_p_chan (for/channel.f90:1026-1234): cp from the current velocity
+// (and scalars), FP64; its work arrays live only for the call.
+static int poisson_p(diablo_ctx* ctx) {
+  int rc;
+  if ((rc = ensure_xs64(ctx))) return rc;
+  const size_t fe = four_elems(ctx) * sizeof(double2), pe = phys_elems(ctx) * sizeof(double);
+  std::vector<void*> mine;
+  auto alloc = [&](void** p, size_t b) -> int {
+    int r = dev_alloc(ctx, p, b);
+    if (!r) mine.push_back(*p);
+    return r;
+  };
+  auto release = [&]() {
+    cudaStreamSynchronize(ctx->stream);
+    for (void* p : mine) {
+      for (size_t i = 0; i < ctx->allocs.size(); ++i)
+        if (ctx->allocs[i] == p) { ctx->allocs.erase(ctx->allocs.begin() + i); break; }
+      cudaFree(p);
+    }
+  };
+  double2* Gf[9];
+  double* Gp[9];
+  double2* Qf[6];
+  double* Qp[6];
+  rc = 0;
+  for (int q = 0; q < 9 && !rc; ++q) rc = alloc((void**)&Gf[q], fe) || alloc((void**)&Gp[q], pe);
+  for (int q = 0; q < 6 && !rc; ++q) rc = alloc((void**)&Qf[q], fe) || alloc((void**)&Qp[q], pe);
+  if (rc) { release(); return DIABLO_ERR_NOMEM; }
+  const FGeom fg{ctx->ny, ctx->nyp2, ctx->nkx1, ctx->nk2, ctx->kp, (size_t)ctx->nkx1 * ctx->kp};
+  const int c = ctx->cur;
+  {
+    PpGradArgs a;
+    for (int q = 0; q < 3; ++q) a.cu[q] = ctx->st[c][q];
+    for (int q = 0; q < 9; ++q) a.G[q] = Gf[q];
+    a.kx = ctx->d_kx; a.kz = ctx->d_kz; a.dyf = ctx->d_dyf; a.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_pp_grad<<<grid1d(four_elems(ctx)), 256, 0, ctx->stream>>>(a);
+  }
+  if (!rc) rc = ifft_batch(ctx, Gf, Gp, 9);
+  if (!rc) {
+    PpProdArgs a;
+    for (int q = 0; q < 9; ++q) a.G[q] = Gp[q];
+    for (int q = 0; q < 6; ++q) a.Q[q] = Qp[q];
+    a.nyp = ctx->ny;
+    a.ps = (size_t)ctx->nz * ctx->nx;
+    Prof pr(ctx, K_OTHER);
+    k_pp_prod<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(a);
+  }
+  if (!rc) rc = fft_batch(ctx, Qp, Qf, 6);
+  if (!rc) {
+    PpSolveArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int q = 0; q < 6; ++q) a.Q[q] = Qf[q];
+    for (int n = 0; n < ctx->nth; ++n) { a.cth[n] = ctx->st[c][4 + n]; a.ri[n] = ctx->p.ri[n]; }
+    a.cp = ctx->st[c][3];
+    a.kx = ctx->d_kx; a.kz = ctx->d_kz; a.met = ctx->d_met; a.gyf = ctx->d_gyf;
+    a.nth = ctx->nth; a.n = ctx->nyp2; a.nyp = ctx->ny; a.nkx1 = ctx->nkx1; a.nk2 = ctx->nk2; a.kp = ctx->kp;
+    a.ncol = ctx->nkx1 * ctx->nk2;
+    const int warps = 4;
+    dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
+    Prof pr(ctx, K_OTHER);
+    switch (rows_per_lane(ctx->nyp2)) {
+#define X(r) case r: k_pp_solve<r><<<grd, blk, 0, ctx->stream>>>(a); break;
+      X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+      default: rc = DIABLO_ERR_SIZE;
+    }
+  }
+  if (!rc && cudaGetLastError() != cudaSuccess) rc = DIABLO_ERR_CUDA;
+  release();
+  return rc;
+}
+
 static int substep(diablo_ctx* ctx, int rk) {
   if (les_active(ctx)) {
     if (ctx->precision != DIABLO_FP64) return DIABLO_ERR_UNSUPPORTED;
@@ -1222,21 +1373,25 @@ static int substep(diablo_ctx* ctx, int rk) {
     add(OP_SOLVE, 3 + n, 0, nullptr, a.cth_out[n], a.cth_in[n]);
   }
   add(OP_POISSON, 0, 0, nullptr, nullptr, nullptr);
-  add(OP_PROJ, 0, 0, a.cu_out[0], a.cu_out[0], nullptr);
-  add(OP_PROJ, 2, 0, a.cu_out[2], a.cu_out[2], nullptr);
-  add(OP_PROJ, 1, 0, a.cu_out[1], a.cu_out[1], nullptr);
+  const bool cfl = courant_due(ctx, rk);
+  if (cfl && (rc = ensure_cfl(ctx))) return rc;
+  add(OP_PROJ, 0, 0, a.cu_out[0], a.cu_out[0], cfl ? ctx->ustar[0] : nullptr);
+  add(OP_PROJ, 2, 0, a.cu_out[2], a.cu_out[2], cfl ? ctx->ustar[2] : nullptr);
+  add(OP_PROJ, 1, 0, a.cu_out[1], a.cu_out[1], cfl ? ctx->ustar[1] : nullptr);
   add(OP_CP, 0, 0, nullptr, a.cp_out, nullptr);
   {
     Prof pr(ctx, K_SOLVE);
     // thermal-wind forcing (flavor 'Front') keeps the general kernel
     if (fits && tiled) rc = launch_tiles(A, ctx->stream);
-    else if (mean_split) rc = DIABLO_ERR_UNSUPPORTED;
+    else if (mean_split || cfl) rc = DIABLO_ERR_UNSUPPORTED;
     else rc = launch_solve(a, false, ctx->stream);
     if (rc) return rc;
   }
   CK(cudaGetLastError());
   ctx->cur = nx_;
   if (a.store_cf) ctx->cf_cur = 1 - ctx->cf_cur;
+  // variable dt: courant on the solved velocities (for/channel.f90:885-888)
+  if (cfl) return courant_four(ctx, ctx->ustar);
   return 0;
 }
 
@@ -1570,7 +1725,6 @@ int diablo_rk_substep(diablo_ctx* ctx, int rk_step) {
 
 int diablo_step(diablo_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return DIABLO_ERR_ARG;
-  if (ctx->p.variable_dt) return DIABLO_ERR_UNSUPPORTED;
   for (int s = 0; s < nsteps; ++s) {
     ctx->time_step += 1;
     for (int rk = 1; rk <= 3; ++rk) {
@@ -1625,7 +1779,6 @@ int diablo_apply_bc_post(diablo_ctx* ctx) {
 
 int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure) {
   if (!ctx) return DIABLO_ERR_ARG;
-  if (compute_pressure || ctx->p.variable_dt) return DIABLO_ERR_UNSUPPORTED;
   // pre_first_step applies the velocity wall values only (for/advance.f90:25)
   int rc = bc_post(ctx, 1, 0);
   if (rc) return rc;
@@ -1635,6 +1788,14 @@ int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure) {
   if ((rc = launch_solve(a, true, ctx->stream))) return rc;
   ctx->launches++;
   CK(cudaGetLastError());
+  // poisson_p_chan for the initial pressure (for/advance.f90:31-33)
+  if (compute_pressure && (rc = poisson_p(ctx))) return rc;
+  // courant on the projected initial field (for/advance.f90:36-41)
+  if (ctx->p.variable_dt) {
+    double2* cu[3] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2]};
+    if ((rc = courant_four(ctx, cu))) return rc;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
   return 0;
 }
 

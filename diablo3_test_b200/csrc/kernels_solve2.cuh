@@ -29,7 +29,7 @@ enum TileOp {
   OP_CFOLD,        // cr += temp3 * tile
   OP_SOLVE,        // pressure gradient, matrix + wall rows, solve, store     arg: field kind
   OP_POISSON,      // phi from the accumulated divergence
-  OP_PROJ,         // tile = new velocity; subtract grad phi; store           arg: comp
+  OP_PROJ,         // tile = new velocity; subtract grad phi; store; src2: keep the tile  arg: comp
   OP_CP            // cp_out = cp_in + phi/temp4
 };
 
@@ -585,6 +585,9 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
           const int j = j0 + r;
           if (j >= n) continue;
           double2 u = TV(j);
+          // src2: keep the solved velocity before the projection (the field
+          // courant reads, for/channel.f90:885-888)
+          if (st.src2 && valid && j >= 1 && j <= nyp) ((double2*)st.src2)[j * ps + cbase + c] = u;
           if (comp != 1 && j >= 1 && j <= nyp) u = u - mul_ik(comp == 0 ? kxm : kzq, cr[r]);
           if (comp == 1 && j >= 2 && j <= nyp) {
             const double2 pm = r == 0 ? phm : cr[r - 1];

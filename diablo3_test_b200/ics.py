@@ -130,3 +130,45 @@ def config_c4():
                                    delta_t=1e-3, f_type=1, px0=-2.0 / 2000.0, grav_y=0.0)
     gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 1.8)
     return p, gy, laminar_dns(p, gy, seed=4, amp=0.05)
+
+
+def _spectral_noise(rng, p: ChannelParams, amp, damp, slope=-5.0 / 3.0):
+    """Random-phase field whose x-z energy spectrum follows k^slope (shell
+    spectrum E(k) ~ k^slope, so |u_hat|^2 ~ k^(slope - 1) in two dimensions),
+    zero mean per plane, rms amp * damp(y)."""
+    f = _empty(p)
+    kx = np.fft.rfftfreq(p.nx, 1.0 / p.nx)
+    kz = np.fft.fftfreq(p.nz, 1.0 / p.nz)
+    k = np.sqrt(kx[None, :] ** 2 + kz[:, None] ** 2)
+    a = np.zeros_like(k)
+    a[k > 0] = k[k > 0] ** ((slope - 1.0) / 2.0)
+    for j in range(p.ny + 2):
+        ph = rng.uniform(0.0, 2.0 * np.pi, k.shape)
+        v = np.fft.irfft2(a * np.exp(1j * ph), s=(p.nz, p.nx))
+        s = v.std()
+        if s > 0:
+            f[j, :p.nz, :p.nx] = amp * damp[j] * v / s
+    return f
+
+
+def config_c3(les_model_type: int = 2):
+    """LES of a Re_tau = 1000 channel: 128 x 129 x 128, Lx = 2pi, Lz = pi,
+    tanh 2.2, velocities only, constant pressure gradient px0 = -1 in wall
+    units (Re = 1000), dt = 2e-4, dynamic Smagorinsky by default, started from a
+    written state (create_new_flow = False, so the LES term acts from step 1).
+    IC: log-law mean plus random-phase fluctuations with a k^-5/3 spectrum of
+    10% of the centreline velocity (seed 3)."""
+    p = ChannelParams.with_scalars(0, nx=128, ny=129, nz=128, lx=2 * math.pi, lz=math.pi, ly=2.0, re=1000.0,
+                                   delta_t=2e-4, f_type=1, px0=-1.0, grav_y=0.0, use_les=True,
+                                   les_model_type=les_model_type, create_new_flow=False)
+    gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.2)
+    _, gyf, _, _ = metrics(gy)
+    rng = np.random.default_rng(3)
+    yp = np.clip((1.0 - np.abs(gyf)) * 1000.0, 0.0, None)
+    with np.errstate(divide="ignore"):
+        ulog = np.where(yp < 11.0, yp, np.log(np.maximum(yp, 1e-30)) / 0.41 + 5.2)
+    ucl = float(ulog.max())
+    damp = np.clip(1.0 - gyf ** 2, 0.0, None)
+    fields = {q: _spectral_noise(rng, p, 0.1 * ucl, damp) for q in ("u1", "u2", "u3")}
+    fields["u1"][:, :p.nz, :p.nx] += ulog[:, None, None]
+    return p, gy, fields

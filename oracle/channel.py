@@ -429,7 +429,8 @@ class OracleChannel:
         for n in range(self.Nth):
             nmax = math.sqrt(abs(p.th_bc_ymin_c1[n]))
             if nmax > 0:
-                dt = min(dt, 0.1 * 2.0 * PI_REF / nmax)
+                # the literal 0.1 is default (single-precision) REAL in the reference
+                dt = min(dt, float(np.float32(0.1)) * 2.0 * PI_REF / nmax)
         dx = p.lx / self.Nx
         dz = p.lz / self.Nz
         J = slice(1, self.Nyp + 1)
