@@ -262,11 +262,26 @@ def ensemble_bench(torch, k, warmup=3):
     torch.cuda.synchronize()
     es = torch.cuda.ExternalStream(ens.stream_handle)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(es)
-    ens.step(k)
-    e1.record(es)
+
+    def time_graph():
+        e0.record(es)
+        ens.step(k)
+        e1.record(es)
+        ens.synchronize()
+        return e0.elapsed_time(e1)
+
+    ms_default = time_graph()
+    # autotuned tiles per member size, scored on this graph (states restored)
+    tiles = {}
+    for (p, _, _), t in zip(cfg, ens.autotune(5)):
+        tiles[f"{p.nx}x{p.ny}x{p.nz}"] = list(t)
+    ens.step(1)
     ens.synchronize()
-    ms_graph = e0.elapsed_time(e1)
+    ms_graph = time_graph()
+    # the members run singly catch up to the same step count, then are timed
+    for ch in one_m:
+        ch.step(k + 1)
+    torch.cuda.synchronize()
     e0.record(s1)
     for ch in one_m:
         ch.step(k)
@@ -289,6 +304,10 @@ def ensemble_bench(torch, k, warmup=3):
             "value": pts * k / (ms_graph * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_graph / k,
             "singly": {"value": pts * k / (ms_one * 1e-3) / 1e6, "ms_per_step": ms_one / k},
             "speedup_vs_singly": ms_one / ms_graph,
+            "default_tiles": {"value": pts * k / (ms_default * 1e-3) / 1e6, "ms_per_step": ms_default / k},
+            "tiles": tiles,
+            "tiles_meaning": "z inverse sequences/block, x inverse rows/block, x forward rows/block, "
+                             "z forward sequences/block (0 = default), tuned per size on the graph",
             "max_rel_diff_vs_singly": diff,
             "graph": "one CUDA graph launch per ensemble step, one branch per member",
             "kernel_launches_total": launches}
@@ -436,8 +455,11 @@ def run_ours(args):
         return
     chm = setup_channel(p, gy, fields, MIXED)
     chd = setup_channel(p, gy, fields, FP64)
-    for ch in (chm, chd):
+    tiles = {}
+    for name, ch in (("mixed", chm), ("fp64", chd)):
         ch.set_stream(stream.cuda_stream)
+        if not args.no_autotune:
+            tiles[name] = list(ch.autotune())
     # warm-up
     chm.step(args.warmup)
     chd.step(args.warmup)
@@ -510,6 +532,7 @@ def run_ours(args):
         "step_roofline": step_roof,
         "kernels": per_kernel,
         "gpu_launches": launches,
+        "tiles": tiles,
         "clocks": clocks,
     }
     if not args.no_e2e:
@@ -558,6 +581,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost section")
     ap.add_argument("--no-les", action="store_true", help="skip the LES section")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default transform tiles")
     ap.add_argument("--ensemble-steps", type=int, default=20,
                     help="timed steps of the 48-member ensemble section (0: skip)")
     ap.add_argument("--acc-steps", type=int, default=100,

@@ -40,10 +40,13 @@ SIGNATURES = {
     "diablo_download_nu_t": (_i, [_vp, _vp]),
     "diablo_adjoint_record": (_i, [_vp, _i, _i]),
     "diablo_adjoint_run": (_i, [_vp, _vp]),
+    "diablo_autotune": (_i, [_vp, _vp]),
+    "diablo_tiles": (_i, [_vp, _vp]),
     "diablo_ensemble_create": (_vp, [_vp, _i, _vp]),
     "diablo_ensemble_step": (_i, [_vp, _i]),
     "diablo_ensemble_synchronize": (_i, [_vp]),
     "diablo_ensemble_stream": (_vp, [_vp]),
+    "diablo_ensemble_autotune": (_i, [_vp, _i]),
     "diablo_ensemble_destroy": (_i, [_vp]),
     "diablo_fft_xz_to_fourier": (_i, [_vp, _vp, _vp]),
     "diablo_fft_xz_to_physical": (_i, [_vp, _vp, _vp]),

@@ -88,6 +88,19 @@ class Channel:
         _lib.check(self.lib.diablo_download_state(self.ctx, field, _ptr(out), layout), "download_state")
         return out
 
+    def tiles_in_use(self):
+        """The context's current transform tiles (0 = default)."""
+        t = (ctypes.c_int * 4)()
+        _lib.check(self.lib.diablo_tiles(self.ctx, t), "tiles")
+        return tuple(t)
+
+    def autotune(self):
+        """Time the transform tile shapes for this grid and precision and keep
+        the fastest; returns (z inverse S, x inverse KT, x forward KT, z forward S)."""
+        t = (ctypes.c_int * 4)()
+        _lib.check(self.lib.diablo_autotune(self.ctx, t), "autotune")
+        return tuple(t)
+
     def adjoint_record(self, nsteps: int, every: int):
         """Advance nsteps steps, keeping checkpoints every `every` steps for
         adjoint_run (velocity-only DNS in FP64)."""
@@ -182,9 +195,11 @@ class Ensemble:
     member's kernels on a parallel branch (``diablo_ensemble_*`` of the C ABI).
     The members stay usable on their own and must outlive the ensemble."""
 
-    def __init__(self, members):
+    def __init__(self, members, autotune: bool = False):
         self.lib = _lib.load()
         self.members = list(members)
+        # tile shapes per member size (cached across members of one size)
+        self.tiles = [m.autotune() for m in self.members] if autotune else None
         arr = (ctypes.c_void_p * len(self.members))(*[m.ctx for m in self.members])
         st = ctypes.c_int(0)
         self.e = self.lib.diablo_ensemble_create(arr, len(self.members), ctypes.byref(st))
@@ -195,6 +210,12 @@ class Ensemble:
 
     def synchronize(self):
         _lib.check(self.lib.diablo_ensemble_synchronize(self.e), "ensemble_synchronize")
+
+    def autotune(self, steps_per_trial: int = 5):
+        """Tune each member size's transform tiles on the ensemble's own graph
+        (the members' states are restored); returns the tiles per member."""
+        _lib.check(self.lib.diablo_ensemble_autotune(self.e, steps_per_trial), "ensemble_autotune")
+        return [tuple(m.tiles_in_use()) for m in self.members]
 
     @property
     def stream_handle(self) -> int:

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <vector>
 
 #include "../../include/diablo_gpu.h"
@@ -80,7 +81,8 @@ struct diablo_ctx {
   std::vector<void*> allocs;
   // opt-in per-kernel timing: events recorded around each step kernel
   int profiling;
-  int generation;           // bumped whenever captured kernel arguments go stale (dt, precision)
+  int generation;           // bumped whenever captured kernel arguments go stale (dt, precision, tiles)
+  int tune[4];              // tile shapes of the step transforms (z inv S, x inv KT, x fwd KT, z fwd S; 0 = default)
   int use_general_solver;   // 1: per-lane-load column kernel instead of the tiled one
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
@@ -571,7 +573,7 @@ static int spectral_inverse(diablo_ctx* ctx, unsigned mean_mask = 0) {
     a.tw = tz;
     a.mean_mask = mean_mask;
     Prof pr(ctx, K_ZINV);
-    if ((rc = launch_zinv<C>(a, ctx->nz, nf, ctx->stream))) return rc;
+    if ((rc = launch_zinv<C>(a, ctx->nz, nf, ctx->stream, ctx->tune[0]))) return rc;
   }
   // 2. x inverse -> physical
   {
@@ -586,7 +588,7 @@ static int spectral_inverse(diablo_ctx* ctx, unsigned mean_mask = 0) {
     a.twM = tm;
     a.twX = tx;
     Prof pr(ctx, K_XINV);
-    if ((rc = launch_xinv<C>(a, ctx->M, ctx->nyp2, nf, ctx->stream))) return rc;
+    if ((rc = launch_xinv<C>(a, ctx->M, ctx->nyp2, nf, ctx->stream, ctx->tune[1]))) return rc;
   }
   return 0;
 }
@@ -617,7 +619,7 @@ static int spectral_nl(diablo_ctx* ctx, bool mean_free_u1 = false) {
     a.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
     a.scale = 1.0 / ctx->nx;
     Prof pr(ctx, K_XFWD_NL);
-    if ((rc = launch_xfwd<T, true>(a, ctx->M, ctx->ny, nf, ctx->stream))) return rc;
+    if ((rc = launch_xfwd<T, true>(a, ctx->M, ctx->ny, nf, ctx->stream, ctx->tune[2]))) return rc;
   }
   // 4. z forward + combine -> NL (planes 1..Ny)
   {
@@ -644,7 +646,7 @@ static int spectral_nl(diablo_ctx* ctx, bool mean_free_u1 = false) {
       a.fps = (size_t)ctx->nkx1 * ctx->kp;
     }
     Prof pr(ctx, K_ZFWD_NL);
-    if ((rc = launch_zfwd<C, C, true>(a, ctx->nz, nf, ctx->stream))) return rc;
+    if ((rc = launch_zfwd<C, C, true>(a, ctx->nz, nf, ctx->stream, ctx->tune[3]))) return rc;
   }
   return 0;
 }
@@ -1822,6 +1824,7 @@ int diablo_set_precision(diablo_ctx* ctx, int precision) {
   }
   ctx->precision = precision;
   ctx->p.precision = precision;
+  for (int q = 0; q < 4; ++q) ctx->tune[q] = 0;   // tiles are per precision
   ctx->generation++;
   return 0;
 }
@@ -2412,6 +2415,187 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam) {
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;
+}
+
+}  // extern "C"
+
+// ==========================================================================
+// Autotuner: the tile shapes of the four step transforms (sequences per
+// block of the z kernels, rows per block of the x kernels) are timed on the
+// context's own scratch for its grid and precision, and the fastest kept.
+// Results are cached per (grid, fields, precision) for the process.
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int, int>, std::array<int, 4>> g_tune_cache;
+
+extern "C" {
+
+int diablo_tiles(diablo_ctx* ctx, int* tiles) {
+  if (!ctx || !tiles) return DIABLO_ERR_ARG;
+  for (int q = 0; q < 4; ++q) tiles[q] = ctx->tune[q];
+  return 0;
+}
+
+int diablo_autotune(diablo_ctx* ctx, int* tiles) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  int rc;
+  if (les_active(ctx)) return DIABLO_ERR_UNSUPPORTED;
+  if ((rc = ensure_scratch(ctx))) return rc;
+  const auto key = std::make_tuple(ctx->nx, ctx->ny, ctx->nz, ctx->nf, ctx->precision);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      for (int q = 0; q < 4; ++q) ctx->tune[q] = it->second[q];
+      ctx->generation++;
+      if (tiles) for (int q = 0; q < 4; ++q) tiles[q] = ctx->tune[q];
+      return 0;
+    }
+  }
+  const bool fp32 = ctx->precision != DIABLO_FP64;
+  SolveArgs sa;
+  fill_solve_args(ctx, sa, 1);
+  const bool mean_split = fp32 && !sa.front && !ctx->use_general_solver;
+  int cand[4][3], nc[4];
+  for (int k = 0; k < 4; ++k) {
+    nc[k] = fft_tile_candidates(k, (k == 0 || k == 3) ? ctx->nz : ctx->M, fp32, cand[k]);
+    if (nc[k] <= 0) return DIABLO_ERR_SIZE;
+  }
+  const int slot[4] = {K_ZINV, K_XINV, K_XFWD_NL, K_ZFWD_NL};
+  double best[4] = {1e300, 1e300, 1e300, 1e300};
+  int pick[4] = {0, 0, 0, 0};
+  const int saved_prof = ctx->profiling;
+  auto run = [&]() -> int {
+    return fp32 ? substep_spectral<float>(ctx, mean_split ? 0x1u : 0u) : substep_spectral<double>(ctx, 0u);
+  };
+  for (int i = 0; i < 3; ++i) {
+    for (int k = 0; k < 4; ++k) ctx->tune[k] = cand[k][i < nc[k] ? i : nc[k] - 1];
+    ctx->profiling = 0;
+    if ((rc = run())) { ctx->profiling = saved_prof; return rc; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    ctx->profiling = 1;
+    for (int sl = 0; sl < K_NSLOTS; ++sl) { ctx->slot_ms[sl] = 0.0; ctx->slot_n[sl] = 0; }
+    for (int r = 0; r < 3 && !rc; ++r) rc = run();
+    if (rc) { ctx->profiling = saved_prof; return rc; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    prof_collect(ctx);
+    for (int k = 0; k < 4; ++k) {
+      if (i >= nc[k]) continue;
+      const double t = ctx->slot_ms[slot[k]];
+      if (t < best[k]) { best[k] = t; pick[k] = cand[k][i]; }
+    }
+  }
+  for (int sl = 0; sl < K_NSLOTS; ++sl) { ctx->slot_ms[sl] = 0.0; ctx->slot_n[sl] = 0; }
+  ctx->profiling = saved_prof;
+  for (int k = 0; k < 4; ++k) ctx->tune[k] = pick[k];
+  ctx->generation++;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune_cache[key] = {pick[0], pick[1], pick[2], pick[3]};
+  }
+  if (tiles) for (int q = 0; q < 4; ++q) tiles[q] = pick[q];
+  return 0;
+}
+
+}  // extern "C"
+
+// ==========================================================================
+// Ensemble autotuner: coordinate descent over the transform tiles of each
+// group of same-size members, scored by the time of the ensemble's own graph
+// (the members' kernels run concurrently there, so isolated kernel times are
+// not the objective).  Member states are restored afterwards.
+
+extern "C" {
+
+int diablo_ensemble_autotune(diablo_ensemble* e, int steps_per_trial) {
+  if (!e || steps_per_trial <= 0) return DIABLO_ERR_ARG;
+  const int n = (int)e->m.size();
+  int rc;
+  // snapshot every member (state fields, counters, tiles)
+  struct Snap { std::vector<double2*> f; double time; int step, cur, cf_cur; int tune[4]; };
+  std::vector<Snap> snap(n);
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    if ((rc = ensure_scratch(c))) return rc;
+    if (les_active(c)) return DIABLO_ERR_UNSUPPORTED;
+    const size_t fe = four_elems(c) * sizeof(double2);
+    snap[i].f.assign(4 + c->nth, nullptr);
+    for (int q = 0; q < 4 + c->nth; ++q) {
+      if ((rc = dev_alloc(c, (void**)&snap[i].f[q], fe))) return rc;
+      if (cudaMemcpyAsync(snap[i].f[q], c->st[c->cur][q], fe, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        return DIABLO_ERR_CUDA;
+    }
+    snap[i].time = c->time; snap[i].step = c->time_step; snap[i].cur = c->cur; snap[i].cf_cur = c->cf_cur;
+    for (int q = 0; q < 4; ++q) snap[i].tune[q] = c->tune[q];
+  }
+  // groups of members sharing a tile configuration
+  std::vector<std::vector<int>> groups;
+  std::vector<std::tuple<int, int, int, int, int>> gkey;
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    auto k = std::make_tuple(c->nx, c->ny, c->nz, c->nf, c->precision);
+    size_t g = 0;
+    while (g < gkey.size() && gkey[g] != k) ++g;
+    if (g == gkey.size()) { gkey.push_back(k); groups.emplace_back(); }
+    groups[g].push_back(i);
+  }
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  auto trial = [&](float* ms) -> int {
+    int r = diablo_ensemble_step(e, 1);      // captures if needed, warms
+    if (r) return r;
+    ECK(cudaEventRecord(t0, e->origin));
+    if ((r = diablo_ensemble_step(e, steps_per_trial))) return r;
+    ECK(cudaEventRecord(t1, e->origin));
+    ECK(cudaEventSynchronize(t1));
+    ECK(cudaEventElapsedTime(ms, t0, t1));
+    return 0;
+  };
+  float best = 0.f;
+  rc = trial(&best);
+  for (size_t g = 0; g < groups.size() && !rc; ++g) {
+    diablo_ctx* c0 = e->m[groups[g][0]];
+    const bool fp32 = c0->precision != DIABLO_FP64;
+    for (int k = 0; k < 4 && !rc; ++k) {
+      int cand[3];
+      const int nc = fft_tile_candidates(k, (k == 0 || k == 3) ? c0->nz : c0->M, fp32, cand);
+      const int keep = c0->tune[k];
+      int pick = keep;
+      for (int ci = 0; ci < nc && !rc; ++ci) {
+        if (cand[ci] == keep || (keep == 0 && ci == 0)) continue;   // the current choice is already scored
+        for (int i : groups[g]) { e->m[i]->tune[k] = cand[ci]; e->m[i]->generation++; }
+        float ms = 0.f;
+        if ((rc = trial(&ms))) break;
+        if (ms < best) { best = ms; pick = cand[ci]; }
+      }
+      for (int i : groups[g]) { e->m[i]->tune[k] = pick; e->m[i]->generation++; }
+    }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  // restore the members' states (the tiles found are kept)
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = rc ? rc : DIABLO_ERR_CUDA;
+    c->cur = snap[i].cur; c->cf_cur = snap[i].cf_cur; c->time = snap[i].time; c->time_step = snap[i].step;
+    const size_t fe = four_elems(c) * sizeof(double2);
+    for (int q = 0; q < 4 + c->nth; ++q) {
+      cudaMemcpyAsync(c->st[c->cur][q], snap[i].f[q], fe, cudaMemcpyDeviceToDevice, c->stream);
+      cudaStreamSynchronize(c->stream);
+      for (size_t a = 0; a < c->allocs.size(); ++a)
+        if (c->allocs[a] == snap[i].f[q]) { c->allocs.erase(c->allocs.begin() + a); break; }
+      cudaFree(snap[i].f[q]);
+    }
+    if (rc) for (int q = 0; q < 4; ++q) c->tune[q] = snap[i].tune[q];
+    c->generation++;
+  }
+  return rc;
 }
 
 }  // extern "C"

@@ -216,6 +216,21 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam);
  * entry points (upload, download, step) stay usable and are ordered with the
  * ensemble's work through the member's stream.
  */
+/*
+ * Autotuner (no reference counterpart).  Times the candidate tile shapes of
+ * the step's four transform kernels (sequences per block of the z transforms,
+ * rows per block of the x transforms) for this context's grid and precision on
+ * its own scratch, and keeps the fastest for the context's later steps.  The
+ * choice is cached per (grid, number of fields, precision) for the life of the
+ * process, so contexts of the same size tune once.  The state is not changed.
+ * tiles (optional, 4 ints) receives the choice.  Not for an active LES
+ * context (DIABLO_ERR_UNSUPPORTED); set the precision first (changing it
+ * resets the tiles to their defaults).
+ */
+int diablo_autotune(diablo_ctx* ctx, int* tiles);
+/* The context's current transform tiles (4 ints, 0 = default). */
+int diablo_tiles(diablo_ctx* ctx, int* tiles);
+
 typedef struct diablo_ensemble diablo_ensemble;
 diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* status);
 int diablo_ensemble_step(diablo_ensemble* e, int nsteps);
@@ -225,6 +240,12 @@ int diablo_ensemble_synchronize(diablo_ensemble* e);
  * it time the ensemble on the device. */
 void* diablo_ensemble_stream(diablo_ensemble* e);
 int diablo_ensemble_destroy(diablo_ensemble* e);
+/* Ensemble autotuner: coordinate descent over the transform tile shapes of
+ * each group of same-size members (the candidates of diablo_autotune), scored
+ * by the time of steps_per_trial steps of the ensemble's own graph.  The
+ * members' states and clocks are restored afterwards; the tiles found stay.
+ * Not for members with an active LES (DIABLO_ERR_UNSUPPORTED). */
+int diablo_ensemble_autotune(diablo_ensemble* e, int steps_per_trial);
 
 #ifdef __cplusplus
 }

@@ -82,3 +82,50 @@ def test_ensemble_rejects_per_step_arguments(cuda_device):
         assert e.value.status == _lib.ERR_UNSUPPORTED
     finally:
         ch.close()
+
+
+def test_autotune_keeps_results_and_caches(cuda_device):
+    from diablo3_test_b200.config import MIXED
+    kw = dict(MEMBERS[2])
+    a, b = _build(kw)
+    try:
+        t1 = a.autotune()
+        assert len(t1) == 4 and all(v > 0 for v in t1)
+        t2 = b.autotune()            # same size and precision: from the cache
+        assert t1 == t2
+        a.step(3)
+        c = _build(kw)
+        try:
+            c[0].step(3)             # default tiles
+            assert _same(a, c[0])
+        finally:
+            for ch in c:
+                ch.close()
+    finally:
+        a.close()
+        b.close()
+
+
+def test_ensemble_autotune_restores_states(cuda_device):
+    from diablo3_test_b200.channel import Ensemble
+    pairs = [_build(kw) for kw in MEMBERS[:3]]
+    try:
+        with Ensemble([p[0] for p in pairs]) as ens:
+            ens.step(2)
+            for a, b in pairs:
+                b.step(2)
+            tiles = ens.autotune(2)
+            assert len(tiles) == 3
+            for i, (a, b) in enumerate(pairs):
+                assert _same(a, b), i
+                assert a.time[1] == 2
+            ens.step(2)
+            ens.synchronize()
+            for a, b in pairs:
+                b.step(2)
+            for i, (a, b) in enumerate(pairs):
+                assert _same(a, b), i
+    finally:
+        for a, b in pairs:
+            a.close()
+            b.close()
