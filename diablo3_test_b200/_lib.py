@@ -54,6 +54,7 @@ SIGNATURES = {
     "diablo_step": (_i, [_vp, _i]),
     "diablo_pre_first_step": (_i, [_vp, _i]),
     "diablo_apply_bc_post": (_i, [_vp]),
+    "diablo_filter_chan": (_i, [_vp, _i]),
     "diablo_set_precision": (_i, [_vp, _i]),
     "diablo_get_time": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_d)]),
     "diablo_set_time": (_i, [_vp, _d, _i, _d]),

@@ -88,6 +88,8 @@ class ChannelParams:
     max_dt: float = 1.0
     precision: int = FP64
     flavor: str = "Basic"
+    filter_th: List[bool] = field(default_factory=list)
+    filter_int: List[int] = field(default_factory=list)
 
     # ------------------------------------------------------------------
     # quantities derived exactly as the reference derives them
@@ -154,7 +156,7 @@ class ChannelParams:
         per = dict(pr=[1.0] * n_th, ri=[0.0] * n_th, th_bc_ymin=[1] * n_th,
                    th_bc_ymax=[1] * n_th, th_bc_ymin_c1=[0.0] * n_th,
                    th_bc_ymax_c1=[0.0] * n_th, dthdx=[0.0] * n_th,
-                   dthdz=[0.0] * n_th)
+                   dthdz=[0.0] * n_th, filter_th=[False] * n_th, filter_int=[1] * n_th)
         for k in list(per):
             if k in kw:
                 per[k] = list(kw.pop(k))
@@ -218,6 +220,7 @@ class CParams(ctypes.Structure):
         ("update_dt", ctypes.c_int), ("max_dt", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("flavor_front", ctypes.c_int),
+        ("filter_th", ctypes.c_int * MAX_TH), ("filter_int", ctypes.c_int * MAX_TH),
     ]
 
 
@@ -265,6 +268,8 @@ def read_input_toml(path: str, nx: int, ny: int, nz: int, n_th: int) -> ChannelP
         use_les=bool(sch["USE_LES"]), les_model_type=int(sch["LES_MODEL_TYPE"]),
         create_new_flow=bool(ic["CREATE_NEW_FLOW"]),
         flavor=str(sch.get("FLAVOUR", "Basic")) or "Basic",
+        filter_th=[bool(s.get("FILTER_TH", False)) for s in scal],
+        filter_int=[int(s.get("FILTER_INT", 1)) for s in scal],
     )
     ic_type = int(ic["IC_TYPE"])
     if n_th:

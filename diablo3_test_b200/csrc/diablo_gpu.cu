@@ -93,6 +93,7 @@ struct diablo_ctx {
   double2* ustar[3];
   double* cfl_phys[3];
   double* d_cfl;
+  double* d_sigma;          // filter_chan transfer function [Nkx+1][2Nkz+1]
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
   struct Les {
@@ -1725,6 +1726,48 @@ int diablo_rk_substep(diablo_ctx* ctx, int rk_step) {
   return substep(ctx, rk_step);
 }
 
+static int filter_chan(diablo_ctx* ctx, int n) {
+  if (!ctx->d_sigma) {
+    const int nkx1 = ctx->nkx1, nk2 = ctx->nk2;
+    std::vector<double> sg((size_t)nkx1 * nk2), kx(nkx1), kz(nk2);
+    CK(cudaMemcpy(kx.data(), ctx->d_kx, nkx1 * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(kz.data(), ctx->d_kz, nk2 * sizeof(double), cudaMemcpyDeviceToHost));
+    const double fx = (double)(float)ctx->nx, fz = (double)(float)ctx->nz;
+    for (int m = 0; m < nkx1; ++m)
+      for (int q = 0; q < nk2; ++q) {
+        const double s0 = 0.5 * (1.0 + cos(sqrt(pow(kx[m] * ctx->p.lx * 1.0 / fx, 2.0) +
+                                                pow(kz[q] * ctx->p.lz * 1.0 / fz, 2.0))));
+        sg[(size_t)m * nk2 + q] = pow(s0, 4.0) * (35.0 - 84.0 * s0 + 70.0 * pow(s0, 2.0) - 20.0 * pow(s0, 3.0));
+      }
+    int rc = dev_alloc(ctx, (void**)&ctx->d_sigma, sg.size() * sizeof(double));
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_sigma, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  const int j0 = ctx->jst[n], j1 = ctx->jet[n];
+  const size_t tot = (size_t)(j1 - j0 + 1) * ctx->nkx1 * ctx->kp;
+  Prof pr(ctx, K_OTHER);
+  k_filter_th<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->st[ctx->cur][4 + n], ctx->d_sigma, j0, j1, ctx->nkx1,
+                                                    ctx->nk2, ctx->kp);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// filter_scalars (for/advance.f90:161-173), after each step
+static int filter_scalars(diablo_ctx* ctx) {
+  for (int n = 0; n < ctx->nth; ++n)
+    if (ctx->p.filter_th[n] && ctx->p.filter_int[n] > 0 && ctx->time_step % ctx->p.filter_int[n] == 0) {
+      int rc = filter_chan(ctx, n);
+      if (rc) return rc;
+    }
+  return 0;
+}
+
+int diablo_filter_chan(diablo_ctx* ctx, int n) {
+  if (!ctx || n < 0 || n >= ctx->nth) return DIABLO_ERR_ARG;
+  return filter_chan(ctx, n);
+}
+
 int diablo_step(diablo_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return DIABLO_ERR_ARG;
   for (int s = 0; s < nsteps; ++s) {
@@ -1734,6 +1777,8 @@ int diablo_step(diablo_ctx* ctx, int nsteps) {
       if (rc) return rc;
     }
     ctx->time += ctx->delta_t;
+    int rc = filter_scalars(ctx);
+    if (rc) return rc;
   }
   return 0;
 }
@@ -2050,6 +2095,8 @@ diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* 
     // kernel arguments that change every step cannot be replayed from a graph
     if (c->p.variable_dt || c->p.f_type == 2 || (c->p.f_type == 4 && c->p.w_bc_ymax != 0))
       st = DIABLO_ERR_UNSUPPORTED;
+    for (int q = 0; q < c->nth; ++q)
+      if (c->p.filter_th[q]) st = DIABLO_ERR_UNSUPPORTED;   // filtered on some steps only
   }
   if (!st) {
     e = new diablo_ensemble();

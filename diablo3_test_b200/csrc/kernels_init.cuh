@@ -169,3 +169,16 @@ __global__ void __launch_bounds__(256) k_plane_absmax(const double* u1, const do
     out[(size_t)j * 3 + threadIdx.x] = v;
   }
 }
+
+// filter_chan (for/channel.f90:1241-1329): cth *= sigma(m, kq) on rows j0..j1
+__global__ void k_filter_th(double2* cth, const double* sigma, int j0, int j1, int nkx1, int nk2, int kp) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t ps = (size_t)nkx1 * kp;
+  const size_t tot = (size_t)(j1 - j0 + 1) * ps;
+  if (idx >= tot) return;
+  const int kq = idx % kp;
+  if (kq >= nk2) return;
+  const int m = (idx / kp) % nkx1;
+  const size_t o = (size_t)j0 * ps + idx;
+  cth[o] = sigma[m * nk2 + kq] * cth[o];
+}

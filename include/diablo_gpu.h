@@ -95,6 +95,11 @@ typedef struct diablo_params {
   double max_dt;
   int precision;      /* DIABLO_FP64 or DIABLO_MIXED */
   int flavor_front;   /* 1 = flavor 'Front' (thermal-wind forcing) */
+  /* filter_scalars (for/advance.f90:161-173): scalar n is filtered by
+   * filter_chan after every step whose number is a multiple of filter_int[n]
+   * when filter_th[n] is set (FILTER_TH / FILTER_INT of input.toml) */
+  int filter_th[DIABLO_MAX_TH];
+  int filter_int[DIABLO_MAX_TH];
 } diablo_params;
 
 typedef struct diablo_ctx diablo_ctx;
@@ -132,6 +137,12 @@ int diablo_step(diablo_ctx* ctx, int nsteps);
 int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure);
 /* Fourier-space wall/ghost values of u and theta (for/boundary.f90:824-855). */
 int diablo_apply_bc_post(diablo_ctx* ctx);
+/* filter_chan (for/channel.f90:1241-1329): the spectral filter
+ * sigma0^4 (35 - 84 sigma0 + 70 sigma0^2 - 20 sigma0^3),
+ * sigma0 = (1 + cos|(kx dx, kz dz)|)/2, on scalar n's rows jstart_th..jend_th.
+ * diablo_step applies it itself as filter_scalars does; this entry point is
+ * the subroutine on its own. */
+int diablo_filter_chan(diablo_ctx* ctx, int n);
 
 int diablo_set_precision(diablo_ctx* ctx, int precision);
 int diablo_get_time(diablo_ctx* ctx, double* time, int* time_step, double* delta_t);
@@ -211,8 +222,9 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam);
  * member's state no longer matches them (a member stepped on its own, a
  * changed delta_t or precision, the LES gate opening).  Members whose kernel
  * arguments change every step are rejected with DIABLO_ERR_UNSUPPORTED:
- * variable_dt, the oscillating pressure gradient (f_type 2) and the
- * time-dependent top-wall u3 (f_type 4 with a Neumann top).  A member's own
+ * variable_dt, the oscillating pressure gradient (f_type 2), the
+ * time-dependent top-wall u3 (f_type 4 with a Neumann top) and filtered
+ * scalars (filter_th).  A member's own
  * entry points (upload, download, step) stay usable and are ordered with the
  * ensemble's work through the member's stream.
  */

@@ -717,11 +717,33 @@ class OracleChannel:
         self.rem_div_chan()                                           # :901
         cp[J, K, I] = cp[J, K, I] + cr1[J, K, I] / temp4              # :905-911
 
+    def filter_chan(self, n):
+        """Spectral filter of scalar n on rows jstart_th..jend_th
+        (for/channel.f90:1241-1329)."""
+        p = self.p
+        Nxp, twoNkz = self.Nxp, self.twoNkz
+        kx = self.kx[:Nxp][None, :]
+        kz = self.kz[:twoNkz + 1][:, None]
+        s0 = 0.5 * (1.0 + np.cos(np.sqrt((kx * p.lx * 1.0 / float(np.float32(self.Nx))) ** 2.0
+                                         + (kz * p.lz * 1.0 / float(np.float32(self.Nz))) ** 2.0)))
+        sigma = s0 ** 4.0 * (35.0 - 84.0 * s0 + 70.0 * s0 ** 2.0 - 20.0 * s0 ** 3.0)
+        J = slice(self.jstart_th[n], self.jend_th[n] + 1)
+        c = self.th[n].c
+        c[J, :twoNkz + 1, :Nxp] = c[J, :twoNkz + 1, :Nxp] * sigma[None]
+
+    def filter_scalars(self):
+        """for/advance.f90:161-173."""
+        p = self.p
+        for n in range(self.Nth):
+            if p.filter_th and p.filter_th[n] and p.filter_int[n] > 0 and self.time_step % p.filter_int[n] == 0:
+                self.filter_chan(n)
+
     def step(self, nsteps=1):
-        """Main-loop body without I/O (for/diablo.f90:98-108)."""
+        """Main-loop body without I/O (for/diablo.f90:98-111)."""
         for _ in range(nsteps):
             self.time_step += 1
             for rk in (1, 2, 3):
                 self.rk_step = rk
                 self.rk_chan_1()
             self.time += self.delta_t
+            self.filter_scalars()

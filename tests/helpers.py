@@ -12,7 +12,8 @@ def small_params(nx=32, ny=33, nz=24, n_th=1, **kw):
     base = dict(nx=nx, ny=ny, nz=nz, lx=2 * np.pi, lz=np.pi, re=200.0, delta_t=2e-3, grav_y=0.5)
     base.update(kw)
     th = {k: base.pop(k) for k in list(base) if k in (
-        "pr", "ri", "th_bc_ymin", "th_bc_ymax", "th_bc_ymin_c1", "th_bc_ymax_c1", "dthdx", "dthdz")}
+        "pr", "ri", "th_bc_ymin", "th_bc_ymax", "th_bc_ymin_c1", "th_bc_ymax_c1", "dthdx", "dthdz",
+        "filter_th", "filter_int")}
     return ChannelParams.with_scalars(n_th, **base, **th)
 
 

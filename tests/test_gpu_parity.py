@@ -94,6 +94,9 @@ CASES = {
     "moving_walls": dict(u_bc_ymin_c1=-0.3, u_bc_ymax_c1=0.4, w_bc_ymin_c1=0.2),
     "front_thermal_wind": dict(flavor="Front", ro=2.0, delta=1.5, dthdx=[0.2], dthdz=[0.05], grav_y=1.0),
     "oscillating_pressure_gradient": dict(f_type=2, px0=-0.2, amp_omega0=0.3, omega0=40.0),
+    "filtered_scalars": dict(n_th=2, pr=[0.71, 1.0], filter_th=[True, False], filter_int=[2, 1],
+                             th_bc_ymin=[0, 1], th_bc_ymax=[0, 1], th_bc_ymin_c1=[-1.0, 0.0],
+                             th_bc_ymax_c1=[1.0, 0.0]),
 }
 
 

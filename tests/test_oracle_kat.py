@@ -176,3 +176,19 @@ def test_stokes_mode_amplification():
     np.testing.assert_allclose(got.real, u * 1e-3 * v, rtol=0, atol=1e-13)
     assert np.abs(got.imag).max() < 1e-16
     assert 0 < u < 1  # it decays
+
+
+def test_scalar_filter_transfer_function():
+    # filter_chan (for/channel.f90:1241-1329): sigma = 1 on the mean mode, a
+    # smooth roll-off in |k| down to near zero at the largest stored modes
+    p, o = _oracle(nx=32, ny=9, nz=24, n_th=1)
+    c = o.th[0].c
+    c[:] = 1.0 + 1.0j
+    o.filter_chan(0)
+    J = slice(o.jstart_th[0], o.jend_th[0] + 1)
+    f = c[J, :o.twoNkz + 1, :o.Nxp]
+    assert np.all(f[:, 0, 0] == 1.0 + 1.0j)
+    assert np.all(np.abs(f) <= np.sqrt(2.0) + 1e-15)
+    assert np.abs(f[:, o.Nkz, o.Nkx]).max() < 0.5
+    # rows outside jstart_th..jend_th are untouched
+    assert np.all(c[:o.jstart_th[0]] == 1.0 + 1.0j)
