@@ -315,29 +315,41 @@ def ensemble_bench(torch, k, warmup=3):
 
 def les_bench(torch, k=5, warmup=2):
     """LES workload (config 3: dynamic Smagorinsky, 128 x 129 x 128, Re_tau =
-    1000, k^-5/3 random-phase start, LES active from step 1), FP64, and the
-    reference's constant-Smagorinsky model on the same state for comparison.
-    CUDA events on the context's stream; nu_t summarised after the timed steps."""
+    1000, k^-5/3 random-phase start, LES active from step 1) in FP64 and in
+    mixed precision (LES model and its transforms FP32; solves, projection and
+    state FP64), with the mixed-vs-FP64 error of the velocity and of nu_t after
+    the same steps; the reference's constant-Smagorinsky model beside it.
+    CUDA events on the context's stream."""
     from diablo3_test_b200 import ics
-    from diablo3_test_b200.config import FP64
+    from diablo3_test_b200.config import FP64, MIXED
     out = {}
     for name, model in (("dynamic_smagorinsky", 2), ("constant_smagorinsky", 1)):
         p, gy, fields = ics.config_c3(model)
-        ch = setup_channel(p, gy, fields, FP64)
-        s = torch.cuda.Stream()
-        ch.set_stream(s.cuda_stream)
-        ch.step(warmup)
-        ms = timed_steps(ch, torch, s, k)
-        nt = ch.download_nu_t()[:, :p.nz, :p.nx]
         pts = p.nx * p.ny * p.nz
-        out[name] = {"value": pts * k / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / k,
-                     "steps": k, "warmup": warmup, "dtype": "f64",
-                     "nu_t_max": float(nt.max()), "nu_t_mean": float(nt.mean()),
-                     "nu_t_positive_fraction": float((nt > 0).mean()), "finite": bool(ch.check_finite())}
-        ch.close()
+        res = {}
+        chans = {}
+        for prec_name, prec in (("fp64", FP64), ("mixed", MIXED)):
+            ch = setup_channel(p, gy, fields, prec)
+            s = torch.cuda.Stream()
+            ch.set_stream(s.cuda_stream)
+            ch.step(warmup)
+            ms = timed_steps(ch, torch, s, k)
+            nt = ch.download_nu_t()[:, :p.nz, :p.nx].copy()
+            res[prec_name] = {"value": pts * k / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / k,
+                              "nu_t_max": float(nt.max()), "nu_t_mean": float(nt.mean()),
+                              "nu_t_positive_fraction": float((nt > 0).mean()),
+                              "finite": bool(ch.check_finite())}
+            chans[prec_name] = (ch, nt)
+        sd, sm = state_sig(chans["fp64"][0]), state_sig(chans["mixed"][0])
+        rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+        res["mixed_vs_fp64"] = {"steps": warmup + k, "velocity_rel_l2": {q: rel(sm[q], sd[q]) for q in sd},
+                                "nu_t_rel_l2": rel(chans["mixed"][1], chans["fp64"][1])}
+        res["mixed_speedup_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+        for ch, _ in chans.values():
+            ch.close()
+        out[name] = res
     out["workload"] = ("Re_tau=1000 channel LES 128x129x128, tanh 2.2, dt=2e-4, log-law mean + "
                        "k^-5/3 random-phase fluctuations (seed 3), LES active from step 1")
-    out["mixed"] = "not built: an LES context in mixed precision returns DIABLO_ERR_UNSUPPORTED"
     return out
 
 

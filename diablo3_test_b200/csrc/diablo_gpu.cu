@@ -109,6 +109,8 @@ struct diablo_ctx {
     double *nu_t, *sf, *sg, *c2, *d2;
     double2* xs[NF_MAX];      // x-spectral scratch of the batched transforms
     double *d_cf, *d_cg, *d_d2f, *d_d2g, *d_sclf, *d_sclg;
+    double* u64[3 + DIABLO_MAX_TH];   // FP64 velocities/scalars for the solve (mixed precision)
+    int nu_t_fp32;                    // nu_t was last written by the FP32 model
     int amd_ready;            // AMD models: rotation, invariant strain, gradients
     double2 *Of[3], *SIf[6], *Gf[9], *Tf[3 * DIABLO_MAX_TH];
     double *Op[3], *SIp[6], *Gp[9], *Tp[3 * DIABLO_MAX_TH];
@@ -685,7 +687,7 @@ static int ensure_les(diablo_ctx* ctx) {
 #define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
   for (int i = 0; i < 6; ++i) { AL(L.S[i], fe); AL(L.Sp[i], pe); }
   for (int i = 0; i < 7; ++i) AL(L.T[i], fe);
-  for (int f = 0; f < ctx->nf; ++f) { AL(L.cr[f], fe); AL(L.r[f], pe); }
+  for (int f = 0; f < ctx->nf; ++f) { AL(L.cr[f], fe); AL(L.r[f], pe); AL(L.u64[f], pe); }
   for (int i = 0; i < 2 * ctx->nth; ++i) { AL(L.thg[i], fe); AL(L.thp[i], pe); }
   AL(L.tmp[0], pe); AL(L.tmp[1], pe);
   AL(L.nu_t, pe); AL(L.sf, pe); AL(L.sg, pe);
@@ -739,61 +741,80 @@ static int ensure_les(diablo_ctx* ctx) {
 }
 
 // batched FP64 transforms between the internal Fourier and physical layouts
-static int ifft_batch(diablo_ctx* ctx, const double2* const* four, double* const* phys, int nf) {
+// Batched transforms between FP64 Fourier arrays and physical arrays of
+// element type P (double, or float for the mixed-precision LES model).
+template <typename P>
+static int ifft_batch_t(diablo_ctx* ctx, const double2* const* four, P* const* phys, int nf) {
+  typedef typename CT<P>::C C;
+  const C* tz = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tz64 : (const void*)ctx->tz32);
+  const C* tm = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tm64 : (const void*)ctx->tm32);
+  const C* tx = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tx64 : (const void*)ctx->tx32);
   for (int b = 0; b < nf; b += NF_MAX) {
     const int m = nf - b < NF_MAX ? nf - b : NF_MAX;
-    ZInvArgs<double2> za;
+    ZInvArgs<C> za;
     memset(&za, 0, sizeof(za));
-    XInvArgs<double2> xa;
+    XInvArgs<C> xa;
     memset(&xa, 0, sizeof(xa));
     for (int f = 0; f < m; ++f) {
       za.src[f] = four[b + f];
-      za.dst[f] = ctx->les.xs[f];
-      xa.src[f] = ctx->les.xs[f];
+      za.dst[f] = (C*)ctx->les.xs[f];
+      xa.src[f] = (const C*)ctx->les.xs[f];
       xa.dst[f] = phys[b + f];
     }
     za.nseq = ctx->nyp2 * ctx->nkx1;
     za.g = ctx->g;
-    za.tw = ctx->tz64;
+    za.tw = tz;
     xa.g = ctx->g;
-    xa.twM = ctx->tm64;
-    xa.twX = ctx->tx64;
+    xa.twM = tm;
+    xa.twX = tx;
     int rc;
-    { Prof pr(ctx, K_ZINV); if ((rc = launch_zinv<double2>(za, ctx->nz, m, ctx->stream))) return rc; }
-    { Prof pr(ctx, K_XINV); if ((rc = launch_xinv<double2>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_ZINV); if ((rc = launch_zinv<C>(za, ctx->nz, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_XINV); if ((rc = launch_xinv<C>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
   }
   return 0;
 }
 
-static int fft_batch(diablo_ctx* ctx, const double* const* phys, double2* const* four, int nf) {
+template <typename P>
+static int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int nf) {
+  typedef typename CT<P>::C C;
+  const C* tz = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tz64 : (const void*)ctx->tz32);
+  const C* tm = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tm64 : (const void*)ctx->tm32);
+  const C* tx = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tx64 : (const void*)ctx->tx32);
   for (int b = 0; b < nf; b += NF_MAX) {
     const int m = nf - b < NF_MAX ? nf - b : NF_MAX;
-    XFwdArgs<double> xa;
+    XFwdArgs<P> xa;
     memset(&xa, 0, sizeof(xa));
-    ZFwdArgs<double2, double2> za;
+    ZFwdArgs<C, double2> za;
     memset(&za, 0, sizeof(za));
     for (int f = 0; f < m; ++f) {
       xa.in[f] = phys[b + f];
-      xa.outA[f] = ctx->les.xs[f];
-      za.srcA[f] = ctx->les.xs[f];
+      xa.outA[f] = (C*)ctx->les.xs[f];
+      za.srcA[f] = (const C*)ctx->les.xs[f];
       za.dst[f] = four[b + f];
     }
     xa.g = ctx->g;
-    xa.twM = ctx->tm64;
-    xa.twX = ctx->tx64;
+    xa.twM = tm;
+    xa.twX = tx;
     xa.kx = ctx->d_kx;
     xa.gm = GridMetrics{ctx->d_dy, ctx->d_dyf};
     xa.scale = 1.0 / ctx->nx;
     za.nseq = ctx->nyp2 * ctx->nkx1;
     za.g = ctx->g;
-    za.tw = ctx->tz64;
+    za.tw = tz;
     za.kz = ctx->d_kz;
     za.scale = 1.0 / ctx->nz;
     int rc;
-    { Prof pr(ctx, K_OTHER); if ((rc = launch_xfwd<double, false>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
-    { Prof pr(ctx, K_OTHER); if ((rc = launch_zfwd<double2, double2, false>(za, ctx->nz, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_OTHER); if ((rc = launch_xfwd<P, false>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
+    { Prof pr(ctx, K_OTHER); if ((rc = launch_zfwd<C, double2, false>(za, ctx->nz, m, ctx->stream))) return rc; }
   }
   return 0;
+}
+
+static int ifft_batch(diablo_ctx* ctx, const double2* const* four, double* const* phys, int nf) {
+  return ifft_batch_t<double>(ctx, four, phys, nf);
+}
+static int fft_batch(diablo_ctx* ctx, const double* const* phys, double2* const* four, int nf) {
+  return fft_batch_t<double>(ctx, phys, four, nf);
 }
 
 static int les_active(const diablo_ctx* ctx) {
@@ -801,6 +822,7 @@ static int les_active(const diablo_ctx* ctx) {
   return ctx->p.use_les && (!ctx->p.create_new_flow || ctx->time_step > 100);
 }
 
+template <typename P>
 static int dynamic_coefficient(diablo_ctx* ctx);
 extern "C" {
 static int bc_post(diablo_ctx* ctx, int do_vel, int do_th);
@@ -831,7 +853,24 @@ static int ensure_cfl(diablo_ctx* ctx);
 static int courant_phys(diablo_ctx* ctx, const double* const* u);
 static bool courant_due(const diablo_ctx* ctx, int rk);
 
-static int substep_les(diablo_ctx* ctx, int rk) {
+// batched transforms of LES work arrays (allocated as FP64, used as P)
+template <typename P>
+static int ifft_to(diablo_ctx* ctx, double2* const* four, double* const* phys, int nf) {
+  P* d[64];
+  for (int f = 0; f < nf; ++f) d[f] = reinterpret_cast<P*>(phys[f]);
+  return ifft_batch_t<P>(ctx, four, d, nf);
+}
+template <typename P>
+static int fft_from(diablo_ctx* ctx, double* const* phys, double2* const* four, int nf) {
+  const P* sp[64];
+  for (int f = 0; f < nf; ++f) sp[f] = reinterpret_cast<const P*>(phys[f]);
+  return fft_batch_t<P>(ctx, sp, four, nf);
+}
+
+template <typename P>
+static int substep_les_t(diablo_ctx* ctx, int rk) {
+  auto PP = [](double* q) { return reinterpret_cast<P*>(q); };
+  ctx->les.nu_t_fp32 = sizeof(P) == 4;
   diablo_ctx::Les& L = ctx->les;
   const int nf = ctx->nf, nth = ctx->nth;
   const int c = ctx->cur, nx_ = 1 - c;
@@ -886,7 +925,7 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     Prof pr(ctx, K_OTHER);
     k_strain<<<grid1d(ftot), 256, 0, ctx->stream>>>(sa);
   }
-  if ((rc = ifft_batch(ctx, L.S, L.Sp, 6))) return rc;
+  if ((rc = ifft_to<P>(ctx, L.S, L.Sp, 6))) return rc;
   const int model = ctx->p.les_model_type;
   const bool amd = model == 4 || model == 5;
   const double dxb = ctx->p.lx / ctx->nx * LES_BETA, dzb = ctx->p.lz / ctx->nz * LES_BETA;
@@ -906,50 +945,50 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     af.deltax = dxb; af.deltaz = dzb;
     af.model = model; af.nth = nth; af.g = fg;
     { Prof pr(ctx, K_OTHER); k_amd_fourier<<<grid1d(ftot), 256, 0, ctx->stream>>>(af); }
-    if ((rc = ifft_batch(ctx, L.Of, L.Op, 3))) return rc;
+    if ((rc = ifft_to<P>(ctx, L.Of, L.Op, 3))) return rc;
     if (model == 5) {
-      if ((rc = ifft_batch(ctx, L.SIf, L.SIp, 6))) return rc;
-      if ((rc = ifft_batch(ctx, L.Gf, L.Gp, 9))) return rc;
-      if (nth > 0 && (rc = ifft_batch(ctx, L.Tf, L.Tp, 3 * nth))) return rc;
+      if ((rc = ifft_to<P>(ctx, L.SIf, L.SIp, 6))) return rc;
+      if ((rc = ifft_to<P>(ctx, L.Gf, L.Gp, 9))) return rc;
+      if (nth > 0 && (rc = ifft_to<P>(ctx, L.Tf, L.Tp, 3 * nth))) return rc;
     }
   }
-  if ((rc = spectral_inverse<double>(ctx))) return rc;       // u, th -> ctx->phys
-  double* const* up = (double* const*)ctx->phys;
+  if ((rc = spectral_inverse<P>(ctx))) return rc;            // u, th -> ctx->phys
+  P* const* up = (P* const*)ctx->phys;
   // 5. |S|, the coefficient (dynamic model), eddy viscosity and stresses
   {
-    LesPointArgs pa;
+    LesPointArgs<P> pa;
     memset(&pa, 0, sizeof(pa));
-    for (int i = 0; i < 6; ++i) pa.S[i] = L.Sp[i];
+    for (int i = 0; i < 6; ++i) pa.S[i] = PP(L.Sp[i]);
     pa.u1 = up[0]; pa.u3 = up[2];
-    pa.nu_t = L.nu_t;
-    pa.tmp[0] = L.tmp[0]; pa.tmp[1] = L.tmp[1];
+    pa.nu_t = PP(L.nu_t);
+    pa.tmp[0] = PP(L.tmp[0]); pa.tmp[1] = PP(L.tmp[1]);
     pa.dy = ctx->d_dy; pa.dyf = ctx->d_dyf;
     pa.cf = L.d_cf; pa.cg = L.d_cg; pa.d2f = L.d_d2f; pa.d2g = L.d_d2g;
     pa.nx = ctx->nx; pa.nz = ctx->nz; pa.nyp = ctx->ny;
     pa.dynamic = model == 2;
     pa.amd = amd;
     if (amd) {
-      AmdCoefArgs ca;
-      for (int q = 0; q < 6; ++q) ca.S[q] = model == 5 ? L.SIp[q] : L.Sp[q];
-      for (int q = 0; q < 3; ++q) ca.O[q] = L.Op[q];
+      AmdCoefArgs<P> ca;
+      for (int q = 0; q < 6; ++q) ca.S[q] = PP(model == 5 ? L.SIp[q] : L.Sp[q]);
+      for (int q = 0; q < 3; ++q) ca.O[q] = PP(L.Op[q]);
       ca.dy = ctx->d_dy; ca.dyf = ctx->d_dyf;
-      ca.sf = L.sf; ca.sg = L.sg;
+      ca.sf = PP(L.sf); ca.sg = PP(L.sg);
       ca.wx = pow(dxb, 2.0); ca.wz = pow(dzb, 2.0);
       ca.model = model; ca.nyp = ctx->ny; ca.jstart = ctx->jstart; ca.jend = ctx->jend;
       ca.ps = (size_t)ctx->nz * ctx->nx;
       Prof pr(ctx, K_OTHER);
-      k_amd_coef<<<grid1d(ptot), 256, 0, ctx->stream>>>(ca);
+      k_amd_coef<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(ca);
     } else {
       Prof pr(ctx, K_OTHER);
-      k_les_norms<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg);
+      k_les_norms<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, PP(L.sf), PP(L.sg));
     }
-    if (model == 2 && (rc = dynamic_coefficient(ctx))) return rc;
-    { Prof pr(ctx, K_OTHER); k_les_point<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, L.sf, L.sg); }
+    if (model == 2 && (rc = dynamic_coefficient<P>(ctx))) return rc;
+    { Prof pr(ctx, K_OTHER); k_les_point<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(pa, PP(L.sf), PP(L.sg)); }
   }
   // 6. stresses to Fourier space, divergence into cf (for/les.f90:245-274, 850-880)
   {
-    const double* src[7] = {L.Sp[0], L.Sp[2], L.Sp[3], L.Sp[4], L.Sp[5], L.tmp[0], L.tmp[1]};
-    if ((rc = fft_batch(ctx, src, L.T, 7))) return rc;
+    const P* src[7] = {PP(L.Sp[0]), PP(L.Sp[2]), PP(L.Sp[3]), PP(L.Sp[4]), PP(L.Sp[5]), PP(L.tmp[0]), PP(L.tmp[1])};
+    if ((rc = fft_batch_t<P>(ctx, src, L.T, 7))) return rc;
     LesDivArgs da;
     for (int i = 0; i < 7; ++i) da.T[i] = L.T[i];
     for (int q = 0; q < 3; ++q) da.cf[q] = cf_out[q];
@@ -962,25 +1001,25 @@ static int substep_les(diablo_ctx* ctx, int rk) {
   // 7. scalar SGS flux: the AMD scalar model (model 5, for/les.f90:1219-1412)
   // or kappa_t = nu_t (for/les.f90:1130-1200)
   if (nth > 0 && model == 5) {
-    AmdThArgs ta;
+    AmdThArgs<P> ta;
     memset(&ta, 0, sizeof(ta));
-    for (int q = 0; q < 9; ++q) ta.G[q] = L.Gp[q];
-    for (int q = 0; q < 3 * nth; ++q) ta.T[q] = L.Tp[q];
+    for (int q = 0; q < 9; ++q) ta.G[q] = PP(L.Gp[q]);
+    for (int q = 0; q < 3 * nth; ++q) ta.T[q] = PP(L.Tp[q]);
     for (int n = 0; n < nth; ++n) {
-      ta.fx[n] = L.fxp[n]; ta.fz[n] = L.fzp[n]; ta.kap[n] = L.kap[n];
+      ta.fx[n] = PP(L.fxp[n]); ta.fz[n] = PP(L.fzp[n]); ta.kap[n] = PP(L.kap[n]);
       ta.jst[n] = ctx->jst[n]; ta.jet[n] = ctx->jet[n];
     }
     ta.dy = ctx->d_dy; ta.dyf = ctx->d_dyf; ta.hdy = L.d_cg;
     ta.deltax = dxb; ta.deltaz = dzb;
     ta.nth = nth; ta.nyp = ctx->ny; ta.ps = (size_t)ctx->nz * ctx->nx;
-    { Prof pr(ctx, K_OTHER); k_amd_th<<<grid1d(ptot), 256, 0, ctx->stream>>>(ta); }
-    double* srcp[2 * DIABLO_MAX_TH];
+    { Prof pr(ctx, K_OTHER); k_amd_th<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(ta); }
+    P* srcp[2 * DIABLO_MAX_TH];
     double2* dstf[2 * DIABLO_MAX_TH];
     for (int n = 0; n < nth; ++n) {
-      srcp[2 * n] = L.fxp[n]; srcp[2 * n + 1] = L.fzp[n];
+      srcp[2 * n] = PP(L.fxp[n]); srcp[2 * n + 1] = PP(L.fzp[n]);
       dstf[2 * n] = L.fxf[n]; dstf[2 * n + 1] = L.fzf[n];
     }
-    if ((rc = fft_batch(ctx, srcp, dstf, 2 * nth))) return rc;
+    if ((rc = fft_batch_t<P>(ctx, srcp, dstf, 2 * nth))) return rc;
     AmdThDivArgs da;
     memset(&da, 0, sizeof(da));
     for (int n = 0; n < nth; ++n) {
@@ -996,19 +1035,19 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     for (int n = 0; n < nth; ++n) { ga.cth[n] = ctx->st[c][4 + n]; ga.gx[n] = L.thg[2 * n]; ga.gz[n] = L.thg[2 * n + 1]; }
     ga.kx = ctx->d_kx; ga.kz = ctx->d_kz; ga.g = fg; ga.nth = nth;
     { Prof pr(ctx, K_OTHER); k_th_grad<<<grid1d(ftot), 256, 0, ctx->stream>>>(ga); }
-    if ((rc = ifft_batch(ctx, L.thg, L.thp, 2 * nth))) return rc;
+    if ((rc = ifft_to<P>(ctx, L.thg, L.thp, 2 * nth))) return rc;
     {
-      ScaleArgs sa;
+      ScaleArgs<P> sa;
       memset(&sa, 0, sizeof(sa));
-      for (int q = 0; q < 2 * nth; ++q) sa.f[q] = L.thp[q];
+      for (int q = 0; q < 2 * nth; ++q) sa.f[q] = PP(L.thp[q]);
       sa.nfield = 2 * nth;
-      sa.w = L.nu_t;                                   // kappa_t = nu_t (:1130-1140)
+      sa.w = PP(L.nu_t);                                   // kappa_t = nu_t (:1130-1140)
       sa.ps = (size_t)ctx->nz * ctx->nx;
       sa.nyp = ctx->ny;
       Prof pr(ctx, K_OTHER);
-      k_scale_by<<<grid1d(ptot), 256, 0, ctx->stream>>>(sa);
+      k_scale_by<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(sa);
     }
-    if ((rc = fft_batch(ctx, L.thp, L.thg, 2 * nth))) return rc;
+    if ((rc = fft_from<P>(ctx, L.thp, L.thg, 2 * nth))) return rc;
     ThDivArgs ta;
     memset(&ta, 0, sizeof(ta));
     for (int n = 0; n < nth; ++n) {
@@ -1020,7 +1059,7 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     k_th_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(ta);
   }
   // 8. nonlinear terms (as the DNS step), cf -= NL, cr += beta h cf
-  if ((rc = spectral_nl<double>(ctx))) return rc;
+  if ((rc = spectral_nl<P>(ctx))) return rc;
   {
     CfFinishArgs fa;
     memset(&fa, 0, sizeof(fa));
@@ -1029,17 +1068,28 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     fa.lo[1] = 2; fa.hi[1] = ctx->ny;
     for (int n = 0; n < nth; ++n) { fa.lo[3 + n] = ctx->jst[n]; fa.hi[3 + n] = ctx->jet[n]; }
     fa.nf = nf; fa.temp5 = a.temp5; fa.g = fg;
+    fa.nl_fp32 = sizeof(P) == 4;
     Prof pr(ctx, K_OTHER);
     k_cf_finish<<<grid1d(ftot), 256, 0, ctx->stream>>>(fa);
   }
   // 9. r = IFFT(cr); CN in y per physical column; 10. u, th back to Fourier
   if ((rc = ifft_batch(ctx, L.cr, L.r, nf))) return rc;
+  // the solve runs in FP64: with the FP32 model, the post-wall-update state
+  // is transformed once more in FP64 for it
+  double* u64[3 + DIABLO_MAX_TH];
+  if (sizeof(P) == 8) {
+    for (int f = 0; f < nf; ++f) u64[f] = reinterpret_cast<double*>(up[f]);
+  } else {
+    const double2* src[3 + DIABLO_MAX_TH];
+    for (int f = 0; f < nf; ++f) { src[f] = ctx->st[c][f < 3 ? f : f + 1]; u64[f] = L.u64[f]; }
+    if ((rc = ifft_batch(ctx, src, u64, nf))) return rc;
+  }
   {
-    PhysSolveArgs sa;
+    PhysSolveArgs<P> sa;
     memset(&sa, 0, sizeof(sa));
-    for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = up[f]; }
-    sa.nu_t = L.nu_t;
-    for (int n = 0; n < nth; ++n) sa.kap[n] = model == 5 ? L.kap[n] : L.nu_t;
+    for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = u64[f]; }
+    sa.nu_t = PP(L.nu_t);
+    for (int n = 0; n < nth; ++n) sa.kap[n] = PP(model == 5 ? L.kap[n] : L.nu_t);
     sa.c2 = L.c2; sa.d2 = L.d2;
     sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf;
     sa.nf = nf; sa.nth = nth; sa.n = ctx->nyp2; sa.nyp = ctx->ny; sa.cols = ctx->nz * ctx->nx;
@@ -1056,16 +1106,16 @@ static int substep_les(diablo_ctx* ctx, int rk) {
     }
     const size_t threads = (size_t)nf * sa.cols;
     Prof pr(ctx, K_SOLVE);
-    k_phys_solve<<<(unsigned)((threads + 127) / 128), 128, 0, ctx->stream>>>(sa);
+    k_phys_solve<P><<<(unsigned)((threads + 127) / 128), 128, 0, ctx->stream>>>(sa);
   }
   // variable dt: courant on the solved physical velocities (for/channel.f90:885-888)
   if (courant_due(ctx, rk)) {
-    if ((rc = ensure_cfl(ctx)) || (rc = courant_phys(ctx, up))) return rc;
+    if ((rc = ensure_cfl(ctx)) || (rc = courant_phys(ctx, u64))) return rc;
   }
   {
     double2* dst[3 + DIABLO_MAX_TH];
     for (int f = 0; f < nf; ++f) dst[f] = ctx->st[nx_][f < 3 ? f : f + 1];
-    if ((rc = fft_batch(ctx, (const double* const*)up, dst, nf))) return rc;
+    if ((rc = fft_batch(ctx, u64, dst, nf))) return rc;
   }
   // 11. projection and pressure update on the new state (for/channel.f90:901-911)
   {
@@ -1104,24 +1154,26 @@ static int ensure_dyn(diablo_ctx* ctx) {
 // build the 21 Germano/Lilly inputs, test-filter them in Fourier space,
 // contract and average over x-z planes.  Needs les.Sp (raw strain), les.sf
 // and the physical velocities in ctx->phys.
+template <typename P>
 static int dynamic_coefficient(diablo_ctx* ctx) {
+  auto PP = [](double* q) { return reinterpret_cast<P*>(q); };
   diablo_ctx::Les& L = ctx->les;
   int rc;
   const size_t ptot = phys_elems(ctx), ftot = four_elems(ctx);
   if ((rc = ensure_dyn(ctx))) return rc;
   const size_t ps = (size_t)ctx->nz * ctx->nx;
   {
-    DynPrepArgs pa;
-    for (int q = 0; q < 3; ++q) pa.u[q] = (const double*)ctx->phys[q];
-    for (int q = 0; q < 6; ++q) pa.S[q] = L.Sp[q];
-    pa.sf = L.sf;
-    for (int q = 0; q < DYN_NF; ++q) pa.out[q] = L.dp[q];
+    DynPrepArgs<P> pa;
+    for (int q = 0; q < 3; ++q) pa.u[q] = (const P*)ctx->phys[q];
+    for (int q = 0; q < 6; ++q) pa.S[q] = PP(L.Sp[q]);
+    pa.sf = PP(L.sf);
+    for (int q = 0; q < DYN_NF; ++q) pa.out[q] = PP(L.dp[q]);
     pa.nyp = ctx->ny;
     pa.ps = ps;
     Prof pr(ctx, K_OTHER);
-    k_dyn_prep<<<grid1d(ptot), 256, 0, ctx->stream>>>(pa);
+    k_dyn_prep<P><<<grid1d(ptot), 256, 0, ctx->stream>>>(pa);
   }
-  if ((rc = fft_batch(ctx, L.dp, L.df, DYN_NF))) return rc;
+  if ((rc = fft_from<P>(ctx, L.dp, L.df, DYN_NF))) return rc;
   const FGeom fg{ctx->ny, ctx->nyp2, ctx->nkx1, ctx->nk2, ctx->kp, (size_t)ctx->nkx1 * ctx->kp};
   for (int b = 0; b < DYN_NF; b += NF_MAX) {
     MaskArgs ma;
@@ -1135,18 +1187,18 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
     Prof pr(ctx, K_OTHER);
     k_test_mask<<<grid1d(ftot), 256, 0, ctx->stream>>>(ma);
   }
-  if ((rc = ifft_batch(ctx, L.df, L.dp, DYN_NF))) return rc;
+  if ((rc = ifft_to<P>(ctx, L.df, L.dp, DYN_NF))) return rc;
   {
-    DynContractArgs ca;
-    for (int q = 0; q < DYN_NF; ++q) ca.F[q] = L.dp[q];
-    for (int q = 0; q < 3; ++q) ca.u[q] = (const double*)ctx->phys[q];
+    DynContractArgs<P> ca;
+    for (int q = 0; q < DYN_NF; ++q) ca.F[q] = PP(L.dp[q]);
+    for (int q = 0; q < 3; ++q) ca.u[q] = (const P*)ctx->phys[q];
     ca.d2f = L.d_d2f;
     ca.sums = L.dsums;
     ca.nyp = ctx->ny;
     ca.ps = ps;
     ca.ratio2 = 4.0;   // (2 Delta / Delta)^2
     Prof pr(ctx, K_OTHER);
-    k_dyn_contract<<<ctx->ny, 256, 0, ctx->stream>>>(ca);
+    k_dyn_contract<P><<<ctx->ny, 256, 0, ctx->stream>>>(ca);
   }
   {
     Prof pr(ctx, K_OTHER);
@@ -1296,10 +1348,11 @@ static int poisson_p(diablo_ctx* ctx) {
 
 static int substep(diablo_ctx* ctx, int rk) {
   if (les_active(ctx)) {
-    if (ctx->precision != DIABLO_FP64) return DIABLO_ERR_UNSUPPORTED;
     const int m = ctx->p.les_model_type;
     if (m != 1 && m != 2 && m != 4 && m != 5) return DIABLO_ERR_UNSUPPORTED;
-    return substep_les(ctx, rk);
+    // mixed precision: the LES model and its transforms in FP32, the
+    // Crank-Nicolson solves, projection and state in FP64
+    return ctx->precision == DIABLO_FP64 ? substep_les_t<double>(ctx, rk) : substep_les_t<float>(ctx, rk);
   }
   int rc = ensure_scratch(ctx);
   if (rc) return rc;
@@ -1688,6 +1741,10 @@ int diablo_download_nu_t(diablo_ctx* ctx, double* buf) {
   if (!ctx->les.ready) {
     CK(cudaMemsetAsync(ctx->b_phys, 0, phys_elems(ctx) * sizeof(double), ctx->stream));
     src = ctx->b_phys;
+  } else if (ctx->les.nu_t_fp32) {
+    k_widen<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(reinterpret_cast<const float*>(ctx->les.nu_t),
+                                                             ctx->b_phys, phys_elems(ctx));
+    src = ctx->b_phys;
   }
   if ((rc = phys_out(ctx, src, buf))) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1981,7 +2038,7 @@ static MemberKey member_key(const diablo_ctx* c) {
 static int prepare_member(diablo_ctx* ctx) {
   int rc;
   if ((rc = ensure_scratch(ctx))) return rc;
-  if (les_active(ctx) && ctx->precision == DIABLO_FP64) {
+  if (les_active(ctx)) {
     if ((rc = ensure_les(ctx))) return rc;
     const int m = ctx->p.les_model_type;
     if ((m == 4 || m == 5) && (rc = ensure_amd(ctx))) return rc;

@@ -199,3 +199,5 @@ template int launch_xinv<float2>(const XInvArgs<float2>&, int, int, int, cudaStr
 template int launch_xfwd<double, false>(const XFwdArgs<double>&, int, int, int, cudaStream_t, int);
 template int launch_xfwd<double, true>(const XFwdArgs<double>&, int, int, int, cudaStream_t, int);
 template int launch_xfwd<float, true>(const XFwdArgs<float>&, int, int, int, cudaStream_t, int);
+template int launch_xfwd<float, false>(const XFwdArgs<float>&, int, int, int, cudaStream_t, int);
+template int launch_zfwd<float2, double2, false>(const ZFwdArgs<float2, double2>&, int, int, cudaStream_t, int);

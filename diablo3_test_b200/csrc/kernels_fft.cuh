@@ -384,7 +384,7 @@ struct XFwdSmem {
 };
 
 template <typename T, int N1, int N2, int KT, bool NL>
-__global__ void __launch_bounds__(N2* KT) k_xr2c(XFwdArgs<T> a) {
+__global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? 5 : 1) k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   constexpr int M = N1 * N2;
   constexpr int ROWC = XFwdSmem<T, N1, N2, KT>::ROWC;

@@ -180,13 +180,14 @@ __global__ void k_strain(StrainArgs a) {
 // S[0..5] in: strain components (S2 is zeroed on output, as the reference
 // does); out: |S| S_ij at GYF (S1, S3, S5), |S|_GY (S_ij - implicit part) at GY
 // (S4, S6); tmp[0] = nu_t dU1/dy, tmp[1] = nu_t dU3/dy at GY; nu_t at GY.
+template <typename P>
 struct LesPointArgs {
-  double* S[6];
-  const double* u1;
-  const double* u3;
-  double* nu_t;
-  double* nu_f;          // dynamic model only: clipped nu_t at GYF (may be null)
-  double* tmp[2];
+  P* S[6];
+  const P* u1;
+  const P* u3;
+  P* nu_t;
+  P* nu_f;               // dynamic model only: clipped nu_t at GYF (may be null)
+  P* tmp[2];
   const double* dy;
   const double* dyf;
   const double* cf;      // C(y) at GYF (constant model: c_s^2 for all j)
@@ -199,7 +200,8 @@ struct LesPointArgs {
 };
 
 // |S| at GYF point j (needs S4, S6 at j and j+1)
-DI double snorm_f(const LesPointArgs& a, size_t o, size_t ps) {
+template <typename P>
+DI double snorm_f(const LesPointArgs<P>& a, size_t o, size_t ps) {
   const double s4 = 0.5 * (a.S[3][o + ps] + a.S[3][o]);
   const double s6 = 0.5 * (a.S[5][o + ps] + a.S[5][o]);
   const double s1 = a.S[0][o], s2 = a.S[1][o], s3 = a.S[2][o], s5 = a.S[4][o];
@@ -207,9 +209,10 @@ DI double snorm_f(const LesPointArgs& a, size_t o, size_t ps) {
               2.0 * (s3 * s3));
 }
 // |S| at GY point j (GYF components interpolated)
-DI double snorm_g(const LesPointArgs& a, size_t o, size_t ps, int j) {
+template <typename P>
+DI double snorm_g(const LesPointArgs<P>& a, size_t o, size_t ps, int j) {
   const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
-  auto I = [&](const double* f) { return (f[o] * w1 + f[o - ps] * w0) / den; };
+  auto I = [&](const P* f) { return (f[o] * w1 + f[o - ps] * w0) / den; };
   const double s1 = I(a.S[0]), s2 = I(a.S[1]), s3 = I(a.S[2]), s5 = I(a.S[4]);
   const double s4 = a.S[3][o], s6 = a.S[5][o];
   return sqrt(2.0 * (s1 * s1) + 4.0 * (s4 * s4) + 4.0 * (s5 * s5) + 2.0 * (s2 * s2) + 4.0 * (s6 * s6) +
@@ -217,7 +220,8 @@ DI double snorm_g(const LesPointArgs& a, size_t o, size_t ps, int j) {
 }
 
 // pass 1: |S| at GYF and GY into scratch (two planes are read per point)
-__global__ void k_les_norms(LesPointArgs a, double* sf, double* sg) {
+template <typename P>
+__global__ void k_les_norms(LesPointArgs<P> a, P* sf, P* sg) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t ps = (size_t)a.nz * a.nx;
   const size_t tot = (size_t)(a.nyp + 2) * ps;
@@ -228,7 +232,8 @@ __global__ void k_les_norms(LesPointArgs a, double* sf, double* sg) {
 }
 
 // pass 2: stresses, nu_t and the implicit-part fluxes
-__global__ void k_les_point(LesPointArgs a, const double* sf, const double* sg) {
+template <typename P>
+__global__ void k_les_point(LesPointArgs<P> a, const P* sf, const P* sg) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t ps = (size_t)a.nz * a.nx;
   const size_t tot = (size_t)(a.nyp + 2) * ps;
@@ -351,15 +356,17 @@ __global__ void k_th_grad(ThGradArgs a) {
 }
 
 // physical: f *= nu_t on planes 1..Nyp+1
+template <typename P>
 struct ScaleArgs {
-  double* f[2 * 8];
+  P* f[2 * 8];
   int nfield;
-  const double* w;
+  const P* w;
   size_t ps;
   int nyp;
 };
 
-__global__ void k_scale_by(ScaleArgs a) {
+template <typename P>
+__global__ void k_scale_by(ScaleArgs<P> a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -429,11 +436,12 @@ __global__ void k_cf_finish(CfFinishArgs a) {
 // (:494-547 explicit half, :625-646 scalars, :657-877 implicit rows, Thomas
 // :1335-1496).  One thread per (field, x-z column); the forward sweep keeps
 // the modified upper diagonal and right-hand side in scratch (c2, d2).
+template <typename P>
 struct PhysSolveArgs {
   const double* r[SOLVE_NF];    // inverse-transformed cr
   double* u[SOLVE_NF];          // in: physical field at the start; out: solution on the write rows
-  const double* nu_t;
-  const double* kap[8];
+  const P* nu_t;                // eddy viscosity / diffusivities (the LES model's precision)
+  const P* kap[8];
   double* c2;                   // scratch [nf][n][cols]
   double* d2;
   const double* dy;
@@ -449,7 +457,8 @@ struct PhysSolveArgs {
   double thc1[8][2];
 };
 
-__global__ void k_phys_solve(PhysSolveArgs a) {
+template <typename P>
+__global__ void k_phys_solve(PhysSolveArgs<P> a) {
   const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= (size_t)a.nf * a.cols) return;
   const int f = gid / a.cols;
@@ -458,7 +467,7 @@ __global__ void k_phys_solve(PhysSolveArgs a) {
   const int n = a.n, nyp = a.nyp;
   const double* r = a.r[f];
   double* u = a.u[f];
-  const double* nt = f < 3 ? a.nu_t : a.kap[f - 3];
+  const P* nt = f < 3 ? a.nu_t : a.kap[f - 3];
   double* c2 = a.c2 + (size_t)f * n * ps + col;
   double* d2 = a.d2 + (size_t)f * n * ps + col;
   int lo, hi, w0, b0, b1;
@@ -560,11 +569,12 @@ __global__ void k_phys_solve(PhysSolveArgs a) {
 //   9..14  U_a U_b  (same pair order)
 //   15..20 |S| S_ab
 #define DYN_NF 21
+template <typename P>
 struct DynPrepArgs {
-  const double* u[3];
-  const double* S[6];     // raw strain components S1..S6 (physical)
-  const double* sf;       // |S| at GYF
-  double* out[DYN_NF];
+  const P* u[3];
+  const P* S[6];          // raw strain components S1..S6 (physical)
+  const P* sf;            // |S| at GYF
+  P* out[DYN_NF];
   int nyp;
   size_t ps;              // Nx * Nz
 };
@@ -572,7 +582,8 @@ struct DynPrepArgs {
 __device__ __constant__ int c_pair_a[6] = {0, 1, 2, 0, 0, 1};
 __device__ __constant__ int c_pair_b[6] = {0, 1, 2, 1, 2, 2};
 
-__global__ void k_dyn_prep(DynPrepArgs a) {
+template <typename P>
+__global__ void k_dyn_prep(DynPrepArgs<P> a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -625,9 +636,10 @@ __global__ void k_test_mask(MaskArgs a) {
 
 // Per-plane Germano/Lilly sums: one block per GYF plane j (blockIdx.x + 1).
 // sums[j][0..5] = sum over the plane of L_ab M_ab per pair, [6..11] of M_ab^2.
+template <typename P>
 struct DynContractArgs {
-  const double* F[DYN_NF];    // test-filtered fields (physical)
-  const double* u[3];         // unfiltered u1, u2 (GY), u3
+  const P* F[DYN_NF];         // test-filtered fields (physical)
+  const P* u[3];              // unfiltered u1, u2 (GY), u3
   const double* d2f;          // Delta^2 at GYF
   double* sums;               // [(Ny+2) * 12]
   int nyp;
@@ -635,7 +647,8 @@ struct DynContractArgs {
   double ratio2;              // (test / grid width)^2
 };
 
-__global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs a) {
+template <typename P>
+__global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs<P> a) {
   const int j = blockIdx.x + 1;
   const size_t base = (size_t)j * a.ps;
   double acc[12];
@@ -818,19 +831,21 @@ DI double amd_ratio(double a1, double a2, double a3, double a4, double a5, doubl
 // Model 4: strain S, weights delta_i^2 with (2 dy(j))^2 in y, GYF rows 1..Nyp,
 // GY rows 2..Nyp+1.  Model 5: invariant strain, unit weights, GYF rows
 // jstart..jend, GY rows 2..Nyp.
+template <typename P>
 struct AmdCoefArgs {
-  const double* S[6];
-  const double* O[3];
+  const P* S[6];
+  const P* O[3];
   const double* dy;
   const double* dyf;
-  double* sf;
-  double* sg;
+  P* sf;
+  P* sg;
   double wx, wz;          // (dx beta)^2, (dz beta)^2 (model 4)
   int model, nyp, jstart, jend;
   size_t ps;
 };
 
-__global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs a) {
+template <typename P>
+__global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs<P> a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -843,7 +858,7 @@ __global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs a) {
   if (j >= f0 && j <= f1) {
     const double wy = m4 ? (a.dy[j] * 2.0) * (a.dy[j] * 2.0) : 1.0;
     const double wx = m4 ? a.wx : 1.0, wz = m4 ? a.wz : 1.0;
-    auto av = [&](const double* f) { return 0.5 * (f[idx + ps] + f[idx]); };
+    auto av = [&](const P* f) { return 0.5 * ((double)f[idx + ps] + (double)f[idx]); };
     sfv = amd_ratio(a.S[0][idx], a.S[1][idx], a.S[2][idx], av(a.S[3]), a.S[4][idx], av(a.S[5]), av(a.O[0]),
                     a.O[1][idx], av(a.O[2]), wx, wy, wz);
   }
@@ -851,7 +866,7 @@ __global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs a) {
     const double wy = m4 ? (a.dy[j] * 2.0) * (a.dy[j] * 2.0) : 1.0;
     const double wx = m4 ? a.wx : 1.0, wz = m4 ? a.wz : 1.0;
     const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
-    auto ip = [&](const double* f) { return (f[idx] * w1 + f[idx - ps] * w0) / den; };
+    auto ip = [&](const P* f) { return ((double)f[idx] * w1 + (double)f[idx - ps] * w0) / den; };
     sgv = amd_ratio(ip(a.S[0]), ip(a.S[1]), ip(a.S[2]), a.S[3][idx], ip(a.S[4]), a.S[5][idx], a.O[0][idx],
                     ip(a.O[1]), a.O[2][idx], wx, wy, wz);
   }
@@ -863,12 +878,13 @@ __global__ void k_amd_coef(const __grid_constant__ AmdCoefArgs a) {
 // fluxes s1_th dth/dx, s1_th dth/dz at GYF rows jstart_th..jend_th into fx, fz
 // (zero elsewhere) and kappa_t = -0.5 delta_y temp_th at GY rows 2..Nyp, zero
 // on planes 0, 1, 2, Nyp, Nyp+1 (ghost_les_th_mpi at one rank).
+template <typename P>
 struct AmdThArgs {
-  const double* G[9];
-  const double* T[3 * 8];
-  double* fx[8];
-  double* fz[8];
-  double* kap[8];
+  const P* G[9];
+  const P* T[3 * 8];
+  P* fx[8];
+  P* fz[8];
+  P* kap[8];
   const double* dy;
   const double* dyf;
   const double* hdy;      // -0.5 delta_y(j)
@@ -878,7 +894,8 @@ struct AmdThArgs {
   size_t ps;
 };
 
-__global__ void k_amd_th(const __grid_constant__ AmdThArgs a) {
+template <typename P>
+__global__ void k_amd_th(const __grid_constant__ AmdThArgs<P> a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -886,15 +903,15 @@ __global__ void k_amd_th(const __grid_constant__ AmdThArgs a) {
   const size_t ps = a.ps;
   const double dx2 = a.deltax * a.deltax, dz2 = a.deltaz * a.deltaz;
   for (int n = 0; n < a.nth; ++n) {
-    const double* tx = a.T[3 * n];
-    const double* ty = a.T[3 * n + 1];
-    const double* tz = a.T[3 * n + 2];
+    const P* tx = a.T[3 * n];
+    const P* ty = a.T[3 * n + 1];
+    const P* tz = a.T[3 * n + 2];
     double s1 = 0.0;
     if (j >= a.jst[n] && j <= a.jet[n]) {
       const double dly = a.dyf[j] * 2.0, dy2 = dly * dly;
       const double tyf = 0.5 * (ty[idx + ps] + ty[idx]);
       const double txj = tx[idx], tzj = tz[idx];
-      auto av = [&](const double* f) { return 0.5 * (f[idx + ps] + f[idx]); };
+      auto av = [&](const P* f) { return 0.5 * ((double)f[idx + ps] + (double)f[idx]); };
       const double num = -(dx2 * a.G[0][idx] * (txj * txj) + dy2 * a.G[1][idx] * (tyf * tyf) +
                            dz2 * a.G[2][idx] * (tzj * tzj) +
                            (dy2 * av(a.G[7]) + dx2 * av(a.G[3])) * txj * tyf +
@@ -914,7 +931,7 @@ __global__ void k_amd_th(const __grid_constant__ AmdThArgs a) {
     if (j >= 3 && j <= a.nyp - 1) {
       const double dly = a.dy[j] * 2.0, dy2 = dly * dly;
       const double w1 = a.dyf[j - 1], w0 = a.dyf[j], den = 2.0 * a.dy[j];
-      auto ip = [&](const double* f) { return (f[idx] * w1 + f[idx - ps] * w0) / den; };
+      auto ip = [&](const P* f) { return ((double)f[idx] * w1 + (double)f[idx - ps] * w0) / den; };
       const double txg = ip(tx), tzg = ip(tz), tyg = ty[idx];
       const double num = -(dx2 * ip(a.G[0]) * (txg * txg) + dy2 * ip(a.G[1]) * (tyg * tyg) +
                            dz2 * ip(a.G[2]) * (tzg * tzg) +
@@ -956,4 +973,10 @@ __global__ void k_amd_th_div(const __grid_constant__ AmdThDivArgs a) {
     if (j < a.jst[n] || j > a.jet[n]) continue;
     a.cfth[n][idx] = a.cfth[n][idx] - mul_ik(a.kx[m], h * a.fx[n][idx]) - mul_ik(a.kz[kq], h * a.fz[n][idx]);
   }
+}
+
+// FP32 -> FP64 copy (the mixed-precision eddy viscosity for the boundary)
+__global__ void k_widen(const float* in, double* out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)in[i];
 }
