@@ -400,6 +400,28 @@ def adjoint_bench(torch, nsteps=50, every=10):
             "note": "adjoint_run includes recomputing every segment from its checkpoint"}
 
 
+def stats_bench(ch, p, peak, reps=5):
+    """save_stats_chan on the workload state: the Parseval plane-reduction
+    kernel's device time (one read of every velocity and scalar) and the whole
+    call (wall values, kernel, partial sums to the host, O(Ny) finish)."""
+    import time
+    ch.stats()   # first call allocates the partial-sum buffer
+    ch.set_profiling(True)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ch.stats()
+    wall_ms = (time.perf_counter() - t0) / reps * 1e3
+    ms, n = ch.kernel_times().get("other", (0.0, 0))
+    ch.set_profiling(False)
+    nkx1, nk2 = p.nx // 3 + 1, 2 * (p.nz // 3) + 1
+    alg = (3 + p.n_th) * 16 * (p.ny + 2) * nkx1 * nk2
+    avg = ms / max(n, 1)
+    gbs = alg / (avg * 1e-3) / 1e9 if avg > 0 else None
+    return {"kernel": "k_stats_modes", "launches": n, "avg_ms": avg, "alg_bytes": alg,
+            "achieved_gbs": gbs, "frac_of_peak": gbs / peak if gbs else None,
+            "call_ms": wall_ms, "note": "plane statistics of the x-homogeneous save_stats_chan"}
+
+
 def e2e_round_trip(ch, torch, k):
     """End to end through the C ABI with pinned host buffers: each step
     uploads the state (u1, u2, u3, p, scalars) from the host in the reference
@@ -549,6 +571,7 @@ def run_ours(args):
     }
     if not args.no_e2e:
         out["e2e"] = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)))
+    out["stats"] = stats_bench(chm, p, peak)
     chm.close()
     chd.close()
     if world == 1 and not args.no_les:

@@ -28,6 +28,14 @@ ERR_NOMEM = -8
 U1, U2, U3, P, TH = 0, 1, 2, 3, 4
 LAYOUT_FOURIER, LAYOUT_PHYSICAL = 0, 1
 
+# diablo_stats output: profile names in the order of the DIABLO_STAT_* enums
+STAT_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw", "wv",
+                 "uu_dudx", "vv_dvdy", "wu_dwdx", "vu_dvdx", "uv_dudy", "wv_dwdy",
+                 "dudy", "dwdy", "cp", "shear", "omega_x", "omega_y", "omega_z",
+                 "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
+STAT_TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
+STAT_SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b")
+
 # every symbol include/diablo_gpu.h declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
@@ -55,6 +63,8 @@ SIGNATURES = {
     "diablo_pre_first_step": (_i, [_vp, _i]),
     "diablo_apply_bc_post": (_i, [_vp]),
     "diablo_filter_chan": (_i, [_vp, _i]),
+    "diablo_stats_size": (_i, [_vp]),
+    "diablo_stats": (_i, [_vp, _i, ctypes.POINTER(_d), _i]),
     "diablo_set_precision": (_i, [_vp, _i]),
     "diablo_get_time": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_d)]),
     "diablo_set_time": (_i, [_vp, _d, _i, _d]),

@@ -39,6 +39,23 @@ def _ptr(a):
     raise TypeError(f"unsupported array type {type(a)!r}")
 
 
+# mean.h5 dataset each statistic is written to (for/statistics.f90:176-273,
+# 490-520, 702, 1066, 1268, 2116; for/les.f90:1074): the reference's y is
+# the wall-normal direction internally but its files label it z, so v and w
+# swap.  Scalar profiles take the scalar number (1-based, two digits).
+MEAN_H5_NAMES = {
+    "ume": "ume", "vme": "wme", "wme": "vme", "mke": "mke", "urms": "urms", "vrms": "wrms",
+    "wrms": "vrms", "uv": "uw", "uw": "uv", "wv": "wv", "uu_dudx": "uu_dudx",
+    "vv_dvdy": "ww_dwdz", "wu_dwdx": "vu_dvdx", "vu_dvdx": "wu_dwdx", "uv_dudy": "uw_dudz",
+    "wv_dwdy": "vw_dvdz", "dudy": "dudz", "dwdy": "dvdz", "cp": "cp", "shear": "shear",
+    "omega_x": "omega_x", "omega_y": "omega_z", "omega_z": "omega_y", "epsilon": "epsilon",
+    "epsilon_m": "epsilon_m", "nu_sgs": "nu_sgs", "eps_sgs2": "eps_sgs2",
+    "thme": "thme{:02d}", "dthdy": "dthdz{:02d}", "thrms": "thrms{:02d}", "thv": "thw{:02d}",
+    "thv_m": "thw{:02d}_m", "pe_diss": "pe_diss{:02d}", "spectrum": "FTx_uu",
+    "u1y_left_b": "u1z_x0", "time": "time",
+}
+
+
 class Channel:
     def __init__(self, params: ChannelParams, gy):
         self.params = params
@@ -121,6 +138,31 @@ class Channel:
             out = self.new_field()
         _lib.check(self.lib.diablo_download_nu_t(self.ctx, _ptr(out)), "download_nu_t")
         return out
+
+    def stats(self, homogeneous_x: bool = True) -> dict:
+        """Plane statistics of save_stats_chan (for/statistics.f90:44-712)
+        for the x-homogeneous case; applies the wall values to the state
+        first, as the reference does.  Returns ``{"profiles": {name: (Ny,)},
+        "th": [{name: (Ny,)} per scalar], "spectrum": (Nx/2,), "scalars":
+        {name: float}}`` with the reference's internal names (MEAN_H5_NAMES
+        gives the dataset each one is written to)."""
+        p = self.params
+        n = self.lib.diablo_stats_size(self.ctx)
+        if n < 0:
+            _lib.check(n, "stats_size")
+        out = np.zeros(n)
+        _lib.check(self.lib.diablo_stats(self.ctx, 1 if homogeneous_x else 0,
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n), "stats")
+        ny, npf, ntp = p.ny, len(_lib.STAT_PROFILES), len(_lib.STAT_TH_PROFILES)
+        prof = {k: out[q * ny:(q + 1) * ny].copy() for q, k in enumerate(_lib.STAT_PROFILES)}
+        th = []
+        for t in range(p.n_th):
+            b = (npf + t * ntp) * ny
+            th.append({k: out[b + r * ny:b + (r + 1) * ny].copy() for r, k in enumerate(_lib.STAT_TH_PROFILES)})
+        b = (npf + p.n_th * ntp) * ny
+        spec = out[b:b + p.nx // 2].copy()
+        sc = {k: float(v) for k, v in zip(_lib.STAT_SCALARS, out[b + p.nx // 2:])}
+        return {"profiles": prof, "th": th, "spectrum": spec, "scalars": sc}
 
     # -- reference surface ---------------------------------------------
     def fft_xz_to_fourier(self, v, vv):

@@ -19,6 +19,7 @@
 #include "kernels_les.cuh"
 #include "kernels_adjoint.cuh"
 #include "kernels_init.cuh"
+#include "kernels_stats.cuh"
 
 static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
 static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
@@ -94,6 +95,8 @@ struct diablo_ctx {
   double* cfl_phys[3];
   double* d_cfl;
   double* d_sigma;          // filter_chan transfer function [Nkx+1][2Nkz+1]
+  double* d_stats;          // plane-statistics partial sums (diablo_stats)
+  size_t stats_doubles;
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
   struct Les {
@@ -1823,6 +1826,230 @@ static int filter_scalars(diablo_ctx* ctx) {
 int diablo_filter_chan(diablo_ctx* ctx, int n) {
   if (!ctx || n < 0 || n >= ctx->nth) return DIABLO_ERR_ARG;
   return filter_chan(ctx, n);
+}
+
+// ---------------------------------------------------------------------------
+// Plane statistics (save_stats_chan, for/statistics.f90:44-712), homogeneous x
+
+int diablo_stats_size(diablo_ctx* ctx) {
+  if (!ctx) return DIABLO_ERR_ARG;
+  return ctx->ny * (DIABLO_STAT_NPROF + ctx->nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2 + DIABLO_STAT_NSCALAR;
+}
+
+int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
+  if (!ctx || !out) return DIABLO_ERR_ARG;
+  if (len < diablo_stats_size(ctx)) return DIABLO_ERR_ARG;
+  if (!homogeneous_x) return DIABLO_ERR_UNSUPPORTED;
+  const diablo_params& p = ctx->p;
+  int rc;
+  // apply_BC_vel_mpi_post / apply_BC_th_mpi_post on the state (:63-64)
+  if ((rc = bc_post(ctx, 1, 1))) return rc;
+  const int ny = ctx->ny, nyp2 = ctx->nyp2, nth = ctx->nth, nkx1 = ctx->nkx1;
+  const int nmodes = nkx1 * ctx->nk2;
+  const size_t pn = (size_t)ctx->nz * ctx->nx;
+  int dev = 0, nsm = 148;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  // about four blocks per SM over all planes
+  int nslice = (4 * nsm + nyp2 - 1) / nyp2;
+  nslice = std::max(1, std::min(nslice, (nmodes + STAT_THREADS - 1) / STAT_THREADS));
+  int lslice = (4 * nsm + nyp2 - 1) / nyp2;
+  lslice = std::max(1, std::min<int>(lslice, (int)((pn + STAT_THREADS - 1) / STAT_THREADS)));
+  const size_t n_part = (size_t)nyp2 * nslice * STAT_NQ, n_means = (size_t)nyp2 * (4 + nth);
+  const size_t n_spec = (size_t)nyp2 * nkx1, n_les = (size_t)nyp2 * lslice * 2;
+  const size_t total = n_part + n_means + n_spec + n_les;
+  if (ctx->stats_doubles < total) {
+    if ((rc = dev_alloc(ctx, (void**)&ctx->d_stats, total * sizeof(double)))) return rc;
+    ctx->stats_doubles = total;
+  }
+  double* d_part = ctx->d_stats;
+  double* d_means = d_part + n_part;
+  double* d_spec = d_means + n_means;
+  double* d_les = d_spec + n_spec;
+  CK(cudaMemsetAsync(ctx->d_stats, 0, total * sizeof(double), ctx->stream));
+  const double d0 = nth > 0 ? p.dthdx[0] : 0.0;
+  // (1/(Ro_inv/delta)) dTHdX(1), the thermal-wind shear; 0 without a background gradient
+  const double tws = d0 == 0.0 ? 0.0 : (1.0 / (ctx->ro_inv / p.delta)) * d0;
+  {
+    StatsArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int q = 0; q < 3; ++q) a.cu[q] = ctx->st[ctx->cur][q];
+    for (int n = 0; n < nth; ++n) {
+      a.cth[n] = ctx->st[ctx->cur][4 + n];
+      a.dthdx[n] = p.dthdx[n];
+      a.dthdz[n] = p.dthdz[n];
+    }
+    a.cp = ctx->st[ctx->cur][3];
+    a.kx = ctx->d_kx;
+    a.kz = ctx->d_kz;
+    a.dy = ctx->d_dy;
+    a.dyf = ctx->d_dyf;
+    a.gy = ctx->d_gy;
+    a.gyf = ctx->d_gyf;
+    a.tws = tws;
+    a.nth = nth;
+    a.nyp = ny;
+    a.nkx1 = nkx1;
+    a.nk2 = ctx->nk2;
+    a.kp = ctx->kp;
+    a.nslice = nslice;
+    a.ps = (size_t)nkx1 * ctx->kp;
+    a.part = d_part;
+    a.means = d_means;
+    a.spec = d_spec;
+    Prof pr(ctx, K_OTHER);
+    const dim3 grid(nslice, nyp2);
+    if (nth == 0) k_stats_modes<0><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
+    else if (nth == 1) k_stats_modes<1><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
+    else if (nth == 2) k_stats_modes<2><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
+    else if (nth <= 4) k_stats_modes<4><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
+    else k_stats_modes<DIABLO_MAX_TH><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
+  const bool les = p.use_les && ctx->les.ready;
+  if (les) {
+    // compute_TKE_diss_les needs physical u1, u2, u3 (all planes) and nu_t
+    diablo_ctx::Les& L = ctx->les;
+    const double2* four[3] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2]};
+    double* phys[3] = {L.r[0], L.r[1], L.r[2]};
+    if ((rc = ifft_batch(ctx, four, phys, 3))) return rc;
+    const double* nt = L.nu_t;
+    if (L.nu_t_fp32) {
+      if ((rc = ensure_bscratch(ctx))) return rc;
+      k_widen<<<grid1d(phys_elems(ctx)), 256, 0, ctx->stream>>>(reinterpret_cast<const float*>(L.nu_t),
+                                                               ctx->b_phys, phys_elems(ctx));
+      ctx->launches++;
+      nt = ctx->b_phys;
+    }
+    StatsLesArgs b;
+    memset(&b, 0, sizeof(b));
+    for (int q = 0; q < 3; ++q) b.u[q] = phys[q];
+    b.nu_t = nt;
+    b.dy = ctx->d_dy;
+    b.dyf = ctx->d_dyf;
+    b.nyp = ny;
+    b.nslice = lslice;
+    b.pn = pn;
+    b.part = d_les;
+    Prof pr(ctx, K_OTHER);
+    k_stats_les<<<dim3(lslice, nyp2), STAT_THREADS, 0, ctx->stream>>>(b);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
+  std::vector<double> h(total);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_stats, total * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+
+  // host finish, O(Ny)
+  const double* part = h.data();
+  const double* means = part + n_part;
+  const double* spec = means + n_means;
+  const double* lpart = spec + n_spec;
+  auto Q = [&](int j, int q) {
+    double s = 0.0;
+    for (int sl = 0; sl < nslice; ++sl) s += part[((size_t)j * nslice + sl) * STAT_NQ + q];
+    return s;
+  };
+  auto LQ = [&](int j, int q) {
+    double s = 0.0;
+    for (int sl = 0; sl < lslice; ++sl) s += lpart[((size_t)j * lslice + sl) * 2 + q];
+    return s;
+  };
+  const std::vector<double>&gy = ctx->h_gy, &gyf = ctx->h_gyf, &dy = ctx->h_dy, &dyf = ctx->h_dyf;
+  auto integrate_y = [&](const std::vector<double>& v) {   // integrate_y_var (:1974-1990)
+    double r = 0.0;
+    for (int j = 2; j <= ny; ++j) r = r + 0.5 * (v[j] + v[j - 1]) * dy[j];
+    return r / p.ly;
+  };
+  std::vector<double> ume(nyp2), vme(nyp2), wme(nyp2);
+  for (int j = 0; j < nyp2; ++j) {
+    ume[j] = means[(size_t)j * (4 + nth) + 0];
+    vme[j] = means[(size_t)j * (4 + nth) + 1];
+    wme[j] = means[(size_t)j * (4 + nth) + 2];
+  }
+  const double nn = (double)ctx->nx * ctx->nz;
+  for (int i = 0, ntot = diablo_stats_size(ctx); i < ntot; ++i) out[i] = 0.0;
+  auto set = [&](int q, int j, double v) { out[(size_t)q * ny + (j - 1)] = v; };
+  std::vector<double> uu(nyp2, 0.0), vv(nyp2, 0.0), ww(nyp2, 0.0);
+  for (int j = 1; j <= ny; ++j) {
+    uu[j] = Q(j, SQ_UU);
+    vv[j] = Q(j, SQ_VV);
+    ww[j] = Q(j, SQ_WW);
+    set(DIABLO_STAT_UME, j, ume[j]);
+    set(DIABLO_STAT_VME, j, vme[j]);
+    set(DIABLO_STAT_WME, j, wme[j]);
+    set(DIABLO_STAT_URMS, j, sqrt(uu[j]));
+    set(DIABLO_STAT_VRMS, j, sqrt(vv[j]));
+    set(DIABLO_STAT_WRMS, j, sqrt(ww[j]));
+    set(DIABLO_STAT_UW, j, Q(j, SQ_UW));
+    set(DIABLO_STAT_DUDY, j, (ume[j] - ume[j - 1]) / (gyf[j] - gyf[j - 1]));
+    set(DIABLO_STAT_DWDY, j, (wme[j] - wme[j - 1]) / (gyf[j] - gyf[j - 1]));
+    set(DIABLO_STAT_CP, j, means[(size_t)j * (4 + nth) + 3]);
+    set(DIABLO_STAT_SHEAR, j, Q(j, SQ_SHEAR));
+    set(DIABLO_STAT_OMEGA_X, j, sqrt(Q(j, SQ_OX)));
+    set(DIABLO_STAT_OMEGA_Y, j, sqrt(Q(j, SQ_OY)));
+    set(DIABLO_STAT_OMEGA_Z, j, sqrt(Q(j, SQ_OZ)));
+    if (les) set(DIABLO_STAT_NU_SGS, j, LQ(j, 0) / nn);
+    if (j < 2) continue;
+    // GY-grid rows (j >= 2)
+    const double uv = Q(j, SQ_UV), wv = Q(j, SQ_WV);
+    set(DIABLO_STAT_UV, j, uv);
+    set(DIABLO_STAT_WV, j, wv);
+    set(DIABLO_STAT_EPSILON, j, ctx->nu * Q(j, SQ_EPS));
+    if (les) set(DIABLO_STAT_EPS_SGS2, j, LQ(j, 1) / nn);
+    if (ctx->nz > 1) {   // production terms (:1475-1543); the dudx_m, dvdx_m, dwdx_m terms are 0
+      set(DIABLO_STAT_VV_DVDY, j, (vme[j + 1] - vme[j - 1]) / (gy[j + 1] - gy[j - 1]) * vv[j]);
+      set(DIABLO_STAT_UV_DUDY, j, (ume[j] - ume[j - 1]) / dy[j] * uv);
+      set(DIABLO_STAT_WV_DWDY, j, ((wme[j] - wme[j - 1]) / dy[j] + tws) * wv);
+    }
+    // MKE on GY (:133-150)
+    const double wa = wme[j] + tws * (gyf[j] - 0.5 * p.ly), wb = wme[j - 1] + tws * (gyf[j - 1] - 0.5 * p.ly);
+    set(DIABLO_STAT_MKE, j,
+        0.5 * ((dyf[j - 1] * ume[j] * ume[j] + dyf[j] * ume[j - 1] * ume[j - 1]) / (2.0 * dy[j]) +
+               (dyf[j - 1] * wa * wa + dyf[j] * wb * wb) / (2.0 * dy[j]) + vme[j] * vme[j]));
+  }
+  double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2;
+  sc[DIABLO_STAT_TIME] = ctx->time;
+  sc[DIABLO_STAT_DT] = ctx->delta_t;
+  sc[DIABLO_STAT_UBULK] = integrate_y(ume);
+  sc[DIABLO_STAT_URMS_B] = sqrt(integrate_y(uu));
+  sc[DIABLO_STAT_VRMS_B] = sqrt(integrate_y(vv));
+  sc[DIABLO_STAT_WRMS_B] = sqrt(integrate_y(ww));
+  for (int n = 0; n < nth; ++n) {
+    double* base = out + (size_t)ny * (DIABLO_STAT_NPROF + n * DIABLO_STAT_NTHPROF);
+    auto tset = [&](int r, int j, double v) { base[(size_t)r * ny + (j - 1)] = v; };
+    std::vector<double> thme(nyp2);
+    for (int j = 0; j < nyp2; ++j) thme[j] = means[(size_t)j * (4 + nth) + 4 + n];
+    for (int j = 1; j <= ny; ++j) {
+      const int q0 = STAT_NQV + STAT_NQT * n;
+      tset(DIABLO_STAT_THME, j, thme[j]);
+      tset(DIABLO_STAT_DTHDY, j, (thme[j] - thme[j - 1]) / (gyf[j] - gyf[j - 1]));
+      tset(DIABLO_STAT_THRMS, j, sqrt(Q(j, q0)));
+      tset(DIABLO_STAT_THV, j, Q(j, q0 + 1));
+      tset(DIABLO_STAT_PE_DISS, j, Q(j, q0 + 2));
+      // thv_m (:377-385), gx(i) = i Lx / Nx
+      double s = 0.0;
+      for (int i = 0; i < ctx->nx; ++i)
+        s = s + (thme[j] + p.dthdx[n] * ((i * p.lx) / ctx->nx - 0.5 * p.lx)) * (0.5 * (vme[j] + vme[j + 1]));
+      tset(DIABLO_STAT_THV_M, j, s / ctx->nx);
+    }
+  }
+  if (nth > 0) {   // u1z_x0 (:418-430)
+    std::vector<double> u1yl(nyp2, 0.0);
+    for (int j = 1; j <= ny; ++j) u1yl[j] = gyf[j] * Q(j, SQ_U1YL);
+    sc[DIABLO_STAT_U1Y_LEFT_B] = integrate_y(u1yl);
+  }
+  // FTx_uu (:650-675): kz = 0 row of u1, integrated over y
+  double* sp = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF);
+  for (int m = 0; m < nkx1 && m < ctx->nx / 2; ++m) {
+    double s = 0.0;
+    for (int j = 2; j <= ny; ++j)
+      s += 0.5 * (spec[(size_t)j * nkx1 + m] + spec[(size_t)(j - 1) * nkx1 + m]) * dy[j];
+    sp[m] = s / p.ly;
+  }
+  return 0;
 }
 
 int diablo_step(diablo_ctx* ctx, int nsteps) {

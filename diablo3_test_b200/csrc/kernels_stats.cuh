@@ -1,0 +1,229 @@
+// Plane statistics of save_stats_chan (for/statistics.f90:44-712) for the
+// x-homogeneous case, FP64.
+//
+// Every statistic the reference forms as a plane average of a product of two
+// (spectrally or finite-difference derived) fields is evaluated here from the
+// Fourier coefficients by Parseval's identity instead of transforming the
+// fields to physical space: for fields f, g with packed coefficients F, G on
+// modes kx <= Nkx, |kz| <= Nkz,
+//   (1/(Nx Nz)) sum_{i,k} f g = sum_{m, kq} w(m) Re(F conj G),  w(0) = 1, w(m>0) = 2.
+// The physical transform keeps only the Hermitian part of the kx = 0 column
+// (the C2R x-transform ignores the anti-Hermitian part), so kx = 0
+// coefficients are read as (F(kq) + conj F(-kq)) / 2.  A fluctuation about
+// the plane mean is the field with its (0,0) coefficient removed.
+//
+// One pass reads the state once (three planes of each velocity and scalar
+// per plane through L2) and writes per-block partial sums; the host adds the
+// partials in a fixed order, so the result is deterministic.
+#pragma once
+#include "common.cuh"
+
+constexpr int STAT_NQV = 12;   // velocity accumulators
+constexpr int STAT_NQT = 3;    // accumulators per scalar
+constexpr int STAT_NQ = STAT_NQV + STAT_NQT * DIABLO_MAX_TH;
+constexpr int STAT_THREADS = 256;
+
+// velocity accumulator slots
+enum {
+  SQ_UU = 0,   // <u1'^2>                          compute_TKE (:1296-1312)
+  SQ_VV,       // <u2'^2>
+  SQ_WW,       // <u3'^2>
+  SQ_UW,       // <u1' u3'>                        compute_TKE_Production (:1413-1423)
+  SQ_UV,       // <I(u1') u2'> on GY, j >= 2         (:1425-1447)
+  SQ_WV,       // <I(u3') u2'> on GY, j >= 2
+  SQ_SHEAR,    // <(du1/dy)^2 + (du3/dy)^2>, central (:159-171)
+  SQ_OX,       // <(omega_x - tws)^2>              compute_Vorticity (:1557-1573)
+  SQ_OY,       // <omega_y^2>                      (:1607-1620)
+  SQ_OZ,       // <omega_z^2>                      (:1654-1668)
+  SQ_EPS,      // sum of the nine gradient squares, j >= 2   compute_TKE_diss (:859-1062)
+  SQ_U1YL      // z-mean of u1 at x = 0 (before the gyf(j) factor) (:420-426)
+};
+
+struct StatsArgs {
+  const double2* cu[3];
+  const double2* cth[DIABLO_MAX_TH];
+  const double2* cp;
+  const double* kx;
+  const double* kz;
+  const double* dy;
+  const double* dyf;
+  const double* gy;
+  const double* gyf;
+  double dthdx[DIABLO_MAX_TH], dthdz[DIABLO_MAX_TH];
+  double tws;           // thermal-wind shear (1/(Ro_inv/delta)) dTHdX(1)
+  int nth, nyp, nkx1, nk2, kp, nslice;
+  size_t ps;
+  double* part;         // [Ny+2][nslice][STAT_NQ]
+  double* means;        // [Ny+2][4 + nth]: Re of the (0,0) coefficient of u1 u2 u3 p th_n
+  double* spec;         // [Ny+2][Nkx+1]: |u1(kx, kz = 0)|^2
+};
+
+HDI double nrm2(double2 a) { return a.x * a.x + a.y * a.y; }
+HDI double re_dot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
+
+// Sum `v[q]` (q < nq) over the block; thread 0 stores the totals to out[q].
+template <int NQ>
+__device__ inline void block_sum_store(double (&v)[NQ], int nq, double* out) {
+  __shared__ double red[NQ][STAT_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    if (q < nq) {
+      double s = v[q];
+      for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+      if (lane == 0) red[q][w] = s;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[q][k];
+    out[q] = s;
+  }
+}
+
+// NT: scalar capacity of the instance (nth <= NT), so the register file holds
+// only the accumulators in use
+template <int NT>
+__global__ void __launch_bounds__(STAT_THREADS) k_stats_modes(const __grid_constant__ StatsArgs a) {
+  constexpr int NQ = STAT_NQV + STAT_NQT * NT;
+  const int j = blockIdx.y;
+  const int nyp = a.nyp;
+  const int nmodes = a.nkx1 * a.nk2;
+  const size_t ps = a.ps;
+  const int nq = STAT_NQV + STAT_NQT * a.nth;
+  double acc[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+  const bool inner = j >= 1 && j <= nyp;
+  const double dyj = a.dy[j], dyfj = a.dyf[j];
+  const double dyfm = j >= 1 ? a.dyf[j - 1] : 0.0;
+  const double dgy = inner && j >= 2 ? a.gy[j + 1] - a.gy[j - 1] : 1.0;
+  const double dgyf = inner ? a.gyf[j + 1] - a.gyf[j - 1] : 1.0;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nmodes; idx += a.nslice * blockDim.x) {
+    const int m = idx / a.nk2, kq = idx - m * a.nk2;
+    const bool m0 = m == 0, is00 = m0 && kq == 0;
+    const int kqm = kq == 0 ? 0 : a.nk2 - kq;
+    const size_t col = (size_t)m * a.kp;
+    // Hermitian part of the kx = 0 column
+    auto ld = [&](const double2* f, int jj) -> double2 {
+      const size_t o = (size_t)jj * ps + col;
+      double2 v = f[o + kq];
+      if (m0) {
+        const double2 u = f[o + kqm];
+        v = make_double2(0.5 * (v.x + u.x), 0.5 * (v.y - u.y));
+      }
+      return v;
+    };
+    const double2 c1 = ld(a.cu[0], j);
+    if (kq == 0) a.spec[(size_t)j * a.nkx1 + m] = nrm2(c1);
+    if (is00) {
+      double* mo = a.means + (size_t)j * (4 + a.nth);
+      mo[0] = c1.x;
+      mo[1] = a.cu[1][(size_t)j * ps].x;
+      mo[2] = a.cu[2][(size_t)j * ps].x;
+      mo[3] = a.cp[(size_t)j * ps].x;
+      for (int n = 0; n < a.nth; ++n) mo[4 + n] = a.cth[n][(size_t)j * ps].x;
+    }
+    if (!inner) continue;
+    const double w = m0 ? 1.0 : 2.0;
+    const double kxm = a.kx[m], kzq = a.kz[kq];
+    const double k2 = kxm * kxm + kzq * kzq;
+    const double2 c1m = ld(a.cu[0], j - 1), c1p = ld(a.cu[0], j + 1);
+    const double2 c2m = ld(a.cu[1], j - 1), c2 = ld(a.cu[1], j), c2p = ld(a.cu[1], j + 1);
+    const double2 c3m = ld(a.cu[2], j - 1), c3 = ld(a.cu[2], j), c3p = ld(a.cu[2], j + 1);
+    const double2 z = make_double2(0.0, 0.0);
+    // fluctuations (the (0,0) coefficient removed)
+    const double2 h1 = is00 ? z : c1, h2 = is00 ? z : c2, h3 = is00 ? z : c3;
+    const double2 h1m = is00 ? z : c1m, h2m = is00 ? z : c2m, h3m = is00 ? z : c3m;
+    const double2 h2p = is00 ? z : c2p;
+    acc[SQ_UU] += w * nrm2(h1);
+    acc[SQ_VV] += w * nrm2(h2);
+    acc[SQ_WW] += w * nrm2(h3);
+    acc[SQ_UW] += w * re_dot(h1, h3);
+    {
+      const double2 d1 = (1.0 / (2.0 * dyfj)) * (c1p - c1m), d3 = (1.0 / (2.0 * dyfj)) * (c3p - c3m);
+      acc[SQ_SHEAR] += w * (nrm2(d1) + nrm2(d3));
+      double2 ox = mul_ik(kzq, 0.5 * (c2p + c2)) - (1.0 / (2.0 * dyfj)) * (c3p - c3m);
+      if (is00) ox.x -= a.tws;
+      acc[SQ_OX] += w * nrm2(ox);
+      acc[SQ_OY] += w * nrm2(mul_ik(kxm, c3) - mul_ik(kzq, c1));
+      acc[SQ_OZ] += w * nrm2(d1 - mul_ik(kxm, 0.5 * (c2p + c2)));
+    }
+    if (j >= 2) {
+      const double2 i1 = (1.0 / (2.0 * dyj)) * (dyfm * h1 + dyfj * h1m);
+      const double2 i3 = (1.0 / (2.0 * dyj)) * (dyfm * h3 + dyfj * h3m);
+      acc[SQ_UV] += w * re_dot(i1, h2);
+      acc[SQ_WV] += w * re_dot(i3, h2);
+      // du/dx, dw/dx, du/dz, dw/dz interpolated to GY; dv/dx, dv/dz at GY;
+      // du/dy, dv/dy, dw/dy of the fluctuations
+      double e = k2 * (dyfm * (nrm2(c1) + nrm2(c3)) + dyfj * (nrm2(c1m) + nrm2(c3m))) / (2.0 * dyj);
+      e += k2 * nrm2(c2);
+      e += (nrm2(h1 - h1m) + nrm2(h3 - h3m)) / (dyj * dyj);
+      e += nrm2(h2p - h2m) / (dgy * dgy);
+      acc[SQ_EPS] += w * e;
+    }
+    if (kq == 0) acc[SQ_U1YL] += m0 ? c1.x : 2.0 * c1.x;
+    // scalars: thrms (:275-286), thv (:331-343), pe_diss (:400-414)
+    const double2 v2 = is00 ? z : 0.5 * (c2 + c2p);
+#pragma unroll
+    for (int n = 0; n < NT; ++n) {
+      if (n < a.nth) {
+        const double2 ct = ld(a.cth[n], j);
+        const double2 ht = is00 ? z : ct;
+        acc[STAT_NQV + STAT_NQT * n + 0] += w * nrm2(ht);
+        acc[STAT_NQV + STAT_NQT * n + 1] += w * re_dot(ht, v2);
+        // the wall-normal gradient is that of scalar 1 for every n (:316)
+        const double2 r2 = (1.0 / dgyf) * (ld(a.cth[0], j + 1) - ld(a.cth[0], j - 1));
+        double2 r1 = mul_ik(kxm, ct), r3 = mul_ik(kzq, ct);
+        if (is00) { r1.x += a.dthdx[n]; r3.x += a.dthdz[n]; }
+        acc[STAT_NQV + STAT_NQT * n + 2] += w * (nrm2(r1) + nrm2(r2) + nrm2(r3));
+      }
+    }
+  }
+  block_sum_store<NQ>(acc, nq, a.part + ((size_t)j * a.nslice + blockIdx.x) * STAT_NQ);
+}
+
+// compute_TKE_diss_les (for/statistics.f90:2054-2120) and the plane mean of
+// nu_t (nu_t_mean, for/les.f90:927-937) from physical u1, u2, u3 and nu_t
+// ([j][k][i], Nz x Nx per plane).  Slot 0: sum of nu_t over plane j
+// (1 <= j <= Ny); slot 1: sum of the GY dissipation term `temp` (2 <= j <= Ny).
+struct StatsLesArgs {
+  const double* u[3];
+  const double* nu_t;
+  const double* dy;
+  const double* dyf;
+  int nyp, nslice;
+  size_t pn;            // Nz * Nx
+  double* part;         // [Ny+2][nslice][2]
+};
+
+__global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_constant__ StatsLesArgs a) {
+  const int j = blockIdx.y;
+  double acc[2] = {0.0, 0.0};
+  if (j >= 1 && j <= a.nyp) {
+    const size_t pn = a.pn;
+    const double* u1 = a.u[0];
+    const double* u2 = a.u[1];
+    const double* u3 = a.u[2];
+    const double* nt = a.nu_t;
+    // s1 at GYF row jj (1 <= jj <= Ny) and point i
+    auto s1 = [&](int jj, size_t i) -> double {
+      const size_t o = (size_t)jj * pn + i, op = o + pn, om = o - pn;
+      const double dyp = a.dy[jj + 1], dy0 = a.dy[jj], df = a.dyf[jj];
+      return u1[o] * ((nt[op] * (u1[op] - u1[o]) / dyp - nt[o] * (u1[o] - u1[om]) / dy0) / df) +
+             u3[o] * ((nt[op] * (u3[op] - u3[o]) / dyp - nt[o] * (u3[o] - u3[om]) / dy0) / df);
+    };
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += (size_t)a.nslice * blockDim.x) {
+      const size_t o = (size_t)j * pn + i, op = o + pn, om = o - pn;
+      acc[0] += nt[o];
+      if (j >= 2) {
+        const double t2 = u2[o] * ((0.5 * (nt[o] + nt[op]) * (u2[op] - u2[o]) / a.dyf[j] -
+                                    0.5 * (nt[o] + nt[om]) * (u2[o] - u2[om]) / a.dyf[j - 1]) /
+                                   a.dy[j]);
+        acc[1] += 0.5 * (s1(j, i) + s1(j - 1, i)) + t2;
+      }
+    }
+  }
+  block_sum_store<2>(acc, 2, a.part + ((size_t)j * a.nslice + blockIdx.x) * 2);
+}

@@ -144,6 +144,47 @@ int diablo_apply_bc_post(diablo_ctx* ctx);
  * the subroutine on its own. */
 int diablo_filter_chan(diablo_ctx* ctx, int n);
 
+/* Plane statistics: save_stats_chan (for/statistics.f90:44-712) with
+ * compute_averages, compute_TKE_diss, compute_MKE_diss, compute_TKE,
+ * compute_TKE_Production, compute_Vorticity and compute_TKE_diss_les, for the
+ * x-homogeneous case (homogeneousX, for/parameters.f90:275-280: IC types other
+ * than 5-8).  Applies the wall values (apply_BC_vel/th_mpi_post) to the state
+ * first, as the reference does.  The profiles are the values the reference
+ * writes to mean.h5 at j = 1..Ny (its internal names; mean.h5 swaps the v/w
+ * labels).  The plane averages are evaluated from the Fourier coefficients
+ * (Parseval), in FP64 in both precisions; the host-side finish is O(Ny).
+ * Not computed: HDF5/movie output, y* binning, compute_BPE, and the z-line
+ * averages of the non-homogeneous branch (homogeneous_x = 0 returns
+ * DIABLO_ERR_UNSUPPORTED).  nu_sgs is the plane mean of the nu_t of the most
+ * recent LES substep and eps_sgs2 uses that nu_t, as compute_TKE_diss_les
+ * does; both are 0 without LES.
+ * Layout of `out` (diablo_stats_size doubles):
+ *   profile q of the velocity set at out[q*Ny + j-1], q < DIABLO_STAT_NPROF;
+ *   then, for scalar n, profile r at out[(NPROF + n*NTHPROF + r)*Ny + j-1];
+ *   then the y-averaged kz = 0 spectrum of u1 (FTx_uu), Nx/2 values;
+ *   then DIABLO_STAT_NSCALAR scalars. */
+enum {
+  DIABLO_STAT_UME = 0, DIABLO_STAT_VME, DIABLO_STAT_WME, DIABLO_STAT_MKE,
+  DIABLO_STAT_URMS, DIABLO_STAT_VRMS, DIABLO_STAT_WRMS,
+  DIABLO_STAT_UV, DIABLO_STAT_UW, DIABLO_STAT_WV,
+  DIABLO_STAT_UU_DUDX, DIABLO_STAT_VV_DVDY, DIABLO_STAT_WU_DWDX,
+  DIABLO_STAT_VU_DVDX, DIABLO_STAT_UV_DUDY, DIABLO_STAT_WV_DWDY,
+  DIABLO_STAT_DUDY, DIABLO_STAT_DWDY, DIABLO_STAT_CP, DIABLO_STAT_SHEAR,
+  DIABLO_STAT_OMEGA_X, DIABLO_STAT_OMEGA_Y, DIABLO_STAT_OMEGA_Z,
+  DIABLO_STAT_EPSILON, DIABLO_STAT_EPSILON_M, DIABLO_STAT_NU_SGS, DIABLO_STAT_EPS_SGS2,
+  DIABLO_STAT_NPROF
+};
+enum {
+  DIABLO_STAT_THME = 0, DIABLO_STAT_DTHDY, DIABLO_STAT_THRMS, DIABLO_STAT_THV,
+  DIABLO_STAT_THV_M, DIABLO_STAT_PE_DISS, DIABLO_STAT_NTHPROF
+};
+enum {
+  DIABLO_STAT_TIME = 0, DIABLO_STAT_DT, DIABLO_STAT_UBULK, DIABLO_STAT_URMS_B,
+  DIABLO_STAT_VRMS_B, DIABLO_STAT_WRMS_B, DIABLO_STAT_U1Y_LEFT_B, DIABLO_STAT_NSCALAR
+};
+int diablo_stats_size(diablo_ctx* ctx);
+int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len);
+
 int diablo_set_precision(diablo_ctx* ctx, int precision);
 int diablo_get_time(diablo_ctx* ctx, double* time, int* time_step, double* delta_t);
 int diablo_set_time(diablo_ctx* ctx, double time, int time_step, double delta_t);

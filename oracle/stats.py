@@ -1,0 +1,263 @@
+"""numpy restatement of the reference's plane statistics (test infrastructure
+only): ``save_stats_chan`` (for/statistics.f90:44-712) with the routines it
+calls -- compute_averages (:713-838), compute_TKE_diss (:839-1129),
+compute_MKE_diss (:1130-1284), compute_TKE (:1285-1393),
+compute_TKE_Production (:1394-1549), compute_Vorticity (:1550-1754),
+integrate_y_var (:1974-1990) and compute_TKE_diss_les (:2054-2120) -- for the
+x-homogeneous case (``homogeneousX``, for/parameters.f90:275-280: every IC type
+but 5-8), one y-rank and one z-rank.
+
+Like the reference, every plane average is formed in PHYSICAL space: the
+fields (and the spectral gradients the reference builds) are transformed with
+``fft_xz_to_physical`` and summed over the Nx x Nz grid points.  The CUDA
+library evaluates the same averages from the Fourier coefficients (Parseval),
+so the two agree to round-off, not bit for bit.
+
+Not restated: HDF5/movie output, the y* binning (Bin_Ystar_and_Write),
+compute_BPE, and the z-line (x-dependent) averages of the non-homogeneous
+branch.  The oracle is the checker of the CUDA library, never the product.
+
+Quirks kept from the reference:
+  * pe_diss uses the wall-normal gradient of scalar 1 for every scalar
+    (``crth(i, k, j +- 1, 1)``, :316).
+  * In the homogeneous branch compute_MKE_diss returns before it fills
+    dudx_m, dvdx_m, dwdx_m (:1147-1149), so uu_dudx, wu_dwdx and vu_dvdx are 0
+    (the arrays are zero-initialised module storage) and epsilon_m is 0.
+  * GY-grid profiles (uv, wv, epsilon, mke, the production terms) are 0 at
+    j = 1, the first row their loops leave untouched.
+  * compute_TKE_diss_les sums the work array ``temp`` over j = 1 too, whose
+    row 1 it never writes; that row is reported as 0.
+
+The thermal-wind shift ``(1/(Ro_inv/delta)) dTHdX(1)`` (:172, :1244, :1539,
+:1587) is taken as 0 when dTHdX(1) = 0: the reference evaluates Inf * 0 = NaN
+there when Ro_inv = 0 and reads past dTHdX when N_th = 0.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .channel import Field, OracleChannel
+
+VEL_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw", "wv",
+                "uu_dudx", "vv_dvdy", "wu_dwdx", "vu_dvdx", "uv_dudy", "wv_dwdy",
+                "dudy", "dwdy", "cp", "shear", "omega_x", "omega_y", "omega_z",
+                "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
+TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
+SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b")
+
+
+def thermal_wind_shear(p) -> float:
+    """(1/(Ro_inv/delta)) * dTHdX(1) in IEEE arithmetic (a signed infinity
+    when Ro_inv = 0), taken as 0 when dTHdX(1) = 0."""
+    d = float(p.dthdx[0]) if p.n_th > 0 else 0.0
+    if d == 0.0:
+        return 0.0
+    q = p.ro_inv / p.delta
+    if q == 0.0:
+        return math.copysign(math.inf, q) * d
+    return (1.0 / q) * d
+
+
+def integrate_y_var(o: OracleChannel, var) -> float:
+    """for/statistics.f90:1974-1990 (one y-rank): trapezoid over GY, / Ly."""
+    res = 0.0
+    for j in range(2, o.Nyp + 1):
+        res = res + 0.5 * (var[j] + var[j - 1]) * o.dy[j]
+    return res / o.p.ly
+
+
+def _phys(o: OracleChannel, c):
+    """fft_xz_to_physical of a complex array laid out like Field.c; returns
+    the physical values [j, k, i] on the Nz x Nx grid."""
+    f = Field(o.Ny, o.Nz, o.Nx)
+    f.c[:] = c
+    o.fft_xz_to_physical(f)
+    return f.r[:, :o.Nz, :o.Nx].copy()
+
+
+def save_stats_chan(o: OracleChannel, nu_t=None) -> dict:
+    """Statistics of the oracle's current (Fourier) state.  Applies the
+    velocity and scalar wall values first, as the reference does (:63-64),
+    which changes the oracle's state the same way.  ``nu_t`` (reference
+    physical layout) enables the LES rows nu_sgs and eps_sgs2."""
+    p = o.p
+    Nx, Nz, Nyp, Nxp, tk = o.Nx, o.Nz, o.Nyp, o.Nxp, o.twoNkz
+    gy, gyf, dy, dyf = o.gy, o.gyf, o.dy, o.dyf
+    NN = float(Nx * Nz)
+    ny2 = Nyp + 2
+    K, I = slice(0, tk + 1), slice(0, Nxp)
+    tws = thermal_wind_shear(p)
+    o.apply_bc_vel_post()
+    o.apply_bc_th_post()
+    cr1, cr2, cr3 = o.u1.c.copy(), o.u2.c.copy(), o.u3.c.copy()
+    crth = [t.c.copy() for t in o.th]
+    u1, u2, u3 = _phys(o, cr1), _phys(o, cr2), _phys(o, cr3)
+    th = [_phys(o, c) for c in crth]
+    cikx = o.cikx[None, None, :Nxp]
+    cikz = o.cikz[None, :tk + 1, None]
+    out = {k: np.zeros(ny2) for k in VEL_PROFILES}
+
+    # compute_averages (:733-746, :811-836)
+    ume, vme, wme = cr1[:, 0, 0].real.copy(), cr2[:, 0, 0].real.copy(), cr3[:, 0, 0].real.copy()
+    thme = [c[:, 0, 0].real.copy() for c in crth]
+    out["ume"][:], out["vme"][:], out["wme"][:] = ume, vme, wme
+    ubulk = integrate_y_var(o, ume)
+
+    def zero_cs():
+        return np.zeros_like(cr1)
+
+    # compute_TKE_diss (:859-1062), k_start = 0
+    eps = np.zeros(ny2)
+
+    def interp_sq(s, j):   # (dyf(j-1) s(j)^2 + dyf(j) s(j-1)^2) / (2 dy(j)), summed
+        return np.sum((dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j]))
+
+    for cr, kfac in ((cr1, cikx), (cr3, cikx), (cr1, cikz), (cr3, cikz)):   # du/dx dw/dx du/dz dw/dz
+        cs = zero_cs()
+        cs[1:Nyp + 1, K, I] = kfac * cr[1:Nyp + 1, K, I]
+        s = _phys(o, cs)
+        for j in range(2, Nyp + 1):
+            eps[j] += interp_sq(s, j)
+    for kfac in (cikx, cikz):                                               # dv/dx dv/dz
+        cs = zero_cs()
+        cs[2:Nyp + 1, K, I] = kfac * cr2[2:Nyp + 1, K, I]
+        s = _phys(o, cs)
+        for j in range(2, Nyp + 1):
+            eps[j] += np.sum(s[j] ** 2)
+    for j in range(2, Nyp + 1):
+        su = ((u1[j] - ume[j]) - (u1[j - 1] - ume[j - 1])) / dy[j]           # du/dy
+        sv = ((u2[j + 1] - vme[j + 1]) - (u2[j - 1] - vme[j - 1])) / (gy[j + 1] - gy[j - 1])
+        sw = ((u3[j] - wme[j]) - (u3[j - 1] - wme[j - 1])) / dy[j]           # dw/dy
+        eps[j] += np.sum(su ** 2) + np.sum(sv ** 2) + np.sum(sw ** 2)
+    out["epsilon"][:] = o.nu * eps / NN
+    # compute_MKE_diss returns early in the homogeneous branch: epsilon_m = 0
+
+    # compute_TKE_diss_les (:2054-2120)
+    if nu_t is not None:
+        nt = nu_t[:, :Nz, :Nx]
+        s1 = np.zeros_like(u1)
+        for j in range(1, Nyp + 1):
+            s1[j] = (u1[j] * ((nt[j + 1] * (u1[j + 1] - u1[j]) / dy[j + 1]
+                               - nt[j] * (u1[j] - u1[j - 1]) / dy[j]) / dyf[j])
+                     + u3[j] * ((nt[j + 1] * (u3[j + 1] - u3[j]) / dy[j + 1]
+                                 - nt[j] * (u3[j] - u3[j - 1]) / dy[j]) / dyf[j]))
+        for j in range(2, Nyp + 1):
+            temp = (0.5 * (s1[j] + s1[j - 1])
+                    + u2[j] * ((0.5 * (nt[j] + nt[j + 1]) * (u2[j + 1] - u2[j]) / dyf[j]
+                                - 0.5 * (nt[j] + nt[j - 1]) * (u2[j] - u2[j - 1]) / dyf[j - 1]) / dy[j]))
+            out["eps_sgs2"][j] = np.sum(temp) / NN
+        # nu_sgs: the plane mean of nu_t (nu_t_mean, for/les.f90:927-937)
+        for j in range(1, Nyp + 1):
+            out["nu_sgs"][j] = np.sum(nt[j]) / NN
+
+    # compute_TKE (:1290-1331)
+    for name, u, me in (("urms", u1, ume), ("vrms", u2, vme), ("wrms", u3, wme)):
+        for j in range(1, Nyp + 1):
+            out[name][j] = np.sum((u[j] - me[j]) ** 2) / NN
+    urms_b = np.sqrt(integrate_y_var(o, out["urms"]))
+    vrms_b = np.sqrt(integrate_y_var(o, out["vrms"]))
+    wrms_b = np.sqrt(integrate_y_var(o, out["wrms"]))
+    vv = out["vrms"].copy()   # vv_xy summed over x / Nx: the plane mean of (u2 - vme)^2
+    for name in ("urms", "vrms", "wrms"):
+        out[name][1:Nyp + 1] = np.sqrt(out[name][1:Nyp + 1])
+
+    # compute_TKE_Production (:1408-1545)
+    for j in range(1, Nyp + 1):
+        out["uw"][j] = np.sum((u1[j] - ume[j]) * (u3[j] - wme[j])) / NN
+    for j in range(2, Nyp + 1):
+        fu = (dyf[j - 1] * (u1[j] - ume[j]) + dyf[j] * (u1[j - 1] - ume[j - 1])) / (2.0 * dy[j])
+        fw = (dyf[j - 1] * (u3[j] - wme[j]) + dyf[j] * (u3[j - 1] - wme[j - 1])) / (2.0 * dy[j])
+        out["uv"][j] = np.sum(fu * (u2[j] - vme[j])) / NN
+        out["wv"][j] = np.sum(fw * (u2[j] - vme[j])) / NN
+    if Nz > 1:
+        for j in range(2, Nyp + 1):
+            out["vv_dvdy"][j] = (vme[j + 1] - vme[j - 1]) / (gy[j + 1] - gy[j - 1]) * vv[j]
+            out["uv_dudy"][j] = (ume[j] - ume[j - 1]) / dy[j] * out["uv"][j]
+            out["wv_dwdy"][j] = ((wme[j] - wme[j - 1]) / dy[j] + tws) * out["wv"][j]
+
+    # MKE on GY (:133-150)
+    for j in range(2, Nyp + 1):
+        out["mke"][j] = 0.5 * ((dyf[j - 1] * ume[j] ** 2 + dyf[j] * ume[j - 1] ** 2) / (2.0 * dy[j])
+                               + (dyf[j - 1] * (wme[j] + tws * (gyf[j] - 0.5 * p.ly)) ** 2
+                                  + dyf[j] * (wme[j - 1] + tws * (gyf[j - 1] - 0.5 * p.ly)) ** 2)
+                               / (2.0 * dy[j])
+                               + vme[j] ** 2)
+    # gradients of the mean (:153-156) and mean-square shear (:159-171)
+    for j in range(1, Nyp + 1):
+        out["dudy"][j] = (ume[j] - ume[j - 1]) / (gyf[j] - gyf[j - 1])
+        out["dwdy"][j] = (wme[j] - wme[j - 1]) / (gyf[j] - gyf[j - 1])
+        out["shear"][j] = np.sum(((u1[j + 1] - u1[j - 1]) / (2.0 * dyf[j])) ** 2
+                                 + ((u3[j + 1] - u3[j - 1]) / (2.0 * dyf[j])) ** 2) / NN
+    out["cp"][:] = o.p_.c[:, 0, 0].real
+
+    # compute_Vorticity (:1555-1752)
+    J = slice(1, Nyp + 1)
+    Jp, Jm = slice(2, Nyp + 2), slice(0, Nyp)
+    cs = zero_cs()
+    cs[J, K, I] = (cikz * 0.5 * (cr2[Jp, K, I] + cr2[J, K, I])
+                   - (cr3[Jp, K, I] - cr3[Jm, K, I]) / (2.0 * dyf[J, None, None]))
+    s = _phys(o, cs) - tws
+    for j in range(1, Nyp + 1):
+        out["omega_x"][j] = np.sqrt(np.sum(s[j] ** 2) / NN)
+    cs = zero_cs()
+    cs[J, K, I] = cikx * cr3[J, K, I] - cikz * cr1[J, K, I]
+    s = _phys(o, cs)
+    for j in range(1, Nyp + 1):
+        out["omega_y"][j] = np.sqrt(np.sum(s[j] ** 2) / NN)
+    cs = zero_cs()
+    cs[J, K, I] = ((cr1[Jp, K, I] - cr1[Jm, K, I]) / (2.0 * dyf[J, None, None])
+                   - cikx * 0.5 * (cr2[Jp, K, I] + cr2[J, K, I]))
+    s = _phys(o, cs)
+    for j in range(1, Nyp + 1):
+        out["omega_z"][j] = np.sqrt(np.sum(s[j] ** 2) / NN)
+
+    # scalars (:248-468)
+    gx = np.array([(i * p.lx) / Nx for i in range(Nx)])
+    ths = []
+    u1y_left_b = 0.0
+    for n in range(o.Nth):
+        prof = {k: np.zeros(ny2) for k in TH_PROFILES}
+        c1 = zero_cs()
+        c1[J, K, I] = cikx * crth[n][J, K, I]
+        c2 = zero_cs()
+        c2[J, K, I] = ((crth[0][Jp, K, I] - crth[0][Jm, K, I])
+                       / (gyf[2:Nyp + 2] - gyf[0:Nyp])[:, None, None])
+        c3 = zero_cs()
+        c3[J, K, I] = cikz * crth[n][J, K, I]
+        r1, r2, r3 = _phys(o, c1), _phys(o, c2), _phys(o, c3)
+        t, tm = th[n], thme[n]
+        for j in range(1, Nyp + 1):
+            prof["thrms"][j] = np.sqrt(np.sum((t[j] - tm[j]) ** 2) / NN)
+            prof["thv"][j] = np.sum((t[j] - tm[j]) * (0.5 * (u2[j] + u2[j + 1])
+                                                      - 0.5 * (vme[j] + vme[j + 1]))) / NN
+            prof["thv_m"][j] = np.sum((tm[j] + p.dthdx[n] * (gx - 0.5 * p.lx))
+                                      * (0.5 * (vme[j] + vme[j + 1]))) / float(Nx)
+            prof["dthdy"][j] = (tm[j] - tm[j - 1]) / (gyf[j] - gyf[j - 1])
+            prof["pe_diss"][j] = np.sum((r1[j] + p.dthdx[n]) ** 2 + r2[j] ** 2
+                                        + (r3[j] + p.dthdz[n]) ** 2) / NN
+        prof["thme"][:] = tm
+        if n == 0:
+            u1y_left = np.zeros(ny2)
+            for j in range(1, Nyp + 1):
+                u1y_left[j] = np.sum(gyf[j] * u1[j, :, 0]) / float(Nz)
+            u1y_left_b = integrate_y_var(o, u1y_left)
+        ths.append(prof)
+
+    # y-averaged spectrum of u1 on the kz = 0 row, after the physical round
+    # trip the reference makes (:650-675)
+    f = Field(o.Ny, Nz, Nx)
+    f.r[:, :Nz, :Nx] = u1
+    o.fft_xz_to_fourier(f)
+    cuu = np.abs(f.c[:, 0, :Nxp]) ** 2
+    spec = np.zeros(Nxp)
+    for j in range(2, Nyp + 1):
+        spec += 0.5 * (cuu[j] + cuu[j - 1]) * dy[j]
+    spec /= p.ly
+
+    scal = dict(time=o.time, dt=o.delta_t, ubulk=ubulk, urms_b=urms_b, vrms_b=vrms_b,
+                wrms_b=wrms_b, u1y_left_b=u1y_left_b)
+    return {"profiles": {k: v[1:Nyp + 1].copy() for k, v in out.items()},
+            "th": [{k: v[1:Nyp + 1].copy() for k, v in d.items()} for d in ths],
+            "spectrum": spec, "scalars": scal}
