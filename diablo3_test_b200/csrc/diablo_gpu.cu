@@ -195,7 +195,7 @@ static void launch_solve_t(const SolveArgs& a, bool project_only, cudaStream_t s
 }
 template <int R>
 static void launch_tiles_t(const Solve2Args& A, cudaStream_t s) {
-  const int smem = ((1 + T2_STAGES) * A.s.n * T2_PITCH + T2_COLS * 32 * R) * (int)sizeof(double2) +
+  const int smem = (T2_STAGES * A.s.n * T2_PITCH + T2_COLS * 32 * (R | 1)) * (int)sizeof(double2) +
                    (A.mean_split ? 2 * A.s.n * (int)sizeof(double) : 0);
   cudaFuncSetAttribute(k_column_tiles<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   const int ngroups = (A.s.nk2 + T2_COLS - 1) / T2_COLS;
@@ -1415,14 +1415,14 @@ static int substep(diablo_ctx* ctx, int rk) {
     add(OP_NL, (comp == 0 && mean_split) ? 0 : f32, 0, ctx->nl[comp], a.store_cf ? a.cf_out[comp] : nullptr,
         nullptr);
     if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[comp], nullptr, nullptr);
-    add(OP_SOLVE, comp, 0, nullptr, a.cu_out[comp], a.cu_in[comp]);
+    add(OP_SOLVE, comp, 0, a.cp_in, a.cu_out[comp], a.cu_in[comp]);   // tile: the pressure
   }
   add(OP_OWN_U2, 1, 0, a.cu_in[1], nullptr, nullptr);
   if (p.grav_y != 0.0)
     for (int n = 0; n < ctx->nth; ++n) add(OP_BUOY, 0, p.grav_y, a.cth_in[n], nullptr, nullptr);
   add(OP_NL, f32, 0, ctx->nl[1], a.store_cf ? a.cf_out[1] : nullptr, nullptr);
   if (rk > 1) add(OP_CFOLD, 0, 0, a.cf_in[1], nullptr, nullptr);
-  add(OP_SOLVE, 1, 0, nullptr, a.cu_out[1], a.cu_in[1]);
+  add(OP_SOLVE, 1, 0, a.cp_in, a.cu_out[1], a.cu_in[1]);
   for (int n = 0; n < ctx->nth; ++n) {
     add(OP_OWN_TH, n, 0, a.cth_in[n], nullptr, nullptr);
     if (p.dthdx[n] != 0.0) add(OP_ADD_CF, 0, -p.dthdx[n], a.cu_in[0], nullptr, nullptr);
@@ -1437,7 +1437,7 @@ static int substep(diablo_ctx* ctx, int rk) {
   add(OP_PROJ, 0, 0, a.cu_out[0], a.cu_out[0], cfl ? ctx->ustar[0] : nullptr);
   add(OP_PROJ, 2, 0, a.cu_out[2], a.cu_out[2], cfl ? ctx->ustar[2] : nullptr);
   add(OP_PROJ, 1, 0, a.cu_out[1], a.cu_out[1], cfl ? ctx->ustar[1] : nullptr);
-  add(OP_CP, 0, 0, nullptr, a.cp_out, nullptr);
+  add(OP_CP, 0, 0, a.cp_in, a.cp_out, nullptr);
   {
     Prof pr(ctx, K_SOLVE);
     // thermal-wind forcing (flavor 'Front') keeps the general kernel

@@ -6,17 +6,19 @@
 // rem_div_chan :946-1023), one warp per (kx, kz) column.  The difference is
 // the data path: a block owns 4 adjacent kz columns of one kx, and every
 // field it needs moves through shared memory as an (Ny+2) x 4 tile copied with
-// cp.async (16-byte pieces, 64-byte rows), double buffered so the next tile is
-// in flight while the current one is consumed.  Lanes then read their own
-// rows (and y-neighbours) from shared memory.  The host builds the list of
-// tiles (`steps`) once per substep; terms whose coefficient is zero are not
-// loaded at all.
+// cp.async (16-byte pieces, 64-byte rows) through a three-stage ring, so two
+// tiles are in flight while one is consumed.  Lanes then read their own rows
+// (and y-neighbours) from shared memory.  The host builds the list of tiles
+// (`steps`) once per substep; terms whose coefficient is zero are not loaded
+// at all.  The pressure arrives as the tile of each velocity solve and of the
+// pressure update rather than staying resident: at Ny = 257 that keeps a
+// block at 71 KB of shared memory, three blocks per SM instead of two.
 #pragma once
 #include "common.cuh"
 #include "kernels_solve.cuh"
 
 #define T2_COLS 4
-#define T2_PITCH 5      // complex elements per tile row (4 + 1 pad)
+#define T2_PITCH 4      // complex elements per tile row (unpadded; see tix)
 #define T2_MAXSTEPS 96
 
 enum TileOp {
@@ -69,6 +71,12 @@ struct Solve2Args {
 
 namespace csolve2 {
 
+// Shared-memory slot of tile element (row j, column c).  Lanes of a warp own
+// rows R apart; a 16-byte slot index 4j + c would put them in only two of the
+// eight 16-byte bank groups of a 128-byte wavefront.  XOR-ing the column with
+// bits 1-2 of the row spreads any 8 consecutive rows over all eight.
+DI int tix(int j, int c) { return j * T2_PITCH + (c ^ ((j >> 1) & 3)); }
+
 DI void cp_async16(void* smem, const void* gmem) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
@@ -88,12 +96,12 @@ DI void load_tile(void* tile, const void* g, bool fp32, size_t ps, size_t cbase,
       const int j = idx >> 2, c = idx & 3;
       if (c < nvalid) {
         if (fp32)
-          cp_async8((float2*)tile + j * T2_PITCH + c, (const float2*)g + j * ps + cbase + c);
+          cp_async8((float2*)tile + tix(j, c), (const float2*)g + j * ps + cbase + c);
         else
-          cp_async16((double2*)tile + j * T2_PITCH + c, (const double2*)g + j * ps + cbase + c);
+          cp_async16((double2*)tile + tix(j, c), (const double2*)g + j * ps + cbase + c);
       } else {
-        if (fp32) ((float2*)tile)[j * T2_PITCH + c] = make_float2(0.f, 0.f);
-        else ((double2*)tile)[j * T2_PITCH + c] = make_double2(0.0, 0.0);
+        if (fp32) ((float2*)tile)[tix(j, c)] = make_float2(0.f, 0.f);
+        else ((double2*)tile)[tix(j, c)] = make_double2(0.0, 0.0);
       }
     }
   }
@@ -346,17 +354,19 @@ __global__ void __launch_bounds__(32) k_factor(const __grid_constant__ SolveArgs
 #define T2_STAGES 3
 
 template <int R>
-__global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ Solve2Args A) {
+__global__ void __launch_bounds__(128, 3) k_column_tiles(const __grid_constant__ Solve2Args A) {
   using namespace csolve;
   using namespace csolve2;
   const SolveArgs& a = A.s;
   extern __shared__ __align__(16) unsigned char t2_smem[];
   const int n = a.n, nyp = a.nyp;
   const int tsz = n * T2_PITCH;
-  double2* Tcp = reinterpret_cast<double2*>(t2_smem);
-  double2* Tbase = Tcp + tsz;                         // T2_STAGES streamed tiles
+  double2* Tbase = reinterpret_cast<double2*>(t2_smem);   // T2_STAGES streamed tiles
   double2* dvs = Tbase + T2_STAGES * tsz;             // lane-private divergence rows
-  double* Um = reinterpret_cast<double*>(dvs + T2_COLS * 32 * R);   // U1, I(U1) (mean_split)
+  // a lane's rows sit (R | 1) slots apart: an odd 16-byte stride keeps the 32
+  // lanes on distinct bank groups for any R
+  constexpr int RP = R | 1;
+  double* Um = reinterpret_cast<double*>(dvs + T2_COLS * 32 * RP);   // U1, I(U1) (mean_split)
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, c = tid >> 5;
   const int ngroups = (a.nk2 + T2_COLS - 1) / T2_COLS;
@@ -375,7 +385,7 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
   const int j0 = lane * R;
   const double v00 = m00 ? 1.0 : 0.0;
   const double* met = A.met;
-  double2* dv = dvs + c * (32 * R) + j0;              // this lane's R rows
+  double2* dv = dvs + c * (32 * RP) + lane * RP;      // this lane's R rows
 
   double2 cr[R], cf[R];
 #pragma unroll
@@ -385,7 +395,6 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
 
   if (A.mean_split)
     for (int j = tid; j < 2 * n; j += nthr) Um[j] = A.prof[j];
-  load_tile(Tcp, a.cp_in, false, ps, cbase, nvalid, n, tid, nthr);
   for (int q = 0; q < T2_STAGES - 1; ++q) {
     const TileStep* st = q < A.nstep ? &A.steps[q] : nullptr;
     load_tile(Tbase + q * tsz, st ? st->src : nullptr, st && st->op == OP_NL && st->arg, ps, cbase,
@@ -403,7 +412,7 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
     __syncthreads();
     double2* T = Tbase + (k % T2_STAGES) * tsz;
     const float2* T32 = reinterpret_cast<const float2*>(T);
-    auto TV = [&](int j) -> double2 { return T[j * T2_PITCH + c]; };
+    auto TV = [&](int j) -> double2 { return T[tix(j, c)]; };
 
     switch (st.op) {
       case OP_OWN_U13:
@@ -454,7 +463,7 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
           const int j = j0 + r;
           if (j >= lo && j <= hi) {
             double2 nl;
-            if (st.arg) { float2 v = T32[j * T2_PITCH + c]; nl = make_double2(v.x, v.y); }
+            if (st.arg) { float2 v = T32[tix(j, c)]; nl = make_double2(v.x, v.y); }
             else nl = TV(j);
             cf[r] = cf[r] - nl;
             cr[r] = cr[r] + a.temp5 * cf[r];
@@ -465,13 +474,13 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int j = j0 + r;
-            if (j < n) T[j * T2_PITCH + c] = cf[r];
+            if (j < n) T[tix(j, c)] = cf[r];
           }
           __syncthreads();
           for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
             const int j = idx >> 2, cc = idx & 3;
             if (cc < nvalid && j >= lo && j <= hi)
-              ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+              ((double2*)st.dst)[j * ps + cbase + cc] = T[tix(j, cc)];
           }
         }
         break;
@@ -502,9 +511,9 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
           if (j >= lo && j <= hi) {
             d = cr[r];
             if (kind == 1) {
-              d = d - a.temp4 * met[MET_IDY * n + j] * (Tcp[j * T2_PITCH + c] - Tcp[(j - 1) * T2_PITCH + c]);
+              d = d - a.temp4 * met[MET_IDY * n + j] * (TV(j) - TV(j - 1));
             } else if (kind == 0 || kind == 2) {
-              d = d - a.temp4 * mul_ik(kind == 0 ? kxm : kzq, Tcp[j * T2_PITCH + c]);
+              d = d - a.temp4 * mul_ik(kind == 0 ? kxm : kzq, TV(j));
               if (kind == 0 && m00) d.x -= a.px;
             }
           }
@@ -540,17 +549,20 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
         }
         const int w0 = (kind == 1) ? 1 : lo - 1;
         const int w1 = nyp + 1;
+        // the tile held the pressure (rows j and j-1 were read above, the
+        // latter possibly another lane's); it now stages the solution
+        __syncwarp();
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int j = j0 + r;
-          if (j < n) T[j * T2_PITCH + c] = cr[r];
+          if (j < n) T[tix(j, c)] = cr[r];
         }
         __syncthreads();
         for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
           const int j = idx >> 2, cc = idx & 3;
           if (cc >= nvalid) continue;
           const size_t o = j * ps + cbase + cc;
-          ((double2*)st.dst)[o] = (j >= w0 && j <= w1) ? T[j * T2_PITCH + cc] : ((const double2*)st.src2)[o];
+          ((double2*)st.dst)[o] = (j >= w0 && j <= w1) ? T[tix(j, cc)] : ((const double2*)st.src2)[o];
         }
         break;
       }
@@ -593,13 +605,13 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
             const double2 pm = r == 0 ? phm : cr[r - 1];
             u = u - met[MET_IDY * n + j] * (cr[r] - pm);
           }
-          T[j * T2_PITCH + c] = u;
+          T[tix(j, c)] = u;
         }
         __syncthreads();
         const int w0 = comp == 1 ? 2 : 1;
         for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
           const int j = idx >> 2, cc = idx & 3;
-          if (cc < nvalid && j >= w0 && j <= nyp) ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+          if (cc < nvalid && j >= w0 && j <= nyp) ((double2*)st.dst)[j * ps + cbase + cc] = T[tix(j, cc)];
         }
         break;
       }
@@ -609,14 +621,14 @@ __global__ void __launch_bounds__(128) k_column_tiles(const __grid_constant__ So
         for (int r = 0; r < R; ++r) {
           const int j = j0 + r;
           if (j >= n) continue;
-          double2 p = Tcp[j * T2_PITCH + c];
+          double2 p = TV(j);
           if (j >= a.jstart && j <= a.jend) p = p + ih * cr[r];
-          T[j * T2_PITCH + c] = p;
+          T[tix(j, c)] = p;
         }
         __syncthreads();
         for (int idx = tid; idx < n * T2_COLS; idx += nthr) {
           const int j = idx >> 2, cc = idx & 3;
-          if (cc < nvalid) ((double2*)st.dst)[j * ps + cbase + cc] = T[j * T2_PITCH + cc];
+          if (cc < nvalid) ((double2*)st.dst)[j * ps + cbase + cc] = T[tix(j, cc)];
         }
         break;
       }
