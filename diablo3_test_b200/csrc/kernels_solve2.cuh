@@ -6,13 +6,13 @@
 // rem_div_chan :946-1023), one warp per (kx, kz) column.  The difference is
 // the data path: a block owns 4 adjacent kz columns of one kx, and every
 // field it needs moves through shared memory as an (Ny+2) x 4 tile copied with
-// cp.async (16-byte pieces, 64-byte rows) through a three-stage ring, so two
-// tiles are in flight while one is consumed.  Lanes then read their own rows
+// cp.async (16-byte pieces, 64-byte rows) through a ring of T2_STAGES tiles,
+// so the next tile is in flight while one is consumed.  Lanes then read their own rows
 // (and y-neighbours) from shared memory.  The host builds the list of tiles
 // (`steps`) once per substep; terms whose coefficient is zero are not loaded
 // at all.  The pressure arrives as the tile of each velocity solve and of the
-// pressure update rather than staying resident: at Ny = 257 that keeps a
-// block at 71 KB of shared memory, three blocks per SM instead of two.
+// pressure update rather than staying resident, which keeps a 257-row block at
+// 56 KB of shared memory.
 #pragma once
 #include "common.cuh"
 #include "kernels_solve.cuh"
@@ -351,10 +351,20 @@ __global__ void __launch_bounds__(32) k_factor(const __grid_constant__ SolveArgs
   factor_rows<R>(Am, Bm, Cm, lane, out + (size_t)kind * Fac<R>::N * 32);
 }
 
-#define T2_STAGES 3
+// Ring depth and blocks per SM.  Occupancy, not prefetch depth, decides this
+// kernel's speed: at Ny = 257 (R = 9) a two-stage ring keeps a block at 56 KB
+// and a 128-register cap fits four blocks (16 warps) per SM, measured 0.84 ms
+// per launch against 0.90 (two stages, three blocks), 0.92 (three stages,
+// three blocks) and 1.08 (four stages, two blocks).  Larger R need more
+// shared memory, so fewer blocks fit and the cap is relaxed.
+#ifndef T2_STAGES
+#define T2_STAGES 2
+#endif
+template <int R>
+constexpr int t2_min_blocks() { return R <= 9 ? 4 : (R <= 13 ? 3 : 2); }
 
 template <int R>
-__global__ void __launch_bounds__(128, 3) k_column_tiles(const __grid_constant__ Solve2Args A) {
+__global__ void __launch_bounds__(128, t2_min_blocks<R>()) k_column_tiles(const __grid_constant__ Solve2Args A) {
   using namespace csolve;
   using namespace csolve2;
   const SolveArgs& a = A.s;
