@@ -5,8 +5,10 @@
 #include "kernels_fft.cuh"
 
 // reference physical v(0:Nx+1, 0:Nz+1, 0:Ny+1) -> internal P[j][k][i]
+// (`rows` rows of Nx+2 per plane in `ref`: Nz+2 for a whole reference array,
+// Nz for its significant rows staged contiguously)
 __global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict__ out,
-                              int nx, int nz, int nyp2) {
+                              int nx, int nz, int nyp2, int rows) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)nyp2 * nz * nx;
   if (idx >= tot) return;
@@ -14,7 +16,7 @@ __global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict
   size_t r = idx / nx;
   int k = r % nz;
   int j = r / nz;
-  out[idx] = ref[((size_t)j * (nz + 2) + k) * (nx + 2) + i];
+  out[idx] = ref[((size_t)j * rows + k) * (nx + 2) + i];
 }
 
 // internal P -> the significant box (i < Nx, k < Nz) of a reference physical array
