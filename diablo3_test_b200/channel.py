@@ -140,9 +140,10 @@ class Channel:
         return out
 
     def stats(self, homogeneous_x: bool = True) -> dict:
-        """Plane statistics of save_stats_chan (for/statistics.f90:44-712)
-        for the x-homogeneous case; applies the wall values to the state
-        first, as the reference does.  Returns ``{"profiles": {name: (Ny,)},
+        """Plane statistics of save_stats_chan (for/statistics.f90:44-712);
+        ``homogeneous_x`` is the reference's homogeneousX (False for IC types
+        5-8).  Applies the wall values to the state first, as the reference
+        does.  Returns ``{"profiles": {name: (Ny,)},
         "th": [{name: (Ny,)} per scalar], "spectrum": (Nx/2,), "scalars":
         {name: float}}`` with the reference's internal names (MEAN_H5_NAMES
         gives the dataset each one is written to)."""

@@ -59,7 +59,7 @@ struct diablo_ctx {
   cudaStream_t stream, own_stream;
   // grid metrics and wavenumbers (device)
   double *d_dy, *d_dyf, *d_gy, *d_gyf, *d_kx, *d_kz;
-  std::vector<double> h_dy, h_dyf, h_gy, h_gyf;
+  std::vector<double> h_dy, h_dyf, h_gy, h_gyf, h_kx;
   // twiddles: exp(-2 pi i m/N) for N = Nz, M = Nx/2, Nx
   double2 *tz64, *tm64, *tx64;
   float2 *tz32, *tm32, *tx32;
@@ -96,6 +96,7 @@ struct diablo_ctx {
   double* d_cfl;
   double* d_sigma;          // filter_chan transfer function [Nkx+1][2Nkz+1]
   double* d_stats;          // plane-statistics partial sums (diablo_stats)
+  double* stats_phys[3];    // physical u1, u2, u3 for the z-line statistics
   size_t stats_doubles;
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
@@ -1551,6 +1552,7 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
   for (int i = 0; i < ctx->nkx1; ++i) hkx[i] = i * (2. * PI_REF) / p->lx;
   for (int k = 0; k <= ctx->nkz; ++k) hkz[k] = k * (2. * PI_REF) / p->lz;
   for (int k = 1; k <= ctx->nkz; ++k) hkz[2 * ctx->nkz + 1 - k] = -k * (2. * PI_REF) / p->lz;
+  ctx->h_kx = hkx;
   auto up = [&](double** d, const std::vector<double>& h) -> int {
     int r = dev_alloc(ctx, (void**)d, h.size() * sizeof(double));
     if (r) return r;
@@ -1834,7 +1836,7 @@ int diablo_filter_chan(diablo_ctx* ctx, int n) {
 }
 
 // ---------------------------------------------------------------------------
-// Plane statistics (save_stats_chan, for/statistics.f90:44-712), homogeneous x
+// Plane statistics (save_stats_chan, for/statistics.f90:44-712)
 
 int diablo_stats_size(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
@@ -1844,14 +1846,17 @@ int diablo_stats_size(diablo_ctx* ctx) {
 int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   if (!ctx || !out) return DIABLO_ERR_ARG;
   if (len < diablo_stats_size(ctx)) return DIABLO_ERR_ARG;
-  if (!homogeneous_x) return DIABLO_ERR_UNSUPPORTED;
   const diablo_params& p = ctx->p;
   int rc;
   // apply_BC_vel_mpi_post / apply_BC_th_mpi_post on the state (:63-64)
   if ((rc = bc_post(ctx, 1, 1))) return rc;
-  const int ny = ctx->ny, nyp2 = ctx->nyp2, nth = ctx->nth, nkx1 = ctx->nkx1;
+  const int ny = ctx->ny, nyp2 = ctx->nyp2, nth = ctx->nth, nkx1 = ctx->nkx1, nx = ctx->nx;
   const int nmodes = nkx1 * ctx->nk2;
-  const size_t pn = (size_t)ctx->nz * ctx->nx;
+  const size_t pn = (size_t)ctx->nz * nx;
+  // x-inhomogeneous branch (IC types 5-8): z-line means when Nz > 1 (:749),
+  // epsilon's x derivatives without the kz = 0 row (:862-866), compute_MKE_diss
+  const bool nonhom = !homogeneous_x;
+  const bool zline = nonhom && ctx->nz > 1;
   int dev = 0, nsm = 148;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1860,9 +1865,13 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   nslice = std::max(1, std::min(nslice, (nmodes + STAT_THREADS - 1) / STAT_THREADS));
   int lslice = (4 * nsm + nyp2 - 1) / nyp2;
   lslice = std::max(1, std::min<int>(lslice, (int)((pn + STAT_THREADS - 1) / STAT_THREADS)));
-  const size_t n_part = (size_t)nyp2 * nslice * STAT_NQ, n_means = (size_t)nyp2 * (4 + nth);
-  const size_t n_spec = (size_t)nyp2 * nkx1, n_les = (size_t)nyp2 * lslice * 2;
-  const size_t total = n_part + n_means + n_spec + n_les;
+  // sub-buffer sizes in doubles, each rounded up to an even count so that
+  // every sub-buffer (the double2 rows among them) starts 16-byte aligned
+  auto even = [](size_t v) { return (v + 1) & ~(size_t)1; };
+  const size_t n_part = even((size_t)nyp2 * nslice * STAT_NQ), n_means = even((size_t)nyp2 * (4 + nth));
+  const size_t n_spec = even((size_t)nyp2 * nkx1), n_les = even((size_t)nyp2 * lslice * 2);
+  const size_t n_rows = (size_t)nyp2 * (3 + nth) * nkx1 * 2, n_xy = (size_t)XY_N * nyp2 * nx;
+  const size_t total = n_part + n_means + n_spec + n_les + n_rows + n_xy;
   if (ctx->stats_doubles < total) {
     if ((rc = dev_alloc(ctx, (void**)&ctx->d_stats, total * sizeof(double)))) return rc;
     ctx->stats_doubles = total;
@@ -1871,6 +1880,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   double* d_means = d_part + n_part;
   double* d_spec = d_means + n_means;
   double* d_les = d_spec + n_spec;
+  double* d_rows = d_les + n_les;
+  double* d_xy = d_rows + n_rows;
   CK(cudaMemsetAsync(ctx->d_stats, 0, total * sizeof(double), ctx->stream));
   const double d0 = nth > 0 ? p.dthdx[0] : 0.0;
   // (1/(Ro_inv/delta)) dTHdX(1), the thermal-wind shear; 0 without a background gradient
@@ -1898,10 +1909,13 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     a.nk2 = ctx->nk2;
     a.kp = ctx->kp;
     a.nslice = nslice;
+    a.rowmean = zline ? 1 : 0;
+    a.kstart1 = nonhom ? 1 : 0;
     a.ps = (size_t)nkx1 * ctx->kp;
     a.part = d_part;
     a.means = d_means;
     a.spec = d_spec;
+    a.rows = reinterpret_cast<double2*>(d_rows);
     Prof pr(ctx, K_OTHER);
     const dim3 grid(nslice, nyp2);
     if (nth == 0) k_stats_modes<0><<<grid, STAT_THREADS, 0, ctx->stream>>>(a);
@@ -1913,12 +1927,27 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     CK(cudaGetLastError());
   }
   const bool les = p.use_les && ctx->les.ready;
+  double* uphys[3] = {nullptr, nullptr, nullptr};
+  if (les || zline) {
+    // physical u1, u2, u3 (all planes): LES work arrays when present, else
+    // three buffers kept for the statistics
+    if (les) {
+      for (int q = 0; q < 3; ++q) uphys[q] = ctx->les.r[q];
+      const double2* four[3] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2]};
+      if ((rc = ifft_batch(ctx, four, uphys, 3))) return rc;
+    } else {
+      if ((rc = ensure_bscratch(ctx))) return rc;
+      for (int q = 0; q < 3; ++q) {
+        if (!ctx->stats_phys[q] &&
+            (rc = dev_alloc(ctx, (void**)&ctx->stats_phys[q], phys_elems(ctx) * sizeof(double))))
+          return rc;
+        uphys[q] = ctx->stats_phys[q];
+        if ((rc = inv_four_to_phys(ctx, ctx->st[ctx->cur][q], ctx->b_xs, uphys[q]))) return rc;
+      }
+    }
+  }
   if (les) {
-    // compute_TKE_diss_les needs physical u1, u2, u3 (all planes) and nu_t
     diablo_ctx::Les& L = ctx->les;
-    const double2* four[3] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2]};
-    double* phys[3] = {L.r[0], L.r[1], L.r[2]};
-    if ((rc = ifft_batch(ctx, four, phys, 3))) return rc;
     const double* nt = L.nu_t;
     if (L.nu_t_fp32) {
       if ((rc = ensure_bscratch(ctx))) return rc;
@@ -1929,7 +1958,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     }
     StatsLesArgs b;
     memset(&b, 0, sizeof(b));
-    for (int q = 0; q < 3; ++q) b.u[q] = phys[q];
+    for (int q = 0; q < 3; ++q) b.u[q] = uphys[q];
     b.nu_t = nt;
     b.dy = ctx->d_dy;
     b.dyf = ctx->d_dyf;
@@ -1942,16 +1971,34 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     ctx->launches++;
     CK(cudaGetLastError());
   }
+  if (zline) {
+    StatsXyArgs c;
+    memset(&c, 0, sizeof(c));
+    for (int q = 0; q < 3; ++q) c.u[q] = uphys[q];
+    c.dy = ctx->d_dy;
+    c.dyf = ctx->d_dyf;
+    c.nx = nx;
+    c.nz = ctx->nz;
+    c.nyp = ny;
+    c.out = d_xy;
+    Prof pr(ctx, K_OTHER);
+    k_stats_xy<<<dim3((nx + 127) / 128, nyp2), 128, 0, ctx->stream>>>(c);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
   std::vector<double> h(total);
   CK(cudaMemcpyAsync(h.data(), ctx->d_stats, total * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
 
-  // host finish, O(Ny)
+  // host finish, O(Ny Nx) (+ O(Ny Nx Nkx) for the mean x gradients of the
+  // inhomogeneous branch)
   const double* part = h.data();
   const double* means = part + n_part;
   const double* spec = means + n_means;
   const double* lpart = spec + n_spec;
+  const double* rows = lpart + n_les;
+  const double* xyd = rows + n_rows;
   auto Q = [&](int j, int q) {
     double s = 0.0;
     for (int sl = 0; sl < nslice; ++sl) s += part[((size_t)j * nslice + sl) * STAT_NQ + q];
@@ -1974,21 +2021,72 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     vme[j] = means[(size_t)j * (4 + nth) + 1];
     wme[j] = means[(size_t)j * (4 + nth) + 2];
   }
-  const double nn = (double)ctx->nx * ctx->nz;
+  const double nn = (double)nx * ctx->nz;
   for (int i = 0, ntot = diablo_stats_size(ctx); i < ntot; ++i) out[i] = 0.0;
   auto set = [&](int q, int j, double v) { out[(size_t)q * ny + (j - 1)] = v; };
-  std::vector<double> uu(nyp2, 0.0), vv(nyp2, 0.0), ww(nyp2, 0.0);
+  std::vector<double> uu(nyp2, 0.0), vv(nyp2, 0.0), ww(nyp2, 0.0), uw(nyp2, 0.0), uv(nyp2, 0.0),
+      wv(nyp2, 0.0);
   for (int j = 1; j <= ny; ++j) {
     uu[j] = Q(j, SQ_UU);
     vv[j] = Q(j, SQ_VV);
     ww[j] = Q(j, SQ_WW);
+    uw[j] = Q(j, SQ_UW);
+    if (j >= 2) { uv[j] = Q(j, SQ_UV); wv[j] = Q(j, SQ_WV); }
+  }
+  // z-line means and covariances at each x, [j][i] (the plane values repeated
+  // along x in the homogeneous branch, :811-836)
+  typedef std::vector<double> Vec;
+  const size_t xyn = (size_t)nyp2 * nx;
+  Vec ume_xy(xyn), vme_xy(xyn), wme_xy(xyn), uu_xy(xyn), vv_xy(xyn), uw_xy(xyn), uv_xy(xyn), wv_xy(xyn);
+  auto XY = [&](const Vec& v, int j, int i) { return v[(size_t)j * nx + i]; };
+  if (zline) {
+    Vec* dst[XY_N] = {&ume_xy, &vme_xy, &wme_xy, &uu_xy, &vv_xy, &uw_xy, &uv_xy, &wv_xy};
+    for (int q = 0; q < XY_N; ++q) std::copy(xyd + q * xyn, xyd + (q + 1) * xyn, dst[q]->begin());
+  } else {
+    for (int j = 0; j < nyp2; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const size_t o = (size_t)j * nx + i;
+        ume_xy[o] = ume[j]; vme_xy[o] = vme[j]; wme_xy[o] = wme[j];
+        uu_xy[o] = uu[j]; vv_xy[o] = vv[j]; uw_xy[o] = uw[j]; uv_xy[o] = uv[j]; wv_xy[o] = wv[j];
+      }
+  }
+  // x profiles of the kz = 0 rows: value or x derivative (ikx, reference
+  // wavenumbers) at x_i, the C2R sum Re c_0 + 2 sum_m Re(c_m e^{2 pi i m i/Nx})
+  const std::vector<double>& hkx = ctx->h_kx;
+  std::vector<double> ctab(nx), stab(nx);
+  for (int t = 0; t < nx; ++t) {
+    ctab[t] = cos(2.0 * M_PI * t / nx);
+    stab[t] = sin(2.0 * M_PI * t / nx);
+  }
+  auto xprof = [&](int field, bool deriv, Vec& dst) {
+    for (int j = 0; j < nyp2; ++j) {
+      const double* r = rows + ((size_t)j * (3 + nth) + field) * nkx1 * 2;
+      for (int i = 0; i < nx; ++i) {
+        double s = deriv ? 0.0 : r[0];
+        for (int m = 1; m < nkx1; ++m) {
+          const int t = (int)(((long long)m * i) % nx);
+          double cr = r[2 * m], ci = r[2 * m + 1];
+          if (deriv) { const double k = hkx[m]; const double tr = -k * ci; ci = k * cr; cr = tr; }
+          s += 2.0 * (cr * ctab[t] - ci * stab[t]);
+        }
+        dst[(size_t)j * nx + i] = s;
+      }
+    }
+  };
+  Vec dudx_m(xyn, 0.0), dvdx_m(xyn, 0.0), dwdx_m(xyn, 0.0);
+  if (nonhom) {
+    xprof(0, true, dudx_m);
+    xprof(1, true, dvdx_m);
+    xprof(2, true, dwdx_m);
+  }
+  for (int j = 1; j <= ny; ++j) {
     set(DIABLO_STAT_UME, j, ume[j]);
     set(DIABLO_STAT_VME, j, vme[j]);
     set(DIABLO_STAT_WME, j, wme[j]);
     set(DIABLO_STAT_URMS, j, sqrt(uu[j]));
     set(DIABLO_STAT_VRMS, j, sqrt(vv[j]));
     set(DIABLO_STAT_WRMS, j, sqrt(ww[j]));
-    set(DIABLO_STAT_UW, j, Q(j, SQ_UW));
+    set(DIABLO_STAT_UW, j, uw[j]);
     set(DIABLO_STAT_DUDY, j, (ume[j] - ume[j - 1]) / (gyf[j] - gyf[j - 1]));
     set(DIABLO_STAT_DWDY, j, (wme[j] - wme[j - 1]) / (gyf[j] - gyf[j - 1]));
     set(DIABLO_STAT_CP, j, means[(size_t)j * (4 + nth) + 3]);
@@ -1997,36 +2095,80 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     set(DIABLO_STAT_OMEGA_Y, j, sqrt(Q(j, SQ_OY)));
     set(DIABLO_STAT_OMEGA_Z, j, sqrt(Q(j, SQ_OZ)));
     if (les) set(DIABLO_STAT_NU_SGS, j, LQ(j, 0) / nn);
+    if (ctx->nz > 1) {   // production terms on GYF (:1486-1494)
+      double a = 0.0, b = 0.0;
+      for (int i = 0; i < nx; ++i) {
+        a += XY(uu_xy, j, i) * XY(dudx_m, j, i);
+        b += XY(uw_xy, j, i) * XY(dwdx_m, j, i);
+      }
+      set(DIABLO_STAT_UU_DUDX, j, a / nx);
+      set(DIABLO_STAT_WU_DWDX, j, b / nx);
+    }
+    if (nonhom) {   // compute_MKE_diss (:1150-1262), rows 1..Ny
+      double e = 0.0;
+      for (int i = 0; i < nx; ++i) {
+        const double su = XY(dudx_m, j, i), sum_ = j >= 2 ? XY(dudx_m, j - 1, i) : 0.0;
+        const double sw = XY(dwdx_m, j, i), swm = j >= 2 ? XY(dwdx_m, j - 1, i) : 0.0;
+        e += (dyf[j - 1] * su * su + dyf[j] * sum_ * sum_) / (2.0 * dy[j]);
+        e += XY(dvdx_m, j, i) * XY(dvdx_m, j, i);
+        e += (dyf[j - 1] * sw * sw + dyf[j] * swm * swm) / (2.0 * dy[j]);
+        if (j >= 2) {
+          const double tu = (XY(ume_xy, j, i) - XY(ume_xy, j - 1, i)) / dy[j];
+          const double tv = (XY(vme_xy, j + 1, i) - XY(vme_xy, j - 1, i)) / (gy[j + 1] - gy[j - 1]);
+          const double tw = (XY(wme_xy, j, i) - XY(wme_xy, j - 1, i)) / dy[j] + tws;
+          e += tu * tu + tv * tv + tw * tw;
+        }
+      }
+      set(DIABLO_STAT_EPSILON_M, j, ctx->nu * e / nx);
+    }
     if (j < 2) continue;
     // GY-grid rows (j >= 2)
-    const double uv = Q(j, SQ_UV), wv = Q(j, SQ_WV);
-    set(DIABLO_STAT_UV, j, uv);
-    set(DIABLO_STAT_WV, j, wv);
+    set(DIABLO_STAT_UV, j, uv[j]);
+    set(DIABLO_STAT_WV, j, wv[j]);
     set(DIABLO_STAT_EPSILON, j, ctx->nu * Q(j, SQ_EPS));
     if (les) set(DIABLO_STAT_EPS_SGS2, j, LQ(j, 1) / nn);
-    if (ctx->nz > 1) {   // production terms (:1475-1543); the dudx_m, dvdx_m, dwdx_m terms are 0
-      set(DIABLO_STAT_VV_DVDY, j, (vme[j + 1] - vme[j - 1]) / (gy[j + 1] - gy[j - 1]) * vv[j]);
-      set(DIABLO_STAT_UV_DUDY, j, (ume[j] - ume[j - 1]) / dy[j] * uv);
-      set(DIABLO_STAT_WV_DWDY, j, ((wme[j] - wme[j - 1]) / dy[j] + tws) * wv);
+    if (ctx->nz > 1) {   // production terms on GY (:1496-1532)
+      double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+      for (int i = 0; i < nx; ++i) {
+        a += XY(uv_xy, j, i) * XY(dvdx_m, j, i);
+        b += (XY(vme_xy, j + 1, i) - XY(vme_xy, j - 1, i)) / (gy[j + 1] - gy[j - 1]) * XY(vv_xy, j, i);
+        c += (XY(ume_xy, j, i) - XY(ume_xy, j - 1, i)) / dy[j] * XY(uv_xy, j, i);
+        d += ((XY(wme_xy, j, i) - XY(wme_xy, j - 1, i)) / dy[j] + tws) * XY(wv_xy, j, i);
+      }
+      set(DIABLO_STAT_VU_DVDX, j, a / nx);
+      set(DIABLO_STAT_VV_DVDY, j, b / nx);
+      set(DIABLO_STAT_UV_DUDY, j, c / nx);
+      set(DIABLO_STAT_WV_DWDY, j, d / nx);
     }
     // MKE on GY (:133-150)
-    const double wa = wme[j] + tws * (gyf[j] - 0.5 * p.ly), wb = wme[j - 1] + tws * (gyf[j - 1] - 0.5 * p.ly);
-    set(DIABLO_STAT_MKE, j,
-        0.5 * ((dyf[j - 1] * ume[j] * ume[j] + dyf[j] * ume[j - 1] * ume[j - 1]) / (2.0 * dy[j]) +
-               (dyf[j - 1] * wa * wa + dyf[j] * wb * wb) / (2.0 * dy[j]) + vme[j] * vme[j]));
+    double mk = 0.0;
+    for (int i = 0; i < nx; ++i) {
+      const double u0 = XY(ume_xy, j, i), u1m = XY(ume_xy, j - 1, i);
+      const double wa = XY(wme_xy, j, i) + tws * (gyf[j] - 0.5 * p.ly);
+      const double wb = XY(wme_xy, j - 1, i) + tws * (gyf[j - 1] - 0.5 * p.ly);
+      const double v0 = XY(vme_xy, j, i);
+      mk += (dyf[j - 1] * u0 * u0 + dyf[j] * u1m * u1m) / (2.0 * dy[j]) +
+            (dyf[j - 1] * wa * wa + dyf[j] * wb * wb) / (2.0 * dy[j]) + v0 * v0;
+    }
+    set(DIABLO_STAT_MKE, j, 0.5 * mk / nx);
   }
-  double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2;
+  double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + nx / 2;
   sc[DIABLO_STAT_TIME] = ctx->time;
   sc[DIABLO_STAT_DT] = ctx->delta_t;
   sc[DIABLO_STAT_UBULK] = integrate_y(ume);
   sc[DIABLO_STAT_URMS_B] = sqrt(integrate_y(uu));
   sc[DIABLO_STAT_VRMS_B] = sqrt(integrate_y(vv));
   sc[DIABLO_STAT_WRMS_B] = sqrt(integrate_y(ww));
+  Vec thme_xy(xyn);
   for (int n = 0; n < nth; ++n) {
     double* base = out + (size_t)ny * (DIABLO_STAT_NPROF + n * DIABLO_STAT_NTHPROF);
     auto tset = [&](int r, int j, double v) { base[(size_t)r * ny + (j - 1)] = v; };
     std::vector<double> thme(nyp2);
     for (int j = 0; j < nyp2; ++j) thme[j] = means[(size_t)j * (4 + nth) + 4 + n];
+    if (zline) xprof(3 + n, false, thme_xy);
+    else
+      for (int j = 0; j < nyp2; ++j)
+        for (int i = 0; i < nx; ++i) thme_xy[(size_t)j * nx + i] = thme[j];
     for (int j = 1; j <= ny; ++j) {
       const int q0 = STAT_NQV + STAT_NQT * n;
       tset(DIABLO_STAT_THME, j, thme[j]);
@@ -2036,9 +2178,10 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
       tset(DIABLO_STAT_PE_DISS, j, Q(j, q0 + 2));
       // thv_m (:377-385), gx(i) = i Lx / Nx
       double s = 0.0;
-      for (int i = 0; i < ctx->nx; ++i)
-        s = s + (thme[j] + p.dthdx[n] * ((i * p.lx) / ctx->nx - 0.5 * p.lx)) * (0.5 * (vme[j] + vme[j + 1]));
-      tset(DIABLO_STAT_THV_M, j, s / ctx->nx);
+      for (int i = 0; i < nx; ++i)
+        s = s + (XY(thme_xy, j, i) + p.dthdx[n] * ((i * p.lx) / nx - 0.5 * p.lx)) *
+                    (0.5 * (XY(vme_xy, j, i) + XY(vme_xy, j + 1, i)));
+      tset(DIABLO_STAT_THV_M, j, s / nx);
     }
   }
   if (nth > 0) {   // u1z_x0 (:418-430)
@@ -2048,7 +2191,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   }
   // FTx_uu (:650-675): kz = 0 row of u1, integrated over y
   double* sp = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF);
-  for (int m = 0; m < nkx1 && m < ctx->nx / 2; ++m) {
+  for (int m = 0; m < nkx1 && m < nx / 2; ++m) {
     double s = 0.0;
     for (int j = 2; j <= ny; ++j)
       s += 0.5 * (spec[(size_t)j * nkx1 + m] + spec[(size_t)(j - 1) * nkx1 + m]) * dy[j];

@@ -52,10 +52,15 @@ struct StatsArgs {
   double dthdx[DIABLO_MAX_TH], dthdz[DIABLO_MAX_TH];
   double tws;           // thermal-wind shear (1/(Ro_inv/delta)) dTHdX(1)
   int nth, nyp, nkx1, nk2, kp, nslice;
+  // x-inhomogeneous branch (IC types 5-8): `rowmean` takes fluctuations about
+  // the z-line means, i.e. drops the whole kz = 0 row instead of the (0,0)
+  // mode; `kstart1` leaves the kz = 0 row out of epsilon's x derivatives
+  int rowmean, kstart1;
   size_t ps;
   double* part;         // [Ny+2][nslice][STAT_NQ]
   double* means;        // [Ny+2][4 + nth]: Re of the (0,0) coefficient of u1 u2 u3 p th_n
   double* spec;         // [Ny+2][Nkx+1]: |u1(kx, kz = 0)|^2
+  double2* rows;        // [Ny+2][3 + nth][Nkx+1]: the kz = 0 rows (Hermitian part at kx = 0)
 };
 
 HDI double nrm2(double2 a) { return a.x * a.x + a.y * a.y; }
@@ -116,7 +121,14 @@ __global__ void __launch_bounds__(STAT_THREADS) k_stats_modes(const __grid_const
       return v;
     };
     const double2 c1 = ld(a.cu[0], j);
-    if (kq == 0) a.spec[(size_t)j * a.nkx1 + m] = nrm2(c1);
+    if (kq == 0) {
+      a.spec[(size_t)j * a.nkx1 + m] = nrm2(c1);
+      double2* ro = a.rows + (size_t)j * (3 + a.nth) * a.nkx1 + m;
+      ro[0] = c1;
+      ro[a.nkx1] = ld(a.cu[1], j);
+      ro[2 * a.nkx1] = ld(a.cu[2], j);
+      for (int n = 0; n < a.nth; ++n) ro[(3 + n) * a.nkx1] = ld(a.cth[n], j);
+    }
     if (is00) {
       double* mo = a.means + (size_t)j * (4 + a.nth);
       mo[0] = c1.x;
@@ -133,10 +145,11 @@ __global__ void __launch_bounds__(STAT_THREADS) k_stats_modes(const __grid_const
     const double2 c2m = ld(a.cu[1], j - 1), c2 = ld(a.cu[1], j), c2p = ld(a.cu[1], j + 1);
     const double2 c3m = ld(a.cu[2], j - 1), c3 = ld(a.cu[2], j), c3p = ld(a.cu[2], j + 1);
     const double2 z = make_double2(0.0, 0.0);
-    // fluctuations (the (0,0) coefficient removed)
-    const double2 h1 = is00 ? z : c1, h2 = is00 ? z : c2, h3 = is00 ? z : c3;
-    const double2 h1m = is00 ? z : c1m, h2m = is00 ? z : c2m, h3m = is00 ? z : c3m;
-    const double2 h2p = is00 ? z : c2p;
+    // fluctuations: the (0,0) coefficient removed, or the kz = 0 row
+    const bool drop = a.rowmean ? kq == 0 : is00;
+    const double2 h1 = drop ? z : c1, h2 = drop ? z : c2, h3 = drop ? z : c3;
+    const double2 h1m = drop ? z : c1m, h2m = drop ? z : c2m, h3m = drop ? z : c3m;
+    const double2 h2p = drop ? z : c2p;
     acc[SQ_UU] += w * nrm2(h1);
     acc[SQ_VV] += w * nrm2(h2);
     acc[SQ_WW] += w * nrm2(h3);
@@ -157,20 +170,22 @@ __global__ void __launch_bounds__(STAT_THREADS) k_stats_modes(const __grid_const
       acc[SQ_WV] += w * re_dot(i3, h2);
       // du/dx, dw/dx, du/dz, dw/dz interpolated to GY; dv/dx, dv/dz at GY;
       // du/dy, dv/dy, dw/dy of the fluctuations
-      double e = k2 * (dyfm * (nrm2(c1) + nrm2(c3)) + dyfj * (nrm2(c1m) + nrm2(c3m))) / (2.0 * dyj);
-      e += k2 * nrm2(c2);
+      // (on the kz = 0 row k2 = kx^2: the x derivatives, left out with kstart1)
+      const double k2e = (a.kstart1 && kq == 0) ? 0.0 : k2;
+      double e = k2e * (dyfm * (nrm2(c1) + nrm2(c3)) + dyfj * (nrm2(c1m) + nrm2(c3m))) / (2.0 * dyj);
+      e += k2e * nrm2(c2);
       e += (nrm2(h1 - h1m) + nrm2(h3 - h3m)) / (dyj * dyj);
       e += nrm2(h2p - h2m) / (dgy * dgy);
       acc[SQ_EPS] += w * e;
     }
     if (kq == 0) acc[SQ_U1YL] += m0 ? c1.x : 2.0 * c1.x;
     // scalars: thrms (:275-286), thv (:331-343), pe_diss (:400-414)
-    const double2 v2 = is00 ? z : 0.5 * (c2 + c2p);
+    const double2 v2 = drop ? z : 0.5 * (c2 + c2p);
 #pragma unroll
     for (int n = 0; n < NT; ++n) {
       if (n < a.nth) {
         const double2 ct = ld(a.cth[n], j);
-        const double2 ht = is00 ? z : ct;
+        const double2 ht = drop ? z : ct;
         acc[STAT_NQV + STAT_NQT * n + 0] += w * nrm2(ht);
         acc[STAT_NQV + STAT_NQT * n + 1] += w * re_dot(ht, v2);
         // the wall-normal gradient is that of scalar 1 for every n (:316)
@@ -226,4 +241,66 @@ __global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_constan
     }
   }
   block_sum_store<2>(acc, 2, a.part + ((size_t)j * a.nslice + blockIdx.x) * 2);
+}
+
+// Z-line statistics of the x-inhomogeneous branch from physical u1, u2, u3
+// ([j][k][i]): per (j, i) the z means ume_xy, vme_xy, wme_xy
+// (compute_averages, for/statistics.f90:749-786) and the z means of the
+// fluctuation products the production terms weight by the mean gradients:
+// uu_xy, vv_xy (compute_TKE :1296-1312), vvar_xy = <u1'u3'>, uvar_xy =
+// <I(u1')u2'>, wvar_xy = <I(u3')u2'> (compute_TKE_Production :1413-1447), the
+// last two on GY (j >= 2).  One thread per (j, i), two passes over k.
+enum { XY_UME = 0, XY_VME, XY_WME, XY_UU, XY_VV, XY_UW, XY_UV, XY_WV, XY_N };
+
+struct StatsXyArgs {
+  const double* u[3];
+  const double* dy;
+  const double* dyf;
+  int nx, nz, nyp;
+  double* out;          // [XY_N][Ny+2][Nx]
+};
+
+__global__ void __launch_bounds__(128) k_stats_xy(const __grid_constant__ StatsXyArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= a.nx) return;
+  const size_t pn = (size_t)a.nz * a.nx;
+  const size_t o = (size_t)j * pn + i;
+  const bool lower = j >= 1;
+  const double* u1 = a.u[0];
+  const double* u2 = a.u[1];
+  const double* u3 = a.u[2];
+  double s1 = 0, s2 = 0, s3 = 0, s1m = 0, s3m = 0;
+  for (int k = 0; k < a.nz; ++k) {
+    const size_t q = o + (size_t)k * a.nx;
+    s1 += u1[q];
+    s2 += u2[q];
+    s3 += u3[q];
+    if (lower) { s1m += u1[q - pn]; s3m += u3[q - pn]; }
+  }
+  const double rz = 1.0 / a.nz;
+  const double m1 = s1 * rz, m2 = s2 * rz, m3 = s3 * rz, m1m = s1m * rz, m3m = s3m * rz;
+  const bool gy = j >= 2 && j <= a.nyp;
+  const double wa = gy ? a.dyf[j - 1] / (2.0 * a.dy[j]) : 0.0, wb = gy ? a.dyf[j] / (2.0 * a.dy[j]) : 0.0;
+  double uu = 0, vv = 0, uw = 0, uv = 0, wv = 0;
+  for (int k = 0; k < a.nz; ++k) {
+    const size_t q = o + (size_t)k * a.nx;
+    const double d1 = u1[q] - m1, d2 = u2[q] - m2, d3 = u3[q] - m3;
+    uu += d1 * d1;
+    vv += d2 * d2;
+    uw += d1 * d3;
+    if (gy) {
+      uv += (wa * d1 + wb * (u1[q - pn] - m1m)) * d2;
+      wv += (wa * d3 + wb * (u3[q - pn] - m3m)) * d2;
+    }
+  }
+  const size_t plane = (size_t)(a.nyp + 2) * a.nx, at = (size_t)j * a.nx + i;
+  a.out[XY_UME * plane + at] = m1;
+  a.out[XY_VME * plane + at] = m2;
+  a.out[XY_WME * plane + at] = m3;
+  a.out[XY_UU * plane + at] = uu * rz;
+  a.out[XY_VV * plane + at] = vv * rz;
+  a.out[XY_UW * plane + at] = uw * rz;
+  a.out[XY_UV * plane + at] = uv * rz;
+  a.out[XY_WV * plane + at] = wv * rz;
 }

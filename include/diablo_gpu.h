@@ -146,18 +146,19 @@ int diablo_filter_chan(diablo_ctx* ctx, int n);
 
 /* Plane statistics: save_stats_chan (for/statistics.f90:44-712) with
  * compute_averages, compute_TKE_diss, compute_MKE_diss, compute_TKE,
- * compute_TKE_Production, compute_Vorticity and compute_TKE_diss_les, for the
- * x-homogeneous case (homogeneousX, for/parameters.f90:275-280: IC types other
- * than 5-8).  Applies the wall values (apply_BC_vel/th_mpi_post) to the state
- * first, as the reference does.  The profiles are the values the reference
- * writes to mean.h5 at j = 1..Ny (its internal names; mean.h5 swaps the v/w
- * labels).  The plane averages are evaluated from the Fourier coefficients
- * (Parseval), in FP64 in both precisions; the host-side finish is O(Ny).
- * Not computed: HDF5/movie output, y* binning, compute_BPE, and the z-line
- * averages of the non-homogeneous branch (homogeneous_x = 0 returns
- * DIABLO_ERR_UNSUPPORTED).  nu_sgs is the plane mean of the nu_t of the most
- * recent LES substep and eps_sgs2 uses that nu_t, as compute_TKE_diss_les
- * does; both are 0 without LES.
+ * compute_TKE_Production, compute_Vorticity and compute_TKE_diss_les.
+ * homogeneous_x is the reference's homogeneousX (for/parameters.f90:275-280:
+ * 0 for IC types 5-8): with 0 the means are z-line averages at each x,
+ * epsilon's x derivatives leave out the kz = 0 row, and compute_MKE_diss and
+ * the production terms use the mean x gradients.  Applies the wall values
+ * (apply_BC_vel/th_mpi_post) to the state first, as the reference does.  The
+ * profiles are the values the reference writes to mean.h5 at j = 1..Ny (its
+ * internal names; mean.h5 swaps the v/w labels).  Plane averages of products
+ * are evaluated from the Fourier coefficients (Parseval), z-line averages and
+ * the LES terms from physical fields, all in FP64 in both precisions.
+ * Not computed: HDF5/movie output, y* binning and compute_BPE.  nu_sgs is the
+ * plane mean of the nu_t of the most recent LES substep and eps_sgs2 uses that
+ * nu_t, as compute_TKE_diss_les does; both are 0 without LES.
  * Layout of `out` (diablo_stats_size doubles):
  *   profile q of the velocity set at out[q*Ny + j-1], q < DIABLO_STAT_NPROF;
  *   then, for scalar n, profile r at out[(NPROF + n*NTHPROF + r)*Ny + j-1];

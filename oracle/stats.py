@@ -5,7 +5,7 @@ compute_MKE_diss (:1130-1284), compute_TKE (:1285-1393),
 compute_TKE_Production (:1394-1549), compute_Vorticity (:1550-1754),
 integrate_y_var (:1974-1990) and compute_TKE_diss_les (:2054-2120) -- for the
 x-homogeneous case (``homogeneousX``, for/parameters.f90:275-280: every IC type
-but 5-8), one y-rank and one z-rank.
+but 5-8) and the non-homogeneous one, one y-rank and one z-rank.
 
 Like the reference, every plane average is formed in PHYSICAL space: the
 fields (and the spectral gradients the reference builds) are transformed with
@@ -13,9 +13,9 @@ fields (and the spectral gradients the reference builds) are transformed with
 library evaluates the same averages from the Fourier coefficients (Parseval),
 so the two agree to round-off, not bit for bit.
 
-Not restated: HDF5/movie output, the y* binning (Bin_Ystar_and_Write),
-compute_BPE, and the z-line (x-dependent) averages of the non-homogeneous
-branch.  The oracle is the checker of the CUDA library, never the product.
+Both branches of ``homogeneousX`` are restated.  Not restated: HDF5/movie
+output, the y* binning (Bin_Ystar_and_Write) and compute_BPE.  The oracle is
+the checker of the CUDA library, never the product.
 
 Quirks kept from the reference:
   * pe_diss uses the wall-normal gradient of scalar 1 for every scalar
@@ -77,11 +77,20 @@ def _phys(o: OracleChannel, c):
     return f.r[:, :o.Nz, :o.Nx].copy()
 
 
-def save_stats_chan(o: OracleChannel, nu_t=None) -> dict:
+def _krows(kfac, k0):
+    """A wavenumber factor broadcast over [j, k, i], restricted to k >= k0."""
+    return kfac if kfac.shape[1] == 1 else kfac[:, k0:, :]
+
+
+def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> dict:
     """Statistics of the oracle's current (Fourier) state.  Applies the
     velocity and scalar wall values first, as the reference does (:63-64),
     which changes the oracle's state the same way.  ``nu_t`` (reference
-    physical layout) enables the LES rows nu_sgs and eps_sgs2."""
+    physical layout) enables the LES rows nu_sgs and eps_sgs2.
+    ``homogeneous_x = False`` is the branch of IC types 5-8: z-line averages
+    ume_xy(x, y) etc. as the means (when Nz > 1), the x derivatives of epsilon
+    without the kz = 0 row, compute_MKE_diss and the production terms that use
+    its mean gradients."""
     p = o.p
     Nx, Nz, Nyp, Nxp, tk = o.Nx, o.Nz, o.Nyp, o.Nxp, o.twoNkz
     gy, gyf, dy, dyf = o.gy, o.gyf, o.dy, o.dyf
@@ -99,40 +108,87 @@ def save_stats_chan(o: OracleChannel, nu_t=None) -> dict:
     cikz = o.cikz[None, :tk + 1, None]
     out = {k: np.zeros(ny2) for k in VEL_PROFILES}
 
-    # compute_averages (:733-746, :811-836)
+    # compute_averages (:733-746, :749-836): plane means, and the z-line means
+    # ume_xy(i, j) etc. that every fluctuation below is taken about
     ume, vme, wme = cr1[:, 0, 0].real.copy(), cr2[:, 0, 0].real.copy(), cr3[:, 0, 0].real.copy()
     thme = [c[:, 0, 0].real.copy() for c in crth]
     out["ume"][:], out["vme"][:], out["wme"][:] = ume, vme, wme
     ubulk = integrate_y_var(o, ume)
+    ume_xy, vme_xy, wme_xy = np.zeros((ny2, Nx)), np.zeros((ny2, Nx)), np.zeros((ny2, Nx))
+    thme_xy = [np.zeros((ny2, Nx)) for _ in crth]
+    if Nz > 1 and not homogeneous_x:
+        for j in range(1, Nyp + 1):
+            ume_xy[j] = np.sum(u1[j], axis=0) / float(Nz)
+            wme_xy[j] = np.sum(u3[j], axis=0) / float(Nz)
+            for n in range(o.Nth):
+                thme_xy[n][j] = np.sum(th[n][j], axis=0) / float(Nz)
+        for j in range(1, Nyp + 2):
+            vme_xy[j] = np.sum(u2[j], axis=0) / float(Nz)
+    else:
+        ume_xy[1:Nyp + 1] = ume[1:Nyp + 1, None]
+        wme_xy[1:Nyp + 1] = wme[1:Nyp + 1, None]
+        vme_xy[1:Nyp + 2] = vme[1:Nyp + 2, None]
+        for n in range(o.Nth):
+            thme_xy[n][1:Nyp + 1] = thme[n][1:Nyp + 1, None]
 
     def zero_cs():
         return np.zeros_like(cr1)
 
-    # compute_TKE_diss (:859-1062), k_start = 0
+    # compute_TKE_diss (:859-1062); the x derivatives skip the kz = 0 row
+    # outside the homogeneous branch (k_start, :862-866)
+    k0 = 0 if homogeneous_x else 1
     eps = np.zeros(ny2)
 
     def interp_sq(s, j):   # (dyf(j-1) s(j)^2 + dyf(j) s(j-1)^2) / (2 dy(j)), summed
         return np.sum((dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j]))
 
-    for cr, kfac in ((cr1, cikx), (cr3, cikx), (cr1, cikz), (cr3, cikz)):   # du/dx dw/dx du/dz dw/dz
-        cs = zero_cs()
-        cs[1:Nyp + 1, K, I] = kfac * cr[1:Nyp + 1, K, I]
+    for cr, kfac, kk in ((cr1, cikx, k0), (cr3, cikx, k0), (cr1, cikz, 0), (cr3, cikz, 0)):
+        cs = zero_cs()                                     # du/dx dw/dx du/dz dw/dz
+        cs[1:Nyp + 1, kk:tk + 1, I] = _krows(kfac, kk) * cr[1:Nyp + 1, kk:tk + 1, I]
         s = _phys(o, cs)
         for j in range(2, Nyp + 1):
             eps[j] += interp_sq(s, j)
-    for kfac in (cikx, cikz):                                               # dv/dx dv/dz
+    for kfac, kk in ((cikx, k0), (cikz, 0)):               # dv/dx dv/dz
         cs = zero_cs()
-        cs[2:Nyp + 1, K, I] = kfac * cr2[2:Nyp + 1, K, I]
+        cs[2:Nyp + 1, kk:tk + 1, I] = _krows(kfac, kk) * cr2[2:Nyp + 1, kk:tk + 1, I]
         s = _phys(o, cs)
         for j in range(2, Nyp + 1):
             eps[j] += np.sum(s[j] ** 2)
     for j in range(2, Nyp + 1):
-        su = ((u1[j] - ume[j]) - (u1[j - 1] - ume[j - 1])) / dy[j]           # du/dy
-        sv = ((u2[j + 1] - vme[j + 1]) - (u2[j - 1] - vme[j - 1])) / (gy[j + 1] - gy[j - 1])
-        sw = ((u3[j] - wme[j]) - (u3[j - 1] - wme[j - 1])) / dy[j]           # dw/dy
+        su = ((u1[j] - ume_xy[j]) - (u1[j - 1] - ume_xy[j - 1])) / dy[j]      # du/dy
+        sv = ((u2[j + 1] - vme_xy[j + 1]) - (u2[j - 1] - vme_xy[j - 1])) / (gy[j + 1] - gy[j - 1])
+        sw = ((u3[j] - wme_xy[j]) - (u3[j - 1] - wme_xy[j - 1])) / dy[j]      # dw/dy
         eps[j] += np.sum(su ** 2) + np.sum(sv ** 2) + np.sum(sw ** 2)
     out["epsilon"][:] = o.nu * eps / NN
-    # compute_MKE_diss returns early in the homogeneous branch: epsilon_m = 0
+
+    # compute_MKE_diss (:1130-1284): returns at once in the homogeneous branch,
+    # leaving epsilon_m and the mean x gradients 0
+    dudx_m, dvdx_m, dwdx_m = np.zeros((ny2, Nx)), np.zeros((ny2, Nx)), np.zeros((ny2, Nx))
+    if not homogeneous_x:
+        epm = np.zeros(ny2)
+
+        def row_phys(cr, jlo):            # x derivative of the kz = 0 row, rows jlo..Nyp
+            cs = zero_cs()
+            cs[jlo:Nyp + 1, 0, I] = o.cikx[:Nxp] * cr[jlo:Nyp + 1, 0, I]
+            return _phys(o, cs)[:, 0, :]
+        s = row_phys(cr1, 1)
+        for j in range(1, Nyp + 1):
+            epm[j] += np.sum((dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j]))
+        dudx_m[1:Nyp + 1] = s[1:Nyp + 1]
+        s = row_phys(cr2, 1)
+        for j in range(1, Nyp + 1):
+            epm[j] += np.sum(s[j] ** 2)
+        dvdx_m[1:Nyp + 1] = s[1:Nyp + 1]
+        for j in range(2, Nyp + 1):
+            epm[j] += np.sum(((ume_xy[j] - ume_xy[j - 1]) / dy[j]) ** 2)
+        s = row_phys(cr3, 1)
+        for j in range(1, Nyp + 1):
+            epm[j] += np.sum((dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j]))
+        dwdx_m[1:Nyp + 1] = s[1:Nyp + 1]
+        for j in range(2, Nyp + 1):
+            epm[j] += np.sum(((vme_xy[j + 1] - vme_xy[j - 1]) / (gy[j + 1] - gy[j - 1])) ** 2)
+            epm[j] += np.sum(((wme_xy[j] - wme_xy[j - 1]) / dy[j] + tws) ** 2)
+        out["epsilon_m"][:] = o.nu * epm / float(Nx)
 
     # compute_TKE_diss_les (:2054-2120)
     if nu_t is not None:
@@ -152,38 +208,55 @@ def save_stats_chan(o: OracleChannel, nu_t=None) -> dict:
         for j in range(1, Nyp + 1):
             out["nu_sgs"][j] = np.sum(nt[j]) / NN
 
-    # compute_TKE (:1290-1331)
-    for name, u, me in (("urms", u1, ume), ("vrms", u2, vme), ("wrms", u3, wme)):
+    # compute_TKE (:1290-1331), with the z means uu_xy, vv_xy at each x
+    uu_xy, vv_xy = np.zeros((ny2, Nx)), np.zeros((ny2, Nx))
+    for name, u, me, xy in (("urms", u1, ume_xy, uu_xy), ("vrms", u2, vme_xy, vv_xy),
+                            ("wrms", u3, wme_xy, None)):
         for j in range(1, Nyp + 1):
-            out[name][j] = np.sum((u[j] - me[j]) ** 2) / NN
+            d2 = (u[j] - me[j]) ** 2
+            out[name][j] = np.sum(d2) / NN
+            if xy is not None:
+                xy[j] = np.sum(d2, axis=0) / float(Nz)
     urms_b = np.sqrt(integrate_y_var(o, out["urms"]))
     vrms_b = np.sqrt(integrate_y_var(o, out["vrms"]))
     wrms_b = np.sqrt(integrate_y_var(o, out["wrms"]))
-    vv = out["vrms"].copy()   # vv_xy summed over x / Nx: the plane mean of (u2 - vme)^2
     for name in ("urms", "vrms", "wrms"):
         out[name][1:Nyp + 1] = np.sqrt(out[name][1:Nyp + 1])
 
-    # compute_TKE_Production (:1408-1545)
+    # compute_TKE_Production (:1408-1545): uw on GYF, uv and wv on GY, each
+    # also as z means at each x (vvar_xy, uvar_xy, wvar_xy)
+    uw_xy, uv_xy, wv_xy = np.zeros((ny2, Nx)), np.zeros((ny2, Nx)), np.zeros((ny2, Nx))
     for j in range(1, Nyp + 1):
-        out["uw"][j] = np.sum((u1[j] - ume[j]) * (u3[j] - wme[j])) / NN
+        prod = (u1[j] - ume_xy[j]) * (u3[j] - wme_xy[j])
+        out["uw"][j] = np.sum(prod) / NN
+        uw_xy[j] = np.sum(prod, axis=0) / float(Nz)
     for j in range(2, Nyp + 1):
-        fu = (dyf[j - 1] * (u1[j] - ume[j]) + dyf[j] * (u1[j - 1] - ume[j - 1])) / (2.0 * dy[j])
-        fw = (dyf[j - 1] * (u3[j] - wme[j]) + dyf[j] * (u3[j - 1] - wme[j - 1])) / (2.0 * dy[j])
-        out["uv"][j] = np.sum(fu * (u2[j] - vme[j])) / NN
-        out["wv"][j] = np.sum(fw * (u2[j] - vme[j])) / NN
+        fu = (dyf[j - 1] * (u1[j] - ume_xy[j]) + dyf[j] * (u1[j - 1] - ume_xy[j - 1])) / (2.0 * dy[j])
+        fw = (dyf[j - 1] * (u3[j] - wme_xy[j]) + dyf[j] * (u3[j - 1] - wme_xy[j - 1])) / (2.0 * dy[j])
+        pu, pw = fu * (u2[j] - vme_xy[j]), fw * (u2[j] - vme_xy[j])
+        out["uv"][j] = np.sum(pu) / NN
+        out["wv"][j] = np.sum(pw) / NN
+        uv_xy[j] = np.sum(pu, axis=0) / float(Nz)
+        wv_xy[j] = np.sum(pw, axis=0) / float(Nz)
     if Nz > 1:
+        for j in range(1, Nyp + 1):
+            out["uu_dudx"][j] = np.sum(uu_xy[j] * dudx_m[j]) / float(Nx)
+            out["wu_dwdx"][j] = np.sum(uw_xy[j] * dwdx_m[j]) / float(Nx)
         for j in range(2, Nyp + 1):
-            out["vv_dvdy"][j] = (vme[j + 1] - vme[j - 1]) / (gy[j + 1] - gy[j - 1]) * vv[j]
-            out["uv_dudy"][j] = (ume[j] - ume[j - 1]) / dy[j] * out["uv"][j]
-            out["wv_dwdy"][j] = ((wme[j] - wme[j - 1]) / dy[j] + tws) * out["wv"][j]
+            out["vu_dvdx"][j] = np.sum(uv_xy[j] * dvdx_m[j]) / float(Nx)
+            out["vv_dvdy"][j] = np.sum((vme_xy[j + 1] - vme_xy[j - 1]) / (gy[j + 1] - gy[j - 1])
+                                       * vv_xy[j]) / float(Nx)
+            out["uv_dudy"][j] = np.sum((ume_xy[j] - ume_xy[j - 1]) / dy[j] * uv_xy[j]) / float(Nx)
+            out["wv_dwdy"][j] = np.sum(((wme_xy[j] - wme_xy[j - 1]) / dy[j] + tws)
+                                       * wv_xy[j]) / float(Nx)
 
     # MKE on GY (:133-150)
     for j in range(2, Nyp + 1):
-        out["mke"][j] = 0.5 * ((dyf[j - 1] * ume[j] ** 2 + dyf[j] * ume[j - 1] ** 2) / (2.0 * dy[j])
-                               + (dyf[j - 1] * (wme[j] + tws * (gyf[j] - 0.5 * p.ly)) ** 2
-                                  + dyf[j] * (wme[j - 1] + tws * (gyf[j - 1] - 0.5 * p.ly)) ** 2)
-                               / (2.0 * dy[j])
-                               + vme[j] ** 2)
+        out["mke"][j] = 0.5 * np.sum(
+            (dyf[j - 1] * ume_xy[j] ** 2 + dyf[j] * ume_xy[j - 1] ** 2) / (2.0 * dy[j])
+            + (dyf[j - 1] * (wme_xy[j] + tws * (gyf[j] - 0.5 * p.ly)) ** 2
+               + dyf[j] * (wme_xy[j - 1] + tws * (gyf[j - 1] - 0.5 * p.ly)) ** 2) / (2.0 * dy[j])
+            + vme_xy[j] ** 2) / float(Nx)
     # gradients of the mean (:153-156) and mean-square shear (:159-171)
     for j in range(1, Nyp + 1):
         out["dudy"][j] = (ume[j] - ume[j - 1]) / (gyf[j] - gyf[j - 1])
@@ -227,13 +300,13 @@ def save_stats_chan(o: OracleChannel, nu_t=None) -> dict:
         c3 = zero_cs()
         c3[J, K, I] = cikz * crth[n][J, K, I]
         r1, r2, r3 = _phys(o, c1), _phys(o, c2), _phys(o, c3)
-        t, tm = th[n], thme[n]
+        t, tm, txy = th[n], thme[n], thme_xy[n]
         for j in range(1, Nyp + 1):
-            prof["thrms"][j] = np.sqrt(np.sum((t[j] - tm[j]) ** 2) / NN)
-            prof["thv"][j] = np.sum((t[j] - tm[j]) * (0.5 * (u2[j] + u2[j + 1])
-                                                      - 0.5 * (vme[j] + vme[j + 1]))) / NN
-            prof["thv_m"][j] = np.sum((tm[j] + p.dthdx[n] * (gx - 0.5 * p.lx))
-                                      * (0.5 * (vme[j] + vme[j + 1]))) / float(Nx)
+            prof["thrms"][j] = np.sqrt(np.sum((t[j] - txy[j]) ** 2) / NN)
+            prof["thv"][j] = np.sum((t[j] - txy[j]) * (0.5 * (u2[j] + u2[j + 1])
+                                                       - 0.5 * (vme_xy[j] + vme_xy[j + 1]))) / NN
+            prof["thv_m"][j] = np.sum((txy[j] + p.dthdx[n] * (gx - 0.5 * p.lx))
+                                      * (0.5 * (vme_xy[j] + vme_xy[j + 1]))) / float(Nx)
             prof["dthdy"][j] = (tm[j] - tm[j - 1]) / (gyf[j] - gyf[j - 1])
             prof["pe_diss"][j] = np.sum((r1[j] + p.dthdx[n]) ** 2 + r2[j] ** 2
                                         + (r3[j] + p.dthdz[n]) ** 2) / NN

@@ -3,8 +3,9 @@ save_stats_chan of for/statistics.f90:44-712) with the oracle
 (oracle/stats.py), through the C ABI.
 
 The device evaluates the plane averages from the Fourier coefficients
-(Parseval); the oracle sums physical grid values as the reference does, so the
-two agree to round-off.  Each case steps the GPU channel, loads its state into
+(Parseval) and the z-line averages of the x-inhomogeneous branch from physical
+fields; the oracle sums physical grid values as the reference does, so the two
+agree to round-off.  Each case steps the GPU channel, loads its state into
 the oracle and compares every profile on the same state: max abs error <=
 1e-10 x the profile's largest magnitude (1e-12 x for the means and scalars).
 At the full 256 x 257 x 256 size the checks are size-independent: the rms
@@ -110,15 +111,57 @@ def test_stats_les_match_oracle(cuda_device, model, precision):
         ch.close()
 
 
-def test_stats_rejects_nonhomogeneous_and_short_buffers(cuda_device):
+NONHOM_CASES = {
+    "front_two_scalars": dict(n_th=2, ro=4.0, delta=0.8, dthdx=[0.25, -0.1], dthdz=[0.05, 0.0],
+                              th_bc_ymin=[0, 1], th_bc_ymin_c1=[0.3, 0.0], pr=[1.0, 0.71]),
+    "no_scalars": dict(n_th=0, grav_y=0.0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(NONHOM_CASES))
+@pytest.mark.parametrize("precision", [0, MIXED])
+def test_stats_nonhomogeneous_match_oracle(cuda_device, case, precision):
+    """The branch of IC types 5-8 (homogeneousX false): z-line means,
+    epsilon_m and the production terms of the mean x gradients."""
+    from oracle.stats import save_stats_chan
+    p = small_params(nx=32, ny=33, nz=24, precision=precision, **NONHOM_CASES[case])
+    gy = grid_for(p)
+    ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=8))
+    try:
+        ch.step(2)
+        o = _oracle_from_gpu(ch, p, gy)
+        sg = ch.stats(homogeneous_x=False)
+        so = save_stats_chan(o, homogeneous_x=False)
+        _compare(sg, so, p)
+        for k in ("epsilon_m", "uu_dudx", "wu_dwdx", "vu_dvdx"):
+            assert np.abs(sg["profiles"][k]).max() > 0, k
+    finally:
+        ch.close()
+
+
+def test_stats_nonhomogeneous_les_matches_oracle(cuda_device):
+    from oracle.stats import save_stats_chan
+    p = small_params(nx=32, ny=33, nz=24, n_th=1, use_les=True, create_new_flow=False, re=400.0,
+                     les_model_type=LES_SMAGORINSKY)
+    gy = grid_for(p)
+    ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=6))
+    try:
+        ch.step(2)
+        nu_t = ch.download_nu_t()
+        o = _oracle_from_gpu(ch, p, gy)
+        sg = ch.stats(homogeneous_x=False)
+        so = save_stats_chan(o, nu_t=nu_t, homogeneous_x=False)
+        _compare(sg, so, p)
+    finally:
+        ch.close()
+
+
+def test_stats_rejects_short_buffers(cuda_device):
     import ctypes
     p = small_params()
     gy = grid_for(p)
     ch = setup_gpu(p, gy, initial_fields(p, gy))
     try:
-        with pytest.raises(_lib.DiabloError) as e:
-            ch.stats(homogeneous_x=False)
-        assert e.value.status == _lib.ERR_UNSUPPORTED
         n = ch.lib.diablo_stats_size(ch.ctx)
         assert n == p.ny * (len(_lib.STAT_PROFILES) + p.n_th * len(_lib.STAT_TH_PROFILES)) \
             + p.nx // 2 + len(_lib.STAT_SCALARS)

@@ -256,3 +256,71 @@ def test_stats_physical_sums_match_parseval(seed):
         close("thrms", s["th"][n]["thrms"], np.sqrt(qt[n]["tt"][J]))
         close("thv", s["th"][n]["thv"], qt[n]["tv"][J])
         close("pe_diss", s["th"][n]["pe_diss"], qt[n]["pe"][J])
+
+
+def test_stats_nonhomogeneous_known_answers():
+    """Branch of IC types 5-8: the means are z-line averages at each x, so a
+    kz = 0 mode is mean flow (no fluctuation), epsilon's x derivatives skip
+    the kz = 0 row, and epsilon_m and the production terms use the mean
+    gradients of those x-dependent means."""
+    from oracle.stats import save_stats_chan
+    p = small_params(nx=32, ny=33, nz=24, n_th=0, grav_y=0.0, re=250.0)
+    gy = grid_for(p)
+    o = _oracle(p, gy)
+    y = o.gyf
+    x = np.arange(o.Nx) * (2 * np.pi / o.Nx)
+    z = np.arange(o.Nz) * (2 * np.pi / o.Nz)
+    cx, sx = np.cos(x)[None, None, :], np.sin(x)[None, None, :]
+    cz = np.cos(z)[None, :, None]
+    one = np.ones((1, o.Nz, o.Nx))
+    U, B, A = 1.0 - y ** 2, 0.2 * np.cos(y), 0.1 * np.sin(2.0 * y)
+    V, D, E = 0.07 * np.cos(y), 0.05 * y, 0.03 * (1 - y ** 2)
+    W = 0.2 * y * (1.0 - y ** 2)
+    c = lambda f: f[:, None, None]
+    _set_phys(o, o.u1, c(U) * one + c(B) * cx + c(A) * cz)
+    _set_phys(o, o.u2, c(V) * cx + cz * (c(D) + c(E) * cx))
+    _set_phys(o, o.u3, c(W) * cx)
+    s = save_stats_chan(o, homogeneous_x=False)
+    c1, c2, c3 = o.u1.c, o.u2.c, o.u3.c
+    U, B, A = c1[:, 0, 0].real, 2 * c1[:, 0, 1].real, 2 * c1[:, 1, 0].real
+    V, D, E = 2 * c2[:, 0, 1].real, 2 * c2[:, 1, 0].real, 4 * c2[:, 1, 1].real
+    W = 2 * c3[:, 0, 1].real
+    gy, gyf, dy, dyf = o.gy, o.gyf, o.dy, o.dyf
+    kx, kz, nu = o.kx[1], o.kz[1], 1.0 / p.re
+    ny = p.ny
+    J = np.arange(1, ny + 1)
+    G = np.arange(2, ny + 1)
+    pr = s["profiles"]
+
+    def close(name, got, want, rel=1e-11):
+        scale = max(np.abs(want).max(), 1e-30)
+        err = np.abs(np.asarray(got) - np.asarray(want)).max() / scale
+        assert err < rel, (name, err)
+    close("urms", pr["urms"], np.abs(A[J]) / math.sqrt(2))
+    close("vrms", pr["vrms"], np.sqrt((D[J] ** 2 + E[J] ** 2 / 2) / 2))
+    assert np.abs(pr["wrms"]).max() < 1e-14
+    IA = (dyf[G - 1] * A[G] + dyf[G] * A[G - 1]) / (2 * dy[G])
+    close("uv", pr["uv"][1:], IA * D[G] / 2)
+    dgy = gy[G + 1] - gy[G - 1]
+    eps = (kx ** 2 * E[G] ** 2 / 4                                                   # dv/dx
+           + kz ** 2 * (dyf[G - 1] * A[G] ** 2 + dyf[G] * A[G - 1] ** 2) / (2 * dy[G]) / 2   # du/dz
+           + kz ** 2 * (D[G] ** 2 + E[G] ** 2 / 2) / 2                              # dv/dz
+           + ((A[G] - A[G - 1]) / dy[G]) ** 2 / 2                                    # du/dy
+           + (((D[G + 1] - D[G - 1]) / dgy) ** 2 + ((E[G + 1] - E[G - 1]) / dgy) ** 2 / 2) / 2)
+    close("epsilon", pr["epsilon"][1:], nu * eps)
+    Bm = np.where(J >= 2, B[J - 1], 0.0)
+    Wm = np.where(J >= 2, W[J - 1], 0.0)
+    epm = (kx ** 2 * (dyf[J - 1] * B[J] ** 2 + dyf[J] * Bm ** 2) / (2 * dy[J]) / 2
+           + kx ** 2 * V[J] ** 2 / 2
+           + kx ** 2 * (dyf[J - 1] * W[J] ** 2 + dyf[J] * Wm ** 2) / (2 * dy[J]) / 2)
+    epm[1:] += (((U[G] - U[G - 1]) / dy[G]) ** 2 + ((B[G] - B[G - 1]) / dy[G]) ** 2 / 2
+                + ((V[G + 1] - V[G - 1]) / dgy) ** 2 / 2 + ((W[G] - W[G - 1]) / dy[G]) ** 2 / 2)
+    close("epsilon_m", pr["epsilon_m"], nu * epm)
+    mke = 0.5 * ((dyf[G - 1] * (U[G] ** 2 + B[G] ** 2 / 2) + dyf[G] * (U[G - 1] ** 2 + B[G - 1] ** 2 / 2))
+                 / (2 * dy[G])
+                 + (dyf[G - 1] * W[G] ** 2 / 2 + dyf[G] * W[G - 1] ** 2 / 2) / (2 * dy[G])
+                 + V[G] ** 2 / 2)
+    close("mke", pr["mke"][1:], mke)
+    close("vv_dvdy", pr["vv_dvdy"][1:], (V[G + 1] - V[G - 1]) / dgy * D[G] * E[G] / 2)
+    for k in ("uu_dudx", "wu_dwdx", "vu_dvdx"):
+        assert np.abs(pr[k]).max() < 1e-13 * max(np.abs(pr["vv_dvdy"]).max(), 1e-30), k
