@@ -98,14 +98,15 @@ template <typename C, typename CO> struct ZFwdArgs {
 };
 
 // Blocks per SM the FP32 z-forward and x-inverse kernels' register caps are
-// set for.  Measured at 256 x 257 x 256: 6 and 7 (80 and 71 registers) took the
-// combine kernel from 0.234 to 0.216 ms and the x inverse from 0.261 to 0.238
-// ms per launch; tighter caps spill and lose part of it.
+// set for.  Measured at 256 x 257 x 256: 6 (80 registers) took the combine
+// kernel from 0.234 to 0.216 ms per launch; tighter caps spill and lose part
+// of it.  The x inverse holds 64 registers without spilling and, with its
+// single row buffer, fits eight blocks per SM.
 #ifndef ZFWD32_MIN_BLOCKS
 #define ZFWD32_MIN_BLOCKS 6
 #endif
 #ifndef XC2R32_MIN_BLOCKS
-#define XC2R32_MIN_BLOCKS 7
+#define XC2R32_MIN_BLOCKS 8
 #endif
 
 template <typename C, typename CO, int N1, int N2, int S, bool COMBINE>
@@ -222,8 +223,17 @@ __global__ void __launch_bounds__(N2* KT, sizeof(C) == 8 ? XC2R32_MIN_BLOCKS : 1
   typedef typename CReal<C>::R T;
   constexpr int M = N1 * N2;
   constexpr int SM = dfft::SmemSize<N1, N2>::v;
-  __shared__ C xs[KT][M + 1];
-  __shared__ C sm[KT][SM];
+  // When the N2 threads of a row share a warp (32 % N2 == 0), one row buffer
+  // holds the spectrum (M + 1 entries) and then the four-step tile: a row is
+  // read and rewritten only by its own threads, so a warp barrier separates
+  // the two uses and the block needs half the shared memory (more blocks per
+  // SM).  Otherwise the two live side by side.
+  constexpr bool ALIAS = 32 % N2 == 0;
+  constexpr int ROW = ALIAS ? (SM > M + 1 ? SM : M + 1) : M + 1 + SM;
+  constexpr int SMOFF = ALIAS ? 0 : M + 1;
+  __shared__ C rowbuf[KT][ROW];
+  auto xs = [&](int rr) -> C* { return rowbuf[rr]; };
+  auto sm = [&](int rr) -> C* { return rowbuf[rr] + SMOFF; };
   const int t = threadIdx.x, r = threadIdx.y;
   const int tid = r * N2 + t;
   const int k0 = blockIdx.x * KT;
@@ -235,29 +245,30 @@ __global__ void __launch_bounds__(N2* KT, sizeof(C) == 8 ? XC2R32_MIN_BLOCKS : 1
     int rr = idx % KT, m = idx / KT;
     C val = czero<C>();
     if (m < nkx1 && k0 + rr < nz) val = src[(size_t)m * nz + k0 + rr];
-    xs[rr][m] = val;
+    xs(rr)[m] = val;
   }
   __syncthreads();
   C v[N1];
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     int m = n1 * N2 + t;
-    C xm = xs[r][m];
-    C xc = conj(xs[r][M - m]);  // m == 0 reads X[M] = 0
+    C xm = xs(r)[m];
+    C xc = conj(xs(r)[M - m]);  // m == 0 reads X[M] = 0
     if (m == 0) xm.y = 0;
     C e = xm + xc;
     C o = xm - xc;
     C w = conj(a.twX[m]);           // exp(+2 pi i m / Nx)
     v[n1] = e + mul_i(cmul(w, o));
   }
-  dfft::step1<N1, N2, +1>(v, t, a.twM, sm[r]);
+  if (ALIAS) __syncwarp();
+  dfft::step1<N1, N2, +1>(v, t, a.twM, sm(r));
   __syncthreads();
   if (k0 + r >= nz) return;
   T* dst = a.dst[f] + ((size_t)j * nz + k0 + r) * a.g.nx;
   C* dstc = reinterpret_cast<C*>(dst);
   for (int k1 = t; k1 < N1; k1 += N2) {
     C u[N2];
-    dfft::step2<N1, N2, +1>(u, k1, sm[r]);
+    dfft::step2<N1, N2, +1>(u, k1, sm(r));
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) dstc[k1 + N1 * k2] = u[k2];
   }
