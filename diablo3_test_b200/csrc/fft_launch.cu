@@ -114,7 +114,7 @@ int launch_xinv(const XInvArgs<C>& a, int m, int nplanes, int nfield, cudaStream
 // ---- x forward ----
 template <typename T, int N1, int N2, bool NL, int KT>
 static void launch_xfwd_k(const XFwdArgs<T>& a, int nplanes, int nfield, cudaStream_t s) {
-  constexpr int SMB = XFwdSmem<T, N1, N2, KT>::bytes;
+  constexpr int SMB = XFwdSmem<T, N1, N2, KT, NL>::bytes;
   cudaFuncSetAttribute(k_xr2c<T, N1, N2, KT, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMB);
   dim3 blk(N2, KT), grd(nfield, (a.g.nz + KT - 1) / KT, nplanes);
   k_xr2c<T, N1, N2, KT, NL><<<grd, blk, SMB, s>>>(a);

@@ -399,19 +399,29 @@ DI void nl_fill(typename CT<T>::C (&v)[N1], const XFwdArgs<T>& a, int f, int q, 
 }
 
 // Shared-memory bytes of k_xr2c for a given configuration.
-template <typename T, int N1, int N2, int KT>
+template <typename T, int N1, int N2, int KT, bool NL = true>
 struct XFwdSmem {
   typedef typename CT<T>::C C;
   static constexpr int M = N1 * N2;
   static constexpr int NKX1 = (2 * M) / 3 + 1;   // upper bound of Nkx+1
   // per row one four-step tile (also used for the natural-order spectrum,
-  // which needs M+1 entries) + the two output tiles
+  // which needs M+1 entries) + the accumulated B output of the NL form (the
+  // A output goes straight to global memory)
   static constexpr int ROWC = dfft::SmemSize<N1, N2>::v > M + 1 ? dfft::SmemSize<N1, N2>::v : M + 1;
-  static constexpr int bytes = (KT * ROWC + 2 * NKX1 * (KT + 1)) * (int)sizeof(C);
+  static constexpr int bytes = (KT * ROWC + (NL ? NKX1 * (KT + 1) : 0)) * (int)sizeof(C);
 };
 
+// Blocks per SM the FP32 products kernel's register cap is set for.  With the
+// A output stored straight to global memory a block holds 30 KB of shared
+// memory, so six fit; at 80 registers (40 bytes spilled) the launch measured
+// 0.660 ms against 0.671 at 96 registers and five blocks (0.726 ms with both
+// outputs staged in shared memory).
+#ifndef XR2C32_MIN_BLOCKS
+#define XR2C32_MIN_BLOCKS 6
+#endif
+
 template <typename T, int N1, int N2, int KT, bool NL>
-__global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? 5 : 1) k_xr2c(XFwdArgs<T> a) {
+__global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BLOCKS : 1) k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   constexpr int M = N1 * N2;
   constexpr int ROWC = XFwdSmem<T, N1, N2, KT>::ROWC;
@@ -421,7 +431,7 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? 5 : 1) k_xr2c
   constexpr int OP = KT + 1;
   extern __shared__ __align__(16) unsigned char xr2c_smem[];
   C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][ROWC] four-step tile / spectrum
-  C* acc = smb + KT * ROWC;                            // [2][NKX1][OP] outputs A, B
+  C* acc = smb + KT * ROWC;                            // [NKX1][OP] output B (NL)
   const int t = threadIdx.x, r = threadIdx.y;
   // field fastest: the blocks that read the same input rows run together
   const int f = blockIdx.x;
@@ -431,6 +441,7 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? 5 : 1) k_xr2c
   const int row = min(k0 + r, nz - 1);
   const size_t ps = (size_t)nz * nx;
   const size_t rowoff = (size_t)j * ps + (size_t)row * nx;
+  C* dstA = a.outA[f] + (size_t)j * nkx1 * nz;
   const T sc = (T)a.scale;
   C* sm = smb + r * ROWC;
   C* zs = sm;  // the natural-order spectrum replaces the tile after step 2
@@ -471,20 +482,21 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? 5 : 1) k_xr2c
         C o = (T)0.5 * (zm - zc);
         C x = sc * (e - mul_i(cmul(a.twX[m], o)));
         // each thread owns its (m, r) entries: no synchronisation needed
-        if (!NL || q == 0) acc[m * OP + r] = x;
-        else if (q == 1) acc[(NKX1 + m) * OP + r] = mul_ik((T)a.kx[m], x);
-        else acc[(NKX1 + m) * OP + r] = acc[(NKX1 + m) * OP + r] + x;
+        // A: straight to global (a warp writes 32-byte runs along k of
+        // 32 / N2 rows for each of its N2 modes)
+        if (!NL || q == 0) { if (k0 + r < nz) dstA[(size_t)m * nz + k0 + r] = x; }
+        else if (q == 1) acc[m * OP + r] = mul_ik((T)a.kx[m], x);
+        else acc[m * OP + r] = acc[m * OP + r] + x;
       }
     }
     __syncthreads();
   }
-  // stores run along k (KT consecutive rows per mode)
-  for (int pass = 0; pass < (NL ? 2 : 1); ++pass) {
-    C* dst = (pass == 0 ? a.outA[f] : a.outB[f]) + (size_t)j * nkx1 * nz;
-    const C* src = acc + pass * NKX1 * OP;
+  // B stores run along k (KT consecutive rows per mode)
+  if (NL) {
+    C* dst = a.outB[f] + (size_t)j * nkx1 * nz;
     for (int idx = r * N2 + t; idx < nkx1 * KT; idx += N2 * KT) {
       int rr = idx % KT, m = idx / KT;
-      if (k0 + rr < nz) dst[(size_t)m * nz + k0 + rr] = src[m * OP + rr];
+      if (k0 + rr < nz) dst[(size_t)m * nz + k0 + rr] = acc[m * OP + rr];
     }
   }
 }
