@@ -110,7 +110,7 @@ struct diablo_ctx {
     double* tmp[2];
     double* thp[2 * DIABLO_MAX_TH];
     double* r[3 + DIABLO_MAX_TH];
-    double *nu_t, *sf, *sg, *c2, *d2;
+    double *nu_t, *sf, *sg;
     double2* xs[NF_MAX];      // x-spectral scratch of the batched transforms
     double *d_cf, *d_cg, *d_d2f, *d_d2g, *d_sclf, *d_sclg;
     double* u64[3 + DIABLO_MAX_TH];   // FP64 velocities/scalars for the solve (mixed precision)
@@ -695,7 +695,7 @@ static int ensure_les(diablo_ctx* ctx) {
   for (int i = 0; i < 2 * ctx->nth; ++i) { AL(L.thg[i], fe); AL(L.thp[i], pe); }
   AL(L.tmp[0], pe); AL(L.tmp[1], pe);
   AL(L.nu_t, pe); AL(L.sf, pe); AL(L.sg, pe);
-  AL(L.c2, pe * ctx->nf); AL(L.d2, pe * ctx->nf);
+
   if ((rc = ensure_xs64(ctx))) return rc;
   const int n = ctx->nyp2;
   AL(L.d_cf, n * sizeof(double)); AL(L.d_cg, n * sizeof(double));
@@ -1094,7 +1094,6 @@ static int substep_les_t(diablo_ctx* ctx, int rk) {
     for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = u64[f]; }
     sa.nu_t = PP(L.nu_t);
     for (int n = 0; n < nth; ++n) sa.kap[n] = PP(model == 5 ? L.kap[n] : L.nu_t);
-    sa.c2 = L.c2; sa.d2 = L.d2;
     sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf;
     sa.nf = nf; sa.nth = nth; sa.n = ctx->nyp2; sa.nyp = ctx->ny; sa.cols = ctx->nz * ctx->nx;
     sa.temp1 = a.temp1; sa.temp2 = a.temp2; sa.nu_v = a.nu_v;
@@ -1108,9 +1107,16 @@ static int substep_les_t(diablo_ctx* ctx, int rk) {
       sa.ubc[i] = a.ubc[i]; sa.vbc[i] = a.vbc[i]; sa.wbc[i] = a.wbc[i];
       sa.uc1[i] = a.uc1[i]; sa.vc1[i] = a.vc1[i]; sa.wc1[i] = a.wc1[i];
     }
-    const size_t threads = (size_t)nf * sa.cols;
+    // one warp per (field, column)
+    const size_t threads = (size_t)nf * sa.cols * 32;
+    const unsigned blocks = (unsigned)((threads + 127) / 128);
     Prof pr(ctx, K_SOLVE);
-    k_phys_solve<P><<<(unsigned)((threads + 127) / 128), 128, 0, ctx->stream>>>(sa);
+    switch (std::max(3, (sa.n + 31) / 32)) {
+#define X(r) case r: k_phys_solve<P, r><<<blocks, 128, 0, ctx->stream>>>(sa); break;
+      X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+      default: return DIABLO_ERR_SIZE;
+    }
   }
   // variable dt: courant on the solved physical velocities (for/channel.f90:885-888)
   if (courant_due(ctx, rk)) {
@@ -1149,7 +1155,8 @@ static int ensure_dyn(diablo_ctx* ctx) {
     if ((rc = dev_alloc(ctx, (void**)&L.dp[q], ptot * sizeof(double)))) return rc;
     if ((rc = dev_alloc(ctx, (void**)&L.df[q], ftot * sizeof(double2)))) return rc;
   }
-  if ((rc = dev_alloc(ctx, (void**)&L.dsums, (size_t)ctx->nyp2 * 12 * sizeof(double)))) return rc;
+  if ((rc = dev_alloc(ctx, (void**)&L.dsums, (size_t)ctx->nyp2 * DYN_MAX_SLICES * 12 * sizeof(double))))
+    return rc;
   L.dyn_ready = 1;
   return 0;
 }
@@ -1192,6 +1199,7 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
     k_test_mask<<<grid1d(ftot), 256, 0, ctx->stream>>>(ma);
   }
   if ((rc = ifft_to<P>(ctx, L.df, L.dp, DYN_NF))) return rc;
+  int nslice_dyn = 1;
   {
     DynContractArgs<P> ca;
     for (int q = 0; q < DYN_NF; ++q) ca.F[q] = PP(L.dp[q]);
@@ -1199,15 +1207,19 @@ static int dynamic_coefficient(diablo_ctx* ctx) {
     ca.d2f = L.d_d2f;
     ca.sums = L.dsums;
     ca.nyp = ctx->ny;
+    // about four blocks per SM over the planes
+    ca.nslice = std::max(1, std::min({DYN_MAX_SLICES, (4 * 148 + ctx->ny - 1) / ctx->ny,
+                                      (int)((ps + 255) / 256)}));
     ca.ps = ps;
     ca.ratio2 = 4.0;   // (2 Delta / Delta)^2
     Prof pr(ctx, K_OTHER);
-    k_dyn_contract<P><<<ctx->ny, 256, 0, ctx->stream>>>(ca);
+    k_dyn_contract<P><<<dim3(ca.nslice, ctx->ny), 256, 0, ctx->stream>>>(ca);
+    nslice_dyn = ca.nslice;
   }
   {
     Prof pr(ctx, K_OTHER);
     k_dyn_coef<<<(ctx->nyp2 + 127) / 128, 128, 0, ctx->stream>>>(L.dsums, ctx->d_dy, ctx->d_dyf, L.d_cf, L.d_cg,
-                                                                  ctx->ny, (double)ps);
+                                                                  ctx->ny, nslice_dyn, (double)ps);
   }
   CK(cudaGetLastError());
   return 0;

@@ -434,16 +434,13 @@ __global__ void k_cf_finish(CfFinishArgs a) {
 // ---------------------------------------------------------------------------
 // Crank-Nicolson in y per physical column with the eddy viscosity
 // (:494-547 explicit half, :625-646 scalars, :657-877 implicit rows, Thomas
-// :1335-1496).  One thread per (field, x-z column); the forward sweep keeps
-// the modified upper diagonal and right-hand side in scratch (c2, d2).
+// :1335-1496).
 template <typename P>
 struct PhysSolveArgs {
   const double* r[SOLVE_NF];    // inverse-transformed cr
   double* u[SOLVE_NF];          // in: physical field at the start; out: solution on the write rows
   const P* nu_t;                // eddy viscosity / diffusivities (the LES model's precision)
   const P* kap[8];
-  double* c2;                   // scratch [nf][n][cols]
-  double* d2;
   const double* dy;
   const double* dyf;
   int nf, nth, n, nyp, cols;
@@ -457,10 +454,18 @@ struct PhysSolveArgs {
   double thc1[8][2];
 };
 
-template <typename P>
-__global__ void k_phys_solve(PhysSolveArgs<P> a) {
-  const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (size_t)a.nf * a.cols) return;
+// One warp per (field, physical column): each lane builds R consecutive rows
+// of the column's system and csolve::warp_tridiag solves it (the partition
+// method of the Fourier-space solves).  Warps of a block take adjacent
+// columns, so the 32-byte sectors of their row loads are shared through L1.
+// Rows past Ny+1 are identity rows; the last real row has no upper
+// coefficient, so they do not couple.
+template <typename P, int R>
+__global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
+  using namespace csolve;
+  const int lane = threadIdx.x & 31;
+  const size_t gid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (gid >= (size_t)a.nf * a.cols) return;   // the whole warp leaves together
   const int f = gid / a.cols;
   const size_t col = gid % a.cols;
   const size_t ps = a.cols;
@@ -468,8 +473,6 @@ __global__ void k_phys_solve(PhysSolveArgs<P> a) {
   const double* r = a.r[f];
   double* u = a.u[f];
   const P* nt = f < 3 ? a.nu_t : a.kap[f - 3];
-  double* c2 = a.c2 + (size_t)f * n * ps + col;
-  double* d2 = a.d2 + (size_t)f * n * ps + col;
   int lo, hi, w0, b0, b1;
   double c0v, c1v, tc;
   if (f == 1) { lo = 2; hi = nyp; w0 = 1; b0 = a.vbc[0]; b1 = a.vbc[1]; c0v = a.vc1[0]; c1v = a.vc1[1]; tc = a.temp1 * a.nu_v; }
@@ -531,29 +534,24 @@ __global__ void k_phys_solve(PhysSolveArgs<P> a) {
       }
     }
   };
-  // Thomas (thomas_forward_real_mpi + thomas_backward_real_mpi at one rank),
-  // kept as x(j) = f(j) - e(j) x(j+1) with e = c/b', f = g'/b' in scratch
-  double A, B, C, D;
-  row(0, A, B, C, D);
-  double bprev = B, cprev = C, gprev = D;
-  c2[0] = C / B;
-  d2[0] = D / B;
-  for (int j = 1; j < n; ++j) {
-    row(j, A, B, C, D);
-    const double aj = -A / bprev;
-    B = B + aj * cprev;
-    D = D + aj * gprev;
-    c2[(size_t)j * ps] = C / B;
-    d2[(size_t)j * ps] = D / B;
-    bprev = B; cprev = C; gprev = D;
+  double Am[R], Bm[R], Cm[R];
+  double2 Dm[R];
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+    const int j = lane * R + rr;
+    double A = 0.0, B = 1.0, C = 0.0, D = 0.0;
+    if (j < n) row(j, A, B, C, D);
+    Am[rr] = A; Bm[rr] = B; Cm[rr] = C; Dm[rr] = make_double2(D, 0.0);
   }
-  // every read of u is done: write the solution on the rows the reference writes
+  warp_tridiag<R>(Am, Bm, Cm, Dm, lane);
+  // every lane's reads of u (its rows and their neighbours) are done: write
+  // the solution on the rows the reference writes
+  __syncwarp();
   const int w1 = nyp + 1;
-  double x = d2[(size_t)(n - 1) * ps];
-  if (n - 1 >= w0 && n - 1 <= w1) u[(size_t)(n - 1) * ps + col] = x;
-  for (int j = n - 2; j >= 0; --j) {
-    x = d2[(size_t)j * ps] - c2[(size_t)j * ps] * x;
-    if (j >= w0 && j <= w1) u[(size_t)j * ps + col] = x;
+#pragma unroll
+  for (int rr = 0; rr < R; ++rr) {
+    const int j = lane * R + rr;
+    if (j < n && j >= w0 && j <= w1) u[(size_t)j * ps + col] = Dm[rr].x;
   }
 }
 
@@ -634,29 +632,33 @@ __global__ void k_test_mask(MaskArgs a) {
   }
 }
 
-// Per-plane Germano/Lilly sums: one block per GYF plane j (blockIdx.x + 1).
-// sums[j][0..5] = sum over the plane of L_ab M_ab per pair, [6..11] of M_ab^2.
+// Per-plane Germano/Lilly sums: `nslice` blocks per GYF plane j
+// (blockIdx.y + 1), each summing a strided share of the plane's points, so a
+// 129-plane grid still fills every SM.  sums[j][slice][0..5] = sum of
+// L_ab M_ab per pair, [6..11] of M_ab^2; k_dyn_coef adds the slices in order.
+constexpr int DYN_MAX_SLICES = 16;
 template <typename P>
 struct DynContractArgs {
   const P* F[DYN_NF];         // test-filtered fields (physical)
   const P* u[3];              // unfiltered u1, u2 (GY), u3
   const double* d2f;          // Delta^2 at GYF
-  double* sums;               // [(Ny+2) * 12]
-  int nyp;
+  double* sums;               // [(Ny+2)][nslice][12]
+  int nyp, nslice;
   size_t ps;
   double ratio2;              // (test / grid width)^2
 };
 
 template <typename P>
 __global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs<P> a) {
-  const int j = blockIdx.x + 1;
+  const int j = blockIdx.y + 1;
   const size_t base = (size_t)j * a.ps;
   double acc[12];
 #pragma unroll
   for (int q = 0; q < 12; ++q) acc[q] = 0.0;
   const double w2[6] = {1.0, 1.0, 1.0, 2.0, 2.0, 2.0};
   const double d2 = a.d2f[j];
-  for (size_t p = threadIdx.x; p < a.ps; p += blockDim.x) {
+  for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.ps;
+       p += (size_t)a.nslice * blockDim.x) {
     const size_t o = base + p;
     double Uh[3], Sh[6];
 #pragma unroll
@@ -687,14 +689,14 @@ __global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs<P> a) {
   if (threadIdx.x < 12) {
     double v = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][threadIdx.x];
-    a.sums[(size_t)j * 12 + threadIdx.x] = v;
+    a.sums[((size_t)j * a.nslice + blockIdx.x) * 12 + threadIdx.x] = v;
   }
 }
 
 // C(y) at GYF from the plane sums, and interpolated to GY (for/les.f90's
 // GYF-to-GY weights); one thread per plane, planes 0..Ny+1.
 __global__ void k_dyn_coef(const double* sums, const double* dy, const double* dyf, double* cf, double* cg,
-                           int nyp, double nps) {
+                           int nyp, int nslice, double nps) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > nyp + 1) return;
   const double w2[6] = {1.0, 1.0, 1.0, 2.0, 2.0, 2.0};
@@ -702,8 +704,13 @@ __global__ void k_dyn_coef(const double* sums, const double* dy, const double* d
     if (jj < 1 || jj > nyp) return 0.0;
     double num = 0.0, den = 0.0;
     for (int q = 0; q < 6; ++q) {
-      num += w2[q] * (sums[(size_t)jj * 12 + q] / nps);
-      den += w2[q] * (sums[(size_t)jj * 12 + 6 + q] / nps);
+      double sn = 0.0, sd = 0.0;
+      for (int sl = 0; sl < nslice; ++sl) {
+        sn += sums[((size_t)jj * nslice + sl) * 12 + q];
+        sd += sums[((size_t)jj * nslice + sl) * 12 + 6 + q];
+      }
+      num += w2[q] * (sn / nps);
+      den += w2[q] * (sd / nps);
     }
     return den > 0.0 ? num / den : 0.0;
   };
