@@ -113,6 +113,7 @@ struct diablo_ctx {
     double *nu_t, *sf, *sg;
     double2* xs[NF_MAX];      // x-spectral scratch of the batched transforms
     double *d_cf, *d_cg, *d_d2f, *d_d2g, *d_sclf, *d_sclg;
+    double *d_idy, *d_idyf;   // 1/dy, 1/dyf (physical-space CN rows)
     double* u64[3 + DIABLO_MAX_TH];   // FP64 velocities/scalars for the solve (mixed precision)
     int nu_t_fp32;                    // nu_t was last written by the FP32 model
     int amd_ready;            // AMD models: rotation, invariant strain, gradients
@@ -701,6 +702,7 @@ static int ensure_les(diablo_ctx* ctx) {
   AL(L.d_cf, n * sizeof(double)); AL(L.d_cg, n * sizeof(double));
   AL(L.d_d2f, n * sizeof(double)); AL(L.d_d2g, n * sizeof(double));
   AL(L.d_sclf, n * sizeof(double)); AL(L.d_sclg, n * sizeof(double));
+  AL(L.d_idy, n * sizeof(double)); AL(L.d_idyf, n * sizeof(double));
 #undef AL
   // filter widths Delta^2 and the constant-model scalings (for/les.f90:224-245)
   std::vector<double> d2f(n, 0.0), d2g(n, 0.0), cf(n, 0.0), cg(n, 0.0), sclf(n, 1.0), sclg(n, 1.0);
@@ -739,6 +741,12 @@ static int ensure_les(diablo_ctx* ctx) {
   CK(cudaMemcpyAsync(L.d_cg, cg.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(L.d_sclf, sclf.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(L.d_sclg, sclg.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  // 1/dy, 1/dyf for the physical-space CN rows (dy(0) is not a grid spacing)
+  std::vector<double> idy(n, 0.0), idyf(n, 0.0);
+  for (int j = 1; j < n; ++j) idy[j] = 1.0 / ctx->h_dy[j];
+  for (int j = 0; j < n; ++j) idyf[j] = 1.0 / ctx->h_dyf[j];
+  CK(cudaMemcpyAsync(L.d_idy, idy.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(L.d_idyf, idyf.data(), n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   L.ready = 1;
   return 0;
@@ -1094,7 +1102,7 @@ static int substep_les_t(diablo_ctx* ctx, int rk) {
     for (int f = 0; f < nf; ++f) { sa.r[f] = L.r[f]; sa.u[f] = u64[f]; }
     sa.nu_t = PP(L.nu_t);
     for (int n = 0; n < nth; ++n) sa.kap[n] = PP(model == 5 ? L.kap[n] : L.nu_t);
-    sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf;
+    sa.dy = ctx->d_dy; sa.dyf = ctx->d_dyf; sa.idy = L.d_idy; sa.idyf = L.d_idyf;
     sa.nf = nf; sa.nth = nth; sa.n = ctx->nyp2; sa.nyp = ctx->ny; sa.cols = ctx->nz * ctx->nx;
     sa.temp1 = a.temp1; sa.temp2 = a.temp2; sa.nu_v = a.nu_v;
     sa.jstart = ctx->jstart; sa.jend = ctx->jend;

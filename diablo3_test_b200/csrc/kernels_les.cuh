@@ -443,6 +443,8 @@ struct PhysSolveArgs {
   const P* kap[8];
   const double* dy;
   const double* dyf;
+  const double* idy;            // 1/dy, 1/dyf
+  const double* idyf;
   int nf, nth, n, nyp, cols;
   double temp1, temp2, nu_v;
   int jstart, jend;
@@ -494,25 +496,28 @@ __global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
       const size_t o = (size_t)j * ps + col;
       const double uc = u[o], um = u[o - ps], up = u[o + ps];
       double rhs = r[o];
+      // the reference's quotients by dy and dyf, as products with the
+      // precomputed reciprocals (FP64 division is a long instruction sequence)
       if (f == 1) {
-        const double dyj = a.dy[j], dyfj = a.dyf[j], dyfm = a.dyf[j - 1];
-        rhs += tc * (((up - uc) / dyfj - (uc - um) / dyfm) / dyj);
+        const double idyj = a.idy[j], idyfj = a.idyf[j], idyfm = a.idyf[j - 1];
         const double ntp = 0.5 * (nt[o] + nt[o + ps]), ntm = 0.5 * (nt[o] + nt[o - ps]);
-        rhs += a.temp2 * ((ntp * (up - uc) / dyfj - ntm * (uc - um) / dyfm) / dyj);
-        A = -tc / (dyfm * dyj) - a.temp2 * ntm / (dyfm * dyj);
-        B = 1. + tc / (dyfj * dyj) + tc / (dyfm * dyj) + a.temp2 * ntp / (dyfj * dyj) + a.temp2 * ntm / (dyfm * dyj);
-        C = -tc / (dyfj * dyj) - a.temp2 * ntp / (dyfj * dyj);
+        const double gp = (up - uc) * idyfj, gm = (uc - um) * idyfm;
+        rhs += tc * ((gp - gm) * idyj);
+        rhs += a.temp2 * ((ntp * gp - ntm * gm) * idyj);
+        const double wp = idyfj * idyj, wm = idyfm * idyj;
+        A = -(tc + a.temp2 * ntm) * wm;
+        B = 1. + (tc + a.temp2 * ntp) * wp + (tc + a.temp2 * ntm) * wm;
+        C = -(tc + a.temp2 * ntp) * wp;
       } else {
-        const double dyj = a.dy[j], dyj1 = a.dy[j + 1], dyfj = a.dyf[j];
-        rhs += tc * (((up - uc) / dyj1 - (uc - um) / dyj) / dyfj);
+        const double idyj = a.idy[j], idyj1 = a.idy[j + 1], idyfj = a.idyf[j];
         const double ntp = nt[o + ps], ntc = nt[o];
-        rhs += a.temp2 * ((ntp * (up - uc) / dyj1 - ntc * (uc - um) / dyj) / dyfj);
-        A = -tc / (dyj * dyfj) - a.temp2 * ntc / (dyj * dyfj);
-        // u1/u3 keep the reference's form of the diagonal (:785), the scalars theirs (:668)
-        B = f < 3 ? 1. - tc * (-1. / (dyj1 * dyfj) - 1. / (dyj * dyfj))
-                  : 1. + tc / (dyj1 * dyfj) + tc / (dyj * dyfj);
-        B = B + a.temp2 * ntp / (dyj1 * dyfj) + a.temp2 * ntc / (dyj * dyfj);
-        C = -tc / (dyj1 * dyfj) - a.temp2 * ntp / (dyj1 * dyfj);
+        const double gp = (up - uc) * idyj1, gm = (uc - um) * idyj;
+        rhs += tc * ((gp - gm) * idyfj);
+        rhs += a.temp2 * ((ntp * gp - ntc * gm) * idyfj);
+        const double wp = idyj1 * idyfj, wm = idyj * idyfj;
+        A = -(tc + a.temp2 * ntc) * wm;
+        B = 1. + (tc + a.temp2 * ntp) * wp + (tc + a.temp2 * ntc) * wm;
+        C = -(tc + a.temp2 * ntp) * wp;
       }
       D = rhs;
     }
