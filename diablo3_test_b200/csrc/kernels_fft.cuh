@@ -99,8 +99,8 @@ template <typename C, typename CO> struct ZFwdArgs {
 
 // Blocks per SM the FP32 z-forward and x-inverse kernels' register caps are
 // set for.  Measured at 256 x 257 x 256: 6 (80 registers) took the combine
-// kernel from 0.234 to 0.216 ms per launch; tighter caps spill and lose part
-// of it.  The x inverse holds 64 registers without spilling and, with its
+// kernel from 0.234 to 0.216 ms per launch; 7 (72 registers) spills and
+// measured 0.220.  The x inverse holds 64 registers without spilling and, with its
 // single row buffer, fits eight blocks per SM.
 #ifndef ZFWD32_MIN_BLOCKS
 #define ZFWD32_MIN_BLOCKS 6
@@ -415,7 +415,8 @@ struct XFwdSmem {
 // A output stored straight to global memory a block holds 30 KB of shared
 // memory, so six fit; at 80 registers (40 bytes spilled) the launch measured
 // 0.660 ms against 0.671 at 96 registers and five blocks (0.726 ms with both
-// outputs staged in shared memory).
+// outputs staged in shared memory) and 0.701 at seven blocks (72 registers,
+// 80 bytes spilled).
 #ifndef XR2C32_MIN_BLOCKS
 #define XR2C32_MIN_BLOCKS 6
 #endif
