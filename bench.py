@@ -515,6 +515,17 @@ def run_ours(args):
     else:
         torch.cuda.set_device(local)
     torch.cuda.init()
+    if args.profile_les:
+        # profiling run of the dynamic-LES workload (128 x 129 x 128), no JSON line
+        p, gy, fields = ics.config_c3(2)
+        ch = setup_channel(p, gy, fields, FP64 if args.precision == "fp64" else MIXED)
+        stream = torch.cuda.Stream()
+        ch.set_stream(stream.cuda_stream)
+        ch.step(args.warmup)
+        ms = timed_steps(ch, torch, stream, args.steps)
+        print(f"profiling run LES 128x129x128 dynamic: {ms / max(args.steps, 1):.3f} ms/step")
+        ch.close()
+        return
     p, gy = ics.config_c2()
     if args.grid:
         import dataclasses
@@ -685,6 +696,8 @@ def main():
                     help="profiling: run a smaller grid of the same workload (no JSON contract)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="profiling: run one precision only")
+    ap.add_argument("--profile-les", action="store_true",
+                    help="profiling: time the dynamic-LES workload instead (mixed unless --precision fp64)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -2006,8 +2006,10 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     ctx->launches++;
     CK(cudaGetLastError());
   }
+  // the z-line arrays come back only when they were formed
   std::vector<double> h(total);
-  CK(cudaMemcpyAsync(h.data(), ctx->d_stats, total * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(h.data(), ctx->d_stats, (zline ? total : total - n_xy) * sizeof(double),
+                     cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
 
@@ -2057,19 +2059,16 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   // along x in the homogeneous branch, :811-836)
   typedef std::vector<double> Vec;
   const size_t xyn = (size_t)nyp2 * nx;
-  Vec ume_xy(xyn), vme_xy(xyn), wme_xy(xyn), uu_xy(xyn), vv_xy(xyn), uw_xy(xyn), uv_xy(xyn), wv_xy(xyn);
-  auto XY = [&](const Vec& v, int j, int i) { return v[(size_t)j * nx + i]; };
+  // (held only in the z-line branch; elsewhere XY falls back to the profile)
+  Vec ume_xy, vme_xy, wme_xy, uu_xy, vv_xy, uw_xy, uv_xy, wv_xy;
+  auto XY = [&](const Vec& v, const Vec& prof, int j, int i) {
+    return v.empty() ? prof[j] : v[(size_t)j * nx + i];
+  };
   if (zline) {
     Vec* dst[XY_N] = {&ume_xy, &vme_xy, &wme_xy, &uu_xy, &vv_xy, &uw_xy, &uv_xy, &wv_xy};
-    for (int q = 0; q < XY_N; ++q) std::copy(xyd + q * xyn, xyd + (q + 1) * xyn, dst[q]->begin());
-  } else {
-    for (int j = 0; j < nyp2; ++j)
-      for (int i = 0; i < nx; ++i) {
-        const size_t o = (size_t)j * nx + i;
-        ume_xy[o] = ume[j]; vme_xy[o] = vme[j]; wme_xy[o] = wme[j];
-        uu_xy[o] = uu[j]; vv_xy[o] = vv[j]; uw_xy[o] = uw[j]; uv_xy[o] = uv[j]; wv_xy[o] = wv[j];
-      }
+    for (int q = 0; q < XY_N; ++q) dst[q]->assign(xyd + q * xyn, xyd + (q + 1) * xyn);
   }
+  const Vec zero(nyp2, 0.0);
   // x profiles of the kz = 0 rows: value or x derivative (ikx, reference
   // wavenumbers) at x_i, the C2R sum Re c_0 + 2 sum_m Re(c_m e^{2 pi i m i/Nx})
   const std::vector<double>& hkx = ctx->h_kx;
@@ -2093,8 +2092,9 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
       }
     }
   };
-  Vec dudx_m(xyn, 0.0), dvdx_m(xyn, 0.0), dwdx_m(xyn, 0.0);
+  Vec dudx_m, dvdx_m, dwdx_m;
   if (nonhom) {
+    dudx_m.assign(xyn, 0.0); dvdx_m.assign(xyn, 0.0); dwdx_m.assign(xyn, 0.0);
     xprof(0, true, dudx_m);
     xprof(1, true, dvdx_m);
     xprof(2, true, dwdx_m);
@@ -2118,8 +2118,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     if (ctx->nz > 1) {   // production terms on GYF (:1486-1494)
       double a = 0.0, b = 0.0;
       for (int i = 0; i < nx; ++i) {
-        a += XY(uu_xy, j, i) * XY(dudx_m, j, i);
-        b += XY(uw_xy, j, i) * XY(dwdx_m, j, i);
+        a += XY(uu_xy, uu, j, i) * XY(dudx_m, zero, j, i);
+        b += XY(uw_xy, uw, j, i) * XY(dwdx_m, zero, j, i);
       }
       set(DIABLO_STAT_UU_DUDX, j, a / nx);
       set(DIABLO_STAT_WU_DWDX, j, b / nx);
@@ -2127,15 +2127,15 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     if (nonhom) {   // compute_MKE_diss (:1150-1262), rows 1..Ny
       double e = 0.0;
       for (int i = 0; i < nx; ++i) {
-        const double su = XY(dudx_m, j, i), sum_ = j >= 2 ? XY(dudx_m, j - 1, i) : 0.0;
-        const double sw = XY(dwdx_m, j, i), swm = j >= 2 ? XY(dwdx_m, j - 1, i) : 0.0;
+        const double su = XY(dudx_m, zero, j, i), sum_ = j >= 2 ? XY(dudx_m, zero, j - 1, i) : 0.0;
+        const double sw = XY(dwdx_m, zero, j, i), swm = j >= 2 ? XY(dwdx_m, zero, j - 1, i) : 0.0;
         e += (dyf[j - 1] * su * su + dyf[j] * sum_ * sum_) / (2.0 * dy[j]);
-        e += XY(dvdx_m, j, i) * XY(dvdx_m, j, i);
+        e += XY(dvdx_m, zero, j, i) * XY(dvdx_m, zero, j, i);
         e += (dyf[j - 1] * sw * sw + dyf[j] * swm * swm) / (2.0 * dy[j]);
         if (j >= 2) {
-          const double tu = (XY(ume_xy, j, i) - XY(ume_xy, j - 1, i)) / dy[j];
-          const double tv = (XY(vme_xy, j + 1, i) - XY(vme_xy, j - 1, i)) / (gy[j + 1] - gy[j - 1]);
-          const double tw = (XY(wme_xy, j, i) - XY(wme_xy, j - 1, i)) / dy[j] + tws;
+          const double tu = (XY(ume_xy, ume, j, i) - XY(ume_xy, ume, j - 1, i)) / dy[j];
+          const double tv = (XY(vme_xy, vme, j + 1, i) - XY(vme_xy, vme, j - 1, i)) / (gy[j + 1] - gy[j - 1]);
+          const double tw = (XY(wme_xy, wme, j, i) - XY(wme_xy, wme, j - 1, i)) / dy[j] + tws;
           e += tu * tu + tv * tv + tw * tw;
         }
       }
@@ -2150,10 +2150,10 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     if (ctx->nz > 1) {   // production terms on GY (:1496-1532)
       double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
       for (int i = 0; i < nx; ++i) {
-        a += XY(uv_xy, j, i) * XY(dvdx_m, j, i);
-        b += (XY(vme_xy, j + 1, i) - XY(vme_xy, j - 1, i)) / (gy[j + 1] - gy[j - 1]) * XY(vv_xy, j, i);
-        c += (XY(ume_xy, j, i) - XY(ume_xy, j - 1, i)) / dy[j] * XY(uv_xy, j, i);
-        d += ((XY(wme_xy, j, i) - XY(wme_xy, j - 1, i)) / dy[j] + tws) * XY(wv_xy, j, i);
+        a += XY(uv_xy, uv, j, i) * XY(dvdx_m, zero, j, i);
+        b += (XY(vme_xy, vme, j + 1, i) - XY(vme_xy, vme, j - 1, i)) / (gy[j + 1] - gy[j - 1]) * XY(vv_xy, vv, j, i);
+        c += (XY(ume_xy, ume, j, i) - XY(ume_xy, ume, j - 1, i)) / dy[j] * XY(uv_xy, uv, j, i);
+        d += ((XY(wme_xy, wme, j, i) - XY(wme_xy, wme, j - 1, i)) / dy[j] + tws) * XY(wv_xy, wv, j, i);
       }
       set(DIABLO_STAT_VU_DVDX, j, a / nx);
       set(DIABLO_STAT_VV_DVDY, j, b / nx);
@@ -2163,10 +2163,10 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     // MKE on GY (:133-150)
     double mk = 0.0;
     for (int i = 0; i < nx; ++i) {
-      const double u0 = XY(ume_xy, j, i), u1m = XY(ume_xy, j - 1, i);
-      const double wa = XY(wme_xy, j, i) + tws * (gyf[j] - 0.5 * p.ly);
-      const double wb = XY(wme_xy, j - 1, i) + tws * (gyf[j - 1] - 0.5 * p.ly);
-      const double v0 = XY(vme_xy, j, i);
+      const double u0 = XY(ume_xy, ume, j, i), u1m = XY(ume_xy, ume, j - 1, i);
+      const double wa = XY(wme_xy, wme, j, i) + tws * (gyf[j] - 0.5 * p.ly);
+      const double wb = XY(wme_xy, wme, j - 1, i) + tws * (gyf[j - 1] - 0.5 * p.ly);
+      const double v0 = XY(vme_xy, vme, j, i);
       mk += (dyf[j - 1] * u0 * u0 + dyf[j] * u1m * u1m) / (2.0 * dy[j]) +
             (dyf[j - 1] * wa * wa + dyf[j] * wb * wb) / (2.0 * dy[j]) + v0 * v0;
     }
@@ -2179,16 +2179,16 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   sc[DIABLO_STAT_URMS_B] = sqrt(integrate_y(uu));
   sc[DIABLO_STAT_VRMS_B] = sqrt(integrate_y(vv));
   sc[DIABLO_STAT_WRMS_B] = sqrt(integrate_y(ww));
-  Vec thme_xy(xyn);
+  Vec thme_xy;
   for (int n = 0; n < nth; ++n) {
     double* base = out + (size_t)ny * (DIABLO_STAT_NPROF + n * DIABLO_STAT_NTHPROF);
     auto tset = [&](int r, int j, double v) { base[(size_t)r * ny + (j - 1)] = v; };
     std::vector<double> thme(nyp2);
     for (int j = 0; j < nyp2; ++j) thme[j] = means[(size_t)j * (4 + nth) + 4 + n];
-    if (zline) xprof(3 + n, false, thme_xy);
-    else
-      for (int j = 0; j < nyp2; ++j)
-        for (int i = 0; i < nx; ++i) thme_xy[(size_t)j * nx + i] = thme[j];
+    if (zline) {
+      thme_xy.assign(xyn, 0.0);
+      xprof(3 + n, false, thme_xy);
+    }
     for (int j = 1; j <= ny; ++j) {
       const int q0 = STAT_NQV + STAT_NQT * n;
       tset(DIABLO_STAT_THME, j, thme[j]);
@@ -2199,8 +2199,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
       // thv_m (:377-385), gx(i) = i Lx / Nx
       double s = 0.0;
       for (int i = 0; i < nx; ++i)
-        s = s + (XY(thme_xy, j, i) + p.dthdx[n] * ((i * p.lx) / nx - 0.5 * p.lx)) *
-                    (0.5 * (XY(vme_xy, j, i) + XY(vme_xy, j + 1, i)));
+        s = s + (XY(thme_xy, thme, j, i) + p.dthdx[n] * ((i * p.lx) / nx - 0.5 * p.lx)) *
+                    (0.5 * (XY(vme_xy, vme, j, i) + XY(vme_xy, vme, j + 1, i)));
       tset(DIABLO_STAT_THV_M, j, s / nx);
     }
   }
