@@ -111,37 +111,39 @@ DI void load_tile(void* tile, const void* g, bool fp32, size_t ps, size_t cbase,
 }  // namespace csolve2
 
 namespace csolve2 {
-// warp_tridiag with b supplied row by row (it is only read by the forward sweep)
-template <int R, typename BF>
-DI void warp_tridiag_b(double (&a)[R], BF bf, double (&c)[R], double2 (&d)[R], int lane) {
+// warp_tridiag with b supplied row by row (it is only read by the forward
+// sweep) and a, c reached through accessors returning double&, so that the
+// caller can keep them in registers it has no other use for at that point
+template <int R, typename AF, typename BF, typename CF>
+DI void warp_tridiag_b(AF a, BF bf, CF c, double2 (&d)[R], int lane) {
   using namespace csolve;
 #pragma unroll
   for (int r = 0; r < 2; ++r) {
     double ib = 1.0 / bf(r);
-    a[r] *= ib; c[r] *= ib; d[r] = ib * d[r];
+    a(r) *= ib; c(r) *= ib; d[r] = ib * d[r];
   }
 #pragma unroll
   for (int r = 2; r < R; ++r) {
-    double ib = 1.0 / (bf(r) - a[r] * c[r - 1]);
-    d[r] = ib * (d[r] - a[r] * d[r - 1]);
-    a[r] = -ib * a[r] * a[r - 1];
-    c[r] = ib * c[r];
+    double ib = 1.0 / (bf(r) - a(r) * c(r - 1));
+    d[r] = ib * (d[r] - a(r) * d[r - 1]);
+    a(r) = -ib * a(r) * a(r - 1);
+    c(r) = ib * c(r);
   }
 #pragma unroll
   for (int r = R - 3; r >= 1; --r) {
-    d[r] = d[r] - c[r] * d[r + 1];
-    a[r] = a[r] - c[r] * a[r + 1];
-    c[r] = -c[r] * c[r + 1];
+    d[r] = d[r] - c(r) * d[r + 1];
+    a(r) = a(r) - c(r) * a(r + 1);
+    c(r) = -c(r) * c(r + 1);
   }
   {
-    double ib = 1.0 / (1.0 - c[0] * a[1]);
-    d[0] = ib * (d[0] - c[0] * d[1]);
-    a[0] = ib * a[0];
-    c[0] = -ib * c[0] * c[1];
+    double ib = 1.0 / (1.0 - c(0) * a(1));
+    d[0] = ib * (d[0] - c(0) * d[1]);
+    a(0) = ib * a(0);
+    c(0) = -ib * c(0) * c(1);
   }
-  const double as = a[0], gs = c[0];
+  const double as = a(0), gs = c(0);
   const double2 ds = d[0];
-  const double ae = a[R - 1], ge = c[R - 1];
+  const double ae = a(R - 1), ge = c(R - 1);
   const double2 de = d[R - 1];
   double ae_m = __shfl_up_sync(0xffffffffu, ae, 1);
   double ge_m = __shfl_up_sync(0xffffffffu, ge, 1);
@@ -176,7 +178,7 @@ DI void warp_tridiag_b(double (&a)[R], BF bf, double (&c)[R], double2 (&d)[R], i
   d[0] = S;
   d[R - 1] = E;
 #pragma unroll
-  for (int r = 1; r < R - 1; ++r) d[r] = d[r] - a[r] * S - c[r] * E;
+  for (int r = 1; r < R - 1; ++r) d[r] = d[r] - a(r) * S - c(r) * E;
 }
 }  // namespace csolve2
 
@@ -577,26 +579,29 @@ __global__ void __launch_bounds__(128, t2_min_blocks<R>()) k_column_tiles(const 
         break;
       }
       case OP_POISSON: {
-        double Am[R], Cm[R];
+        // cf is dead here (every field's NL step has stored it and the next
+        // field's own step resets it): its .x and .y hold the sub- and
+        // super-diagonal, which keeps the solve within the register cap
         const double k2n = -kxm * kxm - kzq * kzq;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int j = j0 + r;
-          Am[r] = 0.0; Cm[r] = 0.0;
+          double am = 0.0, cm = 0.0;
           double2 d = z2;
           if (j >= 1 && j <= nyp) {
-            Am[r] = met[MET_PA * n + j];
-            Cm[r] = met[MET_PC * n + j];
+            am = met[MET_PA * n + j];
+            cm = met[MET_PC * n + j];
             d = dv[r];
           }
-          if (j == 1) { Am[r] = 0; Cm[r] = m00 ? 0.0 : -1.0; d = z2; }
-          if (j == nyp) { Am[r] = 1; Cm[r] = 0; d = z2; }
+          if (j == 1) { am = 0; cm = m00 ? 0.0 : -1.0; d = z2; }
+          if (j == nyp) { am = 1; cm = 0; d = z2; }
+          cf[r] = make_double2(am, cm);
           cr[r] = d;
         }
-        warp_tridiag_b<R>(Am, [&](int r) -> double {
+        warp_tridiag_b<R>([&](int r) -> double& { return cf[r].x; }, [&](int r) -> double {
           const int j = j0 + r;
           return (j == 1) ? 1.0 : (j == nyp ? -1.0 : ((j > 1 && j < nyp) ? k2n + met[MET_PB0 * n + j] : 1.0));
-        }, Cm, cr, lane);  // cr = phi from here on
+        }, [&](int r) -> double& { return cf[r].y; }, cr, lane);  // cr = phi from here on
         break;
       }
       case OP_PROJ: {
