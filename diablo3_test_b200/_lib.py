@@ -34,7 +34,7 @@ STAT_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw",
                  "dudy", "dwdy", "cp", "shear", "omega_x", "omega_y", "omega_z",
                  "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
 STAT_TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
-STAT_SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b")
+STAT_SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b", "bpe")
 
 # every symbol include/diablo_gpu.h declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p

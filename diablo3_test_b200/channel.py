@@ -52,7 +52,8 @@ MEAN_H5_NAMES = {
     "epsilon_m": "epsilon_m", "nu_sgs": "nu_sgs", "eps_sgs2": "eps_sgs2",
     "thme": "thme{:02d}", "dthdy": "dthdz{:02d}", "thrms": "thrms{:02d}", "thv": "thw{:02d}",
     "thv_m": "thw{:02d}_m", "pe_diss": "pe_diss{:02d}", "spectrum": "FTx_uu",
-    "u1y_left_b": "u1z_x0", "time": "time",
+    "u1y_left_b": "u1z_x0", "time": "time", "bpe": "BPE", "th1_pdf": "th1PDF",
+    "th1_bin": "th1bin",
 }
 
 
@@ -146,7 +147,8 @@ class Channel:
         does.  Returns ``{"profiles": {name: (Ny,)},
         "th": [{name: (Ny,)} per scalar], "spectrum": (Nx/2,), "scalars":
         {name: float}}`` with the reference's internal names (MEAN_H5_NAMES
-        gives the dataset each one is written to)."""
+        gives the dataset each one is written to); with scalars also
+        "th1_pdf" and "th1_bin" (Nx,) of compute_BPE and scalars["bpe"]."""
         p = self.params
         n = self.lib.diablo_stats_size(self.ctx)
         if n < 0:
@@ -162,8 +164,16 @@ class Channel:
             th.append({k: out[b + r * ny:b + (r + 1) * ny].copy() for r, k in enumerate(_lib.STAT_TH_PROFILES)})
         b = (npf + p.n_th * ntp) * ny
         spec = out[b:b + p.nx // 2].copy()
-        sc = {k: float(v) for k, v in zip(_lib.STAT_SCALARS, out[b + p.nx // 2:])}
-        return {"profiles": prof, "th": th, "spectrum": spec, "scalars": sc}
+        b += p.nx // 2
+        res = {"profiles": prof, "th": th, "spectrum": spec}
+        if p.n_th > 0:   # compute_BPE's PDF of th_1 and its lower bin edges
+            res["th1_pdf"] = out[b:b + p.nx].copy()
+            res["th1_bin"] = out[b + p.nx:b + 2 * p.nx].copy()
+            b += 2 * p.nx
+        res["scalars"] = {k: float(v) for k, v in zip(_lib.STAT_SCALARS, out[b:])}
+        if p.n_th == 0:
+            del res["scalars"]["bpe"]
+        return res
 
     # -- reference surface ---------------------------------------------
     def fft_xz_to_fourier(self, v, vv):

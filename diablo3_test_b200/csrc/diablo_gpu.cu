@@ -1860,7 +1860,8 @@ int diablo_filter_chan(diablo_ctx* ctx, int n) {
 
 int diablo_stats_size(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
-  return ctx->ny * (DIABLO_STAT_NPROF + ctx->nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2 + DIABLO_STAT_NSCALAR;
+  return ctx->ny * (DIABLO_STAT_NPROF + ctx->nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2 +
+         (ctx->nth > 0 ? 2 * ctx->nx : 0) + DIABLO_STAT_NSCALAR;
 }
 
 int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
@@ -1890,8 +1891,9 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   auto even = [](size_t v) { return (v + 1) & ~(size_t)1; };
   const size_t n_part = even((size_t)nyp2 * nslice * STAT_NQ), n_means = even((size_t)nyp2 * (4 + nth));
   const size_t n_spec = even((size_t)nyp2 * nkx1), n_les = even((size_t)nyp2 * lslice * 2);
-  const size_t n_rows = (size_t)nyp2 * (3 + nth) * nkx1 * 2, n_xy = (size_t)XY_N * nyp2 * nx;
-  const size_t total = n_part + n_means + n_spec + n_les + n_rows + n_xy;
+  const size_t n_rows = (size_t)nyp2 * (3 + nth) * nkx1 * 2, n_bpe = even((size_t)nx);
+  const size_t n_xy = (size_t)XY_N * nyp2 * nx;
+  const size_t total = n_part + n_means + n_spec + n_les + n_rows + n_bpe + n_xy;
   if (ctx->stats_doubles < total) {
     if ((rc = dev_alloc(ctx, (void**)&ctx->d_stats, total * sizeof(double)))) return rc;
     ctx->stats_doubles = total;
@@ -1901,7 +1903,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   double* d_spec = d_means + n_means;
   double* d_les = d_spec + n_spec;
   double* d_rows = d_les + n_les;
-  double* d_xy = d_rows + n_rows;
+  double* d_bpe = d_rows + n_rows;
+  double* d_xy = d_bpe + n_bpe;
   CK(cudaMemsetAsync(ctx->d_stats, 0, total * sizeof(double), ctx->stream));
   const double d0 = nth > 0 ? p.dthdx[0] : 0.0;
   // (1/(Ro_inv/delta)) dTHdX(1), the thermal-wind shear; 0 without a background gradient
@@ -2006,6 +2009,46 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     ctx->launches++;
     CK(cudaGetLastError());
   }
+  // compute_BPE on th_1 (:1755-1876, called for n = 1): its physical FP64 field
+  // in b_phys, after every earlier reader of b_phys in stream order
+  const int nbin = nx;
+  double bthmin = 0.0, bthmax = 0.0, bdth = 0.0, broden = 0.0;
+  if (nth > 0) {
+    if ((rc = ensure_bscratch(ctx))) return rc;
+    if ((rc = inv_four_to_phys(ctx, ctx->st[ctx->cur][4], ctx->b_xs, ctx->b_phys))) return rc;
+    StatsBpeArgs e;
+    memset(&e, 0, sizeof(e));
+    e.th = ctx->b_phys;
+    e.dyf = ctx->d_dyf;
+    e.dthdx = p.dthdx[0];
+    e.lx = p.lx;
+    e.even = nonhom ? 1 : 0;
+    if (nonhom) {
+      // the literal 1.1 is single precision in the reference
+      bthmin = -p.dthdx[0] * 0.5 * p.lx * (double)1.1f;
+      bthmax = p.dthdx[0] * 0.5 * p.lx * (double)1.1f;
+      bdth = (bthmax - bthmin) / nbin + 1.e-14;
+    } else {
+      bthmin = -ctx->ro_inv;
+      bthmax = ctx->ro_inv;
+      broden = ctx->ro_inv + 1.e-14;
+    }
+    e.thmin = bthmin;
+    e.thmax = bthmax;
+    e.dth = bdth;
+    e.roden = broden;
+    e.pi_ref = PI_REF;
+    e.nx = nx;
+    e.nz = ctx->nz;
+    e.jlo = ctx->jst[0];
+    e.jhi = ctx->jet[0];
+    e.nbin = nbin;
+    e.pdf = d_bpe;
+    Prof pr(ctx, K_OTHER);
+    k_stats_bpe<<<4 * nsm, 256, nbin * sizeof(double), ctx->stream>>>(e);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
   // the z-line arrays come back only when they were formed
   std::vector<double> h(total);
   CK(cudaMemcpyAsync(h.data(), ctx->d_stats, (zline ? total : total - n_xy) * sizeof(double),
@@ -2020,7 +2063,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   const double* spec = means + n_means;
   const double* lpart = spec + n_spec;
   const double* rows = lpart + n_les;
-  const double* xyd = rows + n_rows;
+  const double* hpdf = rows + n_rows;
+  const double* xyd = hpdf + n_bpe;
   auto Q = [&](int j, int q) {
     double s = 0.0;
     for (int sl = 0; sl < nslice; ++sl) s += part[((size_t)j * nslice + sl) * STAT_NQ + q];
@@ -2172,7 +2216,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     }
     set(DIABLO_STAT_MKE, j, 0.5 * mk / nx);
   }
-  double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + nx / 2;
+  double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + nx / 2 +
+               (nth > 0 ? 2 * nx : 0);
   sc[DIABLO_STAT_TIME] = ctx->time;
   sc[DIABLO_STAT_DT] = ctx->delta_t;
   sc[DIABLO_STAT_UBULK] = integrate_y(ume);
@@ -2208,6 +2253,23 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     std::vector<double> u1yl(nyp2, 0.0);
     for (int j = 1; j <= ny; ++j) u1yl[j] = gyf[j] * Q(j, SQ_U1YL);
     sc[DIABLO_STAT_U1Y_LEFT_B] = integrate_y(u1yl);
+  }
+  if (nth > 0) {   // compute_BPE's finish (:1840-1860)
+    double* pdf = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + nx / 2;
+    double* bin = pdf + nx;
+    std::vector<double> thb(nbin + 1), yr(nbin + 1, 0.0);
+    for (int i = 0; i <= nbin; ++i)
+      thb[i] = nonhom ? bthmin + i * bdth : -(ctx->ro_inv + 1.e-14) * cos(i * PI_REF / nbin);
+    double tot = 0.0;
+    for (int i = 0; i < nbin; ++i) tot += hpdf[i];
+    for (int i = 0; i < nbin; ++i) pdf[i] = hpdf[i] / tot;
+    for (int i = 1; i <= nbin; ++i) yr[i] = yr[i - 1] + pdf[i - 1];
+    for (int i = 0; i <= nbin; ++i) yr[i] = yr[i] * p.ly;
+    double bpe = 0.0;
+    for (int i = 0; i < nbin; ++i)
+      bpe = bpe - (0.5 * (thb[i + 1] + thb[i]) * 0.5 * (yr[i + 1] + yr[i])) * (yr[i + 1] - yr[i]) / p.ly;
+    for (int i = 0; i < nbin; ++i) bin[i] = thb[i];
+    sc[DIABLO_STAT_BPE] = bpe;
   }
   // FTx_uu (:650-675): kz = 0 row of u1, integrated over y
   double* sp = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF);

@@ -304,3 +304,40 @@ __global__ void __launch_bounds__(128) k_stats_xy(const __grid_constant__ StatsX
   a.out[XY_UV * plane + at] = uv * rz;
   a.out[XY_WV * plane + at] = wv * rz;
 }
+
+// compute_BPE (for/statistics.f90:1755-1876): the y-weighted histogram of
+// s = th_1 + dTHdX(1) (gx - Lx/2) over rows jlo..jhi, into Nbin bins either
+// evenly spaced from thmin (the x-inhomogeneous branch) or acos-spaced in
+// [-Ro_inv, Ro_inv] with the reference's float32 pi.  Bin indices below 0 (th
+// under the evenly spaced range, out of bounds in the reference) go to bin 0.
+// Per-block shared-memory histograms, then one atomic add per bin.
+struct StatsBpeArgs {
+  const double* th;     // physical th_1, [j][k][i]
+  const double* dyf;
+  double dthdx, lx, thmin, thmax, dth, roden, pi_ref;
+  int nx, nz, jlo, jhi, nbin, even;
+  double* pdf;          // [nbin], zeroed by the caller
+};
+
+__global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ StatsBpeArgs a) {
+  extern __shared__ double hist[];
+  for (int b = threadIdx.x; b < a.nbin; b += blockDim.x) hist[b] = 0.0;
+  __syncthreads();
+  const size_t pn = (size_t)a.nz * a.nx;
+  const size_t tot = (size_t)(a.jhi - a.jlo + 1) * pn;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const int j = a.jlo + (int)(q / pn);
+    const size_t r = q % pn;
+    const int i = (int)(r % a.nx);
+    const double s = a.th[(size_t)j * pn + r] + a.dthdx * ((i * a.lx) / a.nx - 0.5 * a.lx);
+    double x = a.even ? (s - a.thmin) / a.dth
+                      : acos(-fmin(fmax(s, a.thmin), a.thmax) / a.roden) * a.nbin / a.pi_ref;
+    // truncation toward zero, then the bin range (clamping first keeps the
+    // conversion in range; fmax also sends NaN to bin 0)
+    x = fmin(fmax(x, 0.0), (double)(a.nbin - 1));
+    atomicAdd(&hist[(int)x], a.dyf[j]);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < a.nbin; b += blockDim.x)
+    if (hist[b] != 0.0) atomicAdd(&a.pdf[b], hist[b]);
+}

@@ -13,8 +13,8 @@ fields (and the spectral gradients the reference builds) are transformed with
 library evaluates the same averages from the Fourier coefficients (Parseval),
 so the two agree to round-off, not bit for bit.
 
-Both branches of ``homogeneousX`` are restated.  Not restated: HDF5/movie
-output, the y* binning (Bin_Ystar_and_Write) and compute_BPE.  The oracle is
+Both branches of ``homogeneousX`` are restated, and compute_BPE.  Not
+restated: HDF5/movie output and the y* binning (Bin_Ystar_and_Write).  The oracle is
 the checker of the CUDA library, never the product.
 
 Quirks kept from the reference:
@@ -331,6 +331,60 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
 
     scal = dict(time=o.time, dt=o.delta_t, ubulk=ubulk, urms_b=urms_b, vrms_b=vrms_b,
                 wrms_b=wrms_b, u1y_left_b=u1y_left_b)
-    return {"profiles": {k: v[1:Nyp + 1].copy() for k, v in out.items()},
-            "th": [{k: v[1:Nyp + 1].copy() for k, v in d.items()} for d in ths],
-            "spectrum": spec, "scalars": scal}
+    res = {"profiles": {k: v[1:Nyp + 1].copy() for k, v in out.items()},
+           "th": [{k: v[1:Nyp + 1].copy() for k, v in d.items()} for d in ths],
+           "spectrum": spec, "scalars": scal}
+    if o.Nth > 0:
+        bpe, pdf, bins = compute_bpe(o, th[0], homogeneous_x)
+        scal["bpe"] = bpe
+        res["th1_pdf"], res["th1_bin"] = pdf, bins
+    return res
+
+
+def compute_bpe(o: OracleChannel, th1, homogeneous_x: bool):
+    """compute_BPE (for/statistics.f90:1755-1876): the background potential
+    energy of Tseng & Ferziger from the y-weighted PDF of th_1 plus its
+    background gradient, on Nbin = Nx bins -- evenly spaced in the
+    x-inhomogeneous branch, acos-spaced in [-Ro_inv, Ro_inv] in the homogeneous
+    one (the reference's comments swap the two labels; the code is what is
+    restated).  ``pi`` is the reference's float32 value and the literal 1.1 is
+    single precision.  A negative bin index (th below the evenly spaced range,
+    out of bounds in the reference) is taken as bin 0.  Returns (BPE, PDF, the
+    lower bin edges th_bin(0:Nbin-1))."""
+    from .channel import PI_REF
+    p = o.p
+    Nx, Nz, Nyp = o.Nx, o.Nz, o.Nyp
+    nbin = Nx
+    d0 = float(p.dthdx[0])
+    gx = np.array([(i * p.lx) / Nx for i in range(Nx)])
+    s1 = th1[:, :, :] + d0 * (gx - 0.5 * p.lx)[None, None, :]
+    pdf = np.zeros(nbin)
+    j0, j1 = o.jstart_th[0], o.jend_th[0]
+    if not homogeneous_x:
+        thmin = -d0 * 0.5 * p.lx * float(np.float32(1.1))
+        thmax = d0 * 0.5 * p.lx * float(np.float32(1.1))
+        dth = (thmax - thmin) / nbin + 1e-14
+        th_bin = np.array([thmin + i * dth for i in range(nbin + 1)])
+        for j in range(j0, j1 + 1):
+            b = np.trunc((s1[j] - thmin) / dth).astype(np.int64)
+            b = np.clip(b, 0, nbin - 1)
+            np.add.at(pdf, b.ravel(), o.dyf[j])
+    else:
+        ro = o.Ro_inv
+        thmin, thmax = -ro, ro
+        th_bin = np.array([-(ro + 1e-14) * math.cos(i * PI_REF / nbin) for i in range(nbin + 1)])
+        for j in range(j0, j1 + 1):
+            arg = -np.minimum(np.maximum(s1[j], thmin), thmax) / (ro + 1e-14)
+            b = np.trunc(np.arccos(arg) * nbin / PI_REF).astype(np.int64)
+            b = np.clip(b, 0, nbin - 1)
+            np.add.at(pdf, b.ravel(), o.dyf[j])
+    pdf = pdf / np.sum(pdf)
+    y_r = np.zeros(nbin + 1)
+    for i in range(1, nbin + 1):
+        y_r[i] = y_r[i - 1] + pdf[i - 1]
+    y_r = y_r * p.ly
+    bpe = 0.0
+    for i in range(nbin):
+        bpe = bpe - (0.5 * (th_bin[i + 1] + th_bin[i]) * 0.5 * (y_r[i + 1] + y_r[i])) * \
+            (y_r[i + 1] - y_r[i]) / p.ly
+    return bpe, pdf, th_bin[:nbin].copy()

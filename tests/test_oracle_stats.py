@@ -324,3 +324,50 @@ def test_stats_nonhomogeneous_known_answers():
     close("vv_dvdy", pr["vv_dvdy"][1:], (V[G + 1] - V[G - 1]) / dgy * D[G] * E[G] / 2)
     for k in ("uu_dudx", "wu_dwdx", "vu_dvdx"):
         assert np.abs(pr[k]).max() < 1e-13 * max(np.abs(pr["vv_dvdy"]).max(), 1e-30), k
+
+
+def test_bpe_single_bin_known_answer():
+    """compute_BPE with th = 0 and no background gradient: every point falls in
+    the acos bin of 0, which the reference's float32 pi puts at Nbin/2 - 1
+    (acos(0) * Nbin / pi = 0.49999998 Nbin), so Y_r jumps from 0 to Ly there and
+    BPE = -Ly/2 times the bin's mid value."""
+    from oracle.channel import PI_REF
+    from oracle.stats import compute_bpe
+    p = small_params(nx=32, ny=25, nz=12, n_th=1, ro=2.0, grav_y=0.0)
+    gy = grid_for(p)
+    o = _oracle(p, gy)
+    th1 = np.zeros((p.ny + 2, p.nz, p.nx))
+    bpe, pdf, bins = compute_bpe(o, th1, True)
+    b = p.nx // 2 - 1
+    assert pdf[b] == pytest.approx(1.0, rel=1e-15) and np.count_nonzero(pdf) == 1
+    edge = lambda i: -(0.5 + 1e-14) * math.cos(i * PI_REF / p.nx)
+    assert bins[b] == edge(b)
+    assert bpe == pytest.approx(-0.5 * p.ly * 0.5 * (edge(b) + edge(b + 1)), rel=1e-14)
+
+
+def test_bpe_evenly_spaced_bins_sorted_profile():
+    """x-inhomogeneous branch: th_1 = 0 and a background gradient dTHdX only, so
+    s = dTHdX (x - Lx/2) is spread evenly over x; the PDF is y-weighted and
+    uniform across the occupied bins, and BPE follows from the bins directly."""
+    from oracle.stats import compute_bpe
+    p = small_params(nx=32, ny=25, nz=12, n_th=1, dthdx=[0.4], grav_y=0.0)
+    gy = grid_for(p)
+    o = _oracle(p, gy)
+    th1 = np.zeros((p.ny + 2, p.nz, p.nx))
+    bpe, pdf, bins = compute_bpe(o, th1, False)
+    assert pdf.sum() == pytest.approx(1.0, rel=1e-14)
+    # the Nx positions x_i fall in bins 1.1 Lx/Nx wide: every bin holds a whole
+    # number of the (equally y-weighted) x columns, and they appear in x order
+    counts = pdf * p.nx
+    assert np.allclose(counts, np.round(counts), atol=1e-9)
+    d0, x = 0.4, np.arange(p.nx) * p.lx / p.nx
+    s = d0 * (x - 0.5 * p.lx)
+    thmin = -d0 * 0.5 * p.lx * float(np.float32(1.1))
+    dth = (-2 * thmin) / p.nx + 1e-14
+    want = np.bincount(np.trunc((s - thmin) / dth).astype(int), minlength=p.nx) / p.nx
+    assert np.allclose(pdf, want, atol=1e-12)
+    y_r = np.concatenate([[0.0], np.cumsum(want)]) * p.ly
+    mids = 0.5 * (np.arange(p.nx + 1)[1:] + np.arange(p.nx)) * dth + thmin
+    ref = -np.sum(mids * 0.5 * (y_r[1:] + y_r[:-1]) * np.diff(y_r)) / p.ly
+    assert bpe == pytest.approx(ref, rel=1e-12)
+    assert bins[0] == thmin
