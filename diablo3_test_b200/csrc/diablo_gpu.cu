@@ -1242,7 +1242,7 @@ static int ensure_cfl(diablo_ctx* ctx) {
     if ((rc = dev_alloc(ctx, (void**)&ctx->ustar[q], four_elems(ctx) * sizeof(double2)))) return rc;
     if ((rc = dev_alloc(ctx, (void**)&ctx->cfl_phys[q], phys_elems(ctx) * sizeof(double)))) return rc;
   }
-  return dev_alloc(ctx, (void**)&ctx->d_cfl, (size_t)3 * ctx->nyp2 * sizeof(double));
+  return dev_alloc(ctx, (void**)&ctx->d_cfl, (size_t)5 * ctx->nyp2 * sizeof(double));
 }
 
 static int courant_phys(diablo_ctx* ctx, const double* const* u) {
@@ -1250,9 +1250,9 @@ static int courant_phys(diablo_ctx* ctx, const double* const* u) {
   const size_t ps = (size_t)ctx->nz * ctx->nx;
   {
     Prof pr(ctx, K_OTHER);
-    k_plane_absmax<<<ctx->ny, 256, 0, ctx->stream>>>(u[0], u[1], u[2], ctx->d_cfl, ps);
+    k_plane_range<<<ctx->ny, 256, 0, ctx->stream>>>(u[0], u[1], u[2], ctx->d_cfl, ps);
   }
-  std::vector<double> mx((size_t)3 * ctx->nyp2);
+  std::vector<double> mx((size_t)5 * ctx->nyp2);
   CK(cudaMemcpyAsync(mx.data(), ctx->d_cfl, mx.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   double dt = p.max_dt;
@@ -1263,15 +1263,34 @@ static int courant_phys(diablo_ctx* ctx, const double* const* u) {
     if (nmax > 0) dt = fmin(dt, (double)0.1f * 2.0 * PI_REF / nmax);
   }
   const double cx = p.cfl * (p.lx / ctx->nx), cz = p.cfl * (p.lz / ctx->nz);
-  double m1 = 0.0, m3 = 0.0, dty = INFINITY;
-  for (int j = 1; j <= ctx->ny; ++j) {
-    m1 = fmax(m1, mx[(size_t)j * 3]);
-    m3 = fmax(m3, mx[(size_t)j * 3 + 2]);
-    const double m2 = mx[(size_t)j * 3 + 1];
-    if (m2 > 0) dty = fmin(dty, p.cfl * ctx->h_dy[j] / m2);
+  // max |u - a| over plane j from its range
+  auto dev = [&](int j, int q, double a) {   // q = 0: u1, q = 3: u3
+    return fmax(mx[(size_t)j * 5 + q + 1] - a, a - mx[(size_t)j * 5 + q]);
+  };
+  if (p.flavor_front) {
+    // 'Front': the thermal wind added to u1 and u3, rows jstart..jend, for
+    // each scalar (for/advance.f90:76-89); no velocity limit without scalars
+    const double rd = ctx->ro_inv / p.delta;
+    for (int n = 0; n < ctx->nth; ++n)
+      for (int j = ctx->jstart; j <= ctx->jend; ++j) {
+        const double m1 = dev(j, 0, p.dthdz[n] * ctx->h_gyf[j] / rd);
+        const double m3 = dev(j, 3, -(1.0 / rd) * p.dthdx[n] * (ctx->h_gyf[j] - 0.5 * p.ly));
+        const double m2 = mx[(size_t)j * 5 + 2];
+        if (m1 > 0) dt = fmin(dt, cx / m1);
+        if (m2 > 0) dt = fmin(dt, p.cfl * ctx->h_dy[j] / m2);
+        if (m3 > 0) dt = fmin(dt, cz / m3);
+      }
+  } else {
+    double m1 = 0.0, m3 = 0.0, dty = INFINITY;
+    for (int j = 1; j <= ctx->ny; ++j) {
+      m1 = fmax(m1, dev(j, 0, 0.0));
+      m3 = fmax(m3, dev(j, 3, 0.0));
+      const double m2 = mx[(size_t)j * 5 + 2];
+      if (m2 > 0) dty = fmin(dty, p.cfl * ctx->h_dy[j] / m2);
+    }
+    const double dtx = m1 > 0 ? cx / m1 : INFINITY, dtz = m3 > 0 ? cz / m3 : INFINITY;
+    dt = fmin(fmin(dt, dtx), fmin(dty, dtz));
   }
-  const double dtx = m1 > 0 ? cx / m1 : INFINITY, dtz = m3 > 0 ? cz / m3 : INFINITY;
-  dt = fmin(fmin(dt, dtx), fmin(dty, dtz));
   double nd;
   if (dt <= 0) nd = 0.00001;
   else if (dt >= 1000.) nd = 1000.;
@@ -1463,8 +1482,12 @@ static int substep(diablo_ctx* ctx, int rk) {
     Prof pr(ctx, K_SOLVE);
     // thermal-wind forcing (flavor 'Front') keeps the general kernel
     if (fits && tiled) rc = launch_tiles(A, ctx->stream);
-    else if (mean_split || cfl) rc = DIABLO_ERR_UNSUPPORTED;
-    else rc = launch_solve(a, false, ctx->stream);
+    else if (mean_split) rc = DIABLO_ERR_UNSUPPORTED;
+    else {
+      if (cfl)
+        for (int q = 0; q < 3; ++q) a.keep[q] = ctx->ustar[q];
+      rc = launch_solve(a, false, ctx->stream);
+    }
     if (rc) return rc;
   }
   CK(cudaGetLastError());

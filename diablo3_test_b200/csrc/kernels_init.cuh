@@ -142,31 +142,38 @@ __global__ void __launch_bounds__(128) k_pp_solve(const __grid_constant__ PpSolv
   }
 }
 
-// Largest |u1|, |u2|, |u3| of each plane j = 1..Ny (one block per plane), the
-// maxima courant turns into the CFL time step.
-__global__ void __launch_bounds__(256) k_plane_absmax(const double* u1, const double* u2, const double* u3,
-                                                      double* out, size_t ps) {
+// Per plane j = 1..Ny (one block per plane): min and max of u1 and u3 and the
+// largest |u2|, out[j][0..4] = (min u1, max u1, max |u2|, min u3, max u3).
+// courant turns them into the CFL time step: max|u - a| over the plane is
+// max(max u - a, a - min u) for any shift a, which covers both the plain
+// branch (a = 0) and the 'Front' branch's thermal-wind shifts.
+__global__ void __launch_bounds__(256) k_plane_range(const double* u1, const double* u2, const double* u3,
+                                                     double* out, size_t ps) {
   const int j = blockIdx.x + 1;
   const size_t base = (size_t)j * ps;
-  double m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  double v[5] = {INFINITY, -INFINITY, 0.0, INFINITY, -INFINITY};
   for (size_t i = threadIdx.x; i < ps; i += blockDim.x) {
-    m1 = fmax(m1, fabs(u1[base + i]));
-    m2 = fmax(m2, fabs(u2[base + i]));
-    m3 = fmax(m3, fabs(u3[base + i]));
+    const double a = u1[base + i], c = u3[base + i];
+    v[0] = fmin(v[0], a); v[1] = fmax(v[1], a);
+    v[2] = fmax(v[2], fabs(u2[base + i]));
+    v[3] = fmin(v[3], c); v[4] = fmax(v[4], c);
   }
-  __shared__ double red[3][8];
+  __shared__ double red[5][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int off = 16; off > 0; off >>= 1) {
-    m1 = fmax(m1, __shfl_down_sync(0xffffffffu, m1, off));
-    m2 = fmax(m2, __shfl_down_sync(0xffffffffu, m2, off));
-    m3 = fmax(m3, __shfl_down_sync(0xffffffffu, m3, off));
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v[q], off);
+      v[q] = (q == 0 || q == 3) ? fmin(v[q], o) : fmax(v[q], o);
+    }
+    if (lane == 0) red[q][w] = v[q];
   }
-  if (lane == 0) { red[0][w] = m1; red[1][w] = m2; red[2][w] = m3; }
   __syncthreads();
-  if (threadIdx.x < 3) {
-    double v = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v = fmax(v, red[threadIdx.x][q]);
-    out[(size_t)j * 3 + threadIdx.x] = v;
+  if (threadIdx.x < 5) {
+    const int q = threadIdx.x;
+    double r = red[q][0];
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) r = (q == 0 || q == 3) ? fmin(r, red[q][k]) : fmax(r, red[q][k]);
+    out[(size_t)j * 5 + q] = r;
   }
 }
 

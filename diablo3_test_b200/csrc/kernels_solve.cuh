@@ -59,6 +59,7 @@ struct SolveArgs {
   const double2* nl64[SOLVE_NF];
   const float2* nl32[SOLVE_NF];
   int store_cf;             // 0 on the last substep (cf is not read again)
+  double2* keep[3];         // if set: the solved u1, u2, u3 before the projection (courant)
 };
 
 namespace csolve {
@@ -164,6 +165,12 @@ DI void project_column(const SolveArgs& a, double2* const* cu, const double2* cp
       u1v[r] = (j < n) ? cu[0][(size_t)j * ps + cidx] : z2;
       u2v[r] = (j < n) ? cu[1][(size_t)j * ps + cidx] : z2;
       u3v[r] = (j < n) ? cu[2][(size_t)j * ps + cidx] : z2;
+      // the velocity courant reads (for/channel.f90:885-888), rows 1..Ny
+      if (a.keep[0] && j >= 1 && j <= nyp) {
+        a.keep[0][(size_t)j * ps + cidx] = u1v[r];
+        a.keep[1][(size_t)j * ps + cidx] = u2v[r];
+        a.keep[2][(size_t)j * ps + cidx] = u3v[r];
+      }
     }
     double2 u2n = shfl_down2(u2v[0], 1);
 #pragma unroll

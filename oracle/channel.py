@@ -421,7 +421,8 @@ class OracleChannel:
 
     def courant(self):
         """CFL time step, velocity in physical space (for/advance.f90:47-158),
-        without the 'Front' thermal-wind branch and event scheduling."""
+        with the 'Front' thermal-wind branch (:76-89), without the output-event
+        scheduling."""
         p = self.p
         dt = p.max_dt
         if self.Ro_inv != 0.0:
@@ -433,15 +434,28 @@ class OracleChannel:
                 dt = min(dt, float(np.float32(0.1)) * 2.0 * PI_REF / nmax)
         dx = p.lx / self.Nx
         dz = p.lz / self.Nz
-        J = slice(1, self.Nyp + 1)
-        with np.errstate(divide="ignore"):
-            u1 = np.abs(self.u1.r[J, :self.Nz, :self.Nx])
-            u2 = np.abs(self.u2.r[J, :self.Nz, :self.Nx])
-            u3 = np.abs(self.u3.r[J, :self.Nz, :self.Nx])
-            dt_x = np.min(p.cfl * dx / u1)
-            dt_y = np.min(p.cfl * self.dy[J, None, None] / u2)
-            dt_z = np.min(p.cfl * dz / u3)
-        dt = min(dt, dt_x, dt_y, dt_z)
+        if p.flavor == "Front":
+            rd = self.Ro_inv / self.delta
+            J = slice(self.jstart, self.jend + 1)
+            gyf = self.gyf[J, None, None]
+            with np.errstate(divide="ignore"):
+                for n in range(self.Nth):
+                    u1 = np.abs(self.u1.r[J, :self.Nz, :self.Nx] - p.dthdz[n] * gyf / rd)
+                    u2 = np.abs(self.u2.r[J, :self.Nz, :self.Nx])
+                    u3 = np.abs(self.u3.r[J, :self.Nz, :self.Nx]
+                                + (1.0 / rd) * p.dthdx[n] * (gyf - 0.5 * p.ly))
+                    dt = min(dt, np.min(p.cfl * dx / u1), np.min(p.cfl * self.dy[J, None, None] / u2),
+                             np.min(p.cfl * dz / u3))
+        else:
+            J = slice(1, self.Nyp + 1)
+            with np.errstate(divide="ignore"):
+                u1 = np.abs(self.u1.r[J, :self.Nz, :self.Nx])
+                u2 = np.abs(self.u2.r[J, :self.Nz, :self.Nx])
+                u3 = np.abs(self.u3.r[J, :self.Nz, :self.Nx])
+                dt_x = np.min(p.cfl * dx / u1)
+                dt_y = np.min(p.cfl * self.dy[J, None, None] / u2)
+                dt_z = np.min(p.cfl * dz / u3)
+            dt = min(dt, dt_x, dt_y, dt_z)
         if dt <= 0:
             self.delta_t = 0.00001
         elif dt >= 1000.:

@@ -62,7 +62,7 @@ def test_initial_pressure_matches_oracle(cuda_device, kw):
         ch.close()
 
 
-@pytest.mark.parametrize("case", ["dns", "dns_every_2", "les", "rotation_scalar"])
+@pytest.mark.parametrize("case", ["dns", "dns_every_2", "les", "rotation_scalar", "front"])
 def test_variable_dt_matches_oracle(cuda_device, case):
     kw = dict(variable_dt=True, update_dt=1, cfl=0.5, max_dt=0.02, delta_t=1e-3, re=300.0)
     n_th = 1
@@ -72,6 +72,9 @@ def test_variable_dt_matches_oracle(cuda_device, case):
         kw.update(use_les=True, create_new_flow=False, les_model_type=LES_SMAGORINSKY)
     elif case == "rotation_scalar":
         kw.update(ro=2.0, th_bc_ymin=[0], th_bc_ymin_c1=[-0.5], th_bc_ymax=[0], th_bc_ymax_c1=[0.5])
+    elif case == "front":
+        # the 'Front' branch of courant: thermal-wind shifts of u1 and u3
+        kw.update(flavor="Front", ro=2.0, delta=1.5, dthdx=[0.2], dthdz=[0.05], grav_y=1.0)
     p = small_params(n_th=n_th, **kw)
     gy = grid_for(p)
     fields = initial_fields(p, gy, kind="turbulent", seed=22)
