@@ -35,6 +35,7 @@ STAT_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw",
                  "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
 STAT_TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
 STAT_SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b", "bpe")
+STAT_ZSTAR = ("shear2", "thw", "chi", "epsilon", "TKE", "KE")
 
 # every symbol include/diablo_gpu.h declares: name -> (restype, argtypes)
 _vp = ctypes.c_void_p

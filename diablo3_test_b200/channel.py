@@ -53,7 +53,7 @@ MEAN_H5_NAMES = {
     "thme": "thme{:02d}", "dthdy": "dthdz{:02d}", "thrms": "thrms{:02d}", "thv": "thw{:02d}",
     "thv_m": "thw{:02d}_m", "pe_diss": "pe_diss{:02d}", "spectrum": "FTx_uu",
     "u1y_left_b": "u1z_x0", "time": "time", "bpe": "BPE", "th1_pdf": "th1PDF",
-    "th1_bin": "th1bin",
+    "th1_bin": "th1bin", "zstar": "<name>_zstar",
 }
 
 
@@ -148,7 +148,8 @@ class Channel:
         "th": [{name: (Ny,)} per scalar], "spectrum": (Nx/2,), "scalars":
         {name: float}}`` with the reference's internal names (MEAN_H5_NAMES
         gives the dataset each one is written to); with scalars also
-        "th1_pdf" and "th1_bin" (Nx,) of compute_BPE and scalars["bpe"]."""
+        "th1_pdf" and "th1_bin" (Nx,) of compute_BPE, scalars["bpe"], and
+        "zstar": {shear2, thw, chi, epsilon, TKE, KE: (Nx,)} bin means."""
         p = self.params
         n = self.lib.diablo_stats_size(self.ctx)
         if n < 0:
@@ -170,6 +171,10 @@ class Channel:
             res["th1_pdf"] = out[b:b + p.nx].copy()
             res["th1_bin"] = out[b + p.nx:b + 2 * p.nx].copy()
             b += 2 * p.nx
+            # Bin_Ystar_and_Write's bin means on the same th_1 bins
+            res["zstar"] = {k: out[b + q * p.nx:b + (q + 1) * p.nx].copy()
+                            for q, k in enumerate(_lib.STAT_ZSTAR)}
+            b += len(_lib.STAT_ZSTAR) * p.nx
         res["scalars"] = {k: float(v) for k, v in zip(_lib.STAT_SCALARS, out[b:])}
         if p.n_th == 0:
             del res["scalars"]["bpe"]

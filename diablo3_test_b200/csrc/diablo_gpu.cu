@@ -97,6 +97,9 @@ struct diablo_ctx {
   double* d_sigma;          // filter_chan transfer function [Nkx+1][2Nkz+1]
   double* d_stats;          // plane-statistics partial sums (diablo_stats)
   double* stats_phys[3];    // physical u1, u2, u3 for the z-line statistics
+  double* stats_der[8];     // y* binning: d/dx, d/dz of u1..u3 and of the last scalar
+  double* stats_thl;        // physical last scalar (z-line branch, N_th > 1)
+  double* stats_thxy;       // its z-line mean [Ny+2][Nx]
   size_t stats_doubles;
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
   // LES substep buffers (FP64), allocated on first use
@@ -1884,7 +1887,7 @@ int diablo_filter_chan(diablo_ctx* ctx, int n) {
 int diablo_stats_size(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
   return ctx->ny * (DIABLO_STAT_NPROF + ctx->nth * DIABLO_STAT_NTHPROF) + ctx->nx / 2 +
-         (ctx->nth > 0 ? 2 * ctx->nx : 0) + DIABLO_STAT_NSCALAR;
+         (ctx->nth > 0 ? (2 + ZS_N) * ctx->nx : 0) + DIABLO_STAT_NSCALAR;
 }
 
 int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
@@ -1915,8 +1918,9 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   const size_t n_part = even((size_t)nyp2 * nslice * STAT_NQ), n_means = even((size_t)nyp2 * (4 + nth));
   const size_t n_spec = even((size_t)nyp2 * nkx1), n_les = even((size_t)nyp2 * lslice * 2);
   const size_t n_rows = (size_t)nyp2 * (3 + nth) * nkx1 * 2, n_bpe = even((size_t)nx);
+  const size_t n_zs = even((size_t)(1 + ZS_N) * nx);
   const size_t n_xy = (size_t)XY_N * nyp2 * nx;
-  const size_t total = n_part + n_means + n_spec + n_les + n_rows + n_bpe + n_xy;
+  const size_t total = n_part + n_means + n_spec + n_les + n_rows + n_bpe + n_zs + n_xy;
   if (ctx->stats_doubles < total) {
     if ((rc = dev_alloc(ctx, (void**)&ctx->d_stats, total * sizeof(double)))) return rc;
     ctx->stats_doubles = total;
@@ -1927,7 +1931,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   double* d_les = d_spec + n_spec;
   double* d_rows = d_les + n_les;
   double* d_bpe = d_rows + n_rows;
-  double* d_xy = d_bpe + n_bpe;
+  double* d_zs = d_bpe + n_bpe;
+  double* d_xy = d_zs + n_zs;
   CK(cudaMemsetAsync(ctx->d_stats, 0, total * sizeof(double), ctx->stream));
   const double d0 = nth > 0 ? p.dthdx[0] : 0.0;
   // (1/(Ro_inv/delta)) dTHdX(1), the thermal-wind shear; 0 without a background gradient
@@ -1974,7 +1979,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   }
   const bool les = p.use_les && ctx->les.ready;
   double* uphys[3] = {nullptr, nullptr, nullptr};
-  if (les || zline) {
+  if (les || zline || nth > 0) {
     // physical u1, u2, u3 (all planes): LES work arrays when present, else
     // three buffers kept for the statistics
     if (les) {
@@ -2072,6 +2077,78 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     ctx->launches++;
     CK(cudaGetLastError());
   }
+  if (nth > 0) {
+    // Bin_Ystar_and_Write (:1877-1972) of six pointwise fields: their spectral
+    // derivatives in physical space first, one field at a time through b_four
+    const size_t pe = phys_elems(ctx) * sizeof(double), ftot = four_elems(ctx);
+    for (int q = 0; q < 8; ++q)
+      if (!ctx->stats_der[q] && (rc = dev_alloc(ctx, (void**)&ctx->stats_der[q], pe))) return rc;
+    const int last = nth - 1;
+    for (int q = 0; q < 8; ++q) {
+      const double2* src = q < 6 ? ctx->st[ctx->cur][q % 3] : ctx->st[ctx->cur][4 + last];
+      const int axis = q < 6 ? q / 3 : q - 6;
+      // epsilon's x derivatives leave out the kz = 0 row outside the homogeneous branch
+      const int drop0 = (q < 3 && nonhom) ? 1 : 0;
+      k_spec_deriv<<<grid1d(ftot), 256, 0, ctx->stream>>>(src, ctx->b_four, ctx->d_kx, ctx->d_kz, axis, drop0,
+                                                         nkx1, ctx->nk2, ctx->kp, ftot);
+      ctx->launches++;
+      if ((rc = inv_four_to_phys(ctx, ctx->b_four, ctx->b_xs, ctx->stats_der[q]))) return rc;
+    }
+    const double* thxy = nullptr;
+    if (zline) {
+      if (!ctx->stats_thxy &&
+          (rc = dev_alloc(ctx, (void**)&ctx->stats_thxy, (size_t)nyp2 * nx * sizeof(double))))
+        return rc;
+      const double* thl = ctx->b_phys;   // th_1 when it is the last scalar
+      if (nth > 1) {
+        if (!ctx->stats_thl && (rc = dev_alloc(ctx, (void**)&ctx->stats_thl, pe))) return rc;
+        if ((rc = inv_four_to_phys(ctx, ctx->st[ctx->cur][4 + last], ctx->b_xs, ctx->stats_thl))) return rc;
+        thl = ctx->stats_thl;
+      }
+      k_zmean<<<dim3((nx + 127) / 128, nyp2), 128, 0, ctx->stream>>>(thl, ctx->stats_thxy, nx, ctx->nz, nyp2);
+      ctx->launches++;
+      thxy = ctx->stats_thxy;
+    }
+    StatsZstarArgs z;
+    memset(&z, 0, sizeof(z));
+    for (int q = 0; q < 3; ++q) z.u[q] = uphys[q];
+    z.th1 = ctx->b_phys;
+    for (int q = 0; q < 6; ++q) z.du[q] = ctx->stats_der[q];
+    z.dthd[0] = ctx->stats_der[6];
+    z.dthd[1] = ctx->stats_der[7];
+    z.means = d_means;
+    z.xy = zline ? d_xy : nullptr;
+    z.thxy = thxy;
+    z.dy = ctx->d_dy;
+    z.dyf = ctx->d_dyf;
+    z.gy = ctx->d_gy;
+    z.gyf = ctx->d_gyf;
+    z.nu = ctx->nu;
+    z.dthdx0 = p.dthdx[0];
+    z.dthdx_l = p.dthdx[last];
+    z.dthdz_l = p.dthdz[last];
+    z.lx = p.lx;
+    z.thmin = bthmin;
+    z.thmax = bthmax;
+    z.dth = bdth;
+    z.roden = broden;
+    z.pi_ref = PI_REF;
+    z.nx = nx;
+    z.nz = ctx->nz;
+    z.nyp = ny;
+    z.nth = nth;
+    z.jlo = ctx->jst[0];
+    z.jhi = ctx->jet[0];
+    z.nbin = nbin;
+    z.even = nonhom ? 1 : 0;
+    z.hist = d_zs;
+    const int zsm = (1 + ZS_N) * nbin * (int)sizeof(double);
+    if (zsm > 48 * 1024) CK(cudaFuncSetAttribute(k_stats_zstar, cudaFuncAttributeMaxDynamicSharedMemorySize, zsm));
+    Prof pr(ctx, K_OTHER);
+    k_stats_zstar<<<4 * nsm, 256, zsm, ctx->stream>>>(z);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
   // the z-line arrays come back only when they were formed
   std::vector<double> h(total);
   CK(cudaMemcpyAsync(h.data(), ctx->d_stats, (zline ? total : total - n_xy) * sizeof(double),
@@ -2087,7 +2164,8 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   const double* lpart = spec + n_spec;
   const double* rows = lpart + n_les;
   const double* hpdf = rows + n_rows;
-  const double* xyd = hpdf + n_bpe;
+  const double* hzs = hpdf + n_bpe;
+  const double* xyd = hzs + n_zs;
   auto Q = [&](int j, int q) {
     double s = 0.0;
     for (int sl = 0; sl < nslice; ++sl) s += part[((size_t)j * nslice + sl) * STAT_NQ + q];
@@ -2240,7 +2318,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     set(DIABLO_STAT_MKE, j, 0.5 * mk / nx);
   }
   double* sc = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF) + nx / 2 +
-               (nth > 0 ? 2 * nx : 0);
+               (nth > 0 ? (2 + ZS_N) * nx : 0);
   sc[DIABLO_STAT_TIME] = ctx->time;
   sc[DIABLO_STAT_DT] = ctx->delta_t;
   sc[DIABLO_STAT_UBULK] = integrate_y(ume);
@@ -2293,6 +2371,11 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
       bpe = bpe - (0.5 * (thb[i + 1] + thb[i]) * 0.5 * (yr[i + 1] + yr[i])) * (yr[i + 1] - yr[i]) / p.ly;
     for (int i = 0; i < nbin; ++i) bin[i] = thb[i];
     sc[DIABLO_STAT_BPE] = bpe;
+    // the y* bin means: field sums over the (unnormalised) dyf sums; an empty
+    // bin is 0/0 = NaN, as the reference writes it
+    double* zs = bin + nx;
+    for (int q = 0; q < ZS_N; ++q)
+      for (int i = 0; i < nbin; ++i) zs[(size_t)q * nx + i] = hzs[(size_t)(1 + q) * nbin + i] / hzs[i];
   }
   // FTx_uu (:650-675): kz = 0 row of u1, integrated over y
   double* sp = out + (size_t)ny * (DIABLO_STAT_NPROF + nth * DIABLO_STAT_NTHPROF);

@@ -341,3 +341,120 @@ __global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ Stats
   for (int b = threadIdx.x; b < a.nbin; b += blockDim.x)
     if (hist[b] != 0.0) atomicAdd(&a.pdf[b], hist[b]);
 }
+
+// i k * F for the y* binning's derivative fields: axis 0 = x (kx), 1 = z (kz);
+// drop0 zeroes the kz = 0 row (epsilon's x derivatives in the x-inhomogeneous
+// branch, k_start = 1).  One thread per stored coefficient.
+__global__ void k_spec_deriv(const double2* __restrict__ src, double2* __restrict__ dst, const double* kx,
+                             const double* kz, int axis, int drop0, int nkx1, int nk2, int kp, size_t tot) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= tot) return;
+  const int kq = (int)(idx % kp);
+  const int m = (int)((idx / kp) % nkx1);
+  double2 v = make_double2(0.0, 0.0);
+  if (kq < nk2 && !(drop0 && kq == 0)) v = mul_ik(axis == 0 ? kx[m] : kz[kq], src[idx]);
+  dst[idx] = v;
+}
+
+// z mean at each (j, i) of a physical field, out[j][i]
+__global__ void k_zmean(const double* __restrict__ f, double* __restrict__ out, int nx, int nz, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= nx || j >= n) return;
+  const size_t o = (size_t)j * nz * nx + i;
+  double s = 0.0;
+  for (int k = 0; k < nz; ++k) s += f[o + (size_t)k * nx];
+  out[(size_t)j * nx + i] = s / nz;
+}
+
+// Bin_Ystar_and_Write (for/statistics.f90:1877-1972) for the six fields the
+// reference bins, evaluated point by point from physical fields: shear2
+// (:159-166), thw (:343-370, th_1 against the last scalar's means), chi
+// (:400-423, the last scalar), epsilon (:859-1072), TKE and KE (:1296-1387).
+// Bins as in k_stats_bpe.  hist[0][b] = sum of dyf, hist[1 + q][b] = sum of
+// field_q dyf over the points of bin b (shared per block, then atomics).
+enum { ZS_SHEAR2 = 0, ZS_THW, ZS_CHI, ZS_EPSILON, ZS_TKE, ZS_KE, ZS_N };
+
+struct StatsZstarArgs {
+  const double* u[3];
+  const double* th1;
+  const double* du[6];      // d/dx u1, u2, u3, then d/dz u1, u2, u3
+  const double* dthd[2];    // d/dx, d/dz of the last scalar
+  const double* means;      // [Ny+2][4 + nth] plane means (homogeneous means)
+  const double* xy;         // [XY_N][Ny+2][Nx] z-line means (zline) or null
+  const double* thxy;       // [Ny+2][Nx] z-line mean of the last scalar (zline) or null
+  const double* dy;
+  const double* dyf;
+  const double* gy;
+  const double* gyf;
+  double nu, dthdx0, dthdx_l, dthdz_l, lx, thmin, thmax, dth, roden, pi_ref;
+  int nx, nz, nyp, nth, jlo, jhi, nbin, even;
+  double* hist;             // [1 + ZS_N][nbin], zeroed by the caller
+};
+
+__global__ void __launch_bounds__(256) k_stats_zstar(const __grid_constant__ StatsZstarArgs a) {
+  extern __shared__ double zh[];
+  const int nb = a.nbin;
+  for (int b = threadIdx.x; b < (1 + ZS_N) * nb; b += blockDim.x) zh[b] = 0.0;
+  __syncthreads();
+  const int nx = a.nx;
+  const size_t pn = (size_t)a.nz * nx;
+  const size_t plane = (size_t)(a.nyp + 2) * nx;
+  const int stride = 4 + a.nth;
+  auto UM = [&](int q, int j, int i) -> double {   // mean of u_{q+1} at (j, i)
+    return a.xy ? a.xy[(size_t)q * plane + (size_t)j * nx + i] : a.means[(size_t)j * stride + q];
+  };
+  auto THM = [&](int j, int i) -> double {
+    return a.thxy ? a.thxy[(size_t)j * nx + i] : a.means[(size_t)j * stride + 4 + a.nth - 1];
+  };
+  const double* u1 = a.u[0];
+  const double* u2 = a.u[1];
+  const double* u3 = a.u[2];
+  const size_t tot = (size_t)(a.jhi - a.jlo + 1) * pn;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    const int j = a.jlo + (int)(q / pn);
+    const size_t r = q % pn;
+    const int i = (int)(r % nx);
+    const size_t o = (size_t)j * pn + r, op = o + pn, om = o - pn;
+    const double s = a.th1[o] + a.dthdx0 * ((i * a.lx) / nx - 0.5 * a.lx);
+    double x = a.even ? (s - a.thmin) / a.dth
+                      : acos(-fmin(fmax(s, a.thmin), a.thmax) / a.roden) * nb / a.pi_ref;
+    x = fmin(fmax(x, 0.0), (double)(nb - 1));
+    const int b = (int)x;
+    const double w = a.dyf[j];
+    double f[ZS_N];
+    {
+      const double d1 = (u1[op] - u1[om]) / (2.0 * a.dyf[j]), d3 = (u3[op] - u3[om]) / (2.0 * a.dyf[j]);
+      f[ZS_SHEAR2] = d1 * d1 + d3 * d3;
+    }
+    f[ZS_THW] = (a.th1[o] - THM(j, i)) * 0.5 * ((u2[o] - UM(1, j, i)) + (u2[op] - UM(1, j + 1, i)));
+    {
+      const double r1 = a.dthd[0][o] + a.dthdx_l, r3 = a.dthd[1][o] + a.dthdz_l;
+      const double r2 = (a.th1[op] - a.th1[om]) / (a.gyf[j + 1] - a.gyf[j - 1]);
+      f[ZS_CHI] = r1 * r1 + r2 * r2 + r3 * r3;
+    }
+    double e = 0.0;
+    if (j >= 2) {
+      const double wa = a.dyf[j - 1] / (2.0 * a.dy[j]), wb = a.dyf[j] / (2.0 * a.dy[j]);
+      auto ip = [&](const double* sfield) { return wa * sfield[o] * sfield[o] + wb * sfield[om] * sfield[om]; };
+      e += ip(a.du[0]) + a.du[1][o] * a.du[1][o] + ip(a.du[2]);
+      e += ip(a.du[3]) + a.du[4][o] * a.du[4][o] + ip(a.du[5]);
+      const double su = ((u1[o] - UM(0, j, i)) - (u1[om] - UM(0, j - 1, i))) / a.dy[j];
+      const double sv = ((u2[op] - UM(1, j + 1, i)) - (u2[om] - UM(1, j - 1, i))) / (a.gy[j + 1] - a.gy[j - 1]);
+      const double sw = ((u3[o] - UM(2, j, i)) - (u3[om] - UM(2, j - 1, i))) / a.dy[j];
+      e += su * su + sv * sv + sw * sw;
+    }
+    f[ZS_EPSILON] = a.nu * e;
+    {
+      const double t1 = u1[o] - UM(0, j, i), t2 = u2[o] - UM(1, j, i), t3 = u3[o] - UM(2, j, i);
+      f[ZS_TKE] = 0.5 * (t1 * t1 + t2 * t2 + t3 * t3);
+      f[ZS_KE] = 0.5 * (u1[o] * u1[o] + u2[o] * u2[o] + u3[o] * u3[o]);
+    }
+    atomicAdd(&zh[b], w);
+#pragma unroll
+    for (int k = 0; k < ZS_N; ++k) atomicAdd(&zh[(1 + k) * nb + b], f[k] * w);
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < (1 + ZS_N) * nb; b += blockDim.x)
+    if (zh[b] != 0.0) atomicAdd(&a.hist[b], zh[b]);
+}

@@ -156,16 +156,21 @@ int diablo_filter_chan(diablo_ctx* ctx, int n);
  * internal names; mean.h5 swaps the v/w labels).  Plane averages of products
  * are evaluated from the Fourier coefficients (Parseval), z-line averages and
  * the LES terms from physical fields, all in FP64 in both precisions.
- * With scalars, compute_BPE's background potential energy (scalar BPE) and
- * its th_1 PDF and bin edges (th1PDF, th1bin) are included.  Not computed:
- * HDF5/movie output and the y* binning.  nu_sgs is the
+ * With scalars, compute_BPE's background potential energy (scalar BPE), its
+ * th_1 PDF and bin edges (th1PDF, th1bin) and Bin_Ystar_and_Write's bin means
+ * of shear2, thw, chi, epsilon, TKE and KE on those th_1 bins are included
+ * (the reference writes thw and chi once per scalar under one name, so the
+ * last scalar's stand; empty bins are NaN, 0/0 as in the reference).  Not
+ * computed: HDF5/movie output.  nu_sgs is the
  * plane mean of the nu_t of the most recent LES substep and eps_sgs2 uses that
  * nu_t, as compute_TKE_diss_les does; both are 0 without LES.
  * Layout of `out` (diablo_stats_size doubles):
  *   profile q of the velocity set at out[q*Ny + j-1], q < DIABLO_STAT_NPROF;
  *   then, for scalar n, profile r at out[(NPROF + n*NTHPROF + r)*Ny + j-1];
  *   then the y-averaged kz = 0 spectrum of u1 (FTx_uu), Nx/2 values;
- *   then, when N_th > 0, th1PDF (Nx values) and th1bin (Nx values);
+ *   then, when N_th > 0, th1PDF (Nx values), th1bin (Nx values) and the six
+ *   y* bin means (Nx values each, in the order shear2, thw, chi, epsilon, TKE,
+ *   KE);
  *   then DIABLO_STAT_NSCALAR scalars (BPE is 0 without scalars). */
 enum {
   DIABLO_STAT_UME = 0, DIABLO_STAT_VME, DIABLO_STAT_WME, DIABLO_STAT_MKE,

@@ -13,8 +13,8 @@ fields (and the spectral gradients the reference builds) are transformed with
 library evaluates the same averages from the Fourier coefficients (Parseval),
 so the two agree to round-off, not bit for bit.
 
-Both branches of ``homogeneousX`` are restated, and compute_BPE.  Not
-restated: HDF5/movie output and the y* binning (Bin_Ystar_and_Write).  The oracle is
+Both branches of ``homogeneousX`` are restated, with compute_BPE and the y*
+binning (Bin_Ystar_and_Write).  Not restated: HDF5/movie output.  The oracle is
 the checker of the CUDA library, never the product.
 
 Quirks kept from the reference:
@@ -139,8 +139,14 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
     k0 = 0 if homogeneous_x else 1
     eps = np.zeros(ny2)
 
+    # pointwise fields the y* binning averages (Bin_Ystar_and_Write, :1877-1972)
+    ptw = {}
+    eps_f1 = np.zeros_like(u1)
+
     def interp_sq(s, j):   # (dyf(j-1) s(j)^2 + dyf(j) s(j-1)^2) / (2 dy(j)), summed
-        return np.sum((dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j]))
+        f = (dyf[j - 1] * s[j] ** 2 + dyf[j] * s[j - 1] ** 2) / (2.0 * dy[j])
+        eps_f1[j] += f
+        return np.sum(f)
 
     for cr, kfac, kk in ((cr1, cikx, k0), (cr3, cikx, k0), (cr1, cikz, 0), (cr3, cikz, 0)):
         cs = zero_cs()                                     # du/dx dw/dx du/dz dw/dz
@@ -154,12 +160,15 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
         s = _phys(o, cs)
         for j in range(2, Nyp + 1):
             eps[j] += np.sum(s[j] ** 2)
+            eps_f1[j] += s[j] ** 2
     for j in range(2, Nyp + 1):
         su = ((u1[j] - ume_xy[j]) - (u1[j - 1] - ume_xy[j - 1])) / dy[j]      # du/dy
         sv = ((u2[j + 1] - vme_xy[j + 1]) - (u2[j - 1] - vme_xy[j - 1])) / (gy[j + 1] - gy[j - 1])
         sw = ((u3[j] - wme_xy[j]) - (u3[j - 1] - wme_xy[j - 1])) / dy[j]      # dw/dy
         eps[j] += np.sum(su ** 2) + np.sum(sv ** 2) + np.sum(sw ** 2)
+        eps_f1[j] += su ** 2 + sv ** 2 + sw ** 2
     out["epsilon"][:] = o.nu * eps / NN
+    ptw["epsilon"] = o.nu * eps_f1
 
     # compute_MKE_diss (:1130-1284): returns at once in the homogeneous branch,
     # leaving epsilon_m and the mean x gradients 0
@@ -210,13 +219,17 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
 
     # compute_TKE (:1290-1331), with the z means uu_xy, vv_xy at each x
     uu_xy, vv_xy = np.zeros((ny2, Nx)), np.zeros((ny2, Nx))
+    tke_f1 = np.zeros_like(u1)
     for name, u, me, xy in (("urms", u1, ume_xy, uu_xy), ("vrms", u2, vme_xy, vv_xy),
                             ("wrms", u3, wme_xy, None)):
         for j in range(1, Nyp + 1):
             d2 = (u[j] - me[j]) ** 2
+            tke_f1[j] += 0.5 * d2
             out[name][j] = np.sum(d2) / NN
             if xy is not None:
                 xy[j] = np.sum(d2, axis=0) / float(Nz)
+    ptw["TKE"] = tke_f1
+    ptw["KE"] = 0.5 * (u1 ** 2 + u2 ** 2 + u3 ** 2)
     urms_b = np.sqrt(integrate_y_var(o, out["urms"]))
     vrms_b = np.sqrt(integrate_y_var(o, out["vrms"]))
     wrms_b = np.sqrt(integrate_y_var(o, out["wrms"]))
@@ -261,6 +274,8 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
     for j in range(1, Nyp + 1):
         out["dudy"][j] = (ume[j] - ume[j - 1]) / (gyf[j] - gyf[j - 1])
         out["dwdy"][j] = (wme[j] - wme[j - 1]) / (gyf[j] - gyf[j - 1])
+        ptw.setdefault("shear2", np.zeros_like(u1))[j] = (((u1[j + 1] - u1[j - 1]) / (2.0 * dyf[j])) ** 2
+                                                          + ((u3[j + 1] - u3[j - 1]) / (2.0 * dyf[j])) ** 2)
         out["shear"][j] = np.sum(((u1[j + 1] - u1[j - 1]) / (2.0 * dyf[j])) ** 2
                                  + ((u3[j + 1] - u3[j - 1]) / (2.0 * dyf[j])) ** 2) / NN
     out["cp"][:] = o.p_.c[:, 0, 0].real
@@ -303,11 +318,16 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
         t, tm, txy = th[n], thme[n], thme_xy[n]
         for j in range(1, Nyp + 1):
             prof["thrms"][j] = np.sqrt(np.sum((t[j] - txy[j]) ** 2) / NN)
+            # thw_zstar bins (th_1 - thme_xy(n)) times the GY-averaged u2 fluctuation (:346-349)
+            ptw.setdefault("thw", np.zeros_like(u1))[j] = (th[0][j] - txy[j]) * 0.5 * (
+                (u2[j] - vme_xy[j]) + (u2[j + 1] - vme_xy[j + 1]))
             prof["thv"][j] = np.sum((t[j] - txy[j]) * (0.5 * (u2[j] + u2[j + 1])
                                                        - 0.5 * (vme_xy[j] + vme_xy[j + 1]))) / NN
             prof["thv_m"][j] = np.sum((txy[j] + p.dthdx[n] * (gx - 0.5 * p.lx))
                                       * (0.5 * (vme_xy[j] + vme_xy[j + 1]))) / float(Nx)
             prof["dthdy"][j] = (tm[j] - tm[j - 1]) / (gyf[j] - gyf[j - 1])
+            ptw.setdefault("chi", np.zeros_like(u1))[j] = ((r1[j] + p.dthdx[n]) ** 2 + r2[j] ** 2
+                                                       + (r3[j] + p.dthdz[n]) ** 2)
             prof["pe_diss"][j] = np.sum((r1[j] + p.dthdx[n]) ** 2 + r2[j] ** 2
                                         + (r3[j] + p.dthdz[n]) ** 2) / NN
         prof["thme"][:] = tm
@@ -338,7 +358,54 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
         bpe, pdf, bins = compute_bpe(o, th[0], homogeneous_x)
         scal["bpe"] = bpe
         res["th1_pdf"], res["th1_bin"] = pdf, bins
+        res["zstar"] = {k: bin_ystar(o, th[0], ptw[k], homogeneous_x) for k in ZSTAR}
     return res
+
+
+# the fields Bin_Ystar_and_Write averages, in the order diablo_stats returns them
+ZSTAR = ("shear2", "thw", "chi", "epsilon", "TKE", "KE")
+
+
+def _th_bins(o: OracleChannel, th1, homogeneous_x: bool):
+    """Bin index of every point of rows jstart_th(1)..jend_th(1) and the bin
+    edges th_bin(0:Nbin), as compute_BPE and Bin_Ystar_and_Write form them."""
+    from .channel import PI_REF
+    p = o.p
+    Nx = o.Nx
+    nbin = Nx
+    d0 = float(p.dthdx[0])
+    gx = np.array([(i * p.lx) / Nx for i in range(Nx)])
+    s1 = th1 + d0 * (gx - 0.5 * p.lx)[None, None, :]
+    j0, j1 = o.jstart_th[0], o.jend_th[0]
+    bins = {}
+    if not homogeneous_x:
+        thmin = -d0 * 0.5 * p.lx * float(np.float32(1.1))
+        thmax = d0 * 0.5 * p.lx * float(np.float32(1.1))
+        dth = (thmax - thmin) / nbin + 1e-14
+        th_bin = np.array([thmin + i * dth for i in range(nbin + 1)])
+        for j in range(j0, j1 + 1):
+            bins[j] = np.clip(np.trunc((s1[j] - thmin) / dth).astype(np.int64), 0, nbin - 1)
+    else:
+        ro = o.Ro_inv
+        th_bin = np.array([-(ro + 1e-14) * math.cos(i * PI_REF / nbin) for i in range(nbin + 1)])
+        for j in range(j0, j1 + 1):
+            arg = -np.minimum(np.maximum(s1[j], -ro), ro) / (ro + 1e-14)
+            bins[j] = np.clip(np.trunc(np.arccos(arg) * nbin / PI_REF).astype(np.int64), 0, nbin - 1)
+    return bins, th_bin
+
+
+def bin_ystar(o: OracleChannel, th1, field, homogeneous_x: bool):
+    """Bin_Ystar_and_Write (for/statistics.f90:1877-1972): the dyf-weighted
+    mean of `field` over the points of each th_1 bin (the bins of compute_BPE);
+    an empty bin gives 0/0 = NaN, as in the reference."""
+    bins, _ = _th_bins(o, th1, homogeneous_x)
+    nbin = o.Nx
+    pdf, fb = np.zeros(nbin), np.zeros(nbin)
+    for j, b in bins.items():
+        np.add.at(pdf, b.ravel(), o.dyf[j])
+        np.add.at(fb, b.ravel(), (field[j, :o.Nz, :o.Nx] * o.dyf[j]).ravel())
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return fb / pdf
 
 
 def compute_bpe(o: OracleChannel, th1, homogeneous_x: bool):
@@ -351,33 +418,12 @@ def compute_bpe(o: OracleChannel, th1, homogeneous_x: bool):
     single precision.  A negative bin index (th below the evenly spaced range,
     out of bounds in the reference) is taken as bin 0.  Returns (BPE, PDF, the
     lower bin edges th_bin(0:Nbin-1))."""
-    from .channel import PI_REF
     p = o.p
-    Nx, Nz, Nyp = o.Nx, o.Nz, o.Nyp
-    nbin = Nx
-    d0 = float(p.dthdx[0])
-    gx = np.array([(i * p.lx) / Nx for i in range(Nx)])
-    s1 = th1[:, :, :] + d0 * (gx - 0.5 * p.lx)[None, None, :]
+    nbin = o.Nx
+    bins, th_bin = _th_bins(o, th1, homogeneous_x)
     pdf = np.zeros(nbin)
-    j0, j1 = o.jstart_th[0], o.jend_th[0]
-    if not homogeneous_x:
-        thmin = -d0 * 0.5 * p.lx * float(np.float32(1.1))
-        thmax = d0 * 0.5 * p.lx * float(np.float32(1.1))
-        dth = (thmax - thmin) / nbin + 1e-14
-        th_bin = np.array([thmin + i * dth for i in range(nbin + 1)])
-        for j in range(j0, j1 + 1):
-            b = np.trunc((s1[j] - thmin) / dth).astype(np.int64)
-            b = np.clip(b, 0, nbin - 1)
-            np.add.at(pdf, b.ravel(), o.dyf[j])
-    else:
-        ro = o.Ro_inv
-        thmin, thmax = -ro, ro
-        th_bin = np.array([-(ro + 1e-14) * math.cos(i * PI_REF / nbin) for i in range(nbin + 1)])
-        for j in range(j0, j1 + 1):
-            arg = -np.minimum(np.maximum(s1[j], thmin), thmax) / (ro + 1e-14)
-            b = np.trunc(np.arccos(arg) * nbin / PI_REF).astype(np.int64)
-            b = np.clip(b, 0, nbin - 1)
-            np.add.at(pdf, b.ravel(), o.dyf[j])
+    for j, b in bins.items():
+        np.add.at(pdf, b.ravel(), o.dyf[j])
     pdf = pdf / np.sum(pdf)
     y_r = np.zeros(nbin + 1)
     for i in range(1, nbin + 1):

@@ -56,6 +56,13 @@ def _compare(sg, so, p):
     if p.n_th > 0:   # compute_BPE: the same bins, the same y-weighted PDF
         assert np.array_equal(sg["th1_bin"], so["th1_bin"])
         assert np.abs(sg["th1_pdf"] - so["th1_pdf"]).max() <= 1e-12
+        for k, a in so["zstar"].items():   # y* bin means; empty bins NaN on both sides
+            b = sg["zstar"][k]
+            assert np.array_equal(np.isnan(a), np.isnan(b)), k
+            ok = ~np.isnan(a)
+            if ok.any():
+                scale = max(np.abs(a[ok]).max(), 1e-300)
+                assert np.abs(b[ok] - a[ok]).max() <= TOL * scale, (k, np.abs(b[ok] - a[ok]).max() / scale)
     for k, a in so["scalars"].items():
         b = sg["scalars"][k]
         assert abs(b - a) <= 1e-12 * max(abs(a), 1e-300) or a == b, (k, a, b)
@@ -167,7 +174,8 @@ def test_stats_rejects_short_buffers(cuda_device):
     try:
         n = ch.lib.diablo_stats_size(ch.ctx)
         assert n == p.ny * (len(_lib.STAT_PROFILES) + p.n_th * len(_lib.STAT_TH_PROFILES)) \
-            + p.nx // 2 + (2 * p.nx if p.n_th > 0 else 0) + len(_lib.STAT_SCALARS)
+            + p.nx // 2 + ((2 + len(_lib.STAT_ZSTAR)) * p.nx if p.n_th > 0 else 0) \
+            + len(_lib.STAT_SCALARS)
         out = np.zeros(n)
         ptr = out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         assert ch.lib.diablo_stats(ch.ctx, 1, ptr, n - 1) == _lib.ERR_ARG

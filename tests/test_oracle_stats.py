@@ -371,3 +371,23 @@ def test_bpe_evenly_spaced_bins_sorted_profile():
     ref = -np.sum(mids * 0.5 * (y_r[1:] + y_r[:-1]) * np.diff(y_r)) / p.ly
     assert bpe == pytest.approx(ref, rel=1e-12)
     assert bins[0] == thmin
+
+
+def test_ystar_binning_single_bin_known_answer():
+    """Bin_Ystar_and_Write with th_1 = 0 and no background gradient: every
+    point lands in one th bin, whose value is the dyf-weighted mean of the field
+    over rows jstart_th..jend_th; the other bins are empty (0/0 = NaN, as the
+    reference writes them)."""
+    from oracle.stats import bin_ystar
+    p = small_params(nx=16, ny=25, nz=12, n_th=1, ro=2.0, grav_y=0.0)
+    gy = grid_for(p)
+    o = _oracle(p, gy)
+    th1 = np.zeros((p.ny + 2, p.nz, p.nx))
+    U = 1.0 - o.gyf ** 2
+    field = np.broadcast_to(0.5 * U[:, None, None] ** 2, (p.ny + 2, p.nz, p.nx))
+    fb = bin_ystar(o, th1, field, True)
+    b = p.nx // 2 - 1
+    J = range(o.jstart_th[0], o.jend_th[0] + 1)
+    want = sum(o.dyf[j] * 0.5 * U[j] ** 2 for j in J) / sum(o.dyf[j] for j in J)
+    assert fb[b] == pytest.approx(want, rel=1e-13)
+    assert np.isnan(np.delete(fb, b)).all()
