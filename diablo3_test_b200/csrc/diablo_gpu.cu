@@ -1118,12 +1118,25 @@ static int substep_les_t(diablo_ctx* ctx, int rk) {
       sa.ubc[i] = a.ubc[i]; sa.vbc[i] = a.vbc[i]; sa.wbc[i] = a.wbc[i];
       sa.uc1[i] = a.uc1[i]; sa.vc1[i] = a.vc1[i]; sa.wc1[i] = a.wc1[i];
     }
-    // one warp per (field, column)
+    // one warp per (field, column); PS_W adjacent columns per block through
+    // shared-memory tiles when a field's columns split evenly into them
     const size_t threads = (size_t)nf * sa.cols * 32;
-    const unsigned blocks = (unsigned)((threads + 127) / 128);
+    const bool tiled = sa.cols % PS_W == 0;
+    const int tpb = tiled ? 32 * PS_W : 128;
+    const unsigned blocks = (unsigned)((threads + tpb - 1) / tpb);
+    const int tsm = tiled ? 3 * sa.n * PS_W * (int)sizeof(double) : 0;
     Prof pr(ctx, K_SOLVE);
     switch (std::max(3, (sa.n + 31) / 32)) {
-#define X(r) case r: k_phys_solve<P, r><<<blocks, 128, 0, ctx->stream>>>(sa); break;
+#define X(r)                                                                                            \
+  case r:                                                                                               \
+    if (tiled) {                                                                                        \
+      if (tsm > 48 * 1024)                                                                              \
+        CK(cudaFuncSetAttribute(k_phys_solve<P, r, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm)); \
+      k_phys_solve<P, r, true><<<blocks, tpb, tsm, ctx->stream>>>(sa);                                  \
+    } else {                                                                                            \
+      k_phys_solve<P, r, false><<<blocks, tpb, 0, ctx->stream>>>(sa);                                   \
+    }                                                                                                   \
+    break;
       X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
 #undef X
       default: return DIABLO_ERR_SIZE;

@@ -458,16 +458,21 @@ struct PhysSolveArgs {
 
 // One warp per (field, physical column): each lane builds R consecutive rows
 // of the column's system and csolve::warp_tridiag solves it (the partition
-// method of the Fourier-space solves).  Warps of a block take adjacent
-// columns, so the 32-byte sectors of their row loads are shared through L1.
-// Rows past Ny+1 are identity rows; the last real row has no upper
-// coefficient, so they do not couple.
-template <typename P, int R>
-__global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
+// method of the Fourier-space solves).  Rows past Ny+1 are identity rows; the
+// last real row has no upper coefficient, so they do not couple.
+// TILED (when the columns of a field are a multiple of PS_W): a block of PS_W
+// warps takes PS_W adjacent columns of one field and first copies their u, r
+// and nu_t rows into shared memory with coalesced PS_W-wide row loads (a lane
+// otherwise reads 8 scattered bytes per row); the solution goes back the same
+// way.  Untiled: each warp reads its column from global memory.
+constexpr int PS_W = 8;
+template <typename P, int R, bool TILED>
+__global__ void __launch_bounds__(TILED ? 32 * PS_W : 128) k_phys_solve(PhysSolveArgs<P> a) {
   using namespace csolve;
+  extern __shared__ double ps_tile[];
   const int lane = threadIdx.x & 31;
   const size_t gid = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (gid >= (size_t)a.nf * a.cols) return;   // the whole warp leaves together
+  if (gid >= (size_t)a.nf * a.cols) return;   // the whole warp (TILED: block) leaves together
   const int f = gid / a.cols;
   const size_t col = gid % a.cols;
   const size_t ps = a.cols;
@@ -475,6 +480,25 @@ __global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
   const double* r = a.r[f];
   double* u = a.u[f];
   const P* nt = f < 3 ? a.nu_t : a.kap[f - 3];
+  // tiles [n][PS_W] of u, r, nu_t; c = this warp's column in them
+  double* tu = ps_tile;
+  double* tr = tu + (size_t)n * PS_W;
+  double* tn = tr + (size_t)n * PS_W;
+  const int c = threadIdx.x >> 5;
+  const size_t col0 = col - c;
+  if (TILED) {
+    for (int idx = threadIdx.x; idx < n * PS_W; idx += blockDim.x) {
+      const size_t o = (size_t)(idx / PS_W) * ps + col0 + idx % PS_W;
+      tu[idx] = u[o];
+      tr[idx] = r[o];
+      tn[idx] = (double)nt[o];
+    }
+    __syncthreads();
+  }
+  // row j (and its neighbours) of u, r, nu_t in this column
+  auto U = [&](int j) -> double { return TILED ? tu[j * PS_W + c] : u[(size_t)j * ps + col]; };
+  auto RR = [&](int j) -> double { return TILED ? tr[j * PS_W + c] : r[(size_t)j * ps + col]; };
+  auto NT = [&](int j) -> double { return TILED ? tn[j * PS_W + c] : (double)nt[(size_t)j * ps + col]; };
   int lo, hi, w0, b0, b1;
   double c0v, c1v, tc;
   if (f == 1) { lo = 2; hi = nyp; w0 = 1; b0 = a.vbc[0]; b1 = a.vbc[1]; c0v = a.vc1[0]; c1v = a.vc1[1]; tc = a.temp1 * a.nu_v; }
@@ -493,14 +517,13 @@ __global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
   auto row = [&](int j, double& A, double& B, double& C, double& D) {
     A = 0.0; B = 1.0; C = 0.0; D = 0.0;
     if (j >= lo && j <= hi) {
-      const size_t o = (size_t)j * ps + col;
-      const double uc = u[o], um = u[o - ps], up = u[o + ps];
-      double rhs = r[o];
+      const double uc = U(j), um = U(j - 1), up = U(j + 1);
+      double rhs = RR(j);
       // the reference's quotients by dy and dyf, as products with the
       // precomputed reciprocals (FP64 division is a long instruction sequence)
       if (f == 1) {
         const double idyj = a.idy[j], idyfj = a.idyf[j], idyfm = a.idyf[j - 1];
-        const double ntp = 0.5 * (nt[o] + nt[o + ps]), ntm = 0.5 * (nt[o] + nt[o - ps]);
+        const double ntp = 0.5 * (NT(j) + NT(j + 1)), ntm = 0.5 * (NT(j) + NT(j - 1));
         const double gp = (up - uc) * idyfj, gm = (uc - um) * idyfm;
         rhs += tc * ((gp - gm) * idyj);
         rhs += a.temp2 * ((ntp * gp - ntm * gm) * idyj);
@@ -510,7 +533,7 @@ __global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
         C = -(tc + a.temp2 * ntp) * wp;
       } else {
         const double idyj = a.idy[j], idyj1 = a.idy[j + 1], idyfj = a.idyf[j];
-        const double ntp = nt[o + ps], ntc = nt[o];
+        const double ntp = NT(j + 1), ntc = NT(j);
         const double gp = (up - uc) * idyj1, gm = (uc - um) * idyj;
         rhs += tc * ((gp - gm) * idyfj);
         rhs += a.temp2 * ((ntp * gp - ntc * gm) * idyfj);
@@ -551,12 +574,26 @@ __global__ void __launch_bounds__(128) k_phys_solve(PhysSolveArgs<P> a) {
   warp_tridiag<R>(Am, Bm, Cm, Dm, lane);
   // every lane's reads of u (its rows and their neighbours) are done: write
   // the solution on the rows the reference writes
-  __syncwarp();
   const int w1 = nyp + 1;
+  if (TILED) {
+    __syncthreads();
 #pragma unroll
-  for (int rr = 0; rr < R; ++rr) {
-    const int j = lane * R + rr;
-    if (j < n && j >= w0 && j <= w1) u[(size_t)j * ps + col] = Dm[rr].x;
+    for (int rr = 0; rr < R; ++rr) {
+      const int j = lane * R + rr;
+      if (j < n && j >= w0 && j <= w1) tu[j * PS_W + c] = Dm[rr].x;
+    }
+    __syncthreads();
+    // rows outside the write range hold the values just read: rewriting them
+    // leaves them unchanged
+    for (int idx = threadIdx.x; idx < n * PS_W; idx += blockDim.x)
+      u[(size_t)(idx / PS_W) * ps + col0 + idx % PS_W] = tu[idx];
+  } else {
+    __syncwarp();
+#pragma unroll
+    for (int rr = 0; rr < R; ++rr) {
+      const int j = lane * R + rr;
+      if (j < n && j >= w0 && j <= w1) u[(size_t)j * ps + col] = Dm[rr].x;
+    }
   }
 }
 
