@@ -325,6 +325,8 @@ __global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ Stats
   __syncthreads();
   const size_t pn = (size_t)a.nz * a.nx;
   const size_t tot = (size_t)(a.jhi - a.jlo + 1) * pn;
+  int cur = -1;
+  double accw = 0.0;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
     const int j = a.jlo + (int)(q / pn);
     const size_t r = q % pn;
@@ -335,8 +337,15 @@ __global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ Stats
     // truncation toward zero, then the bin range (clamping first keeps the
     // conversion in range; fmax also sends NaN to bin 0)
     x = fmin(fmax(x, 0.0), (double)(a.nbin - 1));
-    atomicAdd(&hist[(int)x], a.dyf[j]);
+    const int b = (int)x;
+    if (b != cur) {   // runs in one bin reach shared memory once (see k_stats_zstar)
+      if (cur >= 0) atomicAdd(&hist[cur], accw);
+      cur = b;
+      accw = 0.0;
+    }
+    accw += a.dyf[j];
   }
+  if (cur >= 0) atomicAdd(&hist[cur], accw);
   __syncthreads();
   for (int b = threadIdx.x; b < a.nbin; b += blockDim.x)
     if (hist[b] != 0.0) atomicAdd(&a.pdf[b], hist[b]);
@@ -411,6 +420,10 @@ __global__ void __launch_bounds__(256) k_stats_zstar(const __grid_constant__ Sta
   const double* u2 = a.u[1];
   const double* u3 = a.u[2];
   const size_t tot = (size_t)(a.jhi - a.jlo + 1) * pn;
+  int cur = -1;
+  double accw = 0.0, acc[ZS_N];
+#pragma unroll
+  for (int k = 0; k < ZS_N; ++k) acc[k] = 0.0;
   for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
     const int j = a.jlo + (int)(q / pn);
     const size_t r = q % pn;
@@ -450,9 +463,28 @@ __global__ void __launch_bounds__(256) k_stats_zstar(const __grid_constant__ Sta
       f[ZS_TKE] = 0.5 * (t1 * t1 + t2 * t2 + t3 * t3);
       f[ZS_KE] = 0.5 * (u1[o] * u1[o] + u2[o] * u2[o] + u3[o] * u3[o]);
     }
-    atomicAdd(&zh[b], w);
+    // runs of points in one bin accumulate in registers and reach shared
+    // memory once (a flat or weakly varying th_1 puts most points in a few
+    // bins, where one atomic per point would serialise)
+    if (b != cur) {
+      if (cur >= 0) {
+        atomicAdd(&zh[cur], accw);
 #pragma unroll
-    for (int k = 0; k < ZS_N; ++k) atomicAdd(&zh[(1 + k) * nb + b], f[k] * w);
+        for (int k = 0; k < ZS_N; ++k) atomicAdd(&zh[(1 + k) * nb + cur], acc[k]);
+      }
+      cur = b;
+      accw = 0.0;
+#pragma unroll
+      for (int k = 0; k < ZS_N; ++k) acc[k] = 0.0;
+    }
+    accw += w;
+#pragma unroll
+    for (int k = 0; k < ZS_N; ++k) acc[k] += f[k] * w;
+  }
+  if (cur >= 0) {
+    atomicAdd(&zh[cur], accw);
+#pragma unroll
+    for (int k = 0; k < ZS_N; ++k) atomicAdd(&zh[(1 + k) * nb + cur], acc[k]);
   }
   __syncthreads();
   for (int b = threadIdx.x; b < (1 + ZS_N) * nb; b += blockDim.x)
