@@ -317,6 +317,20 @@ DI Pair<T> ld2(const T* p) {
   return Pair<T>{v.x, v.y};
 }
 
+// Division of a row's products by one per-row denominator.  The FP32 build
+// multiplies by the reciprocal (one rounding more, inside the mixed path's
+// tolerance, and no IEEE divide sequence per element); FP64 divides, so the
+// FP64 path rounds as the reference does.
+template <typename T>
+struct DivBy {
+  T d, inv;
+  DI explicit DivBy(T den) : d(den), inv((T)1 / den) {}
+  DI T operator()(T x) const {
+    if constexpr (sizeof(T) == 4) return x * inv;
+    else return x / d;
+  }
+};
+
 // x(j) * y(j)
 template <typename T, int N1, int N2>
 DI void fill_prod(typename CT<T>::C (&v)[N1], const T* x, const T* y, size_t off, int t) {
@@ -334,13 +348,14 @@ DI void fill_prod(typename CT<T>::C (&v)[N1], const T* x, const T* y, size_t off
 template <typename T, int N1, int N2>
 DI void fill_flux(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t off, size_t ps,
                   T den, int t) {
+  const DivBy<T> dv(den);
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     const size_t o = off + 2 * (n1 * N2 + t);
     Pair<T> p = ld2(uf + o + ps), c = ld2(uf + o), m = ld2(uf + o - ps);
     Pair<T> vp = ld2(u2 + o + ps), vc = ld2(u2 + o);
-    v[n1] = CT<T>::mk((p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a) / den,
-                      (p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b) / den);
+    v[n1] = CT<T>::mk(dv(p.a * vp.a + c.a * vp.a - c.a * vc.a - m.a * vc.a),
+                      dv(p.b * vp.b + c.b * vp.b - c.b * vc.b - m.b * vc.b));
   }
 }
 
@@ -348,24 +363,26 @@ DI void fill_flux(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t o
 template <typename T, int N1, int N2>
 DI void fill_interp(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t off, size_t ps,
                     T dyfj, T dyfm, T den, int t) {
+  const DivBy<T> dv(den);
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     const size_t o = off + 2 * (n1 * N2 + t);
     Pair<T> c = ld2(uf + o), m = ld2(uf + o - ps), w = ld2(u2 + o);
-    v[n1] = CT<T>::mk(((dyfj * c.a + dyfm * m.a) / den) * w.a, ((dyfj * c.b + dyfm * m.b) / den) * w.b);
+    v[n1] = CT<T>::mk(dv(dyfj * c.a + dyfm * m.a) * w.a, dv(dyfj * c.b + dyfm * m.b) * w.b);
   }
 }
 
 // (0.25 (u2(j) + u2(j+1))^2 - 0.25 (u2(j) + u2(j-1))^2) / dy(j)
 template <typename T, int N1, int N2>
 DI void fill_v2(typename CT<T>::C (&v)[N1], const T* u2, size_t off, size_t ps, T dyj, int t) {
+  const DivBy<T> dv(dyj);
 #pragma unroll
   for (int n1 = 0; n1 < N1; ++n1) {
     const size_t o = off + 2 * (n1 * N2 + t);
     Pair<T> p = ld2(u2 + o + ps), c = ld2(u2 + o), m = ld2(u2 + o - ps);
     T sa = c.a + p.a, sb = c.b + p.b, da = c.a + m.a, db = c.b + m.b;
-    v[n1] = CT<T>::mk(((T)0.25 * (sa * sa) - (T)0.25 * (da * da)) / dyj,
-                      ((T)0.25 * (sb * sb) - (T)0.25 * (db * db)) / dyj);
+    v[n1] = CT<T>::mk(dv((T)0.25 * (sa * sa) - (T)0.25 * (da * da)),
+                      dv((T)0.25 * (sb * sb) - (T)0.25 * (db * db)));
   }
 }
 
