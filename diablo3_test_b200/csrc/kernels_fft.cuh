@@ -98,12 +98,19 @@ template <typename C, typename CO> struct ZFwdArgs {
 };
 
 // Blocks per SM the FP32 z-forward and x-inverse kernels' register caps are
-// set for.  Measured at 256 x 257 x 256: 6 (80 registers) took the combine
-// kernel from 0.234 to 0.216 ms per launch; 7 (72 registers) spills and
-// measured 0.220.  The x inverse holds 64 registers without spilling and, with its
-// single row buffer, fits eight blocks per SM.
+// set for, and whether k_zfwd's combine form loads B together with A, before
+// A's transform.  Measured at 256 x 257 x 256 with B loaded after A's
+// transform: 6 blocks (80 registers) took the combine kernel from 0.234 to
+// 0.216 ms per launch; 7 (72 registers) spills and measured 0.220.  Loading B
+// with A: 0.2135 ms at 5 blocks (96 registers), 0.2173 at 6 (spills) and
+// 0.2215 at 4, against 0.2150 without; the FP64 combine kernel went from
+// 0.327 to 0.320 ms.  The x inverse holds 64 registers and, with its single
+// row buffer, fits eight blocks per SM.
 #ifndef ZFWD32_MIN_BLOCKS
-#define ZFWD32_MIN_BLOCKS 6
+#define ZFWD32_MIN_BLOCKS 5
+#endif
+#ifndef ZFWD_PREFETCH
+#define ZFWD_PREFETCH 1
 #endif
 // The FP64 x inverse keeps separate spectrum and tile buffers: sharing them
 // measured 0.693 against 0.677 ms per launch at 256 x 257 x 256.
@@ -125,12 +132,20 @@ __global__ void __launch_bounds__(N2* S, sizeof(C) == 8 ? ZFWD32_MIN_BLOCKS : 1)
   constexpr int NR = (N1 + N2 - 1) / N2;  // step-2 rows per thread
   C ra[NR][N2];
   const T sc = (T)a.scale;
+  // B's loads are issued with A's when ZFWD_PREFETCH is set
+  constexpr bool PF = COMBINE && ZFWD_PREFETCH;
+  C vb[PF ? N1 : 1];
   // transform A
   {
     const C* src = a.srcA[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
     C v[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? src[n1 * N2 + t] : czero<C>();
+    if (PF) {
+      const C* srcb = a.srcB[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) vb[PF ? n1 : 0] = ok ? srcb[n1 * N2 + t] : czero<C>();
+    }
     dfft::step1<N1, N2, -1>(v, t, a.tw, sm[s]);
     __syncthreads();
 #pragma unroll
@@ -141,10 +156,15 @@ __global__ void __launch_bounds__(N2* S, sizeof(C) == 8 ? ZFWD32_MIN_BLOCKS : 1)
   }
   if (COMBINE) {
     __syncthreads();
-    const C* src = a.srcB[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
     C v[N1];
+    if (PF) {
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? src[n1 * N2 + t] : czero<C>();
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = vb[PF ? n1 : 0];
+    } else {
+      const C* src = a.srcB[f] + (size_t)(a.q0 + (ok ? q : 0)) * a.g.nz;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = ok ? src[n1 * N2 + t] : czero<C>();
+    }
     dfft::step1<N1, N2, -1>(v, t, a.tw, sm[s]);
     __syncthreads();
 #pragma unroll
