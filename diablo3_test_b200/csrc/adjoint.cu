@@ -1,0 +1,293 @@
+// Discrete adjoint of diablo_step with checkpoint-and-recompute.
+#include "internal.h"
+#include "kernels_adjoint.cuh"
+
+// ==========================================================================
+// Discrete adjoint of diablo_step (velocity-only DNS, FP64), with
+// checkpoint-and-recompute: diablo_adjoint_record stores the state every
+// `every` steps; diablo_adjoint_run recomputes each segment from its
+// checkpoint (keeping the velocities entering every substep) and runs the
+// substep adjoints backwards through it.
+
+int adj_free(diablo_ctx* ctx) {
+  diablo_ctx::Tape& T = ctx->tape;
+  auto rel = [&](void* p) {
+    if (!p) return;
+    for (size_t i = 0; i < ctx->allocs.size(); ++i)
+      if (ctx->allocs[i] == p) { ctx->allocs.erase(ctx->allocs.begin() + i); break; }
+    cudaFree(p);
+  };
+  for (double2* p : T.ckpt) rel(p);
+  for (double2* p : T.sub) rel(p);
+  T.ckpt.clear();
+  T.sub.clear();
+  T.ready = 0;
+  return 0;
+}
+
+// host-built rows of the substep systems (the forward's expressions)
+void adj_rows(diablo_ctx* ctx, std::vector<double>& cn, std::vector<double>& rmask,
+                     std::vector<double>& pa) {
+  const diablo_params& p = ctx->p;
+  const int n = ctx->nyp2, nyp = ctx->ny;
+  const std::vector<double>& dy = ctx->h_dy;
+  const std::vector<double>& dyf = ctx->h_dyf;
+  cn.assign((size_t)3 * 3 * 3 * n, 0.0);
+  rmask.assign((size_t)3 * n, 0.0);
+  pa.assign((size_t)3 * n, 0.0);
+  for (int j = 2; j <= nyp - 1; ++j) {
+    pa[j] = 1. / (dy[j] * dyf[j]);
+    pa[n + j] = 1. / (dy[j + 1] * dyf[j]);
+    pa[2 * n + j] = -1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]);
+  }
+  for (int rk = 0; rk < 3; ++rk) {
+    const double tc = 0.5 * ctx->nu * ctx->h_bar[rk] * p.nu_v_scale;
+    for (int f = 0; f < 3; ++f) {
+      double* A = &cn[((size_t)rk * 3 + f) * 3 * n];
+      double* B = A + n;
+      double* C = B + n;
+      double* rm = &rmask[(size_t)f * n];
+      for (int j = 0; j < n; ++j) { A[j] = 0.0; B[j] = 1.0; C[j] = 0.0; }
+      if (f != 1) {
+        for (int j = ctx->jstart; j <= ctx->jend; ++j) {
+          A[j] = -tc / (dy[j] * dyf[j]);
+          B[j] = 1. - tc * (-1. / (dy[j + 1] * dyf[j]) - 1. / (dy[j] * dyf[j]));
+          C[j] = -tc / (dy[j + 1] * dyf[j]);
+          rm[j] = 1.0;
+        }
+        const int bmin = f == 0 ? p.u_bc_ymin : p.w_bc_ymin, bmax = f == 0 ? p.u_bc_ymax : p.w_bc_ymax;
+        A[0] = 0; B[0] = 1; C[0] = 0;
+        if (bmin == 0) { A[1] = 0; B[1] = 1; C[1] = 0; } else { A[1] = 0; B[1] = -1; C[1] = 1; }
+        A[nyp + 1] = 0; B[nyp + 1] = 1; C[nyp + 1] = 0;
+        if (bmax == 0) { A[nyp] = 0; B[nyp] = 1; C[nyp] = 0; } else { A[nyp] = -1; B[nyp] = 1; C[nyp] = 0; }
+        rm[0] = rm[1] = rm[nyp] = rm[nyp + 1] = 0.0;
+      } else {
+        for (int j = 2; j <= nyp; ++j) {
+          A[j] = -tc / (dyf[j - 1] * dy[j]);
+          B[j] = 1. + tc / (dyf[j] * dy[j]) + tc / (dyf[j - 1] * dy[j]);
+          C[j] = -tc / (dyf[j] * dy[j]);
+          rm[j] = 1.0;
+        }
+        if (p.v_bc_ymin == 0) {
+          for (int r = 1; r <= 2; ++r) { A[r] = 0; B[r] = 1; C[r] = 0; rm[r] = 0; }
+        } else {
+          A[1] = 0; B[1] = -1; C[1] = 1; rm[1] = 0;
+        }
+        A[0] = 0; B[0] = 1; C[0] = 0; rm[0] = 0;
+        if (p.v_bc_ymax == 0) {
+          for (int r = nyp; r <= nyp + 1; ++r) { A[r] = 0; B[r] = 1; C[r] = 0; rm[r] = 0; }
+        } else {
+          A[nyp + 1] = -1; B[nyp + 1] = 1; C[nyp + 1] = 0; rm[nyp + 1] = 0;
+        }
+      }
+    }
+  }
+}
+
+int adj_supported(const diablo_ctx* ctx) {
+  if (ctx->nth != 0 || ctx->p.use_les || ctx->precision != DIABLO_FP64 || ctx->p.variable_dt)
+    return DIABLO_ERR_UNSUPPORTED;
+  return 0;
+}
+
+int adj_alloc(diablo_ctx* ctx, int nsteps, int every) {
+  diablo_ctx::Tape& T = ctx->tape;
+  const size_t fe = four_elems(ctx) * sizeof(double2), pe = phys_elems(ctx) * sizeof(double);
+  int rc;
+  // the checkpoint and substep buffers are kept while nsteps and every stay the same
+  if (T.ckpt.empty() || T.nsteps != nsteps || T.every != every) {
+    adj_free(ctx);
+    T.nsteps = nsteps;
+    T.every = every;
+    T.nseg = (nsteps + every - 1) / every;
+    T.ckpt.assign((size_t)(T.nseg + 1) * 4, nullptr);
+    for (auto& p : T.ckpt) if ((rc = dev_alloc(ctx, (void**)&p, fe))) return rc;
+    T.sub.assign((size_t)every * 9, nullptr);
+    for (auto& p : T.sub) if ((rc = dev_alloc(ctx, (void**)&p, fe))) return rc;
+    T.ckpt_step.assign(T.nseg + 1, 0);
+    T.ckpt_time.assign(T.nseg + 1, 0.0);
+  }
+  T.ready = 0;
+  if (!T.work_ready) {
+#define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
+    for (int q = 0; q < 4; ++q) { AL(T.lu[q], fe); AL(T.ou[q], fe); }
+    for (int q = 0; q < 3; ++q) { AL(T.lF[q], fe); AL(T.oF[q], fe); AL(T.lnl[q], fe); AL(T.lf3[q], fe);
+                                  AL(T.up[q], pe); AL(T.lp3[q], pe); }
+    for (int q = 0; q < 8; ++q) { AL(T.pf[q], fe); AL(T.pp[q], pe); }
+    AL(T.d_cn, (size_t)27 * ctx->nyp2 * sizeof(double));
+    AL(T.d_rmask, (size_t)3 * ctx->nyp2 * sizeof(double));
+    AL(T.d_pa, (size_t)3 * ctx->nyp2 * sizeof(double));
+#undef AL
+    T.work_ready = 1;
+  }
+  std::vector<double> cn, rm, pa;
+  adj_rows(ctx, cn, rm, pa);
+  CK(cudaMemcpyAsync(T.d_cn, cn.data(), cn.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(T.d_rmask, rm.data(), rm.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(T.d_pa, pa.data(), pa.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int copy_fields(diablo_ctx* ctx, double2* const* dst, double2* const* src, int nf) {
+  const size_t fe = four_elems(ctx) * sizeof(double2);
+  for (int q = 0; q < nf; ++q) CK(cudaMemcpyAsync(dst[q], src[q], fe, cudaMemcpyDeviceToDevice, ctx->stream));
+  return 0;
+}
+
+// Adjoint of substep rk: T.lu (lambda of the substep's output state) and
+// T.lF (lambda of its cf) become the lambdas of its input; u_in are the
+// velocities that entered the substep.
+int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
+  diablo_ctx::Tape& T = ctx->tape;
+  const diablo_params& p = ctx->p;
+  const double h = ctx->h_bar[rk - 1];
+  const FGeom fg{ctx->ny, ctx->nyp2, ctx->nkx1, ctx->nk2, ctx->kp, (size_t)ctx->nkx1 * ctx->kp};
+  const size_t ftot = four_elems(ctx), ptot = phys_elems(ctx);
+  int rc;
+  {
+    AdjColArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < 3; ++f) {
+      a.lu[f] = T.lu[f];
+      a.lF[f] = rk < 3 ? T.lF[f] : nullptr;
+      a.ou[f] = T.ou[f];
+      a.oF[f] = rk > 1 ? T.oF[f] : nullptr;
+      a.onl[f] = T.lnl[f];
+    }
+    a.lp = T.lu[3];
+    a.op = T.ou[3];
+    a.cn = T.d_cn + (size_t)(rk - 1) * 9 * ctx->nyp2;
+    a.rmask = T.d_rmask;
+    a.pa = T.d_pa;
+    a.kx = ctx->d_kx; a.kz = ctx->d_kz; a.dy = ctx->d_dy; a.dyf = ctx->d_dyf;
+    a.t3 = ZETA_BAR[rk - 1] * h; a.t4 = h; a.t5 = BETA_BAR[rk - 1] * h;
+    a.tc = 0.5 * ctx->nu * h * p.nu_v_scale;
+    a.nu = ctx->nu; a.roinvd = ctx->ro_inv / p.delta; a.beta = p.beta;
+    a.n = ctx->nyp2; a.nyp = ctx->ny; a.nkx1 = ctx->nkx1; a.nk2 = ctx->nk2; a.kp = ctx->kp;
+    a.ncol = ctx->nkx1 * ctx->nk2;
+    a.jstart = ctx->jstart; a.jend = ctx->jend; a.rk = rk;
+    Prof pr(ctx, K_OTHER);
+    const int warps = 4;
+    dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
+    switch (rows_per_lane(ctx->nyp2)) {
+#define X(r) case r: k_adj_column<r><<<grd, blk, 0, ctx->stream>>>(a); break;
+      X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+      default: return DIABLO_ERR_SIZE;
+    }
+  }
+  {
+    AdjNlPrepArgs a;
+    for (int f = 0; f < 3; ++f) a.lnl[f] = T.lnl[f];
+    for (int q = 0; q < 8; ++q) a.out[q] = T.pf[q];
+    a.kx = ctx->d_kx; a.kz = ctx->d_kz;
+    a.inv = 1.0 / ((double)ctx->nx * ctx->nz);
+    a.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_adj_nl_prep<<<grid1d(ftot), 256, 0, ctx->stream>>>(a);
+  }
+  if ((rc = ifft_batch(ctx, T.pf, T.pp, 8))) return rc;
+  if ((rc = ifft_batch(ctx, u_in, T.up, 3))) return rc;
+  {
+    AdjNlPointArgs a;
+    for (int q = 0; q < 8; ++q) a.P[q] = T.pp[q];
+    a.u1 = T.up[0]; a.u2 = T.up[1]; a.u3 = T.up[2];
+    a.o1 = T.lp3[0]; a.o2 = T.lp3[1]; a.o3 = T.lp3[2];
+    a.dy = ctx->d_dy; a.dyf = ctx->d_dyf;
+    a.nyp = ctx->ny;
+    a.ps = (size_t)ctx->nz * ctx->nx;
+    Prof pr(ctx, K_OTHER);
+    k_adj_nl_point<<<grid1d(ptot), 256, 0, ctx->stream>>>(a);
+  }
+  if ((rc = fft_batch(ctx, T.lp3, T.lf3, 3))) return rc;
+  {
+    AdjAccArgs a;
+    for (int f = 0; f < 3; ++f) { a.ou[f] = T.ou[f]; a.add[f] = T.lf3[f]; }
+    a.scale = (double)ctx->nx * ctx->nz;
+    a.g = fg;
+    Prof pr(ctx, K_OTHER);
+    k_adj_acc<<<grid1d(ftot), 256, 0, ctx->stream>>>(a);
+  }
+  CK(cudaGetLastError());
+  for (int q = 0; q < 4; ++q) std::swap(T.lu[q], T.ou[q]);
+  for (int q = 0; q < 3; ++q) std::swap(T.lF[q], T.oF[q]);
+  return 0;
+}
+
+extern "C" {
+
+int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every) {
+  if (!ctx || nsteps <= 0 || every <= 0) return DIABLO_ERR_ARG;
+  int rc;
+  if ((rc = adj_supported(ctx))) return rc;
+  if ((rc = ensure_scratch(ctx)) || (rc = ensure_xs64(ctx))) return rc;
+  if ((rc = adj_alloc(ctx, nsteps, every))) return rc;
+  diablo_ctx::Tape& T = ctx->tape;
+  for (int s = 0; s < nsteps; ++s) {
+    if (s % every == 0) {
+      const int k = s / every;
+      double2* src[4] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2], ctx->st[ctx->cur][3]};
+      if ((rc = copy_fields(ctx, &T.ckpt[(size_t)k * 4], src, 4))) return rc;
+      T.ckpt_step[k] = ctx->time_step;
+      T.ckpt_time[k] = ctx->time;
+    }
+    if ((rc = one_step(ctx))) return rc;
+  }
+  double2* src[4] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2], ctx->st[ctx->cur][3]};
+  if ((rc = copy_fields(ctx, &T.ckpt[(size_t)T.nseg * 4], src, 4))) return rc;
+  T.ckpt_step[T.nseg] = ctx->time_step;
+  T.ckpt_time[T.nseg] = ctx->time;
+  T.step_end = ctx->time_step;
+  T.time_end = ctx->time;
+  T.gen_end = ctx->generation;
+  T.ready = 1;
+  return 0;
+}
+
+int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam) {
+  if (!ctx || !lam) return DIABLO_ERR_ARG;
+  for (int q = 0; q < 4; ++q) if (!lam[q]) return DIABLO_ERR_ARG;
+  diablo_ctx::Tape& T = ctx->tape;
+  if (!T.ready || ctx->time_step != T.step_end || ctx->generation != T.gen_end) return DIABLO_ERR_STATE;
+  int rc;
+  if ((rc = ensure_bscratch(ctx))) return rc;
+  const size_t fe = four_elems(ctx) * sizeof(double2);
+  for (int q = 0; q < 4; ++q)
+    if ((rc = four_in(ctx, lam[q], T.lu[q], false))) return rc;
+  for (int q = 0; q < 3; ++q) CK(cudaMemsetAsync(T.lF[q], 0, fe, ctx->stream));
+  for (int k = T.nseg - 1; k >= 0; --k) {
+    // recompute the segment from its checkpoint, keeping each substep's input velocities
+    double2* dst[4] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2], ctx->st[ctx->cur][3]};
+    if ((rc = copy_fields(ctx, dst, &T.ckpt[(size_t)k * 4], 4))) return rc;
+    ctx->time_step = T.ckpt_step[k];
+    ctx->time = T.ckpt_time[k];
+    const int s0 = k * T.every, s1 = std::min(T.nsteps, s0 + T.every);
+    for (int s = s0; s < s1; ++s) {
+      ctx->time_step += 1;
+      for (int rk = 1; rk <= 3; ++rk) {
+        double2** keep = &T.sub[((size_t)(s - s0) * 3 + (rk - 1)) * 3];
+        double2* cu[3] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2]};
+        if ((rc = copy_fields(ctx, keep, cu, 3))) return rc;
+        if ((rc = substep(ctx, rk))) return rc;
+      }
+      ctx->time += ctx->delta_t;
+    }
+    for (int s = s1 - 1; s >= s0; --s)
+      for (int rk = 3; rk >= 1; --rk)
+        if ((rc = adj_substep(ctx, rk, &T.sub[((size_t)(s - s0) * 3 + (rk - 1)) * 3]))) return rc;
+  }
+  // back to the recorded final state
+  double2* dst[4] = {ctx->st[ctx->cur][0], ctx->st[ctx->cur][1], ctx->st[ctx->cur][2], ctx->st[ctx->cur][3]};
+  if ((rc = copy_fields(ctx, dst, &T.ckpt[(size_t)T.nseg * 4], 4))) return rc;
+  ctx->time_step = T.step_end;
+  ctx->time = T.time_end;
+  for (int q = 0; q < 4; ++q)
+    if ((rc = four_out(ctx, T.lu[q], lam[q]))) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return 0;
+}
+
+}  // extern "C"
+

@@ -55,3 +55,7 @@ HDI float2 to_c2(float2 a, float2*) { return a; }
 template <typename CTo, typename CFrom> HDI CTo cvt(CFrom a) { return to_c2(a, (CTo*)nullptr); }
 
 template <typename C> HDI C czero() { C z; z.x = 0; z.y = 0; return z; }
+
+// fields of the dynamic Smagorinsky model's Germano/Lilly contraction
+// (k_dyn_prep builds them, the LES work arrays hold them)
+#define DYN_NF 21

@@ -228,7 +228,7 @@ struct AdjNlPrepArgs {
   FGeom g;
 };
 
-__global__ void k_adj_nl_prep(const __grid_constant__ AdjNlPrepArgs a) {
+static __global__ void k_adj_nl_prep(const __grid_constant__ AdjNlPrepArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -265,7 +265,7 @@ struct AdjNlPointArgs {
   size_t ps;
 };
 
-__global__ void k_adj_nl_point(const __grid_constant__ AdjNlPointArgs a) {
+static __global__ void k_adj_nl_point(const __grid_constant__ AdjNlPointArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -320,7 +320,7 @@ struct AdjAccArgs {
   FGeom g;
 };
 
-__global__ void k_adj_acc(const __grid_constant__ AdjAccArgs a) {
+static __global__ void k_adj_acc(const __grid_constant__ AdjAccArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;

@@ -22,7 +22,7 @@ struct PpGradArgs {
   FGeom g;
 };
 
-__global__ void k_pp_grad(const __grid_constant__ PpGradArgs a) {
+static __global__ void k_pp_grad(const __grid_constant__ PpGradArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -60,7 +60,7 @@ struct PpProdArgs {
   size_t ps;
 };
 
-__global__ void k_pp_prod(const __grid_constant__ PpProdArgs a) {
+static __global__ void k_pp_prod(const __grid_constant__ PpProdArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)(a.nyp + 2) * a.ps;
   if (idx >= tot) return;
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(128) k_pp_solve(const __grid_constant__ PpSolv
 // courant turns them into the CFL time step: max|u - a| over the plane is
 // max(max u - a, a - min u) for any shift a, which covers both the plain
 // branch (a = 0) and the 'Front' branch's thermal-wind shifts.
-__global__ void __launch_bounds__(256) k_plane_range(const double* u1, const double* u2, const double* u3,
+static __global__ void __launch_bounds__(256) k_plane_range(const double* u1, const double* u2, const double* u3,
                                                      double* out, size_t ps) {
   const int j = blockIdx.x + 1;
   const size_t base = (size_t)j * ps;
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(256) k_plane_range(const double* u1, const dou
 }
 
 // filter_chan (for/channel.f90:1241-1329): cth *= sigma(m, kq) on rows j0..j1
-__global__ void k_filter_th(double2* cth, const double* sigma, int j0, int j1, int nkx1, int nk2, int kp) {
+static __global__ void k_filter_th(double2* cth, const double* sigma, int j0, int j1, int nkx1, int nk2, int kp) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t ps = (size_t)nkx1 * kp;
   const size_t tot = (size_t)(j1 - j0 + 1) * ps;

@@ -7,7 +7,7 @@
 // reference physical v(0:Nx+1, 0:Nz+1, 0:Ny+1) -> internal P[j][k][i]
 // (`rows` rows of Nx+2 per plane in `ref`: Nz+2 for a whole reference array,
 // Nz for its significant rows staged contiguously)
-__global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict__ out,
+static __global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict__ out,
                               int nx, int nz, int nyp2, int rows) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)nyp2 * nz * nx;
@@ -20,7 +20,7 @@ __global__ void k_ref_to_phys(const double* __restrict__ ref, double* __restrict
 }
 
 // internal P -> the significant box (i < Nx, k < Nz) of a reference physical array
-__global__ void k_phys_to_ref(const double* __restrict__ in, double* __restrict__ ref,
+static __global__ void k_phys_to_ref(const double* __restrict__ in, double* __restrict__ ref,
                               int nx, int nz, int nyp2) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)nyp2 * nz * nx;
@@ -36,7 +36,7 @@ __global__ void k_phys_to_ref(const double* __restrict__ in, double* __restrict_
 // *bad if a significant mode above Nkx is nonzero.  The source has row pitch
 // `rp` complex elements and `rows` rows per plane (Nxp+1 and Nz+2 for a full
 // reference array, Nxp and 2Nkz+1 for a packed copy of its significant box).
-__global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restrict__ out,
+static __global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restrict__ out,
                               Geom g, int nxp, int rp, int rows, int* bad) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)g.nyp2 * g.nk2 * nxp;
@@ -55,7 +55,7 @@ __global__ void k_ref_to_four(const double2* __restrict__ ref, double2* __restri
 
 // internal F -> the significant box (i < Nxp, k <= 2Nkz) of a Fourier array
 // with row pitch `rp` and `rows` rows per plane; modes above Nkx written as 0
-__global__ void k_four_to_ref(const double2* __restrict__ in, double2* __restrict__ ref,
+static __global__ void k_four_to_ref(const double2* __restrict__ in, double2* __restrict__ ref,
                               Geom g, int nxp, int rp, int rows) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)g.nyp2 * g.nk2 * nxp;
@@ -70,7 +70,7 @@ __global__ void k_four_to_ref(const double2* __restrict__ in, double2* __restric
 }
 
 // any non-finite significant entry -> *bad
-__global__ void k_check_finite(const double2* __restrict__ f, Geom g, int* bad) {
+static __global__ void k_check_finite(const double2* __restrict__ f, Geom g, int* bad) {
   size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t tot = (size_t)g.nyp2 * g.nkx1 * g.kp;
   if (idx >= tot) return;
@@ -94,7 +94,7 @@ struct BcPostArgs {
   int do_vel, do_th;   // apply_BC_vel_mpi_post / apply_BC_th_mpi_post
 };
 
-__global__ void k_bc_post(BcPostArgs a) {
+static __global__ void k_bc_post(BcPostArgs a) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= a.nkx1 * a.nk2) return;
   const int m = idx / a.nk2, kq = idx % a.nk2;
@@ -199,4 +199,10 @@ __global__ void k_bc_post(BcPostArgs a) {
       }
     }
   }
+}
+
+// FP32 -> FP64 copy of n values
+static __global__ void k_widen(const float* in, double* out, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (double)in[i];
 }

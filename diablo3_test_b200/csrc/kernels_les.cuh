@@ -40,7 +40,7 @@ struct ExplicitArgs2 {
   double2* cr[SOLVE_NF];
 };
 
-__global__ void k_explicit2(const __grid_constant__ ExplicitArgs2 E) {
+static __global__ void k_explicit2(const __grid_constant__ ExplicitArgs2 E) {
   const SolveArgs& a = E.s;
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t ps = (size_t)a.nkx1 * a.kp;
@@ -113,7 +113,7 @@ struct LesBcArgs {
   int thbc[8][2];
 };
 
-__global__ void k_les_bc(LesBcArgs a) {
+static __global__ void k_les_bc(LesBcArgs a) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= a.nkx1 * a.nk2) return;
   const int m = idx / a.nk2, kq = idx % a.nk2;
@@ -146,7 +146,7 @@ struct StrainArgs {
   FGeom g;
 };
 
-__global__ void k_strain(StrainArgs a) {
+static __global__ void k_strain(StrainArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -301,7 +301,7 @@ struct LesDivArgs {
   int j1, j2;
 };
 
-__global__ void k_les_div(LesDivArgs a) {
+static __global__ void k_les_div(LesDivArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -340,7 +340,7 @@ struct ThGradArgs {
   int nth;
 };
 
-__global__ void k_th_grad(ThGradArgs a) {
+static __global__ void k_th_grad(ThGradArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -386,7 +386,7 @@ struct ThDivArgs {
   int jst[8], jet[8];
 };
 
-__global__ void k_th_div(ThDivArgs a) {
+static __global__ void k_th_div(ThDivArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -413,7 +413,7 @@ struct CfFinishArgs {
   FGeom g;
 };
 
-__global__ void k_cf_finish(CfFinishArgs a) {
+static __global__ void k_cf_finish(CfFinishArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -608,7 +608,6 @@ __global__ void __launch_bounds__(TILED ? 32 * PS_W : 128) k_phys_solve(PhysSolv
 //   3..8   S_ab     (11, 22, 33, 12, 13, 23; S12, S23 averaged from GY)
 //   9..14  U_a U_b  (same pair order)
 //   15..20 |S| S_ab
-#define DYN_NF 21
 template <typename P>
 struct DynPrepArgs {
   const P* u[3];
@@ -661,7 +660,7 @@ struct MaskArgs {
   FGeom g;
 };
 
-__global__ void k_test_mask(MaskArgs a) {
+static __global__ void k_test_mask(MaskArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -737,7 +736,7 @@ __global__ void __launch_bounds__(256) k_dyn_contract(DynContractArgs<P> a) {
 
 // C(y) at GYF from the plane sums, and interpolated to GY (for/les.f90's
 // GYF-to-GY weights); one thread per plane, planes 0..Ny+1.
-__global__ void k_dyn_coef(const double* sums, const double* dy, const double* dyf, double* cf, double* cg,
+static __global__ void k_dyn_coef(const double* sums, const double* dy, const double* dyf, double* cf, double* cg,
                            int nyp, int nslice, double nps) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j > nyp + 1) return;
@@ -785,7 +784,7 @@ struct AmdFourierArgs {
 DI double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 DI double2 cdiff_over(double2 a, double2 b, double d) { return make_double2((a.x - b.x) / d, (a.y - b.y) / d); }
 
-__global__ void k_amd_fourier(const __grid_constant__ AmdFourierArgs a) {
+static __global__ void k_amd_fourier(const __grid_constant__ AmdFourierArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -1009,7 +1008,7 @@ struct AmdThDivArgs {
   int jst[8], jet[8];
 };
 
-__global__ void k_amd_th_div(const __grid_constant__ AmdThDivArgs a) {
+static __global__ void k_amd_th_div(const __grid_constant__ AmdThDivArgs a) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t tot = (size_t)a.g.n * a.g.ps;
   if (idx >= tot) return;
@@ -1025,7 +1024,3 @@ __global__ void k_amd_th_div(const __grid_constant__ AmdThDivArgs a) {
 }
 
 // FP32 -> FP64 copy (the mixed-precision eddy viscosity for the boundary)
-__global__ void k_widen(const float* in, double* out, size_t n) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = (double)in[i];
-}

@@ -22,45 +22,7 @@
 #pragma once
 #include "common.cuh"
 
-#define SOLVE_MAXTH 8
-#define SOLVE_NF (3 + SOLVE_MAXTH)
-
-struct SolveArgs {
-  int nyp, n;               // Nyp, Ny+2
-  int nkx1, nk2, kp, ncol;  // stored x modes, packed z modes, pitch, columns
-  int nth, rk;
-  double temp1, temp2, temp3, temp4, temp5;
-  double nu, beta, nu_v, roinvd;  // nu, horizontal Laplacian exponent, nu_v_scale, Ro_inv/delta
-  double grav_x, grav_y, grav_z;
-  double px;                // subtracted from cr1 at (0,0): temp4*(px0 [+ oscillation])
-  int jstart, jend;
-  int ubc[2], vbc[2], wbc[2];
-  double uc1[2], vc1[2], wc1[2];  // wc1[1] is the (possibly transient) top value
-  int front;                // thermal-wind advection (flavor 'Front')
-  double ly, front_coef;    // Ly, delta/Ro_inv
-  int jst[SOLVE_MAXTH], jet[SOLVE_MAXTH];
-  int thbc[SOLVE_MAXTH][2];
-  double thc1[SOLVE_MAXTH][2];
-  double pr[SOLVE_MAXTH], dthdx[SOLVE_MAXTH], dthdz[SOLVE_MAXTH];
-  const double* dy;
-  const double* dyf;
-  const double* gy;
-  const double* gyf;
-  const double* kx;
-  const double* kz;
-  const double2* cu_in[3];
-  const double2* cth_in[SOLVE_MAXTH];
-  const double2* cp_in;
-  const double2* cf_in[SOLVE_NF];
-  double2* cu_out[3];
-  double2* cth_out[SOLVE_MAXTH];
-  double2* cp_out;
-  double2* cf_out[SOLVE_NF];
-  const double2* nl64[SOLVE_NF];
-  const float2* nl32[SOLVE_NF];
-  int store_cf;             // 0 on the last substep (cf is not read again)
-  double2* keep[3];         // if set: the solved u1, u2, u3 before the projection (courant)
-};
+#include "solve_args.cuh"
 
 namespace csolve {
 

@@ -213,7 +213,7 @@ struct StatsLesArgs {
   double* part;         // [Ny+2][nslice][2]
 };
 
-__global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_constant__ StatsLesArgs a) {
+static __global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_constant__ StatsLesArgs a) {
   const int j = blockIdx.y;
   double acc[2] = {0.0, 0.0};
   if (j >= 1 && j <= a.nyp) {
@@ -260,7 +260,7 @@ struct StatsXyArgs {
   double* out;          // [XY_N][Ny+2][Nx]
 };
 
-__global__ void __launch_bounds__(128) k_stats_xy(const __grid_constant__ StatsXyArgs a) {
+static __global__ void __launch_bounds__(128) k_stats_xy(const __grid_constant__ StatsXyArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= a.nx) return;
@@ -319,7 +319,7 @@ struct StatsBpeArgs {
   double* pdf;          // [nbin], zeroed by the caller
 };
 
-__global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ StatsBpeArgs a) {
+static __global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ StatsBpeArgs a) {
   extern __shared__ double hist[];
   for (int b = threadIdx.x; b < a.nbin; b += blockDim.x) hist[b] = 0.0;
   __syncthreads();
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256) k_stats_bpe(const __grid_constant__ Stats
 // i k * F for the y* binning's derivative fields: axis 0 = x (kx), 1 = z (kz);
 // drop0 zeroes the kz = 0 row (epsilon's x derivatives in the x-inhomogeneous
 // branch, k_start = 1).  One thread per stored coefficient.
-__global__ void k_spec_deriv(const double2* __restrict__ src, double2* __restrict__ dst, const double* kx,
+static __global__ void k_spec_deriv(const double2* __restrict__ src, double2* __restrict__ dst, const double* kx,
                              const double* kz, int axis, int drop0, int nkx1, int nk2, int kp, size_t tot) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= tot) return;
@@ -366,7 +366,7 @@ __global__ void k_spec_deriv(const double2* __restrict__ src, double2* __restric
 }
 
 // z mean at each (j, i) of a physical field, out[j][i]
-__global__ void k_zmean(const double* __restrict__ f, double* __restrict__ out, int nx, int nz, int n) {
+static __global__ void k_zmean(const double* __restrict__ f, double* __restrict__ out, int nx, int nz, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   if (i >= nx || j >= n) return;
@@ -401,7 +401,7 @@ struct StatsZstarArgs {
   double* hist;             // [1 + ZS_N][nbin], zeroed by the caller
 };
 
-__global__ void __launch_bounds__(256) k_stats_zstar(const __grid_constant__ StatsZstarArgs a) {
+static __global__ void __launch_bounds__(256) k_stats_zstar(const __grid_constant__ StatsZstarArgs a) {
   extern __shared__ double zh[];
   const int nb = a.nbin;
   for (int b = threadIdx.x; b < (1 + ZS_N) * nb; b += blockDim.x) zh[b] = 0.0;

@@ -219,22 +219,28 @@ const char* diablo_status_string(int status);
 int diablo_abi_version(void);
 
 /*
- * fft_xz_to_fourier for callers that cannot allocate device memory.  This
- * entry point has no counterpart in the reference: it is fft_xz_to_fourier
- * (for/fft.f90:247-315) run without a diablo_ctx, for drivers that own every
- * device byte through their own pool, for code that cannot take the device-
- * wide synchronisation of cudaMalloc/cudaFree, and for callers that never
- * create a context.  It allocates nothing: its scratch is one file-scope
- * device array of DIABLO_NOALLOC_SCRATCH_BYTES that every GPU loading the
- * library holds until the process exits.  v and vv are DEVICE arrays in the
- * reference layout (v == vv allowed); the work is queued on `stream`
- * (cudaStream_t, NULL = legacy default stream) and nothing waits for it.
- * Grids whose scratch needs exceed the array return DIABLO_ERR_SIZE (e.g.
- * 128 x 129 x 128 fits, 256 x 257 x 256 does not).  The first call on each
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture.  All calls share the one array:
- * calls whose work overlaps on the GPU (different streams, or different host
- * threads) race and must be serialised by the caller.
+ * The library's forward xz transform without a context, for callers that
+ * cannot allocate device memory.  This entry point has no counterpart in the
+ * reference.  Its callers are drivers that own every device byte through
+ * their own pool, code that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree, and callers that never create a context.  It allocates
+ * nothing: its scratch is one file-scope device array of
+ * DIABLO_NOALLOC_SCRATCH_BYTES (plus a 28 KB twiddle table) that every GPU
+ * loading the library holds until the process exits.
+ * v and vv are DEVICE (or managed) arrays of the current device in the
+ * reference layout (v == vv allowed); host pointers and other devices'
+ * memory return DIABLO_ERR_ARG before anything is queued.  The work is queued
+ * on `stream` (cudaStream_t, NULL = legacy default stream).  Grids whose
+ * scratch needs exceed the array return DIABLO_ERR_SIZE (e.g. 128 x 129 x 128
+ * fits, 256 x 257 x 256 does not).  A CUDA error already pending when the call
+ * starts is left for the caller and the call returns DIABLO_ERR_CUDA without
+ * queueing anything.
+ * The first call on each device does a one-time set-up (the array's device
+ * address by cudaGetSymbolAddress, the twiddle tables by cudaMemcpyToSymbol),
+ * so make that first call before any stream capture begins.  All calls share
+ * the one array and it keeps the last call's contents: calls whose work
+ * overlaps on the GPU (different streams, or different host threads) race
+ * and must be serialised by the caller.
  */
 #define DIABLO_NOALLOC_SCRATCH_BYTES (64u << 20)
 int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, double* vv,

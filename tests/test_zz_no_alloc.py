@@ -54,6 +54,43 @@ def test_noalloc_rejects_grids_beyond_its_scratch(cuda_device):
     import torch
     lib = _lib.load()
     p = small_params(nx=256, ny=257, nz=256, n_th=0)
-    v = torch.zeros(8, dtype=torch.float64, device=cuda_device)
-    # the size check fires before any device access
-    assert _noalloc(lib, p, v, v) == _lib.ERR_SIZE
+    # full reference-layout buffers (about 138 MB each): should the size
+    # check ever regress, the transform stays inside them and the test fails
+    # on the return code
+    shape = (p.ny + 2, p.nz + 2, p.nx + 2)
+    v = torch.zeros(shape, dtype=torch.float64, device=cuda_device)
+    vv = torch.zeros(shape, dtype=torch.float64, device=cuda_device)
+    assert _noalloc(lib, p, v, vv) == _lib.ERR_SIZE
+
+
+def test_noalloc_rejects_host_arrays(cuda_device):
+    # a Fortran caller passing host arrays gets an error code before anything
+    # is queued on the GPU
+    import torch
+    lib = _lib.load()
+    p = small_params(nx=32, ny=33, nz=24, n_th=0)
+    shape = (p.ny + 2, p.nz + 2, p.nx + 2)
+    h = np.zeros(shape)
+    d = torch.zeros(shape, dtype=torch.float64, device=cuda_device)
+    hp = ctypes.c_void_p(h.ctypes.data)
+    dp = ctypes.c_void_p(d.data_ptr())
+    assert lib.diablo_fft_xz_to_fourier_noalloc(p.nx, p.ny, p.nz, hp, dp, None) == _lib.ERR_ARG
+    assert lib.diablo_fft_xz_to_fourier_noalloc(p.nx, p.ny, p.nz, dp, hp, None) == _lib.ERR_ARG
+    assert _noalloc(lib, p, d, d) == _lib.OK
+    torch.cuda.synchronize()
+
+
+def test_noalloc_leaves_free_device_memory_unchanged(cuda_device):
+    import torch
+    lib = _lib.load()
+    p = small_params(nx=64, ny=65, nz=64, n_th=0)
+    shape = (p.ny + 2, p.nz + 2, p.nx + 2)
+    v = torch.randn(shape, dtype=torch.float64, device=cuda_device)
+    vv = torch.zeros_like(v)
+    assert _noalloc(lib, p, v, vv) == _lib.OK   # set-up happens on the first call
+    torch.cuda.synchronize()
+    before = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert _noalloc(lib, p, v, vv) == _lib.OK
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == before
