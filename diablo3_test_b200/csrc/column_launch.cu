@@ -68,15 +68,31 @@ int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s) {
 }
 
 // ---- field-split column step (kernels_field.cuh) ----
+// Both kernels are persistent: as many blocks as fit on the device at once
+// (two per SM at Ny = 257), each walking its share of the tasks.
+template <typename K>
+static int resident_blocks(K kernel, int smem) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, FS_THREADS, smem);
+  return (per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+}
 template <int R>
 static void launch_field_t(const FieldArgs& A, cudaStream_t s) {
-  const int groups = (A.s.ncol + FS_WARPS - 1) / FS_WARPS;
-  k_field_solve<R><<<groups * A.nf, 32 * FS_WARPS, 0, s>>>(A);
+  const int smem = (int)field_smem_bytes(A.s.n);
+  cudaFuncSetAttribute(k_field_solve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int tasks = ((A.s.ncol + FS_COLS - 1) / FS_COLS) * A.nf;
+  const int grid = std::min(tasks, resident_blocks(k_field_solve<R>, smem));
+  k_field_solve<R><<<grid, FS_THREADS, smem, s>>>(A);
 }
 template <int R>
 static void launch_project_t(const FieldArgs& A, cudaStream_t s) {
-  const int groups = (A.s.ncol + FS_WARPS - 1) / FS_WARPS;
-  k_project_cols<R><<<groups, 32 * FS_WARPS, 0, s>>>(A);
+  const int smem = (int)field_smem_bytes(A.s.n);
+  cudaFuncSetAttribute(k_project_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int groups = (A.s.ncol + FS_COLS - 1) / FS_COLS;
+  const int grid = std::min(groups, resident_blocks(k_project_cols<R>, smem));
+  k_project_cols<R><<<grid, FS_THREADS, smem, s>>>(A);
 }
 int launch_field_solve(const FieldArgs& A, cudaStream_t s) {
   switch (rows_per_lane(A.s.n)) {

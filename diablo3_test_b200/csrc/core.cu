@@ -310,7 +310,7 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
   ctx->precision = p->precision;
   {
     const char* e = getenv("DIABLO_GENERAL_SOLVER");
-    ctx->use_general_solver = (e && (e[0] == '0' || e[0] == '1')) ? e[0] - '0' : 2;
+    ctx->use_general_solver = (e && (e[0] == '1' || e[0] == '2')) ? e[0] - '0' : 0;
   }
   int rc = 0;
 #define FAIL(code) do { *status = (code); diablo_destroy(ctx); return nullptr; } while (0)

@@ -9,28 +9,33 @@
 // and the pressure through rem_div_chan (:946-1023).  The column step
 // therefore runs as two kernels:
 //
-//   k_field_solve   one warp per (field, column): explicit RK terms
-//                   (:29-249), cf for the next substep, the explicit
-//                   Crank-Nicolson half (:468-514, :625-633), the pressure
-//                   gradient, the wall rows and the factored implicit solve
-//                   (:657-877); writes the solved velocity u* (the scalars'
-//                   final value);
-//   k_project_cols  one warp per column: divergence of u*, the pressure-
-//                   correction Poisson solve, the projection and cp += phi/h
-//                   (:901-1023).
+//   k_field_solve   a block per (field, 8 adjacent columns), a warp per
+//                   column: explicit RK terms (:29-249), cf for the next
+//                   substep, the explicit Crank-Nicolson half (:468-514,
+//                   :625-633), the pressure gradient, the wall rows and the
+//                   factored implicit solve (:657-877); writes the solved
+//                   velocity u* (the scalars' final value);
+//   k_project_cols  a block per 8 columns, a warp per column: divergence of
+//                   u*, the pressure-correction Poisson solve, the
+//                   projection and cp += phi/h (:901-1023).
 //
-// Five to seven times as many independent warps as a warp-per-column kernel
-// that carries every field, and no block-wide barriers: each warp loads its
-// own rows straight into registers (a lane owns R consecutive rows, its
-// neighbours' edge rows come over shuffles), and the warps of a block take
-// adjacent columns, so each 128-byte row segment is fetched once and served
-// to its eight warps from L1/L2.
+// Data path.  A column's rows lie one plane apart in HBM; adjacent columns are
+// adjacent in memory.  A block therefore moves each array as an
+// (Ny+2) x 8-column tile: cp.async copies of 16 bytes, four 128-byte row
+// segments per warp instruction, into a two-stage shared-memory ring, so the
+// next tile is in flight while the current one is consumed.  Each warp then
+// reads its own column from the tile, a lane owning R consecutive rows
+// (csolve's partition solver), and results leave through a third tile slot
+// with the same coalesced pattern.  Tile slots are XOR-swizzled by the lane
+// that owns the row, so the 32 lanes' 16-byte reads spread over all eight
+// 16-byte bank groups.
 #pragma once
 #include "common.cuh"
 #include "kernels_solve.cuh"
 #include "kernels_solve2.cuh"
 
-#define FS_WARPS 8   // columns (warps) per block of both kernels
+#define FS_COLS 8     // columns (one warp each) per block
+#define FS_THREADS (32 * FS_COLS)
 
 struct FieldArgs {
   SolveArgs s;
@@ -45,230 +50,421 @@ struct FieldArgs {
 namespace cfield {
 using namespace csolve;
 
-DI double2 ldc(const double2* p, size_t i) { return __ldg(p + i); }
-DI double2 ldnl(const FieldArgs& A, int f, size_t i) {
-  const SolveArgs& a = A.s;
-  if (a.nl64[f]) return __ldg(a.nl64[f] + i);
-  const float2 v = __ldg(a.nl32[f] + i);
-  return make_double2(v.x, v.y);
+// tile slot of row j, column c: the XOR key is the owning lane (j / R)
+template <int R>
+DI int slot(int j, int c) { return j * FS_COLS + (c ^ ((j / R) & 7)); }
+
+DI void cp16(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g));
+}
+DI void cp8(void* s, const void* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g));
+}
+DI void commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> DI void wait_groups() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Issue the copies of one tile (rows [0, n), columns q0 .. q0+nvalid-1 of g,
+// plane stride ps elements of ESZ bytes) and close the copy group.
+// g == nullptr closes an empty group, so every step commits exactly one.
+// Thread t copies column t % 8 of rows t / 8, t / 8 + 32, ...
+template <int R, int ESZ>
+DI void load_tile(void* tile, const void* g, size_t ps, int q0, int nvalid, int n, int tid) {
+  if (g) {
+    const int c = tid & 7;
+    const unsigned sbase = (unsigned)__cvta_generic_to_shared(tile);
+    if (c < nvalid) {
+      const char* gp = (const char*)g + ((size_t)(tid >> 3) * ps + q0 + c) * ESZ;
+      const size_t gstep = (size_t)32 * ps * ESZ;
+      for (int j = tid >> 3; j < n; j += 32, gp += gstep) {
+        const unsigned sa = sbase + (unsigned)(j * FS_COLS + (c ^ ((j / R) & 7))) * ESZ;
+        if (ESZ == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gp));
+        else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gp));
+      }
+    } else {
+      for (int j = tid >> 3; j < n; j += 32) {
+        char* sp = (char*)tile + (j * FS_COLS + (c ^ ((j / R) & 7))) * ESZ;
+        if (ESZ == 16) *(double2*)sp = make_double2(0.0, 0.0);
+        else *(float2*)sp = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  commit();
+}
+
+// Store rows [j0, j1] of a double2 tile to g (columns q0 .. q0+nvalid-1).
+// Rows below `jk` are taken from `keep_src` instead (rows a solve leaves as
+// they were), when it is set.
+template <int R>
+DI void store_tile(const double2* tile, double2* g, size_t ps, int q0, int nvalid, int j0, int j1,
+                   int tid, const double2* keep_src = nullptr, int jk = 0) {
+  const int c = tid & 7;
+  if (c >= nvalid) return;
+  const size_t gstep = (size_t)32 * ps;
+  int j = j0 + (tid >> 3);
+  size_t o = (size_t)j * ps + q0 + c;
+  for (; j <= j1; j += 32, o += gstep)
+    g[o] = (keep_src && j < jk) ? __ldg(keep_src + o) : tile[j * FS_COLS + (c ^ ((j / R) & 7))];
 }
 }  // namespace cfield
 
-// Rows per lane R = ceil((Ny+2)/32) >= 3.  Blocks per SM for the register cap:
-// the explicit terms keep only a three-row window of the field, so the live
-// state is the R right-hand sides.
-template <int R>
-constexpr int fs_min_blocks() { return R <= 5 ? 4 : 3; }
+// ---- k_field_solve -------------------------------------------------------------
+enum { FT_OWN = 0, FT_ADD, FT_BUOY, FT_NL, FT_CFOLD, FT_P };
+struct FTile {
+  const void* src;
+  int kind, f32;
+  double coef;
+};
+#define FS_MAXTILES (5 + 2 * SOLVE_MAXTH)
 
+// Shared memory of both kernels: a two-stage input ring and an output slot,
+// each (Ny+2) x FS_COLS complex doubles.
+inline size_t field_smem_bytes(int n) { return (size_t)3 * n * FS_COLS * sizeof(double2); }
+
+namespace cfield {
+// the tiles field f reads, in the order its explicit terms use them
+DI int field_tiles(const SolveArgs& a, int f, FTile* tl) {
+  const int th = f - 3;
+  int ns = 0;
+  tl[ns++] = FTile{f < 3 ? (const void*)a.cu_in[f] : (const void*)a.cth_in[th], FT_OWN, 0, 0.0};
+  if (f == 0 || f == 2) {
+    if (a.roinvd != 0.0) tl[ns++] = FTile{a.cu_in[2 - f], FT_ADD, 0, f == 0 ? a.roinvd : -a.roinvd};
+    const double g = f == 0 ? a.grav_x : a.grav_z;
+    if (g != 0.0)
+      for (int t = 0; t < a.nth; ++t) tl[ns++] = FTile{a.cth_in[t], FT_ADD, 0, g};
+  } else if (f == 1) {
+    if (a.grav_y != 0.0)
+      for (int t = 0; t < a.nth; ++t) tl[ns++] = FTile{a.cth_in[t], FT_BUOY, 0, a.grav_y};
+  } else {
+    if (a.dthdx[th] != 0.0) tl[ns++] = FTile{a.cu_in[0], FT_ADD, 0, -a.dthdx[th]};
+    if (a.dthdz[th] != 0.0) tl[ns++] = FTile{a.cu_in[2], FT_ADD, 0, -a.dthdz[th]};
+  }
+  if (a.nl64[f]) tl[ns++] = FTile{a.nl64[f], FT_NL, 0, 0.0};
+  else tl[ns++] = FTile{a.nl32[f], FT_NL, 1, 0.0};
+  if (a.rk > 1) tl[ns++] = FTile{a.cf_in[f], FT_CFOLD, 0, 0.0};
+  if (f < 3) tl[ns++] = FTile{a.cp_in, FT_P, 0, 0.0};
+  return ns;
+}
 template <int R>
-__global__ void __launch_bounds__(32 * FS_WARPS, fs_min_blocks<R>()) k_field_solve(const __grid_constant__ FieldArgs A) {
+DI void load_ftile(void* slot, const FTile* t, size_t ps, int q0, int nvalid, int n, int tid) {
+  if (t && t->f32) load_tile<R, 8>(slot, t->src, ps, q0, nvalid, n, tid);
+  else load_tile<R, 16>(slot, t ? t->src : nullptr, ps, q0, nvalid, n, tid);
+}
+}  // namespace cfield
+
+// Persistent: block b takes tasks b, b + gridDim.x, ... (task t = field
+// t % N_F of column group t / N_F).  The ring runs on across tasks: the last
+// step of a task already copies the next task's first tile, so the tile is in
+// flight while this task's solve and stores run.
+template <int R>
+__global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_constant__ FieldArgs A) {
   using namespace cfield;
+  extern __shared__ __align__(16) unsigned char fs_smem[];
   const SolveArgs& a = A.s;
-  const int nf = A.nf;
-  // field fastest: the blocks of one column group run together, so the
-  // pressure and coupling rows they share are read from L2
-  const int f = blockIdx.x % nf;
-  const int q = (blockIdx.x / nf) * FS_WARPS + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (q >= a.ncol) return;   // whole warps
   const int n = a.n, nyp = a.nyp;
-  const size_t ps = (size_t)a.ncol;     // plane stride (the Fourier pitch is 2Nkz+1)
-  const int m = q / a.nk2, kq = q % a.nk2;
-  const bool m00 = (q == 0);
-  const double kxm = a.kx[m], kzq = a.kz[kq];
-  const double k2s = kxm * kxm + kzq * kzq;
-  const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+  const int tsz = n * FS_COLS;
+  double2* ring = reinterpret_cast<double2*>(fs_smem);
+  double2* out = ring + 2 * tsz;
+  const int nf = A.nf;
+  const int ntask = ((a.ncol + FS_COLS - 1) / FS_COLS) * nf;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const size_t ps = (size_t)a.ncol;          // plane stride (the Fourier pitch is 2Nkz+1)
   const double2 z2 = make_double2(0.0, 0.0);
   const int j0 = lane * R;
   const double* met = A.met;
-
-  // field kind: solve index (0 u1, 1 u2, 2 u3, 3+n scalar n), row-coefficient
-  // index (0 u1/u3, 1 u2, 2+n scalar n), explicit rows [lo, hi], wall rows
-  const int th = f - 3;
-  const int kc_kind = f == 1 ? 1 : (f < 3 ? 0 : 2 + th);
-  int lo, hi, b0, b1;
-  double c0, c1;
-  if (f == 0) { lo = a.jstart; hi = a.jend; b0 = a.ubc[0]; b1 = a.ubc[1]; c0 = a.uc1[0]; c1 = a.uc1[1]; }
-  else if (f == 2) { lo = a.jstart; hi = a.jend; b0 = a.wbc[0]; b1 = a.wbc[1]; c0 = a.wc1[0]; c1 = a.wc1[1]; }
-  else if (f == 1) { lo = 2; hi = nyp; b0 = a.vbc[0]; b1 = a.vbc[1]; c0 = a.vc1[0]; c1 = a.vc1[1]; }
-  else { lo = a.jst[th]; hi = a.jet[th]; b0 = a.thbc[th][0]; b1 = a.thbc[th][1]; c0 = a.thc1[th][0]; c1 = a.thc1[th][1]; }
-  const double* K = A.kc + (size_t)kc_kind * 3 * n;
-  const double cfc = f >= 3 ? (a.nu / a.pr[th]) * kk : a.nu * kk;
-  const double2* own = f < 3 ? a.cu_in[f] : a.cth_in[th];
-  const double2* cpi = a.cp_in;
-  const double v00 = m00 ? 1.0 : 0.0;
-  // mean-split correction of this field: -ikx U(j) u with U = U1 (u3,
-  // scalars) or its GY interpolation I(U1) (u2); none for u1
-  const double* Up = (A.mean_split && f != 0) ? A.prof + (f == 1 ? n : 0) : nullptr;
-
-  // The own field moves through a three-row window (rows j-1, j, j+1); the
-  // rows next to the lane's chunk come from lanes t-1, t+1.  The pressure
-  // likewise carries one row (u2 needs p(j-1)).
-  auto ldo = [&](int j) -> double2 { return j < n ? ldc(own, (size_t)j * ps + q) : z2; };
-  auto ldp = [&](int j) -> double2 { return j < n ? ldc(cpi, (size_t)j * ps + q) : z2; };
-  const double2 u_first = ldo(j0), u_last = ldo(j0 + R - 1);
-  const double2 u_lo = shfl_up2(u_last, 1);     // row j0 - 1
-  const double2 u_hi = shfl_down2(u_first, 1);  // row j0 + R
-  double2 p_prev = z2;
-  if (f == 1) p_prev = shfl_up2(ldp(j0 + R - 1), 1);
-  double2 um = u_lo, uu = u_first;
-
-  double2 d[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int j = j0 + r;
-    const double2 up = r == R - 1 ? u_hi : (r == R - 2 ? u_last : ldo(j + 1));
-    double2 dv = z2;
-    const size_t o = (size_t)j * ps + q;
-    const double2 pj = (f < 3) ? ldp(j) : z2;
-    if (j >= lo && j <= hi) {
-      double2 cf = -cfc * uu;
-      double2 cr = uu - K[2 * n + j] * (up - uu) + K[j] * (uu - um);
-      if (Up) cf = cf - mul_ik(kxm * __ldg(Up + j), uu);
-      // couplings through the other fields' substep-start values
-      if (f == 0 || f == 2) {
-        if (a.roinvd != 0.0) {
-          const double2 oth = ldc(a.cu_in[2 - f], o);
-          cf = cf + (f == 0 ? a.roinvd : -a.roinvd) * oth;
-        }
-        const double g = f == 0 ? a.grav_x : a.grav_z;
-        if (g != 0.0)
-          for (int t = 0; t < a.nth; ++t) cf = cf + g * ldc(a.cth_in[t], o);
-      } else if (f == 1) {
-        if (a.grav_y != 0.0 && !m00)
-          for (int t = 0; t < a.nth; ++t)
-            cf = cf + a.grav_y * (__ldg(met + MET_WB1 * n + j) * ldc(a.cth_in[t], o) +
-                                  __ldg(met + MET_WB2 * n + j) * ldc(a.cth_in[t], o - ps));
-      } else {
-        if (a.dthdx[th] != 0.0) cf = cf + (-a.dthdx[th]) * ldc(a.cu_in[0], o);
-        if (a.dthdz[th] != 0.0) cf = cf + (-a.dthdz[th]) * ldc(a.cu_in[2], o);
-      }
-      cf = cf - ldnl(A, f, o);
-      if (a.store_cf) a.cf_out[f][o] = cf;
-      cr = cr + a.temp5 * cf;
-      if (a.rk > 1) cr = cr + a.temp3 * ldc(a.cf_in[f], o);
-      if (f == 0) {
-        cr = cr - a.temp4 * mul_ik(kxm, pj);
-        if (m00) cr.x -= a.px;
-      } else if (f == 2) {
-        cr = cr - a.temp4 * mul_ik(kzq, pj);
-      } else if (f == 1) {
-        cr = cr - a.temp4 * __ldg(met + MET_IDY * n + j) * (pj - p_prev);
-      }
-      dv = cr;
-    }
-    p_prev = pj;
-    um = uu;
-    uu = up;
-    // wall rows (for/channel.f90:1545-1876)
-    if (f == 1) {
-      if (b0 == 0 && (j == 1 || j == 2)) dv = make_double2(c0 * v00, 0);
-      if (b0 == 1 && j == 1) dv = make_double2(a.dyf[1] * c0 * v00, 0);
-      if (j == 0) dv = z2;
-      if (b1 == 0 && (j == nyp || j == nyp + 1)) dv = make_double2(c1 * v00, 0);
-      if (b1 == 1 && j == nyp + 1) dv = make_double2(a.dyf[nyp] * c1 * v00, 0);
-    } else {
-      if (j == 0 || j == nyp + 1) dv = z2;
-      if (j == 1) dv = make_double2((b0 == 0 ? c0 : a.dy[2] * c0) * v00, 0);
-      if (j == nyp) dv = make_double2((b1 == 0 ? c1 : a.dy[nyp] * c1) * v00, 0);
-    }
-    d[r] = dv;
+  int t = blockIdx.x;
+  if (t >= ntask) return;
+  FTile tl[FS_MAXTILES];
+  int ns = field_tiles(a, t % nf, tl);
+  int step = 0;
+  {
+    const int q0 = (t / nf) * FS_COLS;
+    load_ftile<R>(ring, &tl[0], ps, q0, min(FS_COLS, a.ncol - q0), n, tid);
   }
-  apply_factored<R>(A.fac + (size_t)f * Fac<R>::N * 32, d, lane);
-  // rows the solve writes: u2 1..Ny+1, the others lo-1..Ny+1; the rest keep
-  // their input value
-  const int w0 = f == 1 ? 1 : lo - 1, w1 = nyp + 1;
-  double2* dst = f < 3 ? a.cu_out[f] : a.cth_out[th];
+  for (; t < ntask; t += gridDim.x) {
+    const int f = t % nf;
+    const int q0 = (t / nf) * FS_COLS;
+    const int nvalid = min(FS_COLS, a.ncol - q0);
+    const int q = min(q0 + w, a.ncol - 1);   // a warp past the last column works on a copy
+    const int m = q / a.nk2, kq = q % a.nk2;
+    const bool m00 = (q0 + w == 0);
+    const double kxm = a.kx[m], kzq = a.kz[kq];
+    const double k2s = kxm * kxm + kzq * kzq;
+    const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+    // field kind: solve index f (0 u1, 1 u2, 2 u3, 3+n scalar n),
+    // row-coefficient index (0 u1/u3, 1 u2, 2+n scalar n), explicit rows
+    // [lo, hi], wall rows
+    const int th = f - 3;
+    const int kc_kind = f == 1 ? 1 : (f < 3 ? 0 : 2 + th);
+    int lo, hi, b0, b1;
+    double c0, c1;
+    if (f == 0) { lo = a.jstart; hi = a.jend; b0 = a.ubc[0]; b1 = a.ubc[1]; c0 = a.uc1[0]; c1 = a.uc1[1]; }
+    else if (f == 2) { lo = a.jstart; hi = a.jend; b0 = a.wbc[0]; b1 = a.wbc[1]; c0 = a.wc1[0]; c1 = a.wc1[1]; }
+    else if (f == 1) { lo = 2; hi = nyp; b0 = a.vbc[0]; b1 = a.vbc[1]; c0 = a.vc1[0]; c1 = a.vc1[1]; }
+    else { lo = a.jst[th]; hi = a.jet[th]; b0 = a.thbc[th][0]; b1 = a.thbc[th][1]; c0 = a.thc1[th][0]; c1 = a.thc1[th][1]; }
+    const double* K = A.kc + (size_t)kc_kind * 3 * n;
+    const double cfc = f >= 3 ? (a.nu / a.pr[th]) * kk : a.nu * kk;
+    // mean-split correction of this field: -ikx U(j) u with U = U1 (u3,
+    // scalars) or its GY interpolation I(U1) (u2); none for u1
+    const double* Up = (A.mean_split && f != 0) ? A.prof + (f == 1 ? n : 0) : nullptr;
+    const int tn = t + gridDim.x;
+
+    double2 cr[R], cf[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int j = j0 + r;
-    if (j < n) dst[(size_t)j * ps + q] = (j >= w0 && j <= w1) ? d[r] : ldo(j);
+    for (int r = 0; r < R; ++r) { cr[r] = z2; cf[r] = z2; }
+    for (int k = 0; k < ns; ++k, ++step) {
+      const FTile tk = tl[k];
+      double2* nslot = ring + ((step + 1) & 1) * tsz;
+      if (k + 1 < ns) {
+        load_ftile<R>(nslot, &tl[k + 1], ps, q0, nvalid, n, tid);
+      } else if (tn < ntask) {
+        // the next task's own-field tile
+        const int fn = tn % nf, qn = (tn / nf) * FS_COLS;
+        const FTile own = FTile{fn < 3 ? (const void*)a.cu_in[fn] : (const void*)a.cth_in[fn - 3], FT_OWN, 0, 0.0};
+        load_ftile<R>(nslot, &own, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
+      } else {
+        load_ftile<R>(nslot, nullptr, ps, q0, nvalid, n, tid);
+      }
+      wait_groups<1>();
+      __syncthreads();
+      const double2* T = ring + (step & 1) * tsz;
+      auto TV = [&](int j) -> double2 { return T[slot<R>(j, w)]; };
+      switch (tk.kind) {
+        case FT_OWN:
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi) {
+              const double2 u = TV(j), um = TV(j - 1), up = TV(j + 1);
+              cf[r] = -cfc * u;
+              cr[r] = u - K[2 * n + j] * (up - u) + K[j] * (u - um);
+              if (Up) cf[r] = cf[r] - mul_ik(kxm * __ldg(Up + j), u);
+            }
+          }
+          break;
+        case FT_ADD:
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi) cf[r] = cf[r] + tk.coef * TV(j);
+          }
+          break;
+        case FT_BUOY:
+          if (!m00) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j >= lo && j <= hi)
+                cf[r] = cf[r] + tk.coef * (__ldg(met + MET_WB1 * n + j) * TV(j) +
+                                           __ldg(met + MET_WB2 * n + j) * TV(j - 1));
+            }
+          }
+          break;
+        case FT_NL: {
+          const float2* T32 = reinterpret_cast<const float2*>(T);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi) {
+              double2 nl;
+              if (tk.f32) { const float2 v = T32[slot<R>(j, w)]; nl = make_double2(v.x, v.y); }
+              else nl = TV(j);
+              cf[r] = cf[r] - nl;
+              cr[r] = cr[r] + a.temp5 * cf[r];
+            }
+          }
+          if (a.store_cf) {   // cf of the next substep, out through the output slot
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j < n) out[slot<R>(j, w)] = cf[r];
+            }
+            __syncthreads();
+            store_tile<R>(out, a.cf_out[f], ps, q0, nvalid, lo, hi, tid);
+          }
+          break;
+        }
+        case FT_CFOLD:
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi) cr[r] = cr[r] + a.temp3 * TV(j);
+          }
+          break;
+        case FT_P:
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= lo && j <= hi) {
+              if (f == 0) {
+                cr[r] = cr[r] - a.temp4 * mul_ik(kxm, TV(j));
+                if (m00) cr[r].x -= a.px;
+              } else if (f == 2) {
+                cr[r] = cr[r] - a.temp4 * mul_ik(kzq, TV(j));
+              } else {
+                cr[r] = cr[r] - a.temp4 * __ldg(met + MET_IDY * n + j) * (TV(j) - TV(j - 1));
+              }
+            }
+          }
+          break;
+        default:
+          break;
+      }
+      __syncthreads();
+    }
+    // right-hand side: explicit terms on the explicit rows, wall values on
+    // the wall rows (for/channel.f90:1545-1876); the matrix is in the factor
+    // table
+    const double v00 = m00 ? 1.0 : 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = j0 + r;
+      double2 d = (j >= lo && j <= hi) ? cr[r] : z2;
+      if (f == 1) {
+        if (b0 == 0 && (j == 1 || j == 2)) d = make_double2(c0 * v00, 0);
+        if (b0 == 1 && j == 1) d = make_double2(a.dyf[1] * c0 * v00, 0);
+        if (j == 0) d = z2;
+        if (b1 == 0 && (j == nyp || j == nyp + 1)) d = make_double2(c1 * v00, 0);
+        if (b1 == 1 && j == nyp + 1) d = make_double2(a.dyf[nyp] * c1 * v00, 0);
+      } else {
+        if (j == 0 || j == nyp + 1) d = z2;
+        if (j == 1) d = make_double2((b0 == 0 ? c0 : a.dy[2] * c0) * v00, 0);
+        if (j == nyp) d = make_double2((b1 == 0 ? c1 : a.dy[nyp] * c1) * v00, 0);
+      }
+      cr[r] = d;
+    }
+    apply_factored<R>(A.fac + (size_t)f * Fac<R>::N * 32, cr, lane);
+    // The solve writes rows w0 .. Ny+1 (u2: from row 1, the others from
+    // lo - 1); rows below keep their input value.
+    const int w0 = f == 1 ? 1 : lo - 1;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = j0 + r;
+      if (j < n) out[slot<R>(j, w)] = cr[r];
+    }
+    __syncthreads();
+    const double2* own = f < 3 ? a.cu_in[f] : a.cth_in[th];
+    store_tile<R>(out, f < 3 ? a.cu_out[f] : a.cth_out[th], ps, q0, nvalid, 0, n - 1, tid, own, w0);
+    if (tn < ntask) ns = field_tiles(a, tn % nf, tl);
   }
 }
 
+// ---- k_project_cols --------------------------------------------------------------
 // Divergence -> pressure-correction Poisson solve -> projection -> pressure
-// update of one column per warp, in place on cu (rem_div_chan,
-// for/channel.f90:946-1023 with the wall rows of :1974-2015; cp += phi/h,
-// :905-911).  keep[q], if set, receives the velocity before the projection
-// (the field courant reads, :885-888).
+// update, in place on cu_out (rem_div_chan, for/channel.f90:946-1023 with the
+// wall rows of :1974-2015; cp_out = cp_in + phi/h, :905-911).  keep[q], if
+// set, receives the velocity before the projection (the field courant reads,
+// :885-888).  Tiles: u1*, u3*, u2* for the divergence; after the solve u1*,
+// u3*, u2* again (from L2) and cp, each updated in its slot and stored.
+// Persistent over column groups like k_field_solve.
 template <int R>
-__global__ void __launch_bounds__(32 * FS_WARPS, 2) k_project_cols(const __grid_constant__ FieldArgs A) {
+__global__ void __launch_bounds__(FS_THREADS, 2) k_project_cols(const __grid_constant__ FieldArgs A) {
   using namespace cfield;
+  extern __shared__ __align__(16) unsigned char fs_smem[];
   const SolveArgs& a = A.s;
-  const int q = blockIdx.x * FS_WARPS + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (q >= a.ncol) return;
   const int n = a.n, nyp = a.nyp;
+  const int tsz = n * FS_COLS;
+  double2* ring = reinterpret_cast<double2*>(fs_smem);
+  const int ngroup = (a.ncol + FS_COLS - 1) / FS_COLS;
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
   const size_t ps = (size_t)a.ncol;
-  const int m = q / a.nk2, kq = q % a.nk2;
-  const bool m00 = (q == 0);
-  const double kxm = a.kx[m], kzq = a.kz[kq];
   const double2 z2 = make_double2(0.0, 0.0);
   const int j0 = lane * R;
   const double* met = A.met;
   double2* const* cu = a.cu_out;
-  // divergence ik.u1 + ik.u3 + (u2(j+1) - u2(j))/dyf(j), rows 1..Ny
-  double2 d[R];
-  {
-    double2 v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int j = j0 + r;
-      v[r] = j < n ? ldc(cu[1], (size_t)j * ps + q) : z2;
-    }
-    const double2 vn = shfl_down2(v[0], 1);
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int j = j0 + r;
-      double2 dv = z2;
-      if (j >= 1 && j <= nyp) {
-        const size_t o = (size_t)j * ps + q;
-        const double2 vp = r == R - 1 ? vn : v[r + 1];
-        dv = mul_ik(kxm, ldc(cu[0], o));
-        dv = dv + mul_ik(kzq, ldc(cu[2], o));
-        dv = dv + __ldg(met + MET_IDYF * n + j) * (vp - v[r]);
-      }
-      d[r] = dv;
-    }
-  }
-  // Poisson rows: interior 1/(dy dyf) terms, Neumann walls, phi(1) = 0 for
-  // the (0,0) mode
-  double al[R], cu_[R];
-  const double k2n = -kxm * kxm - kzq * kzq;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int j = j0 + r;
-    double am = 0.0, cm = 0.0;
-    if (j >= 1 && j <= nyp) { am = __ldg(met + MET_PA * n + j); cm = __ldg(met + MET_PC * n + j); }
-    if (j == 1) { am = 0; cm = m00 ? 0.0 : -1.0; d[r] = z2; }
-    if (j == nyp) { am = 1; cm = 0; d[r] = z2; }
-    al[r] = am;
-    cu_[r] = cm;
-  }
-  csolve2::warp_tridiag_b<R>([&](int r) -> double& { return al[r]; }, [&](int r) -> double {
-    const int j = j0 + r;
-    return (j == 1) ? 1.0 : (j == nyp ? -1.0 : ((j > 1 && j < nyp) ? k2n + __ldg(met + MET_PB0 * n + j) : 1.0));
-  }, [&](int r) -> double& { return cu_[r]; }, d, lane);
-  // d = phi from here on
-  const double2 phm = shfl_up2(d[R - 1], 1);
+  const void* src[7] = {cu[0], cu[2], cu[1], cu[0], cu[2], cu[1], a.cp_in};
   const double ih = 1.0 / a.temp4;
+  int g = blockIdx.x;
+  if (g >= ngroup) return;
+  load_tile<R, 16>(ring, src[0], ps, g * FS_COLS, min(FS_COLS, a.ncol - g * FS_COLS), n, tid);
+  int step = 0;
+  for (; g < ngroup; g += gridDim.x) {
+    const int q0 = g * FS_COLS;
+    const int nvalid = min(FS_COLS, a.ncol - q0);
+    const int q = min(q0 + w, a.ncol - 1);
+    const int m = q / a.nk2, kq = q % a.nk2;
+    const bool m00 = (q0 + w == 0);
+    const double kxm = a.kx[m], kzq = a.kz[kq];
+    const int gn = g + gridDim.x;
+    double2 d[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int j = j0 + r;
-    if (j >= n) continue;
-    const size_t o = (size_t)j * ps + q;
-    if (j >= 1 && j <= nyp) {
-      double2 u1 = ldc(cu[0], o), u2 = ldc(cu[1], o), u3 = ldc(cu[2], o);
-      if (a.keep[0]) { a.keep[0][o] = u1; a.keep[1][o] = u2; a.keep[2][o] = u3; }
-      cu[0][o] = u1 - mul_ik(kxm, d[r]);
-      cu[2][o] = u3 - mul_ik(kzq, d[r]);
-      if (j >= 2) {
-        const double2 pm = r == 0 ? phm : d[r - 1];
-        cu[1][o] = u2 - __ldg(met + MET_IDY * n + j) * (d[r] - pm);
+    for (int r = 0; r < R; ++r) d[r] = z2;
+    double2 phm = z2;
+    for (int k = 0; k < 7; ++k, ++step) {
+      double2* nslot = ring + ((step + 1) & 1) * tsz;
+      if (k + 1 < 7) load_tile<R, 16>(nslot, src[k + 1], ps, q0, nvalid, n, tid);
+      else if (gn < ngroup) load_tile<R, 16>(nslot, src[0], ps, gn * FS_COLS, min(FS_COLS, a.ncol - gn * FS_COLS), n, tid);
+      else load_tile<R, 16>(nslot, nullptr, ps, q0, nvalid, n, tid);
+      wait_groups<1>();
+      __syncthreads();
+      double2* T = ring + (step & 1) * tsz;
+      if (k < 3) {
+        // divergence ik.u1 + ik.u3 + (u2(j+1) - u2(j))/dyf(j), rows 1..Ny,
+        // in the order the solves of the fused step accumulated it
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= 1 && j <= nyp) {
+            if (k == 0) d[r] = d[r] + mul_ik(kxm, T[slot<R>(j, w)]);
+            else if (k == 1) d[r] = d[r] + mul_ik(kzq, T[slot<R>(j, w)]);
+            else d[r] = d[r] + __ldg(met + MET_IDYF * n + j) * (T[slot<R>(j + 1, w)] - T[slot<R>(j, w)]);
+          }
+        }
+        if (k == 2) {
+          // Poisson rows: interior 1/(dy dyf) terms, Neumann walls, phi(1) = 0
+          // for the (0,0) mode
+          double al[R], cm[R];
+          const double k2n = -kxm * kxm - kzq * kzq;
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            double am = 0.0, cc = 0.0;
+            if (j >= 1 && j <= nyp) { am = __ldg(met + MET_PA * n + j); cc = __ldg(met + MET_PC * n + j); }
+            if (j == 1) { am = 0; cc = m00 ? 0.0 : -1.0; d[r] = z2; }
+            if (j == nyp) { am = 1; cc = 0; d[r] = z2; }
+            al[r] = am;
+            cm[r] = cc;
+          }
+          csolve2::warp_tridiag_b<R>([&](int r) -> double& { return al[r]; }, [&](int r) -> double {
+            const int j = j0 + r;
+            return (j == 1) ? 1.0 : (j == nyp ? -1.0 : ((j > 1 && j < nyp) ? k2n + __ldg(met + MET_PB0 * n + j) : 1.0));
+          }, [&](int r) -> double& { return cm[r]; }, d, lane);
+          phm = shfl_up2(d[R - 1], 1);   // phi of the row below the lane's first
+        }
+      } else if (k < 6) {
+        const int comp = k == 3 ? 0 : (k == 4 ? 2 : 1);
+        if (a.keep[0]) {
+          store_tile<R>(T, a.keep[comp], ps, q0, nvalid, 1, nyp, tid);
+          __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (comp != 1 && j >= 1 && j <= nyp) {
+            double2& u = T[slot<R>(j, w)];
+            u = u - mul_ik(comp == 0 ? kxm : kzq, d[r]);
+          }
+          if (comp == 1 && j >= 2 && j <= nyp) {
+            double2& u = T[slot<R>(j, w)];
+            u = u - __ldg(met + MET_IDY * n + j) * (d[r] - (r == 0 ? phm : d[r - 1]));
+          }
+        }
+        __syncthreads();
+        store_tile<R>(T, cu[comp], ps, q0, nvalid, comp == 1 ? 2 : 1, nyp, tid);
+      } else {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int j = j0 + r;
+          if (j >= a.jstart && j <= a.jend) {
+            double2& p = T[slot<R>(j, w)];
+            p = p + ih * d[r];
+          }
+        }
+        __syncthreads();
+        store_tile<R>(T, a.cp_out, ps, q0, nvalid, 0, n - 1, tid);
       }
+      __syncthreads();
     }
-    double2 p = ldc(a.cp_in, o);
-    if (j >= a.jstart && j <= a.jend) p = p + ih * d[r];
-    a.cp_out[o] = p;
   }
 }
