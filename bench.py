@@ -13,8 +13,9 @@ every rank runs an independent replica (the step does not shard).
 
 The reference arm (`--impl reference`) times the CPU restatement of the
 reference's step (the Fortran cannot be built on this image) on all host
-cores, one RK substep of the same workload restricted to 33 wall-normal
-planes per timed step.
+cores: whole RK3 steps of the same workload restricted to 33 of its 257
+wall-normal planes per timed step, with one full-size substep beside it as a
+calibration of the per-point rate (kept out of the value).
 """
 from __future__ import annotations
 
@@ -158,10 +159,12 @@ def kernel_bytes(p, nf, mixed):
         # (state u1, u3, u2 on two planes read; 8 more bytes written per mode)
         "z_forward_combine": 2 * nf * ny * xsp * cs + nf * ny * four * cs
                              + (ny * four * (4 * 16 + 8) if mixed else 0),
-        # state (3 u + p + scalars) in and out, NL in, cf in on 2 of 3 substeps
-        # and out on 2 of 3 substeps
-        "column_solve": nyp2 * four * (2 * (4 + nth) * 16 + nf * cs + (16 - cs if mixed else 0)
+        # field solves: every field in and its solved value out, the pressure
+        # in (once), NL in, cf in on 2 of 3 substeps and out on 2 of 3
+        "column_solve": nyp2 * four * (2 * nf * 16 + 16 + nf * cs + (16 - cs if mixed else 0)
                                        + 2 * (2.0 / 3.0) * nf * 16),
+        # projection: solved u1, u2, u3 and p in, projected u1, u2, u3 and p out
+        "projection": nyp2 * four * (4 * 16 * 2),
     }
 
 
@@ -240,49 +243,66 @@ def timed_steps(ch, torch, stream, k, dist=None):
     return e0.elapsed_time(e1)
 
 
-def cpu_baseline(steps=3, warmup=1):
-    """The CPU oracle on all host cores: RK substeps of the benchmark workload
-    restricted to SAMPLE_NY wall-normal planes."""
+def _oracle_slice(ny, cores):
     import dataclasses
     from diablo3_test_b200 import ics
     from diablo3_test_b200.grid import create_grid, TANH_ENDS_SYMMETRIC
     from tests.helpers import setup_oracle
     p, _ = ics.config_c2()
-    p = dataclasses.replace(p, ny=SAMPLE_NY)
+    p = dataclasses.replace(p, ny=ny)
     gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 2.0)
     fields = ics.log_law_turbulent(p, gy)
+    return p, setup_oracle(p, gy, fields, workers=cores)
+
+
+def cpu_baseline(steps=1, warmup=1):
+    """The CPU oracle on all host cores: whole RK3 steps (three substeps) of
+    the benchmark workload restricted to SAMPLE_NY wall-normal planes."""
     cores = os.cpu_count() or 1
-    o = setup_oracle(p, gy, fields, workers=cores)
+    p, o = _oracle_slice(SAMPLE_NY, cores)
     times = []
     for s in range(warmup + steps):
-        o.rk_step = 1 + s % 3
         t = time.perf_counter()
-        o.rk_chan_1()
+        o.step(1)
         dt = time.perf_counter() - t
         if s >= warmup:
             times.append(dt)
-    t_sub = sum(times) / len(times)
-    value = p.nx * p.ny * p.nz / 3.0 / t_sub / 1e6
+    t_step = sum(times) / len(times)
+    value = p.nx * p.ny * p.nz / t_step / 1e6
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"oracle RK substeps of the workload on {SAMPLE_NY} of 257 planes "
-                      f"(256x{SAMPLE_NY}x256), mean of {steps} after {warmup} warm-up; "
-                      f"one substep = 1/3 step", "s_per_substep": t_sub}
+            "sample": f"oracle RK3 steps (3 substeps each) of the workload on {SAMPLE_NY} of 257 "
+                      f"planes (256x{SAMPLE_NY}x256), mean of {steps} after {warmup} warm-up",
+            "s_per_step": t_step}
+
+
+def cpu_calibration(cores):
+    """One RK substep of the full 257-plane workload on the CPU oracle, to
+    check the slice's per-point rate (not part of any reported value)."""
+    p, o = _oracle_slice(257, cores)
+    o.rk_step = 1
+    t = time.perf_counter()
+    o.rk_chan_1()
+    dt = time.perf_counter() - t
+    return {"full_planes_substep_s": dt,
+            "full_planes_rate": p.nx * p.ny * p.nz / 3.0 / dt / 1e6, "unit": UNIT}
 
 
 def read_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/*.md lines 'traffic_per_launch <kernel> <bytes>')."""
+    """Per-launch DRAM bytes of each profiled kernel from the committed ncu
+    summaries (profiles/*.md lines 'traffic_per_launch <kernel> <bytes>
+    <how the figure was obtained>'): {kernel: (bytes, source)}.  These are
+    captured offline, not in this run."""
     out = {}
     pdir = os.path.join(ROOT, "profiles")
     if not os.path.isdir(pdir):
         return out
-    for fn in os.listdir(pdir):
+    for fn in sorted(os.listdir(pdir)):
         if not fn.endswith(".md"):
             continue
         for line in open(os.path.join(pdir, fn)):
-            m = re.match(r"\s*traffic_per_launch\s+(\S+)\s+(\d+)", line)
+            m = re.match(r"\s*traffic_per_launch\s+(\S+)\s+(\d+)\s*(.*)$", line)
             if m:
-                out[m.group(1)] = int(m.group(2))
+                out[m.group(1)] = (int(m.group(2)), f"profiles/{fn}: {m.group(3).strip()}")
     return out
 
 
@@ -430,9 +450,12 @@ def adjoint_bench(torch, nsteps=50, every=10):
     timed(lambda: ch.step(nsteps))                     # warm-up
     t_fwd = min(timed(lambda: ch.step(nsteps)) for _ in range(3))
     timed(lambda: ch.adjoint_record(nsteps, every))    # first call allocates the checkpoints
-    t_rec = timed(lambda: ch.adjoint_record(nsteps, every))
+    # one untimed backward sweep first: it allocates the adjoint work arrays
+    # and loads the adjoint kernels
     for l in lam:
         l.normal_()
+    ch.adjoint_run([l.clone() for l in lam])
+    t_rec = timed(lambda: ch.adjoint_record(nsteps, every))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(s)
     ch.adjoint_run(lam)
@@ -600,10 +623,11 @@ def run_ours(args):
             per_kernel[name] = {"launches": n, "avg_ms": avg, "share": ms / max(ms_mixed, 1e-9),
                                 "alg_bytes": kb[name], "achieved_gbs": kb[name] / (avg * 1e-3) / 1e9}
     dom = max(per_kernel, key=lambda k: per_kernel[k]["avg_ms"] * per_kernel[k]["launches"])
-    traffic = read_traffic().get(dom)
+    traffic, traffic_src = read_traffic().get(dom, (None, None))
     achieved = per_kernel[dom]["achieved_gbs"]
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs"}
+                "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic_source": traffic_src}
     # whole-step roofline against the 3*(8NF+9)*s bytes-per-point-step model
     alg64 = 3 * (8 * nf + 9) * 8
     value = pts * world * args.steps / (ms_mixed * 1e-3) / 1e6
@@ -663,14 +687,18 @@ def run_reference(args):
     if rank != 0:
         return
     cb = cpu_baseline(steps=args.steps, warmup=args.warmup)
+    cal = cpu_calibration(cb["cores"])
     out = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": cb["s_per_substep"] * 3e3, "higher_is_better": True,
+           "warmup": args.warmup, "ms_per_step": cb["s_per_step"] * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
            "data": "synthetic (seeded log-law mean + 10% perturbations, projected)",
-           "config": {"workload": WORKLOAD, "precision": "fp64",
-                      "sample": f"256x{SAMPLE_NY}x256 slice of the workload, one RK substep per timed step"},
+           "config": {"workload": WORKLOAD + f"; timed on its 256x{SAMPLE_NY}x256 slice "
+                                             f"({SAMPLE_NY} of 257 wall-normal planes), whole RK3 steps",
+                      "precision": "fp64",
+                      "sample": f"256x{SAMPLE_NY}x256 slice of the workload, one whole RK3 step per timed step"},
            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "calibration": dict(cal, note="one full 257-plane substep, outside the timed steps and the value"),
            "note": "reference Fortran (gfortran+MPI+FFTW+HDF5+toml-f) cannot be built on this image; "
                    "the CPU restatement of its step (oracle/) is timed instead"}
     print(json.dumps(out))

@@ -69,30 +69,37 @@ int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s) {
 
 // ---- field-split column step (kernels_field.cuh) ----
 // Both kernels are persistent: as many blocks as fit on the device at once
-// (two per SM at Ny = 257), each walking its share of the tasks.
+// (two per SM at Ny = 257), each walking its share of the tasks.  The shared-
+// memory attribute and the resident block count are set up once per device
+// and instantiation, for the largest system of its R (32 R rows), so a launch
+// makes no extra runtime calls beyond cudaGetDevice.
 template <typename K>
-static int resident_blocks(K kernel, int smem) {
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
+static int resident_blocks(K kernel, int smem, int* cache) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) dev = 0;
+  int v = __atomic_load_n(&cache[dev], __ATOMIC_ACQUIRE);
+  if (v > 0) return v;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  int sms = 0, per = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, FS_THREADS, smem);
-  return (per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+  v = (per > 0 ? per : 1) * (sms > 0 ? sms : 1);
+  __atomic_store_n(&cache[dev], v, __ATOMIC_RELEASE);
+  return v;
 }
 template <int R>
 static void launch_field_t(const FieldArgs& A, cudaStream_t s) {
-  const int smem = (int)field_smem_bytes(A.s.n);
-  cudaFuncSetAttribute(k_field_solve<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  static int cache[64];
+  const int resident = resident_blocks(k_field_solve<R>, (int)field_smem_bytes(32 * R), cache);
   const int tasks = ((A.s.ncol + FS_COLS - 1) / FS_COLS) * A.nf;
-  const int grid = std::min(tasks, resident_blocks(k_field_solve<R>, smem));
-  k_field_solve<R><<<grid, FS_THREADS, smem, s>>>(A);
+  k_field_solve<R><<<std::min(tasks, resident), FS_THREADS, field_smem_bytes(A.s.n), s>>>(A);
 }
 template <int R>
 static void launch_project_t(const FieldArgs& A, cudaStream_t s) {
-  const int smem = (int)field_smem_bytes(A.s.n);
-  cudaFuncSetAttribute(k_project_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  static int cache[64];
+  const int resident = resident_blocks(k_project_cols<R>, (int)field_smem_bytes(32 * R), cache);
   const int groups = (A.s.ncol + FS_COLS - 1) / FS_COLS;
-  const int grid = std::min(groups, resident_blocks(k_project_cols<R>, smem));
-  k_project_cols<R><<<grid, FS_THREADS, smem, s>>>(A);
+  k_project_cols<R><<<std::min(groups, resident), FS_THREADS, field_smem_bytes(A.s.n), s>>>(A);
 }
 int launch_field_solve(const FieldArgs& A, cudaStream_t s) {
   switch (rows_per_lane(A.s.n)) {

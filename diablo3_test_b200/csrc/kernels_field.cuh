@@ -118,16 +118,19 @@ struct FTile {
 };
 #define FS_MAXTILES (5 + 2 * SOLVE_MAXTH)
 
-// Shared memory of both kernels: a two-stage input ring and an output slot,
-// each (Ny+2) x FS_COLS complex doubles.
-inline size_t field_smem_bytes(int n) { return (size_t)3 * n * FS_COLS * sizeof(double2); }
+// Shared memory of both kernels: a two-stage ring of (Ny+2) x FS_COLS complex
+// doubles.  Results leave through the slot just consumed.
+inline size_t field_smem_bytes(int n) { return (size_t)2 * n * FS_COLS * sizeof(double2); }
 
 namespace cfield {
-// the tiles field f reads, in the order its explicit terms use them
+// The tiles field f reads, in the order its explicit terms use them: the
+// nonlinear terms and couplings first, so that cf is complete when the
+// field's own tile arrives and its registers turn into the right-hand side's.
 DI int field_tiles(const SolveArgs& a, int f, FTile* tl) {
   const int th = f - 3;
   int ns = 0;
-  tl[ns++] = FTile{f < 3 ? (const void*)a.cu_in[f] : (const void*)a.cth_in[th], FT_OWN, 0, 0.0};
+  if (a.nl64[f]) tl[ns++] = FTile{a.nl64[f], FT_NL, 0, 0.0};
+  else tl[ns++] = FTile{a.nl32[f], FT_NL, 1, 0.0};
   if (f == 0 || f == 2) {
     if (a.roinvd != 0.0) tl[ns++] = FTile{a.cu_in[2 - f], FT_ADD, 0, f == 0 ? a.roinvd : -a.roinvd};
     const double g = f == 0 ? a.grav_x : a.grav_z;
@@ -140,8 +143,7 @@ DI int field_tiles(const SolveArgs& a, int f, FTile* tl) {
     if (a.dthdx[th] != 0.0) tl[ns++] = FTile{a.cu_in[0], FT_ADD, 0, -a.dthdx[th]};
     if (a.dthdz[th] != 0.0) tl[ns++] = FTile{a.cu_in[2], FT_ADD, 0, -a.dthdz[th]};
   }
-  if (a.nl64[f]) tl[ns++] = FTile{a.nl64[f], FT_NL, 0, 0.0};
-  else tl[ns++] = FTile{a.nl32[f], FT_NL, 1, 0.0};
+  tl[ns++] = FTile{f < 3 ? (const void*)a.cu_in[f] : (const void*)a.cth_in[th], FT_OWN, 0, 0.0};
   if (a.rk > 1) tl[ns++] = FTile{a.cf_in[f], FT_CFOLD, 0, 0.0};
   if (f < 3) tl[ns++] = FTile{a.cp_in, FT_P, 0, 0.0};
   return ns;
@@ -153,19 +155,24 @@ DI void load_ftile(void* slot, const FTile* t, size_t ps, int q0, int nvalid, in
 }
 }  // namespace cfield
 
+// Blocks per SM the register cap is set for: three fit in 80 registers
+// without spills up to R = 6; at R = 9 the solve spills under that cap
+// (0.545 against 0.477 ms per launch at 256 x 257 x 256), so two.
+template <int R>
+constexpr int fs_min_blocks() { return R <= 6 ? 3 : 2; }
+
 // Persistent: block b takes tasks b, b + gridDim.x, ... (task t = field
 // t % N_F of column group t / N_F).  The ring runs on across tasks: the last
 // step of a task already copies the next task's first tile, so the tile is in
 // flight while this task's solve and stores run.
 template <int R>
-__global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_constant__ FieldArgs A) {
+__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_field_solve(const __grid_constant__ FieldArgs A) {
   using namespace cfield;
   extern __shared__ __align__(16) unsigned char fs_smem[];
   const SolveArgs& a = A.s;
   const int n = a.n, nyp = a.nyp;
   const int tsz = n * FS_COLS;
   double2* ring = reinterpret_cast<double2*>(fs_smem);
-  double2* out = ring + 2 * tsz;
   const int nf = A.nf;
   const int ntask = ((a.ncol + FS_COLS - 1) / FS_COLS) * nf;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -219,30 +226,49 @@ __global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_cons
       if (k + 1 < ns) {
         load_ftile<R>(nslot, &tl[k + 1], ps, q0, nvalid, n, tid);
       } else if (tn < ntask) {
-        // the next task's own-field tile
+        // the next task's first tile (its nonlinear terms)
         const int fn = tn % nf, qn = (tn / nf) * FS_COLS;
-        const FTile own = FTile{fn < 3 ? (const void*)a.cu_in[fn] : (const void*)a.cth_in[fn - 3], FT_OWN, 0, 0.0};
-        load_ftile<R>(nslot, &own, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
+        const FTile first = a.nl64[fn] ? FTile{a.nl64[fn], FT_NL, 0, 0.0} : FTile{a.nl32[fn], FT_NL, 1, 0.0};
+        load_ftile<R>(nslot, &first, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
       } else {
         load_ftile<R>(nslot, nullptr, ps, q0, nvalid, n, tid);
       }
       wait_groups<1>();
       __syncthreads();
-      const double2* T = ring + (step & 1) * tsz;
+      double2* T = ring + (step & 1) * tsz;
       auto TV = [&](int j) -> double2 { return T[slot<R>(j, w)]; };
       switch (tk.kind) {
-        case FT_OWN:
+        case FT_OWN: {
+          // cf is complete here; it leaves through this slot, overwriting the
+          // field row by row: a lane takes its two neighbour rows (other
+          // lanes' rows of the same column) before the warp writes anything,
+          // and reads row j+1 before overwriting row j
+          // (lanes whose rows lie past the system read nothing)
+          const double2 h_lo = (j0 >= 1 && j0 - 1 < n) ? TV(j0 - 1) : z2;
+          const double2 h_hi = j0 + R < n ? TV(j0 + R) : z2;
+          __syncwarp();
+          double2 um = h_lo, u = j0 < n ? TV(j0) : z2;
 #pragma unroll
           for (int r = 0; r < R; ++r) {
             const int j = j0 + r;
+            const double2 up = r == R - 1 ? h_hi : (j + 1 < n ? TV(j + 1) : z2);
+            double2 c = cf[r];
             if (j >= lo && j <= hi) {
-              const double2 u = TV(j), um = TV(j - 1), up = TV(j + 1);
-              cf[r] = -cfc * u;
+              c = c - cfc * u;
+              if (Up) c = c - mul_ik(kxm * __ldg(Up + j), u);
               cr[r] = u - K[2 * n + j] * (up - u) + K[j] * (u - um);
-              if (Up) cf[r] = cf[r] - mul_ik(kxm * __ldg(Up + j), u);
+              cr[r] = cr[r] + a.temp5 * c;
             }
+            if (a.store_cf && j < n) T[slot<R>(j, w)] = c;
+            um = u;
+            u = up;
+          }
+          if (a.store_cf) {
+            __syncthreads();
+            store_tile<R>(T, a.cf_out[f], ps, q0, nvalid, lo, hi, tid);
           }
           break;
+        }
         case FT_ADD:
 #pragma unroll
           for (int r = 0; r < R; ++r) {
@@ -270,18 +296,8 @@ __global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_cons
               double2 nl;
               if (tk.f32) { const float2 v = T32[slot<R>(j, w)]; nl = make_double2(v.x, v.y); }
               else nl = TV(j);
-              cf[r] = cf[r] - nl;
-              cr[r] = cr[r] + a.temp5 * cf[r];
+              cf[r] = -nl;
             }
-          }
-          if (a.store_cf) {   // cf of the next substep, out through the output slot
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-              const int j = j0 + r;
-              if (j < n) out[slot<R>(j, w)] = cf[r];
-            }
-            __syncthreads();
-            store_tile<R>(out, a.cf_out[f], ps, q0, nvalid, lo, hi, tid);
           }
           break;
         }
@@ -338,6 +354,7 @@ __global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_cons
     // The solve writes rows w0 .. Ny+1 (u2: from row 1, the others from
     // lo - 1); rows below keep their input value.
     const int w0 = f == 1 ? 1 : lo - 1;
+    double2* out = ring + ((step - 1) & 1) * tsz;   // the slot of the last step
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = j0 + r;
@@ -346,6 +363,7 @@ __global__ void __launch_bounds__(FS_THREADS, 2) k_field_solve(const __grid_cons
     __syncthreads();
     const double2* own = f < 3 ? a.cu_in[f] : a.cth_in[th];
     store_tile<R>(out, f < 3 ? a.cu_out[f] : a.cth_out[th], ps, q0, nvalid, 0, n - 1, tid, own, w0);
+    __syncthreads();   // the next task's second tile goes to this slot
     if (tn < ntask) ns = field_tiles(a, tn % nf, tl);
   }
 }
