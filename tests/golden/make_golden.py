@@ -6,7 +6,7 @@ the first argument; h5py and matplotlib, which only that tool's file writer
 and plotter use, are stubbed).  The GPU box never runs this script; the tests
 read the committed .npz.
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /path/to/reference
 """
 import os
 import sys
@@ -52,4 +52,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+    main(sys.argv[1])
