@@ -519,6 +519,43 @@ def e2e_round_trip(ch, torch, k):
             "path": "diablo_upload_state x6 (host, pinned) + diablo_step + diablo_download_state x6"}
 
 
+def profile_other(args, torch):
+    """Profiling runs (no JSON line), for launch lists and ncu sections, at
+    --grid: the adjoint with the adjoint workload's parameters (velocity-only
+    FP64; diablo_adjoint_record over --steps steps, a checkpoint every step,
+    then diablo_adjoint_run), and the statistics (diablo_stats --steps times)
+    on the Re_tau = 180 workload's state."""
+    import dataclasses
+    from diablo3_test_b200 import ics, _lib
+    from diablo3_test_b200.config import FP64, MIXED
+    from diablo3_test_b200.grid import create_grid, TANH_ENDS_SYMMETRIC
+    if args.profile_adjoint:
+        p, gy, _ = ics.config_c4()      # velocity-only FP64 parameters
+    else:
+        p, gy = ics.config_c2()
+    if args.grid:
+        p = dataclasses.replace(p, nx=args.grid[0], ny=args.grid[1], nz=args.grid[2])
+        gy, _ = create_grid(p.ny, 2.0, TANH_ENDS_SYMMETRIC, 1.8 if args.profile_adjoint else 2.0)
+    fields = ics.laminar_dns(p, gy, seed=4, amp=0.05) if args.profile_adjoint else ics.log_law_turbulent(p, gy)
+    ch = setup_channel(p, gy, fields, FP64 if args.profile_adjoint else MIXED)
+    stream = torch.cuda.Stream()
+    ch.set_stream(stream.cuda_stream)
+    ch.step(args.warmup)
+    t0 = time.perf_counter()
+    if args.profile_adjoint:
+        ids = (_lib.U1, _lib.U2, _lib.U3, _lib.P)
+        lam = [torch.randn(ch.shape_phys, dtype=torch.float64, device="cuda") for _ in ids]
+        ch.adjoint_record(args.steps, 1)
+        ch.adjoint_run(lam)
+    else:
+        for _ in range(args.steps):
+            ch.stats()
+    ch.synchronize()
+    what = "adjoint" if args.profile_adjoint else "statistics"
+    print(f"profiling run {what} {p.nx}x{p.ny}x{p.nz}: {time.perf_counter() - t0:.3f} s")
+    ch.close()
+
+
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
@@ -537,6 +574,9 @@ def run_ours(args):
     else:
         torch.cuda.set_device(local)
     torch.cuda.init()
+    if args.profile_adjoint or args.profile_stats:
+        profile_other(args, torch)
+        return
     if args.profile_les:
         # profiling run of the dynamic-LES workload (128 x 129 x 128), no JSON line
         p, gy, fields = ics.config_c3(2)
@@ -725,6 +765,10 @@ def main():
                     help="profiling: run one precision only")
     ap.add_argument("--profile-les", action="store_true",
                     help="profiling: time the dynamic-LES workload instead (mixed unless --precision fp64)")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="profiling: record and run the adjoint on the --grid workload (velocities, FP64)")
+    ap.add_argument("--profile-stats", action="store_true",
+                    help="profiling: save_stats_chan on the --grid workload state")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -72,6 +72,7 @@ SIGNATURES = {
     "diablo_set_stream": (_i, [_vp, _vp]),
     "diablo_synchronize": (_i, [_vp]),
     "diablo_check_finite": (_i, [_vp]),
+    "diablo_set_wait_bound": (_i, [_vp, ctypes.c_longlong, _i]),
     "diablo_kernel_launches": (ctypes.c_longlong, [_vp]),
     "diablo_set_profiling": (_i, [_vp, _i]),
     "diablo_kernel_times": (_i, [_vp, _i, ctypes.POINTER(_d), ctypes.POINTER(ctypes.c_longlong)]),

@@ -88,6 +88,13 @@ static int resident_blocks(K kernel, int smem, int* cache) {
   return v;
 }
 template <int R>
+static void launch_column_step_t(const FieldArgs& A, cudaStream_t s) {
+  static int cache[64];
+  const int resident = resident_blocks(k_column_step<R>, (int)field_smem_bytes(32 * R), cache);
+  const int groups = (A.s.ncol + FS_COLS - 1) / FS_COLS;
+  k_column_step<R><<<std::min(groups * (A.nf + 1), resident), FS_THREADS, field_smem_bytes(A.s.n), s>>>(A);
+}
+template <int R>
 static void launch_field_t(const FieldArgs& A, cudaStream_t s) {
   static int cache[64];
   const int resident = resident_blocks(k_field_solve<R>, (int)field_smem_bytes(32 * R), cache);
@@ -112,6 +119,22 @@ int launch_field_solve(const FieldArgs& A, cudaStream_t s) {
 int launch_project_cols(const FieldArgs& A, cudaStream_t s) {
   switch (rows_per_lane(A.s.n)) {
 #define X(r) case r: launch_project_t<r>(A, s); return 0;
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return DIABLO_ERR_SIZE;
+  }
+}
+int column_step_resident(int n) {
+  switch (rows_per_lane(n)) {
+#define X(r) case r: { static int cache[64]; return resident_blocks(k_column_step<r>, (int)field_smem_bytes(32 * r), cache); }
+    X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
+#undef X
+    default: return 0;
+  }
+}
+int launch_column_step(const FieldArgs& A, cudaStream_t s) {
+  switch (rows_per_lane(A.s.n)) {
+#define X(r) case r: launch_column_step_t<r>(A, s); return 0;
     X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16) X(17)
 #undef X
     default: return DIABLO_ERR_SIZE;

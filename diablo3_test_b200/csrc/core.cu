@@ -243,6 +243,19 @@ int les_active(const diablo_ctx* ctx) {
 }
 // ==========================================================================
 // C ABI
+// The column step's status word: DIABLO_ERR_TIMEOUT (and the word cleared)
+// if a bounded device wait gave up since the last check.  Waits for the
+// context's stream.
+int sched_status(diablo_ctx* ctx) {
+  int v = 0;
+  CK(cudaMemcpyAsync(&v, ctx->d_sched, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (!v) return 0;
+  CK(cudaMemsetAsync(ctx->d_sched, 0, sizeof(int), ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DIABLO_ERR_TIMEOUT;
+}
+
 extern "C" {
 
 int diablo_abi_version(void) { return DIABLO_ABI_VERSION; }
@@ -310,7 +323,7 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
   ctx->precision = p->precision;
   {
     const char* e = getenv("DIABLO_GENERAL_SOLVER");
-    ctx->use_general_solver = (e && (e[0] == '1' || e[0] == '2')) ? e[0] - '0' : 0;
+    ctx->use_general_solver = (e && e[0] >= '1' && e[0] <= '3') ? e[0] - '0' : 0;
   }
   int rc = 0;
 #define FAIL(code) do { *status = (code); diablo_destroy(ctx); return nullptr; } while (0)
@@ -360,6 +373,11 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
       if ((rc = dev_alloc(ctx, (void**)&ctx->cf[b][f], four_elems(ctx) * sizeof(double2)))) FAIL(rc);
   }
   if ((rc = dev_alloc(ctx, (void**)&ctx->d_flag, sizeof(int)))) FAIL(rc);
+  // column-step scheduler: status, task counter, one count per column group
+  ctx->sched_ints = 2 + (size_t)(ctx->nkx1 * ctx->nk2 + FS_COLS - 1) / FS_COLS;
+  if ((rc = dev_alloc(ctx, (void**)&ctx->d_sched, ctx->sched_ints * sizeof(int)))) FAIL(rc);
+  ctx->wait_spins = 1LL << 24;   // about a second of 100 ns sleeps
+  ctx->wait_withhold = 0;
   if ((rc = upload_coefficients(ctx))) FAIL(rc);
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) FAIL(DIABLO_ERR_CUDA);
 #undef FAIL
@@ -576,7 +594,8 @@ int diablo_fft_xz_to_physical(diablo_ctx* ctx, double* vv, double* v) {
 
 int diablo_rk_substep(diablo_ctx* ctx, int rk_step) {
   if (!ctx || rk_step < 1 || rk_step > 3) return DIABLO_ERR_ARG;
-  return substep(ctx, rk_step);
+  const int rc = substep(ctx, rk_step);
+  return rc ? rc : sched_status(ctx);
 }
 
 static int filter_chan(diablo_ctx* ctx, int n) {
@@ -633,7 +652,7 @@ int diablo_step(diablo_ctx* ctx, int nsteps) {
     int rc = filter_scalars(ctx);
     if (rc) return rc;
   }
-  return 0;
+  return sched_status(ctx);
 }
 
 extern "C++" int bc_post(diablo_ctx* ctx, int do_vel, int do_th) {
@@ -757,6 +776,14 @@ int diablo_synchronize(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
+  return sched_status(ctx);
+}
+
+int diablo_set_wait_bound(diablo_ctx* ctx, long long max_spins, int withheld_arrivals) {
+  if (!ctx || max_spins < 1 || withheld_arrivals < 0) return DIABLO_ERR_ARG;
+  ctx->wait_spins = max_spins;
+  ctx->wait_withhold = withheld_arrivals;
+  ctx->generation++;   // captured kernel arguments change
   return 0;
 }
 

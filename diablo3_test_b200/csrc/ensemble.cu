@@ -211,7 +211,12 @@ int diablo_ensemble_synchronize(diablo_ensemble* e) {
   ECK(cudaStreamSynchronize(e->origin));
   for (diablo_ctx* c : e->m) ECK(cudaStreamSynchronize(c->stream));
   ECK(cudaGetLastError());
-  return 0;
+  int rc = 0;
+  for (diablo_ctx* c : e->m) {   // a member's column-step wait that gave up
+    const int r = sched_status(c);
+    if (r && !rc) rc = r;
+  }
+  return rc;
 }
 
 int diablo_ensemble_destroy(diablo_ensemble* e) {

@@ -83,7 +83,10 @@ struct diablo_ctx {
   int profiling;
   int generation;           // bumped whenever captured kernel arguments go stale (dt, precision, tiles)
   int tune[4];              // tile shapes of the step transforms (z inv S, x inv KT, x fwd KT, z fwd S; 0 = default)
-  int use_general_solver;   // 0: field-split column kernels, 1: the general kernel, 2: the tiled kernel
+  // column step (DIABLO_GENERAL_SOLVER): 0 the field-split kernels in two
+  // launches, 1 the general kernel, 2 the fused tiled kernel, 3 the
+  // field-split step in one launch with bounded waits
+  int use_general_solver;
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
@@ -101,6 +104,12 @@ struct diablo_ctx {
   double* stats_thxy;       // its z-line mean [Ny+2][Nx]
   size_t stats_doubles;
   double* d_fac[3];         // factored field systems per RK substep (k_factor)
+  // k_column_step's scheduler words (task counter, status, per-group counts),
+  // the bound of its waits and the arrivals withheld by the failure hook
+  int* d_sched;
+  size_t sched_ints;
+  long long wait_spins;
+  int wait_withhold;
   // LES substep buffers (FP64), allocated on first use
   struct Les {
     int ready;
@@ -227,6 +236,9 @@ int launch_solve(const SolveArgs& a, bool project_only, cudaStream_t s);
 struct FieldArgs;
 int launch_field_solve(const FieldArgs& A, cudaStream_t s);
 int launch_project_cols(const FieldArgs& A, cudaStream_t s);
+int launch_column_step(const FieldArgs& A, cudaStream_t s);
+int column_step_resident(int n);   // blocks of k_column_step resident at once
+int sched_status(diablo_ctx* ctx);  // DIABLO_ERR_TIMEOUT if a device wait gave up (clears it)
 
 // ---- the step (step.cu) ------------------------------------------------------
 int upload_coefficients(diablo_ctx* ctx);

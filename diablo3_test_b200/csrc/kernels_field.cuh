@@ -34,8 +34,6 @@
 #include "kernels_solve.cuh"
 #include "kernels_solve2.cuh"
 
-#define FS_COLS 8     // columns (one warp each) per block
-#define FS_THREADS (32 * FS_COLS)
 
 struct FieldArgs {
   SolveArgs s;
@@ -45,6 +43,12 @@ struct FieldArgs {
   int nf;              // 3 + N_th
   int mean_split;      // see Solve2Args::mean_split
   const double* prof;  // [2][n] U1(j), I(U1)(j)
+  // k_column_step's scheduler: [0] status (1 = a wait gave up), [1] task
+  // counter, [2 + g] velocity solves done in column group g
+  int* sched;
+  int need;            // solves a projection waits for (3)
+  int lag;             // column groups between a group's solves and its projection
+  long long max_spins; // bound of a projection's wait
 };
 
 namespace cfield {
@@ -155,18 +159,24 @@ DI void load_ftile(void* slot, const FTile* t, size_t ps, int q0, int nvalid, in
 }
 }  // namespace cfield
 
-// Blocks per SM the register cap is set for: three fit in 80 registers
-// without spills up to R = 6; at R = 9 the solve spills under that cap
-// (0.545 against 0.477 ms per launch at 256 x 257 x 256), so two.
+// Blocks per SM the register cap of k_column_step is set for: three fit in
+// 80 registers without spills up to R = 4; beyond that the projection's
+// Poisson rows and the solve spill under that cap, so two.
 template <int R>
-constexpr int fs_min_blocks() { return R <= 6 ? 3 : 2; }
+constexpr int fs_min_blocks() { return R <= 4 ? 3 : 2; }
+
+// Blocks per SM the register cap of k_field_solve is set for: three fit in
+// 80 registers without spills up to R = 6; at R = 9 the solve spills under
+// that cap (0.545 against 0.477 ms per launch at 256 x 257 x 256), so two.
+template <int R>
+constexpr int fs_field_min_blocks() { return R <= 6 ? 3 : 2; }
 
 // Persistent: block b takes tasks b, b + gridDim.x, ... (task t = field
 // t % N_F of column group t / N_F).  The ring runs on across tasks: the last
 // step of a task already copies the next task's first tile, so the tile is in
 // flight while this task's solve and stores run.
 template <int R>
-__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_field_solve(const __grid_constant__ FieldArgs A) {
+__global__ void __launch_bounds__(FS_THREADS, fs_field_min_blocks<R>()) k_field_solve(const __grid_constant__ FieldArgs A) {
   using namespace cfield;
   extern __shared__ __align__(16) unsigned char fs_smem[];
   const SolveArgs& a = A.s;
@@ -485,4 +495,389 @@ __global__ void __launch_bounds__(FS_THREADS, 2) k_project_cols(const __grid_con
       __syncthreads();
     }
   }
+}
+
+// ---- k_column_step --------------------------------------------------------------
+// Both halves of the column step in one persistent launch.  Tasks are claimed
+// in order from a counter: the field tasks of column group s (one per field)
+// are followed, LAG groups later, by the projection task of group s - LAG, so
+// the solved velocities it reads were written shortly before and are still
+// in L2.  A projection task waits until its group's three velocity tasks have
+// published their completion (a release/acquire count per group).  It can
+// only wait on tasks claimed before it by blocks that are running, and field
+// tasks never wait, so the wait always ends; it is still bounded by
+// max_spins, after which the task sets the status word and leaves its group
+// untouched, later waits give up at once, and the host reports
+// DIABLO_ERR_TIMEOUT.
+// Scheduler words: the status stays set across launches until the host has
+// read it (a later launch's waits then give up at once); the task counter and
+// the per-group counts are zeroed before every launch.
+enum { SCHED_STATUS = 0, SCHED_COUNTER = 1, SCHED_DONE = 2 };
+
+namespace cfield {
+struct Task {
+  int kind;   // 0 field solve, 1 projection, 2 none left
+  int g, f;   // column group, field
+};
+DI Task decode_task(int t, int ngroup, int nf, int lag) {
+  const int a0 = lag * nf, a1 = a0 + (ngroup - lag) * (nf + 1), a2 = a1 + lag;
+  if (t < a0) return Task{0, t / nf, t % nf};
+  if (t < a1) {
+    const int u = t - a0, s = lag + u / (nf + 1), r = u % (nf + 1);
+    return r < nf ? Task{0, s, r} : Task{1, s - lag, 0};
+  }
+  if (t < a2) return Task{1, ngroup - lag + (t - a1), 0};
+  return Task{2, 0, 0};
+}
+DI int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+}  // namespace cfield
+
+template <int R>
+__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(const __grid_constant__ FieldArgs A) {
+  using namespace cfield;
+  extern __shared__ __align__(16) unsigned char fs_smem[];
+  __shared__ int s_next, s_ok;
+  const SolveArgs& a = A.s;
+  const int n = a.n, nyp = a.nyp;
+  const int tsz = n * FS_COLS;
+  double2* ring = reinterpret_cast<double2*>(fs_smem);
+  const int nf = A.nf;
+  const int ngroup = (a.ncol + FS_COLS - 1) / FS_COLS;
+  const int lag = min(A.lag, ngroup);
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const size_t ps = (size_t)a.ncol;          // plane stride (the Fourier pitch is 2Nkz+1)
+  const double2 z2 = make_double2(0.0, 0.0);
+  const int j0 = lane * R;
+  const double* met = A.met;
+  double2* const* cu = a.cu_out;
+  const void* src[7] = {cu[0], cu[2], cu[1], cu[0], cu[2], cu[1], a.cp_in};
+  const double ih = 1.0 / a.temp4;
+  auto claim = [&]() -> Task {
+    if (tid == 0) s_next = atomicAdd(A.sched + SCHED_COUNTER, 1);
+    __syncthreads();
+    const int t = s_next;
+    return decode_task(t, ngroup, nf, lag);
+  };
+  Task cur = claim();
+  bool pre = false;   // the current task's first tile is already in flight
+  int step = 0;
+  while (cur.kind != 2) {
+    if (cur.kind == 0) {
+      const int f = cur.f;
+      const int q0 = cur.g * FS_COLS;
+      const int nvalid = min(FS_COLS, a.ncol - q0);
+      const int q = min(q0 + w, a.ncol - 1);   // a warp past the last column works on a copy
+      const int m = q / a.nk2, kq = q % a.nk2;
+      const bool m00 = (q0 + w == 0);
+      const double kxm = a.kx[m], kzq = a.kz[kq];
+      const double k2s = kxm * kxm + kzq * kzq;
+      const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+      // field kind: solve index f (0 u1, 1 u2, 2 u3, 3+n scalar n),
+      // row-coefficient index (0 u1/u3, 1 u2, 2+n scalar n), explicit rows
+      // [lo, hi], wall rows
+      const int th = f - 3;
+      const int kc_kind = f == 1 ? 1 : (f < 3 ? 0 : 2 + th);
+      int lo, hi, b0, b1;
+      double c0, c1;
+      if (f == 0) { lo = a.jstart; hi = a.jend; b0 = a.ubc[0]; b1 = a.ubc[1]; c0 = a.uc1[0]; c1 = a.uc1[1]; }
+      else if (f == 2) { lo = a.jstart; hi = a.jend; b0 = a.wbc[0]; b1 = a.wbc[1]; c0 = a.wc1[0]; c1 = a.wc1[1]; }
+      else if (f == 1) { lo = 2; hi = nyp; b0 = a.vbc[0]; b1 = a.vbc[1]; c0 = a.vc1[0]; c1 = a.vc1[1]; }
+      else { lo = a.jst[th]; hi = a.jet[th]; b0 = a.thbc[th][0]; b1 = a.thbc[th][1]; c0 = a.thc1[th][0]; c1 = a.thc1[th][1]; }
+      const double* K = A.kc + (size_t)kc_kind * 3 * n;
+      const double cfc = f >= 3 ? (a.nu / a.pr[th]) * kk : a.nu * kk;
+      // mean-split correction of this field: -ikx U(j) u with U = U1 (u3,
+      // scalars) or its GY interpolation I(U1) (u2); none for u1
+      const double* Up = (A.mean_split && f != 0) ? A.prof + (f == 1 ? n : 0) : nullptr;
+      FTile tl[FS_MAXTILES];
+      const int ns = field_tiles(a, f, tl);
+      if (!pre) load_ftile<R>(ring + (step & 1) * tsz, &tl[0], ps, q0, nvalid, n, tid);
+      Task nxt{2, 0, 0};
+
+      double2 cr[R], cf[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) { cr[r] = z2; cf[r] = z2; }
+      for (int k = 0; k < ns; ++k, ++step) {
+        const FTile tk = tl[k];
+        double2* nslot = ring + ((step + 1) & 1) * tsz;
+        if (k + 1 < ns) {
+          load_ftile<R>(nslot, &tl[k + 1], ps, q0, nvalid, n, tid);
+        } else {
+          // claim the next task; a field task's first tile (its nonlinear
+          // terms) goes in flight now, a projection's waits for its inputs
+          nxt = claim();
+          if (nxt.kind == 0) {
+            const int qn = nxt.g * FS_COLS;
+            const FTile first = a.nl64[nxt.f] ? FTile{a.nl64[nxt.f], FT_NL, 0, 0.0}
+                                              : FTile{a.nl32[nxt.f], FT_NL, 1, 0.0};
+            load_ftile<R>(nslot, &first, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
+          } else {
+            load_ftile<R>(nslot, nullptr, ps, q0, nvalid, n, tid);
+          }
+        }
+        wait_groups<1>();
+        __syncthreads();
+        double2* T = ring + (step & 1) * tsz;
+        auto TV = [&](int j) -> double2 { return T[slot<R>(j, w)]; };
+        switch (tk.kind) {
+          case FT_OWN: {
+            // cf is complete here; it leaves through this slot, overwriting the
+            // field row by row: a lane takes its two neighbour rows (other
+            // lanes' rows of the same column) before the warp writes anything,
+            // and reads row j+1 before overwriting row j
+            // (lanes whose rows lie past the system read nothing)
+            const double2 h_lo = (j0 >= 1 && j0 - 1 < n) ? TV(j0 - 1) : z2;
+            const double2 h_hi = j0 + R < n ? TV(j0 + R) : z2;
+            __syncwarp();
+            double2 um = h_lo, u = j0 < n ? TV(j0) : z2;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              const double2 up = r == R - 1 ? h_hi : (j + 1 < n ? TV(j + 1) : z2);
+              double2 c = cf[r];
+              if (j >= lo && j <= hi) {
+                c = c - cfc * u;
+                if (Up) c = c - mul_ik(kxm * __ldg(Up + j), u);
+                cr[r] = u - K[2 * n + j] * (up - u) + K[j] * (u - um);
+                cr[r] = cr[r] + a.temp5 * c;
+              }
+              if (a.store_cf && j < n) T[slot<R>(j, w)] = c;
+              um = u;
+              u = up;
+            }
+            if (a.store_cf) {
+              __syncthreads();
+              store_tile<R>(T, a.cf_out[f], ps, q0, nvalid, lo, hi, tid);
+            }
+            break;
+          }
+          case FT_ADD:
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j >= lo && j <= hi) cf[r] = cf[r] + tk.coef * TV(j);
+            }
+            break;
+          case FT_BUOY:
+            if (!m00) {
+#pragma unroll
+              for (int r = 0; r < R; ++r) {
+                const int j = j0 + r;
+                if (j >= lo && j <= hi)
+                  cf[r] = cf[r] + tk.coef * (__ldg(met + MET_WB1 * n + j) * TV(j) +
+                                             __ldg(met + MET_WB2 * n + j) * TV(j - 1));
+              }
+            }
+            break;
+          case FT_NL: {
+            const float2* T32 = reinterpret_cast<const float2*>(T);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j >= lo && j <= hi) {
+                double2 nl;
+                if (tk.f32) { const float2 v = T32[slot<R>(j, w)]; nl = make_double2(v.x, v.y); }
+                else nl = TV(j);
+                cf[r] = -nl;
+              }
+            }
+            break;
+          }
+          case FT_CFOLD:
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j >= lo && j <= hi) cr[r] = cr[r] + a.temp3 * TV(j);
+            }
+            break;
+          case FT_P:
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              if (j >= lo && j <= hi) {
+                if (f == 0) {
+                  cr[r] = cr[r] - a.temp4 * mul_ik(kxm, TV(j));
+                  if (m00) cr[r].x -= a.px;
+                } else if (f == 2) {
+                  cr[r] = cr[r] - a.temp4 * mul_ik(kzq, TV(j));
+                } else {
+                  cr[r] = cr[r] - a.temp4 * __ldg(met + MET_IDY * n + j) * (TV(j) - TV(j - 1));
+                }
+              }
+            }
+            break;
+          default:
+            break;
+        }
+        __syncthreads();
+      }
+      // right-hand side: explicit terms on the explicit rows, wall values on
+      // the wall rows (for/channel.f90:1545-1876); the matrix is in the factor
+      // table
+      const double v00 = m00 ? 1.0 : 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int j = j0 + r;
+        double2 d = (j >= lo && j <= hi) ? cr[r] : z2;
+        if (f == 1) {
+          if (b0 == 0 && (j == 1 || j == 2)) d = make_double2(c0 * v00, 0);
+          if (b0 == 1 && j == 1) d = make_double2(a.dyf[1] * c0 * v00, 0);
+          if (j == 0) d = z2;
+          if (b1 == 0 && (j == nyp || j == nyp + 1)) d = make_double2(c1 * v00, 0);
+          if (b1 == 1 && j == nyp + 1) d = make_double2(a.dyf[nyp] * c1 * v00, 0);
+        } else {
+          if (j == 0 || j == nyp + 1) d = z2;
+          if (j == 1) d = make_double2((b0 == 0 ? c0 : a.dy[2] * c0) * v00, 0);
+          if (j == nyp) d = make_double2((b1 == 0 ? c1 : a.dy[nyp] * c1) * v00, 0);
+        }
+        cr[r] = d;
+      }
+      apply_factored<R>(A.fac + (size_t)f * Fac<R>::N * 32, cr, lane);
+      // The solve writes rows w0 .. Ny+1 (u2: from row 1, the others from
+      // lo - 1); rows below keep their input value.
+      const int w0 = f == 1 ? 1 : lo - 1;
+      double2* out = ring + ((step - 1) & 1) * tsz;   // the slot of the last step
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int j = j0 + r;
+        if (j < n) out[slot<R>(j, w)] = cr[r];
+      }
+      __syncthreads();
+      const double2* own = f < 3 ? a.cu_in[f] : a.cth_in[th];
+      store_tile<R>(out, f < 3 ? a.cu_out[f] : a.cth_out[th], ps, q0, nvalid, 0, n - 1, tid, own, w0);
+      // publish a velocity field's completion to its group's projection: every
+      // thread's stores are ordered before the count (the next task's second
+      // tile also goes to this slot only after the barrier)
+      __threadfence();
+      __syncthreads();
+      if (f < 3 && tid == 0) atomicAdd(A.sched + SCHED_DONE + cur.g, 1);
+      pre = nxt.kind == 0;
+      cur = nxt;
+    } else {
+      const int g = cur.g;
+      const int q0 = g * FS_COLS;
+      const int nvalid = min(FS_COLS, a.ncol - q0);
+      const int q = min(q0 + w, a.ncol - 1);
+      const int m = q / a.nk2, kq = q % a.nk2;
+      const bool m00 = (q0 + w == 0);
+      const double kxm = a.kx[m], kzq = a.kz[kq];
+      // wait (bounded) until the three velocity solves of this group are done
+      if (tid == 0) {
+        int ok = 1;
+        long long it = 0;
+        while (ld_acquire(A.sched + SCHED_DONE + g) < A.need) {
+          if (*(volatile int*)(A.sched + SCHED_STATUS) != 0 || ++it > A.max_spins) {
+            ok = 0;
+            atomicExch(A.sched + SCHED_STATUS, 1);
+            break;
+          }
+          __nanosleep(100);
+        }
+        __threadfence();
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (!s_ok) {   // timed out: this group is left as it is
+        cur = claim();
+        pre = false;
+        continue;
+      }
+      load_tile<R, 16>(ring + (step & 1) * tsz, src[0], ps, q0, nvalid, n, tid);
+      Task nxt{2, 0, 0};
+      double2 d[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) d[r] = z2;
+      double2 phm = z2;
+      for (int k = 0; k < 7; ++k, ++step) {
+        double2* nslot = ring + ((step + 1) & 1) * tsz;
+        if (k + 1 < 7) load_tile<R, 16>(nslot, src[k + 1], ps, q0, nvalid, n, tid);
+        else {
+          nxt = claim();
+          if (nxt.kind == 0) {
+            const int qn = nxt.g * FS_COLS;
+            const FTile first = a.nl64[nxt.f] ? FTile{a.nl64[nxt.f], FT_NL, 0, 0.0}
+                                              : FTile{a.nl32[nxt.f], FT_NL, 1, 0.0};
+            load_ftile<R>(nslot, &first, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
+          } else {
+            load_tile<R, 16>(nslot, nullptr, ps, q0, nvalid, n, tid);
+          }
+        }
+        wait_groups<1>();
+        __syncthreads();
+        double2* T = ring + (step & 1) * tsz;
+        if (k < 3) {
+          // divergence ik.u1 + ik.u3 + (u2(j+1) - u2(j))/dyf(j), rows 1..Ny,
+          // in the order the solves of the fused step accumulated it
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= 1 && j <= nyp) {
+              if (k == 0) d[r] = d[r] + mul_ik(kxm, T[slot<R>(j, w)]);
+              else if (k == 1) d[r] = d[r] + mul_ik(kzq, T[slot<R>(j, w)]);
+              else d[r] = d[r] + __ldg(met + MET_IDYF * n + j) * (T[slot<R>(j + 1, w)] - T[slot<R>(j, w)]);
+            }
+          }
+          if (k == 2) {
+            // Poisson rows: interior 1/(dy dyf) terms, Neumann walls, phi(1) = 0
+            // for the (0,0) mode
+            double al[R], cm[R];
+            const double k2n = -kxm * kxm - kzq * kzq;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int j = j0 + r;
+              double am = 0.0, cc = 0.0;
+              if (j >= 1 && j <= nyp) { am = __ldg(met + MET_PA * n + j); cc = __ldg(met + MET_PC * n + j); }
+              if (j == 1) { am = 0; cc = m00 ? 0.0 : -1.0; d[r] = z2; }
+              if (j == nyp) { am = 1; cc = 0; d[r] = z2; }
+              al[r] = am;
+              cm[r] = cc;
+            }
+            csolve2::warp_tridiag_b<R>([&](int r) -> double& { return al[r]; }, [&](int r) -> double {
+              const int j = j0 + r;
+              return (j == 1) ? 1.0 : (j == nyp ? -1.0 : ((j > 1 && j < nyp) ? k2n + __ldg(met + MET_PB0 * n + j) : 1.0));
+            }, [&](int r) -> double& { return cm[r]; }, d, lane);
+            phm = shfl_up2(d[R - 1], 1);   // phi of the row below the lane's first
+          }
+        } else if (k < 6) {
+          const int comp = k == 3 ? 0 : (k == 4 ? 2 : 1);
+          if (a.keep[0]) {
+            store_tile<R>(T, a.keep[comp], ps, q0, nvalid, 1, nyp, tid);
+            __syncthreads();
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (comp != 1 && j >= 1 && j <= nyp) {
+              double2& u = T[slot<R>(j, w)];
+              u = u - mul_ik(comp == 0 ? kxm : kzq, d[r]);
+            }
+            if (comp == 1 && j >= 2 && j <= nyp) {
+              double2& u = T[slot<R>(j, w)];
+              u = u - __ldg(met + MET_IDY * n + j) * (d[r] - (r == 0 ? phm : d[r - 1]));
+            }
+          }
+          __syncthreads();
+          store_tile<R>(T, cu[comp], ps, q0, nvalid, comp == 1 ? 2 : 1, nyp, tid);
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int j = j0 + r;
+            if (j >= a.jstart && j <= a.jend) {
+              double2& p = T[slot<R>(j, w)];
+              p = p + ih * d[r];
+            }
+          }
+          __syncthreads();
+          store_tile<R>(T, a.cp_out, ps, q0, nvalid, 0, n - 1, tid);
+        }
+        __syncthreads();
+      }
+      pre = nxt.kind == 0;
+      cur = nxt;
+    }
+  }
+  wait_groups<0>();
 }

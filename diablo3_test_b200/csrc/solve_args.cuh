@@ -95,3 +95,8 @@ struct Solve2Args {
   int nstep;
   TileStep steps[T2_MAXSTEPS];
 };
+
+// Columns (one warp each) per block of the field-split column step
+// (kernels_field.cuh); the host sizes the step's scheduler by it.
+#define FS_COLS 8
+#define FS_THREADS (32 * FS_COLS)

@@ -469,9 +469,8 @@ int substep(diablo_ctx* ctx, int rk) {
   a.store_cf = rk < 3 ? 1 : 0;
   const bool cfl = courant_due(ctx, rk);
   if (cfl && (rc = ensure_cfl(ctx))) return rc;
-  if (tiled && ctx->use_general_solver == 0) {
-    // default: one warp per (field, column), then one per column for the
-    // projection (kernels_field.cuh)
+  if (tiled && (ctx->use_general_solver == 0 || ctx->use_general_solver >= 3)) {
+    // default: the field-split column step (kernels_field.cuh)
     FieldArgs F;
     memset(&F, 0, sizeof(F));
     F.s = a;
@@ -484,13 +483,29 @@ int substep(diablo_ctx* ctx, int rk) {
     F.nf = ctx->nf;
     F.mean_split = mean_split ? 1 : 0;
     F.prof = ctx->d_prof;
-    {
+    // Two launches (field solves, then projections) by default.  The single
+    // launch (k_column_step: both, with a bounded wait per column group) is
+    // opt-in: it measured slower at 256 x 257 x 256 (0.71 against 0.59 ms
+    // per substep, mixed) and for the 64 x 97 x 64 adjoint case (13.9 against
+    // 12.5 ms for 50 steps), and equal on the 48-member ensemble.
+    if (ctx->use_general_solver == 3) {
+      const int resident = column_step_resident(ctx->nyp2);
+      F.sched = ctx->d_sched;
+      F.need = 3 + ctx->wait_withhold;
+      F.max_spins = ctx->wait_spins;
+      F.lag = std::max(1, resident / ctx->nf);
+      CK(cudaMemsetAsync(ctx->d_sched + 1, 0, (ctx->sched_ints - 1) * sizeof(int), ctx->stream));
       Prof pr(ctx, K_SOLVE);
-      if ((rc = launch_field_solve(F, ctx->stream))) return rc;
-    }
-    {
-      Prof pr(ctx, K_PROJ);
-      if ((rc = launch_project_cols(F, ctx->stream))) return rc;
+      if ((rc = launch_column_step(F, ctx->stream))) return rc;
+    } else {
+      {
+        Prof pr(ctx, K_SOLVE);
+        if ((rc = launch_field_solve(F, ctx->stream))) return rc;
+      }
+      {
+        Prof pr(ctx, K_PROJ);
+        if ((rc = launch_project_cols(F, ctx->stream))) return rc;
+      }
     }
     CK(cudaGetLastError());
     ctx->cur = nx_;

@@ -212,6 +212,13 @@ module diablo_gpu
       type(c_ptr), value :: ctx
       integer(c_int) :: diablo_check_finite
     end function diablo_check_finite
+    function diablo_set_wait_bound(ctx, max_spins, withheld_arrivals) bind(C, name="diablo_set_wait_bound")
+      import :: c_ptr, c_int, c_long_long
+      type(c_ptr), value :: ctx
+      integer(c_long_long), value :: max_spins
+      integer(c_int), value :: withheld_arrivals
+      integer(c_int) :: diablo_set_wait_bound
+    end function diablo_set_wait_bound
 
     ! ---- tracing and status text
     function diablo_kernel_launches(ctx) bind(C, name="diablo_kernel_launches")

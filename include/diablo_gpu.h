@@ -48,7 +48,7 @@ enum diablo_status {
   DIABLO_ERR_SIZE = -2,         /* grid size the kernels do not support */
   DIABLO_ERR_CUDA = -3,         /* a CUDA runtime call failed */
   DIABLO_ERR_NONFINITE = -4,    /* NaN/Inf found in the state */
-  DIABLO_ERR_TIMEOUT = -5,      /* a bounded device wait gave up */
+  DIABLO_ERR_TIMEOUT = -5,      /* a bounded device wait gave up (diablo_set_wait_bound) */
   DIABLO_ERR_UNSUPPORTED = -6,  /* option not implemented on the device */
   DIABLO_ERR_STATE = -7,        /* uploaded state violates the layout contract */
   DIABLO_ERR_NOMEM = -8         /* device allocation failed */
@@ -131,7 +131,9 @@ int diablo_fft_xz_to_physical(diablo_ctx* ctx, double* vv, double* v);
 
 /* One RK substep, rk_step in {1,2,3} (for/channel.f90:10-917). */
 int diablo_rk_substep(diablo_ctx* ctx, int rk_step);
-/* nsteps full steps: 3 substeps each, time += delta_t (for/diablo.f90:98-108). */
+/* nsteps full steps: 3 substeps each, time += delta_t (for/diablo.f90:98-108).
+ * Returns when the steps have finished on the device (it reads the column
+ * step's wait status, see diablo_set_wait_bound). */
 int diablo_step(diablo_ctx* ctx, int nsteps);
 /* Wall values, projection, optional initial pressure (for/advance.f90:17-44). */
 int diablo_pre_first_step(diablo_ctx* ctx, int compute_pressure);
@@ -203,6 +205,19 @@ int diablo_synchronize(diablo_ctx* ctx);
 /* DIABLO_ERR_NONFINITE if any significant Fourier entry of the state is NaN
  * or Inf, 0 otherwise. */
 int diablo_check_finite(diablo_ctx* ctx);
+/* The column step can run as one persistent kernel (opt-in: environment
+ * variable DIABLO_GENERAL_SOLVER=3 when the context is created; the default
+ * two launches measured faster) in which each column group's projection
+ * waits on a device counter until the group's three velocity solves are
+ * done.  That wait always ends (it only waits on work already running), and
+ * it is also bounded: after max_spins polls (100 ns apart; default 2^24,
+ * about a second) the kernel records a timeout, leaves the group unprojected
+ * and returns, and diablo_step, diablo_rk_substep and diablo_synchronize
+ * return DIABLO_ERR_TIMEOUT (reading the record clears it; the state is then
+ * invalid).  withheld_arrivals > 0 makes every projection wait for that many
+ * more arrivals than will come: failure injection from the host, to test
+ * that path.  No reference counterpart. */
+int diablo_set_wait_bound(diablo_ctx* ctx, long long max_spins, int withheld_arrivals);
 /* number of kernels this context has launched since creation */
 long long diablo_kernel_launches(const diablo_ctx* ctx);
 
