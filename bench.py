@@ -675,8 +675,12 @@ def run_ours(args):
     # the mixed step as a whole: algorithmic bytes of every timed kernel launch
     # per step over the step's own time
     mixed_bytes = sum(v["launches"] * v["alg_bytes"] for v in per_kernel.values()) / args.steps
+    # The 4-pass model counts only state arrays, which are FP64 in both
+    # precisions here (mixed precision keeps its FP32 arrays inside the
+    # transforms), so the model's bytes per point-step are the same for both.
     step_roof = {"model_bytes_per_point_step_fp64": alg64,
                  "fp64_frac": alg64 * pts / (ms_fp64 / args.steps * 1e-3) / 1e9 / peak,
+                 "mixed_model_frac": alg64 * pts / (ms_mixed / args.steps * 1e-3) / 1e9 / peak,
                  "mixed_alg_bytes_per_step": mixed_bytes,
                  "mixed_achieved_gbs": mixed_bytes / (ms_mixed / args.steps * 1e-3) / 1e9,
                  "mixed_frac": mixed_bytes / (ms_mixed / args.steps * 1e-3) / 1e9 / peak}
