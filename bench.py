@@ -225,6 +225,24 @@ def accuracy_report(sm, sd, p, gy):
     return out
 
 
+def max_over_ranks(vals, torch, dist=None, device="cuda"):
+    """Element-wise maximum of per-rank timings over every rank (identity
+    without a process group).  `device` is where the reduction tensor lives:
+    "cuda" for NCCL, "cpu" for gloo."""
+    if dist is None:
+        return [float(v) for v in vals]
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def aggregate_rate(points_per_step, world, steps, ms):
+    """Whole-job Mpoint-steps/s: every rank advanced its own replica of
+    `points_per_step` points `steps` times in `ms` milliseconds (the maximum
+    over ranks)."""
+    return points_per_step * world * steps / (ms * 1e-3) / 1e6
+
+
 def timed_steps(ch, torch, stream, k, dist=None):
     """K steps between barriers, CUDA events on the context's stream."""
     ch.synchronize()
@@ -491,10 +509,13 @@ def stats_bench(ch, p, peak, reps=5):
             "note": "x-homogeneous save_stats_chan with compute_BPE and the y* binning"}
 
 
-def e2e_round_trip(ch, torch, k):
+def e2e_round_trip(ch, torch, k, stream, dist=None, world=1):
     """End to end through the C ABI with pinned host buffers: each step
     uploads the state (u1, u2, u3, p, scalars) from the host in the reference
-    layout, advances one step and downloads the state again."""
+    layout, advances one step and downloads the state again.  Every copy runs
+    on the context's stream, so CUDA events on that stream bracket the copies
+    and the steps; under torchrun every rank runs its replica between barriers
+    and the time is the maximum over ranks."""
     from diablo3_test_b200 import _lib
     p = ch.params
     ids = [_lib.U1, _lib.U2, _lib.U3, _lib.P] + [_lib.TH + n for n in range(p.n_th)]
@@ -504,19 +525,30 @@ def e2e_round_trip(ch, torch, k):
         ch.download(fid, out=b)
     ch.synchronize()
     box = (p.ny + 2) * (2 * (p.nz // 3) + 1) * (p.nx // 2) * 16
-    t0 = time.perf_counter()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
     for _ in range(k):
         for b, fid in zip(bufs, ids):
             ch.upload(fid, b)
         ch.step(1)
         for b, fid in zip(bufs, ids):
             ch.download(fid, out=b)
+    e1.record(stream)
+    e1.synchronize()
     ch.synchronize()
-    dt = time.perf_counter() - t0
+    ms = max_over_ranks([e0.elapsed_time(e1)], torch, dist)[0]
+    if dist is not None:
+        dist.barrier()
     pts = p.nx * p.ny * p.nz
-    return {"value": pts * k / dt / 1e6, "unit": UNIT, "h2d_bytes_per_step": box * len(ids),
-            "d2h_bytes_per_step": box * len(ids), "ms_per_step": dt / k * 1e3,
-            "path": "diablo_upload_state x6 (host, pinned) + diablo_step + diablo_download_state x6"}
+    return {"value": aggregate_rate(pts, world, k, ms), "unit": UNIT,
+            "h2d_bytes_per_step": box * len(ids) * world,
+            "d2h_bytes_per_step": box * len(ids) * world, "ms_per_step": ms / k,
+            "path": "diablo_upload_state x6 (host, pinned) + diablo_step + diablo_download_state x6",
+            "timing": "CUDA events on the context's stream, max over ranks"}
 
 
 def profile_other(args, torch):
@@ -632,10 +664,7 @@ def run_ours(args):
     ktimes64 = chd.kernel_times()
     chd.set_profiling(False)
     clocks = sampler.stop()
-    if dist is not None:
-        t = torch.tensor([ms_mixed, ms_fp64], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_mixed, ms_fp64 = float(t[0]), float(t[1])
+    ms_mixed, ms_fp64 = max_over_ranks([ms_mixed, ms_fp64], torch, dist)
     # mixed vs FP64 after the same W+K steps from the same state
     sm, sd = state_sig(chm), state_sig(chd)
     err = {k: float(np.linalg.norm(sm[k] - sd[k]) / np.linalg.norm(sd[k])) for k in sm}
@@ -647,6 +676,9 @@ def run_ours(args):
         chd.step(args.acc_steps - done)
         acc = accuracy_report(state_sig(chm, True), state_sig(chd, True), p, gy)
         acc["steps"] = args.acc_steps
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)), stream, dist, world)
     if rank != 0:
         chm.close()
         chd.close()
@@ -670,8 +702,8 @@ def run_ours(args):
                 "traffic_source": traffic_src}
     # whole-step roofline against the 3*(8NF+9)*s bytes-per-point-step model
     alg64 = 3 * (8 * nf + 9) * 8
-    value = pts * world * args.steps / (ms_mixed * 1e-3) / 1e6
-    v64 = pts * world * args.steps / (ms_fp64 * 1e-3) / 1e6
+    value = aggregate_rate(pts, world, args.steps, ms_mixed)
+    v64 = aggregate_rate(pts, world, args.steps, ms_fp64)
     # the mixed step as a whole: algorithmic bytes of every timed kernel launch
     # per step over the step's own time
     mixed_bytes = sum(v["launches"] * v["alg_bytes"] for v in per_kernel.values()) / args.steps
@@ -706,8 +738,8 @@ def run_ours(args):
         "tiles": tiles,
         "clocks": clocks,
     }
-    if not args.no_e2e:
-        out["e2e"] = e2e_round_trip(chm, torch, max(2, min(args.steps, 5)))
+    if e2e is not None:
+        out["e2e"] = e2e
     out["stats"] = stats_bench(chm, p, peak)
     chm.close()
     chd.close()

@@ -385,6 +385,16 @@ DI void fill_prod(typename CT<T>::C (&v)[N1], const T* x, const T* y, size_t off
   for (int n1 = 0; n1 < N1; ++n1) v[n1] = CT<T>::mk(px[n1].a * py[n1].a, px[n1].b * py[n1].b);
 }
 
+// x(j)^2 (u1 u1 and u3 u3): one load per element
+template <typename T, int N1, int N2>
+DI void fill_sq(typename CT<T>::C (&v)[N1], const T* x, size_t off, int t) {
+  Pair<T> px[N1];
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) px[n1] = ld2(x + off + 2 * (n1 * N2 + t));
+#pragma unroll
+  for (int n1 = 0; n1 < N1; ++n1) v[n1] = CT<T>::mk(px[n1].a * px[n1].a, px[n1].b * px[n1].b);
+}
+
 // (uf(j+1)u2(j+1) + uf(j)u2(j+1) - uf(j)u2(j) - uf(j-1)u2(j)) / (2 dyf(j))
 template <typename T, int N1, int N2>
 DI void fill_flux(typename CT<T>::C (&v)[N1], const T* uf, const T* u2, size_t off, size_t ps,
@@ -449,24 +459,53 @@ DI void nl_fill(typename CT<T>::C (&v)[N1], const XFwdArgs<T>& a, int f, int q, 
     fill_flux<T, N1, N2>(v, own, u2, off, ps, (T)(2.0 * a.gm.dyf[j]), t);
   } else if (q == 0) {
     // f=0: u3*u1; f=2: u3*u3; scalar: th*u3
-    fill_prod<T, N1, N2>(v, f == 0 ? u3 : own, f == 0 ? u1 : u3, off, t);
+    if (f == 2) fill_sq<T, N1, N2>(v, u3, off, t);
+    else fill_prod<T, N1, N2>(v, f == 0 ? u3 : own, f == 0 ? u1 : u3, off, t);
   } else {
     // f=0: u1*u1; f=2: u3*u1; scalar: th*u1
-    fill_prod<T, N1, N2>(v, own, u1, off, t);
+    if (f == 0) fill_sq<T, N1, N2>(v, u1, off, t);
+    else fill_prod<T, N1, N2>(v, own, u1, off, t);
   }
 }
 
-// Shared-memory bytes of k_xr2c for a given configuration.
+// Whether k_xr2c finishes the real-to-complex split in registers.  The split
+// needs Z[m] and Z[M - m] together.  With N1 = 2 N2 a thread can own step-2
+// rows k1 and N1 - k1 (thread 0: rows 0 and N1/2), and row k1 holds
+// Z[k1 + N1 k2] while row N1 - k1 holds Z[M - k1 - N1 k2] at k2' = N2-1-k2:
+// every pair (m, M - m) then lies in one thread, and the spectrum needs no
+// natural-order copy in shared memory.  At 256 x 257 x 256 (FP32 products,
+// 16 rows per block) this and the accumulator pitch below took the launch
+// from 0.615 to 0.494 ms; with a separate code path for thread 0 (run
+// serially beside the other threads' in every warp) it had measured 0.689.
+#ifndef XR2C_PAIRED
+#define XR2C_PAIRED 1
+#endif
+#ifndef XR2C_PAD_OP
+#define XR2C_PAD_OP 1
+#endif
+
+// Shared-memory layout of k_xr2c for a given configuration.
 template <typename T, int N1, int N2, int KT, bool NL = true>
 struct XFwdSmem {
   typedef typename CT<T>::C C;
   static constexpr int M = N1 * N2;
   static constexpr int NKX1 = (2 * M) / 3 + 1;   // upper bound of Nkx+1
-  // per row one four-step tile (also used for the natural-order spectrum,
-  // which needs M+1 entries) + the accumulated B output of the NL form (the
-  // A output goes straight to global memory)
-  static constexpr int ROWC = dfft::SmemSize<N1, N2>::v > M + 1 ? dfft::SmemSize<N1, N2>::v : M + 1;
-  static constexpr int bytes = (KT * ROWC + (NL ? NKX1 * (KT + 1) : 0)) * (int)sizeof(C);
+  static constexpr bool PAIRED = XR2C_PAIRED && N1 == 2 * N2;
+  // per row one four-step tile (without the register split also the
+  // natural-order spectrum, which needs M+1 entries)
+  static constexpr int ROWC = (PAIRED || dfft::SmemSize<N1, N2>::v > M + 1) ? dfft::SmemSize<N1, N2>::v : M + 1;
+  // Pitch of the accumulated B output [m][row] of the NL form (the A output
+  // goes straight to global memory).  Shared memory serves 128 bytes per
+  // wavefront: W = 128 / sizeof(C) threads, that is G = W / N2 rows of N2
+  // threads with consecutive modes m.  Entry (m, row) sits at m OP + row, so
+  // the W threads hit distinct banks when OP / G is odd; OP is the smallest
+  // such pitch >= KT (18 against KT + 1 = 17 for the FP32 products: 0.494
+  // against 0.501 ms per launch).
+  static constexpr int W = 128 / (int)sizeof(C);
+  static constexpr int G = W / N2 > 1 ? W / N2 : 1;
+  static constexpr int OPG = (KT + G - 1) / G;
+  static constexpr int OP = !XR2C_PAD_OP ? KT + 1 : G * (OPG % 2 ? OPG : OPG + 1);
+  static constexpr int bytes = (KT * ROWC + (NL ? NKX1 * OP : 0)) * (int)sizeof(C);
 };
 
 // Blocks per SM the FP32 products kernel's register cap is set for.  With the
@@ -478,16 +517,27 @@ struct XFwdSmem {
 #ifndef XR2C32_MIN_BLOCKS
 #define XR2C32_MIN_BLOCKS 6
 #endif
+// Whether k_xr2c separates the phases of one row's transform with a warp
+// barrier instead of a block barrier.  The N2 threads of a row share a warp
+// when 32 % N2 == 0, and every shared-memory entry a phase reads was written
+// by the same row's threads; only the B output's final store reads other
+// rows' entries.  At 256 x 257 x 256 (FP32, before the register split) the
+// warp barrier measured 5.057 against 5.101 ms per step.
+#ifndef XR2C_WARP_SYNC
+#define XR2C_WARP_SYNC 1
+#endif
 
 template <typename T, int N1, int N2, int KT, bool NL>
 __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BLOCKS : 1) k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
+  typedef XFwdSmem<T, N1, N2, KT, NL> L;
   constexpr int M = N1 * N2;
-  constexpr int ROWC = XFwdSmem<T, N1, N2, KT>::ROWC;
-  constexpr int NKX1 = XFwdSmem<T, N1, N2, KT>::NKX1;
+  constexpr int ROWC = L::ROWC;
+  constexpr int NKX1 = L::NKX1;
   constexpr int NS = (NKX1 + N2 - 1) / N2;  // output slots per thread
   constexpr int NR = (N1 + N2 - 1) / N2;    // step-2 rows per thread
-  constexpr int OP = KT + 1;
+  constexpr int OP = L::OP;
+  constexpr bool PAIRED = L::PAIRED;
   extern __shared__ __align__(16) unsigned char xr2c_smem[];
   C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][ROWC] four-step tile / spectrum
   C* acc = smb + KT * ROWC;                            // [NKX1][OP] output B (NL)
@@ -505,6 +555,28 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BL
   C* sm = smb + r * ROWC;
   C* zs = sm;  // the natural-order spectrum replaces the tile after step 2
   constexpr int NQ = NL ? 3 : 1;
+  constexpr bool WROW = XR2C_WARP_SYNC && 32 % N2 == 0;
+  auto rowsync = [] { if constexpr (WROW) __syncwarp(); else __syncthreads(); };
+  // output X[m] of transform q: A straight to global (a warp writes 32-byte
+  // runs along k of 32 / N2 rows for each of its N2 modes); Bx and B0 into the
+  // accumulator, each (m, row) entry always by the same thread
+  auto put = [&](int q, int m, C x) {
+    if (!NL || q == 0) { if (k0 + r < nz) dstA[(size_t)m * nz + k0 + r] = x; }
+    else if (q == 1) acc[m * OP + r] = mul_ik((T)a.kx[m], x);
+    else acc[m * OP + r] = acc[m * OP + r] + x;
+  };
+  // the pair (m, M - m) from zm = Z[m], zp = Z[M - m]:
+  //   X[m] = sc (e - i w o),  X[M - m] = sc conj(e + i w o)
+  // with e = (zm + conj zp)/2, o = (zm - conj zp)/2, w = exp(-2 pi i m / Nx)
+  // (w(M - m) = -conj w(m) gives the second form)
+  auto put_pair = [&](int q, int m, C zm, C zp) {
+    const C zc = conj(zp);
+    const C e = (T)0.5 * (zm + zc);
+    const C o = (T)0.5 * (zm - zc);
+    const C wo = cmul(a.twX[m], o);
+    if (m < nkx1) put(q, m, sc * (e - mul_i(wo)));
+    if (2 * m != M && M - m < nkx1) put(q, M - m, sc * conj(e + mul_i(wo)));
+  };
 #pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
     C v[N1];
@@ -516,42 +588,72 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BL
         v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * (n1 * N2 + t));
     }
     dfft::step1<N1, N2, -1>(v, t, a.twM, sm);
-    __syncthreads();
-    C u[NR][N2];
+    rowsync();
+    if constexpr (PAIRED) {
+      // thread t owns rows t and N1 - t; thread 0 rows 0 and N1/2
+      C ua[N2], ub[N2];
+      dfft::step2<N1, N2, -1>(ua, t, sm);
+      dfft::step2<N1, N2, -1>(ub, t == 0 ? N1 / 2 : N1 - t, sm);
+      rowsync();  // the tile is free for the next transform
+      // N2 pair slots per thread, the same code path in every thread (a
+      // separate path for thread 0 would run serially beside the others'):
+      //   t != 0:  Z[t + N1 k2] with Z[(N1 - t) + N1 (N2-1-k2)]
+      //   t == 0:  slots k2 < N2/2: row N1/2, Z[N1/2 + N1 k2] with
+      //            Z[N1/2 + N1 (N2-1-k2)]; slots k2 >= N2/2: row 0,
+      //            Z[N1 i] with Z[N1 (N2 - i)], i = k2 - N2/2 + 1 (i = N2/2
+      //            pairs Z[M/2] with itself)
+      // and X[0] = sc (Re Z[0] + Im Z[0]) from thread 0 besides.
+      const bool t0 = t == 0;
 #pragma unroll
-    for (int rr = 0; rr < NR; ++rr)
-      if (t + rr * N2 < N1) dfft::step2<N1, N2, -1>(u[rr], t + rr * N2, sm);
-    __syncthreads();
-#pragma unroll
-    for (int rr = 0; rr < NR; ++rr) {
-      const int k1 = t + rr * N2;
-      if (k1 < N1) {
-#pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) zs[k1 + N1 * k2] = u[rr][k2];
+      for (int k2 = 0; k2 < N2; ++k2) {
+        constexpr int H = N2 / 2;
+        const int i = k2 - H + 1;  // row-0 index of thread 0's upper slots
+        C zm, zp;
+        int m;
+        if (k2 < H) {
+          zm = t0 ? ub[k2] : ua[k2];
+          zp = ub[N2 - 1 - k2];
+          m = t0 ? N1 / 2 + N1 * k2 : t + N1 * k2;
+        } else {
+          zm = t0 ? ua[i < 0 ? 0 : i] : ua[k2];
+          zp = t0 ? ua[(N2 - i) % N2] : ub[N2 - 1 - k2];
+          m = t0 ? N1 * i : t + N1 * k2;
+        }
+        put_pair(q, m, zm, zp);
       }
-    }
-    if (t == 0) zs[M] = u[0][0];
-    __syncthreads();
+      if (t0) put(q, 0, CT<T>::mk(sc * (ua[0].x + ua[0].y), (T)0));
+    } else {
+      C u[NR][N2];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      int m = t + s * N2;
-      if (m < nkx1) {
-        C zm = zs[m], zc = conj(zs[M - m]);
-        C e = (T)0.5 * (zm + zc);
-        C o = (T)0.5 * (zm - zc);
-        C x = sc * (e - mul_i(cmul(a.twX[m], o)));
-        // each thread owns its (m, r) entries: no synchronisation needed
-        // A: straight to global (a warp writes 32-byte runs along k of
-        // 32 / N2 rows for each of its N2 modes)
-        if (!NL || q == 0) { if (k0 + r < nz) dstA[(size_t)m * nz + k0 + r] = x; }
-        else if (q == 1) acc[m * OP + r] = mul_ik((T)a.kx[m], x);
-        else acc[m * OP + r] = acc[m * OP + r] + x;
+      for (int rr = 0; rr < NR; ++rr)
+        if (t + rr * N2 < N1) dfft::step2<N1, N2, -1>(u[rr], t + rr * N2, sm);
+      rowsync();
+#pragma unroll
+      for (int rr = 0; rr < NR; ++rr) {
+        const int k1 = t + rr * N2;
+        if (k1 < N1) {
+#pragma unroll
+          for (int k2 = 0; k2 < N2; ++k2) zs[k1 + N1 * k2] = u[rr][k2];
+        }
       }
+      if (t == 0) zs[M] = u[0][0];
+      rowsync();
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        int m = t + s * N2;
+        if (m < nkx1) {
+          C zm = zs[m], zc = conj(zs[M - m]);
+          C e = (T)0.5 * (zm + zc);
+          C o = (T)0.5 * (zm - zc);
+          put(q, m, sc * (e - mul_i(cmul(a.twX[m], o))));
+        }
+      }
+      rowsync();
     }
-    __syncthreads();
   }
   // B stores run along k (KT consecutive rows per mode)
   if (NL) {
+    if constexpr (WROW) __syncthreads();
     C* dst = a.outB[f] + (size_t)j * nkx1 * nz;
     for (int idx = r * N2 + t; idx < nkx1 * KT; idx += N2 * KT) {
       int rr = idx % KT, m = idx / KT;
