@@ -1,15 +1,16 @@
 """torch.autograd.Function over libdiablo_gpu's step and its hand-written
 discrete adjoint (diablo_adjoint_record / diablo_adjoint_run).
 
-    u1, u2, u3, p = ChannelSteps.apply(channel, nsteps, every, u1, u2, u3, p)
+    u1, u2, u3, p, *th = ChannelSteps.apply(channel, nsteps, every, u1, u2, u3, p, *th)
 
 takes and returns the Fourier state in the reference layout (float64 CUDA
 tensors of shape (Ny+2, Nz+2, Nx+2), each complex coefficient stored as two
-reals, the layout of ``vv(0:Nxp, 0:Nz+1, 0:Nyp+1)``).  The forward advances
-`channel` by nsteps steps keeping checkpoints every `every` steps; backward
-recomputes each segment from its checkpoint and runs the adjoint substeps
-backwards (no autograd graph of the step is built).  Velocity-only DNS in
-FP64 (for/channel.f90:rk_chan_1 without scalars or LES).
+reals, the layout of ``vv(0:Nxp, 0:Nz+1, 0:Nyp+1)``), one tensor per scalar
+after p.  The forward advances `channel` by nsteps steps keeping checkpoints
+every `every` steps; backward recomputes each segment from its checkpoint and
+runs the adjoint substeps backwards (no autograd graph of the step is built).
+DNS in FP64 with velocities and scalars (for/channel.f90:rk_chan_1 without
+LES, 'Front' forcing or the scalar filter).
 """
 from __future__ import annotations
 
@@ -20,13 +21,16 @@ from . import _lib
 
 class ChannelSteps(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, channel, nsteps: int, every: int, u1, u2, u3, p):
-        for fid, t in ((_lib.U1, u1), (_lib.U2, u2), (_lib.U3, u3), (_lib.P, p)):
+    def forward(ctx, channel, nsteps: int, every: int, *state):
+        fids = [_lib.U1, _lib.U2, _lib.U3, _lib.P] + [_lib.TH + n for n in range(channel.params.n_th)]
+        if len(state) != len(fids):
+            raise ValueError(f"{len(fids)} state tensors: u1, u2, u3, p and one per scalar")
+        for fid, t in zip(fids, state):
             channel.upload(fid, t.detach().contiguous(), _lib.LAYOUT_FOURIER)
         channel.adjoint_record(nsteps, every)
         outs = []
-        for fid in (_lib.U1, _lib.U2, _lib.U3, _lib.P):
-            o = torch.zeros_like(u1)
+        for fid in fids:
+            o = torch.zeros_like(state[0])
             channel.download(fid, _lib.LAYOUT_FOURIER, out=o)
             outs.append(o)
         channel.synchronize()
@@ -34,9 +38,9 @@ class ChannelSteps(torch.autograd.Function):
         return tuple(outs)
 
     @staticmethod
-    def backward(ctx, g1, g2, g3, gp):
-        lam = [g.detach().clone().contiguous() if g is not None else None for g in (g1, g2, g3, gp)]
+    def backward(ctx, *grads):
+        lam = [g.detach().clone().contiguous() if g is not None else None for g in grads]
         ref = next(t for t in lam if t is not None)
         lam = [t if t is not None else torch.zeros_like(ref) for t in lam]
         ctx.channel.adjoint_run(lam)
-        return None, None, None, lam[0], lam[1], lam[2], lam[3]
+        return (None, None, None) + tuple(lam)

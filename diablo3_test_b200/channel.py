@@ -121,16 +121,17 @@ class Channel:
 
     def adjoint_record(self, nsteps: int, every: int):
         """Advance nsteps steps, keeping checkpoints every `every` steps for
-        adjoint_run (velocity-only DNS in FP64)."""
+        adjoint_run (DNS with velocities and scalars in FP64)."""
         _lib.check(self.lib.diablo_adjoint_record(self.ctx, nsteps, every), "adjoint_record")
 
     def adjoint_run(self, lam):
-        """lam: four reference-layout Fourier arrays (numpy or torch) holding
-        dJ/d(u1, u2, u3, p) of the recorded final state; overwritten with
-        dJ/d of the recorded initial state."""
-        if len(lam) != 4:
-            raise ValueError("four arrays: u1, u2, u3, p")
-        arr = (ctypes.c_void_p * 4)(*[_ptr(a) for a in lam])
+        """lam: 4 + N_th reference-layout Fourier arrays (numpy or torch)
+        holding dJ/d(u1, u2, u3, p, th_0, ..) of the recorded final state;
+        overwritten with dJ/d of the recorded initial state."""
+        ns = 4 + self.params.n_th
+        if len(lam) != ns:
+            raise ValueError(f"{ns} arrays: u1, u2, u3, p and one per scalar")
+        arr = (ctypes.c_void_p * ns)(*[_ptr(a) for a in lam])
         _lib.check(self.lib.diablo_adjoint_run(self.ctx, arr), "adjoint_run")
 
     def download_nu_t(self, out=None) -> np.ndarray:

@@ -63,7 +63,7 @@ struct diablo_ctx {
   double2 *tz64, *tm64, *tx64;
   float2 *tz32, *tm32, *tx32;
   // Fourier state, double buffered: [u1, u2, u3, p, th0..]
-  double2* st[2][3 + DIABLO_MAX_TH];
+  double2* st[2][4 + DIABLO_MAX_TH];
   double2* cf[2][3 + DIABLO_MAX_TH];
   int cur;      // index of the current state buffer
   int cf_cur;   // index of the buffer holding the last substep's cf
@@ -142,14 +142,17 @@ struct diablo_ctx {
     int ready, nsteps, every, nseg;
     int step_end, gen_end;
     double time_end;
-    std::vector<double2*> ckpt;       // (nseg + 1) x 4 fields (u1, u2, u3, p); the last is the final state
+    std::vector<double2*> ckpt;       // (nseg + 1) x (4 + nth) fields (u1, u2, u3, p, th..); the last is the final state
     std::vector<int> ckpt_step;
     std::vector<double> ckpt_time;
-    std::vector<double2*> sub;        // every x 3 substeps x 3 velocity inputs
-    double2 *lu[4], *ou[4], *lF[3], *oF[3], *lnl[3], *pf[8], *lf3[3];
+    std::vector<double2*> sub;        // every x 3 substeps x (3 + nth) inputs (u1, u2, u3, th..)
+    // lambdas of the state [u1, u2, u3, p, th..], of cf and NL [u1, u2, u3, th..],
+    // the product adjoints (8 + 3 nth) and the physical fields of the substep
+    double2 *lu[4 + DIABLO_MAX_TH], *ou[4 + DIABLO_MAX_TH], *lF[3 + DIABLO_MAX_TH], *oF[3 + DIABLO_MAX_TH];
+    double2 *lnl[3 + DIABLO_MAX_TH], *pf[8 + 3 * DIABLO_MAX_TH], *lf3[3 + DIABLO_MAX_TH];
     int work_ready;
-    double *pp[8], *up[3], *lp3[3];
-    double *d_cn, *d_rmask, *d_pa;    // [3 rk][3 field][3][n], [3][n], [3][n]
+    double *pp[8 + 3 * DIABLO_MAX_TH], *up[3 + DIABLO_MAX_TH], *lp3[3 + DIABLO_MAX_TH];
+    double *d_cn, *d_rmask, *d_pa;    // [3 rk][3 + nth field][3][n], [3 + nth][n], [3][n]
   } tape;
   struct Timed { int slot; cudaEvent_t a, b; };
   std::vector<Timed> timed;        // pending (recorded, not yet read)

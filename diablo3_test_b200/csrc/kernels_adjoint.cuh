@@ -1,4 +1,4 @@
-// Discrete adjoint of the velocity-only DNS substep (FP64).
+// Discrete adjoint of the DNS substep with velocities and scalars (FP64).
 //
 // Forward substep in Fourier-column form (for/channel.f90:29-917 with
 // rem_div_chan :946-1023), per (kx, kz) column, rows J = jstart..jend for
@@ -9,6 +9,11 @@
 //   u*  = A^-1 [r on the rows A takes it; wall-row constants]
 //   u_s = u* on rows >= w0, u on rows < w0
 //   phi = Lp^-1 div(u_s);  u' = u_s - grad phi;  p' = p + phi/h on J
+// and per scalar th (rows Jt = jstart_th..Ny, :156-249, :553-710):
+//   cf2 += grav_y I(th) (rows J2, not the (0,0) mode), cf1 += grav_x th,
+//   cf3 += grav_z th (rows J)
+//   cft = -nu/Pr k^2b th - dTHdX u1 - dTHdZ u3 - NL_th                 Jt
+//   th' = At^-1 [th + zeta h cft_prev + beta h cft + tc/Pr L th]        Jt
 // The adjoint takes lambda (the real gradient of the objective packed as a
 // complex number, dJ/dRe + i dJ/dIm) of (u', p', cf) back to (u, p, cf_prev)
 // and to the nonlinear terms; a complex factor a in y = a x gives
@@ -215,17 +220,140 @@ __global__ void __launch_bounds__(128) k_adj_column(const __grid_constant__ AdjC
   }
 }
 
+// Adjoint of one scalar's column work, after k_adj_column: lambda of the new
+// th and of this substep's cf_th become lambda of the old th (linear part),
+// of the previous cf_th and of NL_th; the buoyancy terms take lambda cf of
+// the velocities (k_adj_column's -onl) into lambda th, and the background
+// gradients add -dTHdX lambda cf_th to lambda u1 and -dTHdZ lambda cf_th to
+// lambda u3 (read-modify-write of k_adj_column's output, so scalars run one
+// launch after another).
+struct AdjScalarArgs {
+  const double2* lth;       // in: lambda of the new th
+  const double2* lF;        // in: lambda of this substep's cf_th (null: none)
+  const double2* vnl[3];    // in: lambda NL of u1, u2, u3 (= -lambda cf)
+  double2* oth;             // out: linear part of lambda of the old th
+  double2* oF;              // out: lambda of the previous substep's cf_th (null at rk 1)
+  double2* onl;             // out: lambda of NL_th (rows Jt; zero elsewhere)
+  double2* ou1;             // in/out: lambda u1 (k_adj_column's output)
+  double2* ou3;             // in/out: lambda u3
+  const double* cn;         // [A, B, C][n] of the scalar's CN system
+  const double* rmask;      // [n]
+  const double* kx;
+  const double* kz;
+  const double* dy;
+  const double* dyf;
+  double t3, t5, tc, nu_pr, beta, gx, gy, gz, dthdx, dthdz;
+  int n, nyp, nkx1, nk2, kp, ncol, jst, jet;
+};
+
+template <int R>
+__global__ void __launch_bounds__(128) k_adj_scalar(const __grid_constant__ AdjScalarArgs a) {
+  using namespace csolve;
+  const int lane = threadIdx.x & 31;
+  const int col = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (col >= a.ncol) return;
+  const int m = col / a.nk2, kq = col % a.nk2;
+  const size_t ps = (size_t)a.nkx1 * a.kp;
+  const size_t c0 = (size_t)m * a.kp + kq;
+  const int n = a.n;
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double k2s = kxm * kxm + kzq * kzq;
+  const double kk = a.beta == 1.0 ? k2s : pow(k2s, a.beta);
+  const bool m00 = m == 0 && kq == 0;
+  const int j0 = lane * R;
+  const double2 z = make_double2(0.0, 0.0);
+  auto ld = [&](const double2* f, int j) -> double2 { return (j >= 0 && j < n) ? f[(size_t)j * ps + c0] : z; };
+  auto st = [&](double2* f, int j, double2 v) { if (j < n) f[(size_t)j * ps + c0] = v; };
+  auto up1 = [&](const double2 (&v)[R], int r) -> double2 {
+    double2 nx = shfl_down2(v[0], 1);
+    if (lane == 31) nx = z;
+    return r + 1 < R ? v[r + 1] : nx;
+  };
+  auto dn1 = [&](const double2 (&v)[R], int r) -> double2 {
+    double2 pv = shfl_up2(v[R - 1], 1);
+    if (lane == 0) pv = z;
+    return r > 0 ? v[r - 1] : pv;
+  };
+  auto DY = [&](int j) { return (j >= 1 && j < n) ? a.dy[j] : 1.0; };
+  auto DYF = [&](int j) { return (j >= 0 && j < n) ? a.dyf[j] : 1.0; };
+  double2 LS[R], OU[R];
+  const int w0 = a.jst - 1;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 + r;
+    LS[r] = ld(a.lth, j);
+    OU[r] = z;
+    if (j < w0) { OU[r] = LS[r]; LS[r] = z; }
+  }
+  // At^-T lambda th*
+  {
+    const double* cn = a.cn;
+    double at[R], bt[R], ct[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = j0 + r;
+      at[r] = (j - 1 >= 0 && j - 1 < n) ? cn[2 * n + j - 1] : 0.0;
+      bt[r] = j < n ? cn[n + j] : 1.0;
+      ct[r] = j + 1 < n ? cn[j + 1] : 0.0;
+    }
+    warp_tridiag<R>(at, bt, ct, LS, lane);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 + r;
+    if (!(j < n && a.rmask[j] != 0.0)) LS[r] = z;   // now lambda r (= lambda cr)
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = j0 + r;
+    const double2 lm = dn1(LS, r), lp = up1(LS, r);
+    const double alm = 1.0 / (DY(j) * DYF(j - 1)), al = 1.0 / (DY(j + 1) * DYF(j));
+    const double ga = 1.0 / (DY(j) * DYF(j)), gap = 1.0 / (DY(j + 1) * DYF(j + 1));
+    double2 o = OU[r] + LS[r] - (a.tc * (al + ga)) * LS[r];
+    if (j >= 1) o = o + (a.tc * alm) * lm;
+    if (j + 1 < n) o = o + (a.tc * gap) * lp;
+    if (a.oF) st(a.oF, j, a.t3 * LS[r]);
+    double2 lcf = z;
+    if (j >= a.jst && j <= a.jet) {
+      lcf = a.t5 * LS[r];
+      if (a.lF) lcf = lcf + ld(a.lF, j);
+    }
+    st(a.onl, j, -1.0 * lcf);
+    o = o - (a.nu_pr * kk) * lcf;
+    // cf_th -= dTHdX u1 + dTHdZ u3
+    if (j < n && (a.dthdx != 0.0 || a.dthdz != 0.0)) {
+      const size_t q = (size_t)j * ps + c0;
+      if (a.dthdx != 0.0) a.ou1[q] = a.ou1[q] - a.dthdx * lcf;
+      if (a.dthdz != 0.0) a.ou3[q] = a.ou3[q] - a.dthdz * lcf;
+    }
+    // buoyancy: lambda cf_f = -lambda NL_f, zero off each equation's rows
+    o = o - a.gx * ld(a.vnl[0], j) - a.gz * ld(a.vnl[2], j);
+    if (!m00 && a.gy != 0.0) {
+      // cf2(i) += gy (th(i) dyf(i-1) + th(i-1) dyf(i)) / (2 dy(i)), rows 2..Ny
+      const double2 b0 = ld(a.vnl[1], j), b1 = ld(a.vnl[1], j + 1);
+      if (j >= 2) o = o - (a.gy * DYF(j - 1) / (2.0 * DY(j))) * b0;
+      if (j + 1 >= 2 && j + 1 < n) o = o - (a.gy * DYF(j + 1) / (2.0 * DY(j + 1))) * b1;
+    }
+    OU[r] = o;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) st(a.oth, j0 + r, OU[r]);
+}
+
 // lambda NL -> the eight physical-space product adjoints, in Fourier space,
 // scaled by the forward transform's transpose (1/(NxNz), halved for kx > 0):
 //   0 u1u3: -ikz l1 - ikx l3   1 u1u1: -ikx l1   2 u3u3: -ikz l3
 //   3 Y(u1,u2): l1   4 Y(u3,u2): l3   5 I(u1)u2: -ikx l2   6 I(u3)u2: -ikz l2   7 V(u2): l2
+// and per scalar s (NL_s = ikx F(th u1) + ikz F(th u3) + F(Y(th, u2))):
+//   8+3s th u1: -ikx ls   9+3s th u3: -ikz ls   10+3s Y(th,u2): ls
 struct AdjNlPrepArgs {
-  const double2* lnl[3];
-  double2* out[8];
+  const double2* lnl[3 + DIABLO_MAX_TH];
+  double2* out[8 + 3 * DIABLO_MAX_TH];
   const double* kx;
   const double* kz;
   double inv;       // 1/(Nx Nz)
   FGeom g;
+  int nth;
 };
 
 static __global__ void k_adj_nl_prep(const __grid_constant__ AdjNlPrepArgs a) {
@@ -246,22 +374,30 @@ static __global__ void k_adj_nl_prep(const __grid_constant__ AdjNlPrepArgs a) {
   a.out[5][idx] = w * mul_ik(-kxm, l2);
   a.out[6][idx] = w * mul_ik(-kzq, l2);
   a.out[7][idx] = w * l2;
+  for (int s = 0; s < a.nth; ++s) {
+    const double2 ls = a.lnl[3 + s][idx];
+    a.out[8 + 3 * s][idx] = w * mul_ik(-kxm, ls);
+    a.out[9 + 3 * s][idx] = w * mul_ik(-kzq, ls);
+    a.out[10 + 3 * s][idx] = w * ls;
+  }
 }
 
 // Product rule in physical space, gathered per point (planes 0..Ny+1): the
-// adjoints of u1, u2, u3 from the eight product adjoints P[0..7] (zero off
-// planes 1..Ny) and the forward velocities.
+// adjoints of u1, u2, u3 and of each scalar from the product adjoints P
+// (zero off planes 1..Ny) and the forward velocities and scalars.
 struct AdjNlPointArgs {
-  const double* P[8];
+  const double* P[8 + 3 * DIABLO_MAX_TH];
   const double* u1;
   const double* u2;
   const double* u3;
+  const double* th[DIABLO_MAX_TH];
   double* o1;
   double* o2;
   double* o3;
+  double* oth[DIABLO_MAX_TH];
   const double* dy;
   const double* dyf;
-  int nyp;
+  int nyp, nth;
   size_t ps;
 };
 
@@ -307,6 +443,17 @@ static __global__ void k_adj_nl_point(const __grid_constant__ AdjNlPointArgs a) 
   if (j >= 1 && j <= nyp) lv += 0.5 * (vp - U(a.u2, j - 1)) / a.dy[j] * P(7, j);
   if (j - 1 >= 1) lv += 0.5 * (U(a.u2, j - 1) + v) / a.dy[j - 1] * P(7, j - 1);
   if (j + 1 <= nyp) lv -= 0.5 * (v + vp) / a.dy[j + 1] * P(7, j + 1);
+  // scalars: th u1, th u3 and Y(th, u2), the same rules as u1 u3 and Y(u1, u2)
+  for (int s = 0; s < a.nth; ++s) {
+    const int q = 8 + 3 * s;
+    const double th = U(a.th[s], j);
+    double lt = u1 * P(q, j) + u3 * P(q + 1, j);
+    l1 += th * P(q, j);
+    l3 += th * P(q + 1, j);
+    lt += v * D(j - 1) * P(q + 2, j - 1) + (vp - v) * D(j) * P(q + 2, j) - vp * D(j + 1) * P(q + 2, j + 1);
+    if (j >= 1) lv += (th + U(a.th[s], j - 1)) * (D(j - 1) * P(q + 2, j - 1) - D(j) * P(q + 2, j));
+    a.oth[s][idx] = lt;
+  }
   a.o1[idx] = l1;
   a.o2[idx] = lv;
   a.o3[idx] = l3;
@@ -314,10 +461,11 @@ static __global__ void k_adj_nl_point(const __grid_constant__ AdjNlPointArgs a) 
 
 // ou[f] += w(m) Nx Nz * F(lambda u_f physical)  (the inverse transform's transpose)
 struct AdjAccArgs {
-  double2* ou[3];
-  const double2* add[3];
+  double2* ou[3 + DIABLO_MAX_TH];
+  const double2* add[3 + DIABLO_MAX_TH];
   double scale;     // Nx Nz
   FGeom g;
+  int nf;
 };
 
 static __global__ void k_adj_acc(const __grid_constant__ AdjAccArgs a) {
@@ -328,5 +476,5 @@ static __global__ void k_adj_acc(const __grid_constant__ AdjAccArgs a) {
   if (kq >= a.g.nk2) return;
   const int m = (idx / a.g.kp) % a.g.nkx1;
   const double w = a.scale * (m > 0 ? 2.0 : 1.0);
-  for (int f = 0; f < 3; ++f) a.ou[f][idx] = a.ou[f][idx] + w * a.add[f][idx];
+  for (int f = 0; f < a.nf; ++f) a.ou[f][idx] = a.ou[f][idx] + w * a.add[f][idx];
 }

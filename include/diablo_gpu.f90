@@ -259,8 +259,8 @@ module diablo_gpu
       integer(c_int) :: diablo_abi_version
     end function diablo_abi_version
 
-    ! ---- discrete adjoint; lam(1:4) hold the addresses of the four Fourier
-    ! arrays dJ/d(u1, u2, u3, p)
+    ! ---- discrete adjoint; lam(1:4+N_th) hold the addresses of the Fourier
+    ! arrays dJ/d(u1, u2, u3, p, th_1, ..)
     function diablo_adjoint_record(ctx, nsteps, every) bind(C, name="diablo_adjoint_record")
       import :: c_ptr, c_int
       type(c_ptr), value :: ctx
@@ -270,7 +270,7 @@ module diablo_gpu
     function diablo_adjoint_run(ctx, lam) bind(C, name="diablo_adjoint_run")
       import :: c_ptr, c_int
       type(c_ptr), value :: ctx
-      type(c_ptr), intent(in) :: lam(4)
+      type(c_ptr), intent(in) :: lam(*)
       integer(c_int) :: diablo_adjoint_run
     end function diablo_adjoint_run
 

@@ -263,12 +263,14 @@ int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, do
 
 /*
  * Discrete adjoint of diablo_step.  No reference counterpart: the reference
- * has no adjoint.  For velocity-only DNS contexts in FP64 (n_th = 0, no LES,
- * fixed delta_t); other contexts get DIABLO_ERR_UNSUPPORTED.
+ * has no adjoint.  For DNS contexts in FP64 with velocities and any number of
+ * scalars (buoyancy, background gradients, scalar transport), fixed delta_t;
+ * LES, the 'Front' forcing, the scalar filter and mixed precision get
+ * DIABLO_ERR_UNSUPPORTED.
  * diablo_adjoint_record advances nsteps steps exactly as diablo_step does and
- * keeps the state (u1, u2, u3, p) every `every` steps on the device.
- * diablo_adjoint_run takes lam[0..3] = dJ/d(u1, u2, u3, p) of the recorded
- * final state for any objective J and overwrites them with dJ/d of the state
+ * keeps the state (u1, u2, u3, p, th_0..) every `every` steps on the device.
+ * diablo_adjoint_run takes lam[0..3+n_th] = dJ/d(u1, u2, u3, p, th_0..) of the
+ * recorded final state for any objective J and overwrites them with dJ/d of the state
  * the recording started from.  It recomputes each segment of `every` steps
  * from its checkpoint and runs the hand-written adjoint of every RK substep
  * backwards through it (transposed tridiagonal solves, adjoint transforms,

@@ -3,15 +3,20 @@ torch.autograd (test infrastructure only: the reference gradient that the
 hand-written adjoint of libdiablo_gpu is checked against).
 
 The step is for/channel.f90:rk_chan_1 (:10-917) with rem_div_chan
-(:946-1023) for velocities only (no scalars, no LES), written in Fourier
-space the way the CUDA path runs it: the Crank-Nicolson operator and the wall
-rows act along y only, so the reference's physical-space solves per (x, z)
-column equal solves per (kx, kz) column.  The nonlinear products are formed in
-physical space with the reference's dealiased transforms (for/fft.f90:247-382,
-float32 pi in the wavenumbers).
+(:946-1023) for velocities and scalars (no LES, no 'Front' forcing), written
+in Fourier space the way the CUDA path runs it: the Crank-Nicolson operator
+and the wall rows act along y only, so the reference's physical-space solves
+per (x, z) column equal solves per (kx, kz) column.  The nonlinear products
+are formed in physical space with the reference's dealiased transforms
+(for/fft.f90:247-382, float32 pi in the wavenumbers).  Scalars follow
+:156-249 (buoyancy grav_y I(th) into cf2 outside the (0,0) mode, grav_x th
+and grav_z th into cf1 and cf3, -nu/Pr k^2b th, the background gradients
+-u1 dTHdX - u3 dTHdZ) and :553-710 (products th u1, th u3, the y-flux of
+th u2, the implicit solve with apply_bc_th's wall rows, :1797-1876).
 
-State: complex128 tensors u1, u2, u3, p of shape (Ny+2, 2Nkz+1, Nkx+1)
-(plane j, packed kz index, kx index) -- the significant Fourier box.
+State: complex128 tensors u1, u2, u3, p, th_0 .. th_{N_th-1} of shape
+(Ny+2, 2Nkz+1, Nkx+1) (plane j, packed kz index, kx index) -- the
+significant Fourier box.
 """
 from __future__ import annotations
 
@@ -23,8 +28,10 @@ from oracle.channel import PI_REF, BETA_BAR, ZETA_BAR, H_FRAC, grid_metrics
 
 class TorchChannel:
     def __init__(self, p, gy_file, device="cpu"):
-        if p.n_th != 0 or p.use_les:
-            raise NotImplementedError("velocity-only DNS")
+        if p.use_les or getattr(p, "flavor", "Basic") == "Front":
+            raise NotImplementedError("DNS without the 'Front' forcing")
+        self.nth = p.n_th
+        self.jst = [p.jstart_th(n) for n in range(p.n_th)]
         self.p = p
         self.dev = device
         self.Nx, self.Ny, self.Nz = p.nx, p.ny, p.nz
@@ -86,15 +93,18 @@ class TorchChannel:
             x[j] = (g[j] - c[j] * x[j + 1]) / b[j]
         return x
 
-    def _solve_rows(self, kind, r, rk):
-        """The implicit CN system of u1/u3 (kind 0) or u2 (kind 1) with its
-        wall rows (for/channel.f90:716-877, 1545-1792), solved per column."""
+    def _solve_rows(self, kind, r, rk, pr=1.0, j0=None):
+        """The implicit CN system of u1/u3 or a scalar (kind 0; the scalar's
+        diffusivity is nu/pr and its rows start at j0, :657-707) or u2
+        (kind 1) with its wall rows (for/channel.f90:716-877, 1545-1792),
+        solved per column."""
         p, Nyp, n = self.p, self.Nyp, self.n
         dy, dyf = self.dy_np, self.dyf_np
         h = H_FRAC[rk - 1] * p.delta_t
-        tc = 0.5 * self.nu * h * p.nu_v_scale
+        tc = 0.5 * self.nu * h * p.nu_v_scale / pr
         A = np.zeros(n); B = np.ones(n); C = np.zeros(n)
-        rows = range(self.jstart, self.jend + 1) if kind == 0 else range(2, Nyp + 1)
+        j0 = self.jstart if j0 is None else j0
+        rows = range(j0, self.jend + 1) if kind == 0 else range(2, Nyp + 1)
         for j in rows:
             if kind == 0:
                 A[j] = -tc / (dy[j] * dyf[j])
@@ -140,7 +150,9 @@ class TorchChannel:
             A[Nyp + 1], B[Nyp + 1], C[Nyp + 1], vec[Nyp + 1] = -1., 1., 0., dyf[Nyp] * p.v_bc_ymax_c1 * m
 
     # -- nonlinear terms (for/channel.f90:299-459) ----------------------
-    def nonlinear(self, u1c, u2c, u3c):
+    def nonlinear(self, u1c, u2c, u3c, thc=()):
+        """NL of u1, u2, u3 (:299-459) and of each scalar (:553-608); the
+        scalars' rows are masked by the caller."""
         Nyp = self.Nyp
         u1, u2, u3 = self.to_physical(u1c), self.to_physical(u2c), self.to_physical(u3c)
         dy = self.dy[:, None, None]
@@ -163,18 +175,27 @@ class TorchChannel:
         nl1 = torch.cat([z, ikz * p13 + ikx * p11 + y1, z])
         nl3 = torch.cat([z, ikx * p13 + ikz * p33 + y3, z])
         nl2 = torch.cat([z, ikx * q1 + ikz * q3 + v, z])
-        return nl1, nl2, nl3
+        nlth = []
+        for c in thc:
+            th = self.to_physical(c)
+            a1 = F(th[J] * u1[J])
+            a3 = F(th[J] * u3[J])
+            yt = F((th[Jp] * u2[Jp] + th[J] * u2[Jp] - th[J] * u2[J] - th[Jm] * u2[J]) / (2.0 * dyf[J]))
+            nlth.append(torch.cat([z, ikx * a1 + ikz * a3 + yt, z]))
+        return (nl1, nl2, nl3) + tuple(nlth)
 
     # -- one RK substep -------------------------------------------------
     def substep(self, st, fprev, rk):
         p, Nyp, n = self.p, self.Nyp, self.n
-        u1, u2, u3, pr = st
+        u1, u2, u3, pr = st[:4]
+        ths = st[4:]
         h = H_FRAC[rk - 1] * p.delta_t
         t3, t4, t5 = ZETA_BAR[rk - 1] * h, h, BETA_BAR[rk - 1] * h
         tc = 0.5 * self.nu * h * p.nu_v_scale
         ikx, ikz = 1j * self.kx, 1j * self.kz
         dy, dyf = self.dy[:, None, None], self.dyf[:, None, None]
-        nl1, nl2, nl3 = self.nonlinear(u1, u2, u3)
+        nls = self.nonlinear(u1, u2, u3, ths)
+        nl1, nl2, nl3 = nls[:3]
         js, je = self.jstart, self.jend
         rows13 = torch.zeros(n, 1, 1, dtype=torch.float64, device=self.dev)
         rows13[js:je + 1] = 1.0
@@ -185,6 +206,19 @@ class TorchChannel:
         cf1 = rows13 * (-self.nu * self.kk * u1 + self.roinvd * u3 - nl1)
         cf3 = rows13 * (-self.nu * self.kk * u3 - self.roinvd * u1 - nl3)
         cf2 = rows2 * (-self.nu * self.kk * u2 - nl2)
+        # scalars' explicit terms (:156-249) and their products (:553-608)
+        dyfm = torch.cat([self.dyf[:1], self.dyf[:-1]])[:, None, None]
+        cfth = []
+        for q, th in enumerate(ths):
+            thm = torch.cat([th[:1], th[:-1]])
+            buoy = p.grav_y * (th * dyfm + thm * dyf) / (2.0 * dy)
+            cf2 = cf2 + rows2 * (1.0 - self.m00) * buoy
+            cf1 = cf1 + rows13 * p.grav_x * th
+            cf3 = cf3 + rows13 * p.grav_z * th
+            rowst = torch.zeros(n, 1, 1, dtype=torch.float64, device=self.dev)
+            rowst[self.jst[q]:je + 1] = 1.0
+            cfth.append(rowst * (-(self.nu / p.pr[q]) * self.kk * th - u1 * p.dthdx[q]
+                                 - u3 * p.dthdz[q] - nls[3 + q]))
         px = 0.0
         if p.f_type == 1:
             px = t4 * p.px0
@@ -198,7 +232,6 @@ class TorchChannel:
         up = lambda u: torch.cat([u[1:], u[-1:]])
         um = lambda u: torch.cat([u[:1], u[:-1]])
         dyp = torch.cat([self.dy[1:], self.dy[-1:]])[:, None, None]
-        dyfm = torch.cat([self.dyf[:1], self.dyf[:-1]])[:, None, None]
         r1 = cr1 + tc * (((up(u1) - u1) / dyp - (u1 - um(u1)) / dy) / dyf)
         r3 = cr3 + tc * (((up(u3) - u3) / dyp - (u3 - um(u3)) / dy) / dyf)
         r2 = cr2 + tc * (((up(u2) - u2) / dyf - (u2 - um(u2)) / dyfm) / dy)
@@ -216,6 +249,19 @@ class TorchChannel:
             x = self.thomas(A, B, C, vec, 0, n - 1)
             out.append(torch.stack([u[j] if j < w0 else x[j] for j in range(n)]))
         u1s, u2s, u3s = out
+        # scalars: cr, the CN half and the implicit solve (:553-710)
+        thn = []
+        for q, th in enumerate(ths):
+            crt = th + t5 * cfth[q]
+            if rk > 1:
+                crt = crt + t3 * fprev[3 + q]
+            rt = crt + (tc / p.pr[q]) * (((up(th) - th) / dyp - (th - um(th)) / dy) / dyf)
+            A, B, C, vec = self._solve_rows(0, rt, rk, p.pr[q], self.jst[q])
+            self._bc13(A, B, C, vec, p.th_bc_ymin[q], p.th_bc_ymin_c1[q],
+                       p.th_bc_ymax[q], p.th_bc_ymax_c1[q])
+            x = self.thomas(A, B, C, vec, 0, n - 1)
+            w0 = self.jst[q] - 1
+            thn.append(torch.stack([th[j] if j < w0 else x[j] for j in range(n)]))
         # projection (rem_div_chan, for/channel.f90:946-1023)
         kx2, kz2 = self.kx ** 2, self.kz ** 2
         zero = torch.zeros_like(u1s[0])
@@ -247,7 +293,7 @@ class TorchChannel:
         phim = torch.cat([phi[:1], phi[:-1]])
         u2n = u2s - J2 * (phi - phim) / dy
         prn = pr + rows13 * phi / t4
-        return (u1n, u2n, u3n, prn), (cf1, cf2, cf3)
+        return (u1n, u2n, u3n, prn) + tuple(thn), (cf1, cf2, cf3) + tuple(cfth)
 
     def step(self, st, nsteps=1):
         for _ in range(nsteps):
@@ -261,12 +307,15 @@ class TorchChannel:
         """J = 1/2 <u.u>: the volume average of the kinetic energy of the
         dealiased field, by Parseval over the stored half spectrum (weight 2
         for kx > 0), u1, u3 on GYF planes 1..Ny (weights dyf), u2 on GY planes
-        2..Ny (weights dy)."""
+        2..Ny (weights dy).  Entries of st beyond the third (scalars) count
+        like u1: 1/2 <th^2> on GYF planes."""
         u1, u2, u3 = st[0], st[1], st[2]
         w = torch.full((u1.shape[2],), 2.0, dtype=torch.float64, device=u1.device)
         w[0] = 1.0
         ny = p.ny
         e13 = ((u1.abs() ** 2 + u3.abs() ** 2) * w).sum(dim=(1, 2))
+        for th in st[3:]:
+            e13 = e13 + ((th.abs() ** 2) * w).sum(dim=(1, 2))
         e2 = ((u2.abs() ** 2) * w).sum(dim=(1, 2))
         ly = dyf[1:ny + 1].sum()
         return 0.5 * ((e13[1:ny + 1] * dyf[1:ny + 1]).sum() + (e2[2:ny + 1] * dy[2:ny + 1]).sum()) / ly
