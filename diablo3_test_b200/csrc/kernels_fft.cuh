@@ -468,6 +468,105 @@ DI void nl_fill(typename CT<T>::C (&v)[N1], const XFwdArgs<T>& a, int f, int q, 
   }
 }
 
+// 16-byte row loads for the FP32 transforms with N1 = 2 N2 (XR2C_VEC4).
+// Thread t of a row loads float4 number N2 i + t (i < N1/2): the N2 threads
+// of the row read 16 N2 contiguous bytes per instruction (128 bytes at
+// N2 = 8, against 64 with the 8-byte pair loads), so a warp's load covers
+// whole 128-byte lines.  Element e = 2i + b of the thread is then the complex
+// point z[2 N2 i + 2t + b].
+DI float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+template <int N1, int N2>
+DI size_t v4off(int i, int t) { return (size_t)4 * (N2 * i + t); }
+
+template <int N1, int N2>
+DI void fill4_prod(float2 (&v)[N1], const float* x, const float* y, size_t off, int t) {
+  float4 px[N1 / 2], py[N1 / 2];
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) { px[i] = ld4(x + off + v4off<N1, N2>(i, t)); py[i] = ld4(y + off + v4off<N1, N2>(i, t)); }
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) {
+    v[2 * i] = make_float2(px[i].x * py[i].x, px[i].y * py[i].y);
+    v[2 * i + 1] = make_float2(px[i].z * py[i].z, px[i].w * py[i].w);
+  }
+}
+template <int N1, int N2>
+DI void fill4_sq(float2 (&v)[N1], const float* x, size_t off, int t) {
+  float4 px[N1 / 2];
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) px[i] = ld4(x + off + v4off<N1, N2>(i, t));
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) {
+    v[2 * i] = make_float2(px[i].x * px[i].x, px[i].y * px[i].y);
+    v[2 * i + 1] = make_float2(px[i].z * px[i].z, px[i].w * px[i].w);
+  }
+}
+template <int N1, int N2>
+DI void fill4_flux(float2 (&v)[N1], const float* uf, const float* u2, size_t off, size_t ps, float den, int t) {
+  const DivBy<float> dv(den);
+  auto f = [&](float p, float c, float m, float vp, float vc) { return dv(p * vp + c * vp - c * vc - m * vc); };
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) {
+    const size_t o = off + v4off<N1, N2>(i, t);
+    const float4 p = ld4(uf + o + ps), c = ld4(uf + o), m = ld4(uf + o - ps);
+    const float4 vp = ld4(u2 + o + ps), vc = ld4(u2 + o);
+    v[2 * i] = make_float2(f(p.x, c.x, m.x, vp.x, vc.x), f(p.y, c.y, m.y, vp.y, vc.y));
+    v[2 * i + 1] = make_float2(f(p.z, c.z, m.z, vp.z, vc.z), f(p.w, c.w, m.w, vp.w, vc.w));
+  }
+}
+template <int N1, int N2>
+DI void fill4_interp(float2 (&v)[N1], const float* uf, const float* u2, size_t off, size_t ps, float dyfj,
+                     float dyfm, float den, int t) {
+  const DivBy<float> dv(den);
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) {
+    const size_t o = off + v4off<N1, N2>(i, t);
+    const float4 c = ld4(uf + o), m = ld4(uf + o - ps), w = ld4(u2 + o);
+    v[2 * i] = make_float2(dv(dyfj * c.x + dyfm * m.x) * w.x, dv(dyfj * c.y + dyfm * m.y) * w.y);
+    v[2 * i + 1] = make_float2(dv(dyfj * c.z + dyfm * m.z) * w.z, dv(dyfj * c.w + dyfm * m.w) * w.w);
+  }
+}
+template <int N1, int N2>
+DI void fill4_v2(float2 (&v)[N1], const float* u2, size_t off, size_t ps, float dyj, int t) {
+  const DivBy<float> dv(dyj);
+  auto f = [&](float p, float c, float m) {
+    const float sa = c + p, da = c + m;
+    return dv(0.25f * (sa * sa) - 0.25f * (da * da));
+  };
+#pragma unroll
+  for (int i = 0; i < N1 / 2; ++i) {
+    const size_t o = off + v4off<N1, N2>(i, t);
+    const float4 p = ld4(u2 + o + ps), c = ld4(u2 + o), m = ld4(u2 + o - ps);
+    v[2 * i] = make_float2(f(p.x, c.x, m.x), f(p.y, c.y, m.y));
+    v[2 * i + 1] = make_float2(f(p.z, c.z, m.z), f(p.w, c.w, m.w));
+  }
+}
+// nl_fill with the 16-byte loads (same products, same operation order)
+template <int N1, int N2>
+DI void nl_fill4(float2 (&v)[N1], const XFwdArgs<float>& a, int f, int q, int j, size_t off, size_t ps, int t) {
+  const float* u1 = a.in[0];
+  const float* u2 = a.in[1];
+  const float* u3 = a.in[2];
+  if (f == 1) {
+    if (q == 2) {
+      fill4_v2<N1, N2>(v, u2, off, ps, (float)a.gm.dy[j], t);
+    } else {
+      fill4_interp<N1, N2>(v, q == 0 ? u3 : u1, u2, off, ps, (float)a.gm.dyf[j], (float)a.gm.dyf[j - 1],
+                           (float)(2.0 * a.gm.dy[j]), t);
+    }
+    return;
+  }
+  const float* own = f == 0 ? u1 : (f == 2 ? u3 : a.in[f]);
+  if (q == 2) {
+    fill4_flux<N1, N2>(v, own, u2, off, ps, (float)(2.0 * a.gm.dyf[j]), t);
+  } else if (q == 0) {
+    if (f == 2) fill4_sq<N1, N2>(v, u3, off, t);
+    else fill4_prod<N1, N2>(v, f == 0 ? u3 : own, f == 0 ? u1 : u3, off, t);
+  } else {
+    if (f == 0) fill4_sq<N1, N2>(v, u1, off, t);
+    else fill4_prod<N1, N2>(v, own, u1, off, t);
+  }
+}
+
 // Whether k_xr2c finishes the real-to-complex split in registers.  The split
 // needs Z[m] and Z[M - m] together.  With N1 = 2 N2 a thread can own step-2
 // rows k1 and N1 - k1 (thread 0: rows 0 and N1/2), and row k1 holds
@@ -483,6 +582,21 @@ DI void nl_fill(typename CT<T>::C (&v)[N1], const XFwdArgs<T>& a, int f, int q, 
 #ifndef XR2C_PAD_OP
 #define XR2C_PAD_OP 1
 #endif
+// Whether the FP32 paired transforms use the 16-byte row loads.  The loads
+// give each thread the columns n2 = c0, c0 + 1 (c0 = 2t mod N2) of the
+// four-step split n = n2 + N2 n1, the even n1 (t < N2/2) or the odd n1
+// (t >= N2/2).  Step 1 is then a radix-2 split of the length-N1 DFT: the
+// thread transforms its two half sequences (length N1/2 = N2), E_c or O_c,
+// and stores E'[c][k] = E_c[k] w_M^(c k) or O'[c][k] = O_c[k] w_M^((N2+c) k);
+// the step-2 thread of row k1 forms E' + O' (k1 < N1/2, k = k1) or
+// (E' - O') w_M^(N2 c) (k1 >= N1/2, k = k1 - N1/2) and transforms along c.
+// Tile entry (h, c, k) sits at h HP + c CP + k with CP = N2 + 1 and
+// HP = N2 CP + 1: at N2 = 8 both the stores (fixed c, k per instruction)
+// and the step-2 reads (fixed c, consecutive k) of the warp's four rows fill
+// two 128-byte wavefronts each.
+#ifndef XR2C_VEC4
+#define XR2C_VEC4 1
+#endif
 
 // Shared-memory layout of k_xr2c for a given configuration.
 template <typename T, int N1, int N2, int KT, bool NL = true>
@@ -491,9 +605,15 @@ struct XFwdSmem {
   static constexpr int M = N1 * N2;
   static constexpr int NKX1 = (2 * M) / 3 + 1;   // upper bound of Nkx+1
   static constexpr bool PAIRED = XR2C_PAIRED && N1 == 2 * N2;
+  static constexpr bool VEC = XR2C_VEC4 && PAIRED && sizeof(T) == 4;
+  static constexpr int VCP = N2 + 1, VHP = N2 * VCP + 1;
+  static constexpr int VRAW = 2 * VHP;
+  // the E'/O' tile padded like dfft::SmemSize: rows start 64 bytes apart modulo 128
+  static constexpr int VROW = VRAW + ((((VRAW * 8) % 128) == 64) ? 0 : ((128 + 64 - (VRAW * 8) % 128) % 128) / 8);
   // per row one four-step tile (without the register split also the
   // natural-order spectrum, which needs M+1 entries)
-  static constexpr int ROWC = (PAIRED || dfft::SmemSize<N1, N2>::v > M + 1) ? dfft::SmemSize<N1, N2>::v : M + 1;
+  static constexpr int ROWC = VEC ? VROW
+                            : ((PAIRED || dfft::SmemSize<N1, N2>::v > M + 1) ? dfft::SmemSize<N1, N2>::v : M + 1);
   // Pitch of the accumulated B output [m][row] of the NL form (the A output
   // goes straight to global memory).  Shared memory serves 128 bytes per
   // wavefront: W = 128 / sizeof(C) threads, that is G = W / N2 rows of N2
@@ -538,6 +658,7 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BL
   constexpr int NR = (N1 + N2 - 1) / N2;    // step-2 rows per thread
   constexpr int OP = L::OP;
   constexpr bool PAIRED = L::PAIRED;
+  constexpr bool VEC = L::VEC;
   extern __shared__ __align__(16) unsigned char xr2c_smem[];
   C* smb = reinterpret_cast<C*>(xr2c_smem);          // [KT][ROWC] four-step tile / spectrum
   C* acc = smb + KT * ROWC;                            // [NKX1][OP] output B (NL)
@@ -580,20 +701,64 @@ __global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BL
 #pragma unroll 1
   for (int q = 0; q < NQ; ++q) {
     C v[N1];
-    if (NL) {
-      nl_fill<T, N1, N2>(v, a, f, q, j, rowoff, ps, t);
-    } else {
+    if constexpr (VEC) {
+      if (NL) {
+        nl_fill4<N1, N2>(v, a, f, q, j, rowoff, ps, t);
+      } else {
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1)
-        v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * (n1 * N2 + t));
+        for (int i = 0; i < N1 / 2; ++i) {
+          const float4 x = ld4(a.in[f] + rowoff + v4off<N1, N2>(i, t));
+          v[2 * i] = CT<T>::mk(x.x, x.y);
+          v[2 * i + 1] = CT<T>::mk(x.z, x.w);
+        }
+      }
+      // step 1: the half sequences of columns c0 and c0 + 1
+      constexpr int H = N1 / 2, CP = L::VCP, HP = L::VHP;
+      const int h = t >= N2 / 2 ? 1 : 0;
+      const int c0 = 2 * (t - h * (N2 / 2));
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        C sq[H];
+#pragma unroll
+        for (int i = 0; i < H; ++i) sq[i] = v[2 * i + b];
+        dfft::RegDFT<H, -1, C>::run(sq);
+        const int c = c0 + b;
+        C* dst = sm + h * HP + c * CP;
+        dst[0] = sq[0];
+        const int tws = h * N2 + c;
+#pragma unroll
+        for (int k = 1; k < H; ++k) dst[k] = cmul(sq[k], a.twM[tws * k]);
+      }
+    } else {
+      if (NL) {
+        nl_fill<T, N1, N2>(v, a, f, q, j, rowoff, ps, t);
+      } else {
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1)
+          v[n1] = *reinterpret_cast<const C*>(a.in[f] + rowoff + 2 * (n1 * N2 + t));
+      }
+      dfft::step1<N1, N2, -1>(v, t, a.twM, sm);
     }
-    dfft::step1<N1, N2, -1>(v, t, a.twM, sm);
     rowsync();
     if constexpr (PAIRED) {
       // thread t owns rows t and N1 - t; thread 0 rows 0 and N1/2
       C ua[N2], ub[N2];
-      dfft::step2<N1, N2, -1>(ua, t, sm);
-      dfft::step2<N1, N2, -1>(ub, t == 0 ? N1 / 2 : N1 - t, sm);
+      if constexpr (VEC) {
+        constexpr int H = N1 / 2, CP = L::VCP, HP = L::VHP;
+        const int ka = t, kb = (H - t) % H;   // rows t (< H) and N1 - t or H (>= H)
+#pragma unroll
+        for (int c = 0; c < N2; ++c) {
+          const C ea = sm[c * CP + ka], oa = sm[HP + c * CP + ka];
+          const C eb = sm[c * CP + kb], ob = sm[HP + c * CP + kb];
+          ua[c] = ea + oa;
+          ub[c] = c == 0 ? eb - ob : cmul(eb - ob, a.twM[N2 * c]);
+        }
+        dfft::RegDFT<N2, -1, C>::run(ua);
+        dfft::RegDFT<N2, -1, C>::run(ub);
+      } else {
+        dfft::step2<N1, N2, -1>(ua, t, sm);
+        dfft::step2<N1, N2, -1>(ub, t == 0 ? N1 / 2 : N1 - t, sm);
+      }
       rowsync();  // the tile is free for the next transform
       // N2 pair slots per thread, the same code path in every thread (a
       // separate path for thread 0 would run serially beside the others'):
