@@ -327,8 +327,12 @@ def read_traffic():
 def ensemble_bench(torch, k, warmup=3):
     """The uneven-grid ensemble (48 mixed-precision members cycling four grid
     sizes, 23.5 M points per ensemble step): one graph launch per step for all
-    members against the same members run one at a time on one stream.  Both
-    are timed with CUDA events; their final states are compared."""
+    members, in the persistent mode (every member's column step of a substep
+    in one persistent launch per rows-per-lane class) and in the branches mode
+    (each member's whole step on its own graph branch), against the same
+    members run one at a time on one stream.  All are timed with CUDA events;
+    the final states are compared."""
+    from diablo3_test_b200 import _lib
     from diablo3_test_b200 import ics
     from diablo3_test_b200.channel import Ensemble
     from diablo3_test_b200.config import MIXED
@@ -362,10 +366,18 @@ def ensemble_bench(torch, k, warmup=3):
         tiles[f"{p.nx}x{p.ny}x{p.nz}"] = list(t)
     ens.step(1)
     ens.synchronize()
+    mode = ens.mode
     ms_graph = time_graph()
+    # the other mode on the same members
+    ens.mode = _lib.ENSEMBLE_BRANCHES if mode == _lib.ENSEMBLE_PERSISTENT else _lib.ENSEMBLE_PERSISTENT
+    ens.step(1)
+    ens.synchronize()
+    ms_other = time_graph()
+    other_mode = ens.mode
+    ens.mode = mode
     # the members run singly catch up to the same step count, then are timed
     for ch in one_m:
-        ch.step(k + 1)
+        ch.step(2 * k + 2)
     torch.cuda.synchronize()
     e0.record(s1)
     for ch in one_m:
@@ -394,7 +406,12 @@ def ensemble_bench(torch, k, warmup=3):
             "tiles_meaning": "z inverse sequences/block, x inverse rows/block, x forward rows/block, "
                              "z forward sequences/block (0 = default), tuned per size on the graph",
             "max_rel_diff_vs_singly": diff,
-            "graph": "one CUDA graph launch per ensemble step, one branch per member",
+            "mode": "persistent" if mode == _lib.ENSEMBLE_PERSISTENT else "branches",
+            "other_mode": {"mode": "persistent" if other_mode == _lib.ENSEMBLE_PERSISTENT else "branches",
+                           "value": pts * k / (ms_other * 1e-3) / 1e6, "ms_per_step": ms_other / k},
+            "graph": "one CUDA graph launch per ensemble step; persistent: per substep the members' "
+                     "transforms on parallel branches, then one k_column_step_ens launch per "
+                     "rows-per-lane class walking the member table; branches: one branch per member",
             "kernel_launches_total": launches}
 
 

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdiablo_g
 
 # status codes (enum diablo_status)
 OK = 0
+ENSEMBLE_BRANCHES, ENSEMBLE_PERSISTENT = 0, 1
 ERR_ARG = -1
 ERR_SIZE = -2
 ERR_CUDA = -3
@@ -56,6 +57,8 @@ SIGNATURES = {
     "diablo_ensemble_synchronize": (_i, [_vp]),
     "diablo_ensemble_stream": (_vp, [_vp]),
     "diablo_ensemble_autotune": (_i, [_vp, _i]),
+    "diablo_ensemble_set_mode": (_i, [_vp, _i]),
+    "diablo_ensemble_mode": (_i, [_vp]),
     "diablo_ensemble_destroy": (_i, [_vp]),
     "diablo_fft_xz_to_fourier": (_i, [_vp, _vp, _vp]),
     "diablo_fft_xz_to_physical": (_i, [_vp, _vp, _vp]),

@@ -250,9 +250,13 @@ class Channel:
 
 class Ensemble:
     """Independent channels (any mix of grids, parameters and precisions)
-    stepped together: one CUDA graph launch per step for all members, each
-    member's kernels on a parallel branch (``diablo_ensemble_*`` of the C ABI).
-    The members stay usable on their own and must outlive the ensemble."""
+    stepped together: one CUDA graph launch per step for all members
+    (``diablo_ensemble_*`` of the C ABI).  In the persistent mode (the
+    default when every member qualifies) each substep's column steps of all
+    members run in one persistent launch per rows-per-lane class after the
+    members' transforms, which run on parallel branches; in the branches mode
+    each member's whole step is one branch.  The members stay usable on their
+    own and must outlive the ensemble."""
 
     def __init__(self, members, autotune: bool = False):
         self.lib = _lib.load()
@@ -269,6 +273,15 @@ class Ensemble:
 
     def synchronize(self):
         _lib.check(self.lib.diablo_ensemble_synchronize(self.e), "ensemble_synchronize")
+
+    @property
+    def mode(self) -> int:
+        """_lib.ENSEMBLE_PERSISTENT or _lib.ENSEMBLE_BRANCHES."""
+        return self.lib.diablo_ensemble_mode(self.e)
+
+    @mode.setter
+    def mode(self, mode: int):
+        _lib.check(self.lib.diablo_ensemble_set_mode(self.e, mode), "ensemble_set_mode")
 
     def autotune(self, steps_per_trial: int = 5):
         """Tune each member size's transform tiles on the ensemble's own graph

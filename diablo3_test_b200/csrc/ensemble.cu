@@ -1,6 +1,7 @@
 // Ensembles of independent channels stepped by CUDA graph launches, and the
 // tile autotuner of the step transforms.
 #include "internal.h"
+#include "kernels_field.cuh"
 
 // ==========================================================================
 // Ensembles: independent members stepped by one CUDA graph launch per step.
@@ -15,8 +16,30 @@ struct MemberKey {
   }
 };
 
+// One launch of the ensemble column step: the members of one rows-per-lane
+// class R at one substep of one graph parity.  The member arguments are built
+// on the host during capture and copied to the device after it.
+struct EnsTable {
+  int R = 0, ntask = 0;
+  std::vector<int> members;        // indices into diablo_ensemble::m
+  std::vector<FieldArgs> args;     // host copy, in member order
+  std::vector<int> prefix;         // [nmem + 1] first task of each member
+  FieldArgs* d_args = nullptr;
+  int* d_prefix = nullptr;
+  int* d_counter = nullptr;
+};
+
 struct diablo_ensemble {
   std::vector<diablo_ctx*> m;
+  // DIABLO_ENSEMBLE_PERSISTENT: every member's column step of a substep in
+  // one persistent launch per rows-per-lane class; DIABLO_ENSEMBLE_BRANCHES:
+  // each member's whole step on its own graph branch
+  int mode = DIABLO_ENSEMBLE_PERSISTENT;
+  std::vector<EnsTable> tables[2][3];   // [graph parity][substep]
+  // per rows-per-lane class (R = 3..9): the stream its column launches are
+  // captured on and the event the class's members wait on
+  cudaStream_t cstream[10] = {};
+  cudaEvent_t cevent[10] = {};
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> joins;
   cudaStream_t origin = nullptr;
@@ -112,6 +135,160 @@ int capture(diablo_ensemble* e, int w) {
   return 0;
 }
 
+// Whether every member's substep takes the field-split column step that the
+// ensemble kernel runs: DNS (LES gate never opening), no 'Front' forcing,
+// the default column path, and 3..9 rows per lane.
+bool persistent_ok(const diablo_ensemble* e) {
+  for (const diablo_ctx* c : e->m) {
+    if (c->p.use_les || (c->p.flavor_front && c->ro_inv != 0.0)) return false;
+    if (!(c->use_general_solver == 0 || c->use_general_solver == 3)) return false;
+    const int R = rows_per_lane(c->nyp2);
+    if (R < 3 || R > 9 || column_step_ens_resident(R) <= 0) return false;
+  }
+  return true;
+}
+
+void free_tables(diablo_ensemble* e, int w) {
+  for (int rk = 0; rk < 3; ++rk) {
+    for (EnsTable& t : e->tables[w][rk]) {
+      if (t.d_args) cudaFree(t.d_args);
+      if (t.d_prefix) cudaFree(t.d_prefix);
+      if (t.d_counter) cudaFree(t.d_counter);
+    }
+    e->tables[w][rk].clear();
+  }
+}
+
+// Capture one step of every member into exec[w] with the column steps of
+// each substep launched together: per substep, each member's transforms and
+// nonlinear terms on its own branch, then (after all branches) one
+// k_column_step_ens launch per rows-per-lane class, then the next substep's
+// branches.  The host state is advanced as the step would advance it.
+int capture_persistent(diablo_ensemble* e, int w) {
+  const int n = (int)e->m.size();
+  for (diablo_ctx* c : e->m) {
+    const int R = rows_per_lane(c->nyp2);
+    if (!e->cstream[R] && (cudaStreamCreateWithFlags(&e->cstream[R], cudaStreamNonBlocking) != cudaSuccess ||
+                           cudaEventCreateWithFlags(&e->cevent[R], cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      return DIABLO_ERR_CUDA;
+    }
+  }
+  // classes and their device tables (allocated before capture begins)
+  free_tables(e, w);
+  for (int rk = 0; rk < 3; ++rk) {
+    std::vector<EnsTable>& tb = e->tables[w][rk];
+    for (int i = 0; i < n; ++i) {
+      const int R = rows_per_lane(e->m[i]->nyp2);
+      EnsTable* t = nullptr;
+      for (EnsTable& x : tb) if (x.R == R) t = &x;
+      if (!t) { tb.emplace_back(); t = &tb.back(); t->R = R; }
+      t->members.push_back(i);
+    }
+    for (EnsTable& t : tb) {
+      const size_t k = t.members.size();
+      t.args.assign(k, FieldArgs{});
+      t.prefix.assign(k + 1, 0);
+      if (cudaMalloc((void**)&t.d_args, k * sizeof(FieldArgs)) != cudaSuccess ||
+          cudaMalloc((void**)&t.d_prefix, (k + 1) * sizeof(int)) != cudaSuccess ||
+          cudaMalloc((void**)&t.d_counter, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        free_tables(e, w);
+        return DIABLO_ERR_NOMEM;
+      }
+    }
+  }
+  std::vector<cudaStream_t> saved(n);
+  std::vector<int> prof(n);
+  e->key[w].resize(n);
+  e->nlaunch[w].assign(n, 0);
+  std::vector<long long> l0(n);
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    saved[i] = c->stream;
+    prof[i] = c->profiling;
+    c->profiling = 0;
+    c->stream = e->streams[i];
+    e->key[w][i] = member_key(c);
+    l0[i] = c->launches;
+  }
+  cudaGraph_t graph = nullptr;
+  int rc = 0;
+  cudaError_t ce = cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    cudaEventRecord(e->fork, e->origin);
+    for (int rk = 1; rk <= 3 && !rc; ++rk) {
+      std::vector<EnsTable>& tb = e->tables[w][rk - 1];
+      for (EnsTable& t : tb) {
+        for (size_t k = 0; k < t.members.size() && !rc; ++k) {
+          diablo_ctx* c = e->m[t.members[k]];
+          // the step's start, or this class's column step of the substep before
+          cudaStreamWaitEvent(c->stream, rk == 1 ? e->fork : e->cevent[t.R], 0);
+          if (rk == 1) c->time_step += 1;
+          c->defer_col = &t.args[k];
+          c->defer_filled = 0;
+          rc = substep(c, rk);
+          c->defer_col = nullptr;
+          if (!rc && !c->defer_filled) rc = DIABLO_ERR_UNSUPPORTED;
+          if (rk == 3) c->time += c->delta_t;
+          cudaEventRecord(e->joins[t.members[k]], c->stream);
+          cudaStreamWaitEvent(e->cstream[t.R], e->joins[t.members[k]], 0);
+        }
+      }
+      for (EnsTable& t : tb) {
+        if (rc) break;
+        const int res = column_step_ens_resident(t.R);
+        int tot = 0;
+        for (size_t k = 0; k < t.members.size(); ++k) {
+          FieldArgs& F = t.args[k];
+          const int ngroup = (F.s.ncol + FS_COLS - 1) / FS_COLS;
+          F.lag = std::max(1, res / F.nf);
+          t.prefix[k] = tot;
+          tot += ngroup * (F.nf + 1);
+        }
+        t.prefix[t.members.size()] = tot;
+        t.ntask = tot;
+        EnsColArgs E;
+        E.mem = t.d_args;
+        E.prefix = t.d_prefix;
+        E.counter = t.d_counter;
+        E.nmem = (int)t.members.size();
+        E.tsz = 32 * t.R * FS_COLS;
+        rc = launch_column_step_ens(E, t.R, tot, e->cstream[t.R]);
+        e->nlaunch[w][t.members[0]] += 2;
+        cudaEventRecord(e->cevent[t.R], e->cstream[t.R]);
+      }
+    }
+    // the step ends when every class's last column step has
+    for (EnsTable& t : e->tables[w][2]) cudaStreamWaitEvent(e->origin, e->cevent[t.R], 0);
+    ce = cudaStreamEndCapture(e->origin, &graph);
+  }
+  for (int i = 0; i < n; ++i) {
+    diablo_ctx* c = e->m[i];
+    e->nlaunch[w][i] += c->launches - l0[i];
+    c->launches = l0[i];
+    c->stream = saved[i];
+    c->profiling = prof[i];
+  }
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return rc;
+  }
+  ECK(ce);
+  // the member tables the graph's kernels read
+  for (int rk = 0; rk < 3; ++rk)
+    for (EnsTable& t : e->tables[w][rk]) {
+      ECK(cudaMemcpy(t.d_args, t.args.data(), t.args.size() * sizeof(FieldArgs), cudaMemcpyHostToDevice));
+      ECK(cudaMemcpy(t.d_prefix, t.prefix.data(), t.prefix.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+  if (e->exec[w]) { cudaGraphExecDestroy(e->exec[w]); e->exec[w] = nullptr; }
+  ce = cudaGraphInstantiate(&e->exec[w], graph, 0);
+  cudaGraphDestroy(graph);
+  ECK(ce);
+  return 0;
+}
+
 // (Re)capture both graphs from the members' current state, leaving the
 // members' host state as it was.
 int capture_both(diablo_ensemble* e) {
@@ -125,8 +302,9 @@ int capture_both(diablo_ensemble* e) {
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return DIABLO_ERR_CUDA;
     sv[i] = Saved{c->time, c->time_step, c->cur, c->cf_cur, c->w_top_transient};
   }
-  int rc = capture(e, 0);
-  if (!rc) rc = capture(e, 1);
+  const bool pers = e->mode == DIABLO_ENSEMBLE_PERSISTENT;
+  int rc = pers ? capture_persistent(e, 0) : capture(e, 0);
+  if (!rc) rc = pers ? capture_persistent(e, 1) : capture(e, 1);
   for (int i = 0; i < n; ++i) {
     diablo_ctx* c = e->m[i];
     c->time = sv[i].time; c->time_step = sv[i].time_step;
@@ -163,6 +341,7 @@ diablo_ensemble* diablo_ensemble_create(diablo_ctx* const* members, int n, int* 
       ok = cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking) == cudaSuccess &&
            cudaEventCreateWithFlags(&e->joins[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) { st = DIABLO_ERR_CUDA; diablo_ensemble_destroy(e); e = nullptr; }
+    else e->mode = persistent_ok(e) ? DIABLO_ENSEMBLE_PERSISTENT : DIABLO_ENSEMBLE_BRANCHES;
   }
   if (status) *status = st;
   return e;
@@ -206,6 +385,21 @@ int diablo_ensemble_step(diablo_ensemble* e, int nsteps) {
 
 void* diablo_ensemble_stream(diablo_ensemble* e) { return e ? (void*)e->origin : nullptr; }
 
+int diablo_ensemble_set_mode(diablo_ensemble* e, int mode) {
+  if (!e || (mode != DIABLO_ENSEMBLE_BRANCHES && mode != DIABLO_ENSEMBLE_PERSISTENT)) return DIABLO_ERR_ARG;
+  if (mode == DIABLO_ENSEMBLE_PERSISTENT && !persistent_ok(e)) return DIABLO_ERR_UNSUPPORTED;
+  if (mode == e->mode) return 0;
+  ECK(cudaStreamSynchronize(e->origin));
+  for (int k = 0; k < 2; ++k) {
+    if (e->exec[k]) { cudaGraphExecDestroy(e->exec[k]); e->exec[k] = nullptr; }
+    e->key[k].clear();
+  }
+  e->mode = mode;
+  return 0;
+}
+
+int diablo_ensemble_mode(const diablo_ensemble* e) { return e ? e->mode : DIABLO_ERR_ARG; }
+
 int diablo_ensemble_synchronize(diablo_ensemble* e) {
   if (!e) return DIABLO_ERR_ARG;
   ECK(cudaStreamSynchronize(e->origin));
@@ -224,6 +418,11 @@ int diablo_ensemble_destroy(diablo_ensemble* e) {
   if (e->origin) cudaStreamSynchronize(e->origin);
   for (int k = 0; k < 2; ++k)
     if (e->exec[k]) cudaGraphExecDestroy(e->exec[k]);
+  for (int k = 0; k < 2; ++k) free_tables(e, k);
+  for (int r = 0; r < 10; ++r) {
+    if (e->cstream[r]) cudaStreamDestroy(e->cstream[r]);
+    if (e->cevent[r]) cudaEventDestroy(e->cevent[r]);
+  }
   for (cudaStream_t s : e->streams)
     if (s) cudaStreamDestroy(s);
   for (cudaEvent_t v : e->joins)

@@ -20,6 +20,8 @@
 #include "kernels_fft.cuh"
 #include "solve_args.cuh"
 
+struct FieldArgs;   // the field-split column step's arguments (kernels_field.cuh)
+
 static_assert(DIABLO_MAX_TH <= SOLVE_MAXTH, "scalar capacity");
 static_assert(3 + DIABLO_MAX_TH <= NF_MAX, "field capacity");
 
@@ -87,6 +89,11 @@ struct diablo_ctx {
   // launches, 1 the general kernel, 2 the fused tiled kernel, 3 the
   // field-split step in one launch with bounded waits
   int use_general_solver;
+  // ensemble capture: when set, substep stores the arguments of its
+  // field-split column step here (and sets defer_filled) instead of
+  // launching it; the ensemble launches every member's column step at once
+  FieldArgs* defer_col;
+  int defer_filled;
   Solve2Args solve2;        // tile schedule of the current substep
   double* d_kc[3];          // implicit-row coefficients per RK substep [2+nth][3][n]
   double* d_met;            // Poisson and metric rows [MET_N][n]
@@ -241,6 +248,11 @@ int launch_field_solve(const FieldArgs& A, cudaStream_t s);
 int launch_project_cols(const FieldArgs& A, cudaStream_t s);
 int launch_column_step(const FieldArgs& A, cudaStream_t s);
 int column_step_resident(int n);   // blocks of k_column_step resident at once
+// the ensemble column step (column_ens.cu): one launch for every member of a
+// rows-per-lane class R (3..9); resident blocks of that launch
+struct EnsColArgs;
+int column_step_ens_resident(int R);
+int launch_column_step_ens(const EnsColArgs& E, int R, int ntask, cudaStream_t s);
 int sched_status(diablo_ctx* ctx);  // DIABLO_ERR_TIMEOUT if a device wait gave up (clears it)
 
 // ---- the step (step.cu) ------------------------------------------------------

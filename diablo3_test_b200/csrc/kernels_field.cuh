@@ -518,16 +518,17 @@ namespace cfield {
 struct Task {
   int kind;   // 0 field solve, 1 projection, 2 none left
   int g, f;   // column group, field
+  int mem;    // member (context) of the task
 };
 DI Task decode_task(int t, int ngroup, int nf, int lag) {
   const int a0 = lag * nf, a1 = a0 + (ngroup - lag) * (nf + 1), a2 = a1 + lag;
-  if (t < a0) return Task{0, t / nf, t % nf};
+  if (t < a0) return Task{0, t / nf, t % nf, 0};
   if (t < a1) {
     const int u = t - a0, s = lag + u / (nf + 1), r = u % (nf + 1);
-    return r < nf ? Task{0, s, r} : Task{1, s - lag, 0};
+    return r < nf ? Task{0, s, r, 0} : Task{1, s - lag, 0, 0};
   }
-  if (t < a2) return Task{1, ngroup - lag + (t - a1), 0};
-  return Task{2, 0, 0};
+  if (t < a2) return Task{1, ngroup - lag + (t - a1), 0, 0};
+  return Task{2, 0, 0, 0};
 }
 DI int ld_acquire(const int* p) {
   int v;
@@ -536,36 +537,40 @@ DI int ld_acquire(const int* p) {
 }
 }  // namespace cfield
 
-template <int R>
-__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(const __grid_constant__ FieldArgs A) {
+// The body of the single-launch column step, shared by the one-context
+// kernel (k_column_step) and the ensemble kernel (k_column_step_ens):
+// args_of(i) gives member i's arguments, claim() the next task (with its
+// member), tsz the ring's slot stride in complex elements (at least the
+// largest member's (Ny+2) x FS_COLS).  A task's own member fixes its sizes;
+// the first tile of the next task is fetched with that task's member's.
+template <int R, class ArgsOf, class Claim>
+DI void column_step_body(ArgsOf args_of, Claim claim, double2* ring, int tsz) {
   using namespace cfield;
-  extern __shared__ __align__(16) unsigned char fs_smem[];
-  __shared__ int s_next, s_ok;
-  const SolveArgs& a = A.s;
-  const int n = a.n, nyp = a.nyp;
-  const int tsz = n * FS_COLS;
-  double2* ring = reinterpret_cast<double2*>(fs_smem);
-  const int nf = A.nf;
-  const int ngroup = (a.ncol + FS_COLS - 1) / FS_COLS;
-  const int lag = min(A.lag, ngroup);
+  __shared__ int s_ok;
   const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-  const size_t ps = (size_t)a.ncol;          // plane stride (the Fourier pitch is 2Nkz+1)
   const double2 z2 = make_double2(0.0, 0.0);
   const int j0 = lane * R;
-  const double* met = A.met;
-  double2* const* cu = a.cu_out;
-  const void* src[7] = {cu[0], cu[2], cu[1], cu[0], cu[2], cu[1], a.cp_in};
-  const double ih = 1.0 / a.temp4;
-  auto claim = [&]() -> Task {
-    if (tid == 0) s_next = atomicAdd(A.sched + SCHED_COUNTER, 1);
-    __syncthreads();
-    const int t = s_next;
-    return decode_task(t, ngroup, nf, lag);
-  };
   Task cur = claim();
   bool pre = false;   // the current task's first tile is already in flight
   int step = 0;
+  // the next task's first tile (its nonlinear terms), from its own member
+  auto prefetch_next = [&](double2* nslot, const Task& nxt, int n_cur, size_t ps_cur, int q0, int nvalid) {
+    if (nxt.kind == 0) {
+      const SolveArgs& an = args_of(nxt.mem).s;
+      const int qn = nxt.g * FS_COLS;
+      const FTile first = an.nl64[nxt.f] ? FTile{an.nl64[nxt.f], FT_NL, 0, 0.0}
+                                         : FTile{an.nl32[nxt.f], FT_NL, 1, 0.0};
+      load_ftile<R>(nslot, &first, (size_t)an.ncol, qn, min(FS_COLS, an.ncol - qn), an.n, tid);
+    } else {
+      load_tile<R, 16>(nslot, nullptr, ps_cur, q0, nvalid, n_cur, tid);
+    }
+  };
   while (cur.kind != 2) {
+    const FieldArgs& A = args_of(cur.mem);
+    const SolveArgs& a = A.s;
+    const int n = a.n, nyp = a.nyp;
+    const size_t ps = (size_t)a.ncol;          // plane stride (the Fourier pitch is 2Nkz+1)
+    const double* met = A.met;
     if (cur.kind == 0) {
       const int f = cur.f;
       const int q0 = cur.g * FS_COLS;
@@ -609,14 +614,7 @@ __global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(
           // claim the next task; a field task's first tile (its nonlinear
           // terms) goes in flight now, a projection's waits for its inputs
           nxt = claim();
-          if (nxt.kind == 0) {
-            const int qn = nxt.g * FS_COLS;
-            const FTile first = a.nl64[nxt.f] ? FTile{a.nl64[nxt.f], FT_NL, 0, 0.0}
-                                              : FTile{a.nl32[nxt.f], FT_NL, 1, 0.0};
-            load_ftile<R>(nslot, &first, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
-          } else {
-            load_ftile<R>(nslot, nullptr, ps, q0, nvalid, n, tid);
-          }
+          prefetch_next(nslot, nxt, n, ps, q0, nvalid);
         }
         wait_groups<1>();
         __syncthreads();
@@ -757,6 +755,9 @@ __global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(
       pre = nxt.kind == 0;
       cur = nxt;
     } else {
+      double2* const* cu = a.cu_out;
+      const void* src[7] = {cu[0], cu[2], cu[1], cu[0], cu[2], cu[1], a.cp_in};
+      const double ih = 1.0 / a.temp4;
       const int g = cur.g;
       const int q0 = g * FS_COLS;
       const int nvalid = min(FS_COLS, a.ncol - q0);
@@ -796,14 +797,7 @@ __global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(
         if (k + 1 < 7) load_tile<R, 16>(nslot, src[k + 1], ps, q0, nvalid, n, tid);
         else {
           nxt = claim();
-          if (nxt.kind == 0) {
-            const int qn = nxt.g * FS_COLS;
-            const FTile first = a.nl64[nxt.f] ? FTile{a.nl64[nxt.f], FT_NL, 0, 0.0}
-                                              : FTile{a.nl32[nxt.f], FT_NL, 1, 0.0};
-            load_ftile<R>(nslot, &first, ps, qn, min(FS_COLS, a.ncol - qn), n, tid);
-          } else {
-            load_tile<R, 16>(nslot, nullptr, ps, q0, nvalid, n, tid);
-          }
+          prefetch_next(nslot, nxt, n, ps, q0, nvalid);
         }
         wait_groups<1>();
         __syncthreads();
@@ -880,4 +874,65 @@ __global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(
     }
   }
   wait_groups<0>();
+}
+
+template <int R>
+__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step(const __grid_constant__ FieldArgs A) {
+  using namespace cfield;
+  extern __shared__ __align__(16) unsigned char fs_smem[];
+  __shared__ int s_next;
+  const int ngroup = (A.s.ncol + FS_COLS - 1) / FS_COLS;
+  const int lag = min(A.lag, ngroup);
+  auto args_of = [&](int) -> const FieldArgs& { return A; };
+  auto claim = [&]() -> Task {
+    if (threadIdx.x == 0) s_next = atomicAdd(A.sched + SCHED_COUNTER, 1);
+    __syncthreads();
+    return decode_task(s_next, ngroup, A.nf, lag);
+  };
+  column_step_body<R>(args_of, claim, reinterpret_cast<double2*>(fs_smem), A.s.n * FS_COLS);
+}
+
+// ---- k_column_step_ens -------------------------------------------------------------
+// The column step of every member of an ensemble whose systems have R rows
+// per lane, in one persistent launch: a member table, and one task counter
+// over all members' tasks (member i's tasks are numbers prefix[i] ..
+// prefix[i+1]-1, in k_column_step's order).  Each member keeps its own
+// scheduler words (per-group counts, status) and wait bound; a projection
+// task waits, bounded, on its own member's group counts only, for tasks
+// claimed before it by running blocks, so the wait ends as in k_column_step.
+struct EnsColArgs {
+  const FieldArgs* mem;   // [nmem] member arguments (device)
+  const int* prefix;      // [nmem + 1] first task of each member (device)
+  int* counter;           // the launch's task counter (zeroed before it)
+  int nmem;
+  int tsz;                // ring slot stride: 32 R FS_COLS
+};
+
+template <int R>
+__global__ void __launch_bounds__(FS_THREADS, fs_min_blocks<R>()) k_column_step_ens(const __grid_constant__ EnsColArgs E) {
+  using namespace cfield;
+  extern __shared__ __align__(16) unsigned char fs_smem[];
+  __shared__ int s_next, s_mem;
+  auto args_of = [&](int i) -> const FieldArgs& { return E.mem[i]; };
+  auto claim = [&]() -> Task {
+    if (threadIdx.x == 0) {
+      const int t = atomicAdd(E.counter, 1);
+      int lo = 0, hi = E.nmem;   // the member i with prefix[i] <= t < prefix[i+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (E.prefix[mid] <= t) lo = mid; else hi = mid;
+      }
+      s_next = t;
+      s_mem = t < E.prefix[E.nmem] ? lo : -1;
+    }
+    __syncthreads();
+    const int i = s_mem;
+    if (i < 0) return Task{2, 0, 0, 0};
+    const FieldArgs& A = E.mem[i];
+    const int ngroup = (A.s.ncol + FS_COLS - 1) / FS_COLS;
+    Task k = decode_task(s_next - E.prefix[i], ngroup, A.nf, min(A.lag, ngroup));
+    k.mem = i;
+    return k;
+  };
+  column_step_body<R>(args_of, claim, reinterpret_cast<double2*>(fs_smem), E.tsz);
 }

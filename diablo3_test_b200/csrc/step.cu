@@ -488,7 +488,16 @@ int substep(diablo_ctx* ctx, int rk) {
     // opt-in: it measured slower at 256 x 257 x 256 (0.71 against 0.59 ms
     // per substep, mixed) and for the 64 x 97 x 64 adjoint case (13.9 against
     // 12.5 ms for 50 steps), and equal on the 48-member ensemble.
-    if (ctx->use_general_solver == 3) {
+    if (ctx->defer_col) {
+      // ensemble capture: the ensemble launches this column step with the
+      // other members' (k_column_step_ens); lag is set there
+      if (cfl) return DIABLO_ERR_UNSUPPORTED;
+      F.sched = ctx->d_sched;
+      F.need = 3 + ctx->wait_withhold;
+      F.max_spins = ctx->wait_spins;
+      *ctx->defer_col = F;
+      ctx->defer_filled = 1;
+    } else if (ctx->use_general_solver == 3) {
       const int resident = column_step_resident(ctx->nyp2);
       F.sched = ctx->d_sched;
       F.need = 3 + ctx->wait_withhold;

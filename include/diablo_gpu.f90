@@ -44,6 +44,9 @@ module diablo_gpu
   ! buffer layouts (enum diablo_layout)
   integer(c_int), parameter :: DIABLO_LAYOUT_FOURIER = 0
   integer(c_int), parameter :: DIABLO_LAYOUT_PHYSICAL = 1
+  ! ensemble stepping modes
+  integer(c_int), parameter :: DIABLO_ENSEMBLE_BRANCHES = 0
+  integer(c_int), parameter :: DIABLO_ENSEMBLE_PERSISTENT = 1
 
   ! Run parameters: field order and kinds exactly as struct diablo_params.
   type, bind(C) :: diablo_params
@@ -317,6 +320,17 @@ module diablo_gpu
       type(c_ptr), value :: e
       integer(c_int) :: diablo_ensemble_destroy
     end function diablo_ensemble_destroy
+    function diablo_ensemble_set_mode(e, mode) bind(C, name="diablo_ensemble_set_mode")
+      import :: c_ptr, c_int
+      type(c_ptr), value :: e
+      integer(c_int), value :: mode
+      integer(c_int) :: diablo_ensemble_set_mode
+    end function diablo_ensemble_set_mode
+    function diablo_ensemble_mode(e) bind(C, name="diablo_ensemble_mode")
+      import :: c_ptr, c_int
+      type(c_ptr), value :: e
+      integer(c_int) :: diablo_ensemble_mode
+    end function diablo_ensemble_mode
     function diablo_ensemble_autotune(e, steps_per_trial) bind(C, name="diablo_ensemble_autotune")
       import :: c_ptr, c_int
       type(c_ptr), value :: e

@@ -290,8 +290,16 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam);
  * contexts from diablo_create with any mix of grid sizes, parameters and
  * precisions; they stay owned by the caller and must outlive the ensemble.
  * diablo_ensemble_step advances every member by nsteps steps with one CUDA
- * graph launch per step, the members' kernel chains on parallel branches of
- * the graph.  The graphs are captured on first use and again whenever a
+ * graph launch per step.  In DIABLO_ENSEMBLE_PERSISTENT mode (the default
+ * when every member qualifies: DNS without LES or the 'Front' forcing, the
+ * default column path, Ny + 2 <= 288) each substep runs the members'
+ * transforms and nonlinear terms on parallel branches of the graph and then
+ * the column step of every member in ONE persistent launch per rows-per-lane
+ * class: the launch walks a member table, and each projection task waits,
+ * bounded by the member's diablo_set_wait_bound, for its own member's solves
+ * (a wait that gives up makes diablo_ensemble_synchronize return
+ * DIABLO_ERR_TIMEOUT).  In DIABLO_ENSEMBLE_BRANCHES mode each member's whole
+ * step is one branch of the graph.  The graphs are captured on first use and again whenever a
  * member's state no longer matches them (a member stepped on its own, a
  * changed delta_t or precision, the LES gate opening).  Members whose kernel
  * arguments change every step are rejected with DIABLO_ERR_UNSUPPORTED:
@@ -325,6 +333,13 @@ int diablo_ensemble_synchronize(diablo_ensemble* e);
  * it time the ensemble on the device. */
 void* diablo_ensemble_stream(diablo_ensemble* e);
 int diablo_ensemble_destroy(diablo_ensemble* e);
+/* Stepping mode (see above): DIABLO_ENSEMBLE_PERSISTENT or
+ * DIABLO_ENSEMBLE_BRANCHES.  Persistent mode is refused with
+ * DIABLO_ERR_UNSUPPORTED when a member does not qualify.  The graphs are
+ * captured again at the next step. */
+enum diablo_ensemble_mode { DIABLO_ENSEMBLE_BRANCHES = 0, DIABLO_ENSEMBLE_PERSISTENT = 1 };
+int diablo_ensemble_set_mode(diablo_ensemble* e, int mode);
+int diablo_ensemble_mode(const diablo_ensemble* e);
 /* Ensemble autotuner: coordinate descent over the transform tile shapes of
  * each group of same-size members (the candidates of diablo_autotune), scored
  * by the time of steps_per_trial steps of the ensemble's own graph.  The

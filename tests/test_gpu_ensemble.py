@@ -129,3 +129,78 @@ def test_ensemble_autotune_restores_states(cuda_device):
         for a, b in pairs:
             a.close()
             b.close()
+
+
+# members without LES: the persistent mode (the column steps of every member
+# of a rows-per-lane class in one launch per substep); Ny = 97 gives a second
+# class (four rows per lane) beside the three-row members
+PERSISTENT_MEMBERS = MEMBERS[:3] + [dict(nx=32, ny=97, nz=24, n_th=1, re=700.0, precision=MIXED)]
+
+
+def test_persistent_ensemble_matches_members_run_singly(cuda_device):
+    from diablo3_test_b200.channel import Ensemble
+    pairs = [_build(kw) for kw in PERSISTENT_MEMBERS]
+    try:
+        with Ensemble([p[0] for p in pairs]) as ens:
+            assert ens.mode == _lib.ENSEMBLE_PERSISTENT
+            ens.step(3)
+            ens.synchronize()
+            for a, b in pairs:
+                b.step(3)
+            for i, (a, b) in enumerate(pairs):
+                assert _same(a, b), i
+            # a member stepped on its own, then the branches mode and back
+            pairs[1][0].step(1)
+            pairs[1][1].step(1)
+            ens.mode = _lib.ENSEMBLE_BRANCHES
+            ens.step(1)
+            ens.mode = _lib.ENSEMBLE_PERSISTENT
+            ens.step(2)
+            ens.synchronize()
+            for a, b in pairs:
+                b.step(3)
+            for i, (a, b) in enumerate(pairs):
+                assert _same(a, b), i
+                assert a.check_finite()
+    finally:
+        for a, b in pairs:
+            a.close()
+            b.close()
+
+
+def test_persistent_ensemble_wait_times_out_and_recovers(cuda_device):
+    """One member withholds an arrival (failure injected from the host): its
+    projection tasks' bounded waits give up, the launch returns on its own
+    and the ensemble reports DIABLO_ERR_TIMEOUT; with the bound restored and
+    the member's state reloaded the ensemble steps bit-identically again."""
+    from diablo3_test_b200.channel import Ensemble
+    pairs = [_build(kw) for kw in PERSISTENT_MEMBERS[:2]]
+    try:
+        with Ensemble([p[0] for p in pairs]) as ens:
+            assert ens.mode == _lib.ENSEMBLE_PERSISTENT
+            victim = pairs[1][0]
+            assert victim.lib.diablo_set_wait_bound(victim.ctx, 2000, 1) == _lib.OK
+            ens.step(1)
+            with pytest.raises(_lib.DiabloError) as e:
+                ens.synchronize()
+            assert e.value.status == _lib.ERR_TIMEOUT
+            ens.synchronize()                    # the record was read and cleared
+            assert victim.lib.diablo_set_wait_bound(victim.ctx, 1 << 24, 0) == _lib.OK
+            pairs[0][1].step(1)
+            ref = pairs[1][1]
+            ref.step(1)
+            fids = [_lib.U1, _lib.U2, _lib.U3, _lib.P] + [_lib.TH + n for n in range(ref.params.n_th)]
+            for fid in fids:
+                victim.upload(fid, ref.download(fid), _lib.LAYOUT_FOURIER)
+            t, n, dt = ref.time
+            victim.set_time(t, n, dt)
+            ens.step(2)
+            ens.synchronize()
+            for a, b in pairs:
+                b.step(2)
+            for i, (a, b) in enumerate(pairs):
+                assert _same(a, b), i
+    finally:
+        for a, b in pairs:
+            a.close()
+            b.close()
