@@ -502,7 +502,7 @@ def adjoint_bench(torch, nsteps=50, every=10):
             "forward_ms": t_fwd, "record_ms": t_rec, "adjoint_run_ms": t_run,
             "adjoint_over_forward": t_run / t_fwd,
             "record_plus_adjoint_over_forward": (t_rec + t_run) / t_fwd,
-            "note": "adjoint_run includes recomputing every segment from its checkpoint"}
+            "note": "adjoint_run includes recomputing every segment but the last from its checkpoint (the record keeps the last segment's substep inputs)"}
 
 
 def stats_bench(ch, p, peak, reps=5):

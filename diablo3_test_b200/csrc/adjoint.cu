@@ -9,6 +9,13 @@
 // checkpoint (keeping the velocities entering every substep) and runs the
 // substep adjoints backwards through it.
 
+// Warps (columns) per block of the adjoint column kernels.  The adjoint
+// workload's grids are small (946 columns at 64 x 97 x 64): fewer warps per
+// block spread the columns over more SMs.
+#ifndef ADJ_COLUMN_WARPS
+#define ADJ_COLUMN_WARPS 2
+#endif
+
 int adj_free(diablo_ctx* ctx) {
   diablo_ctx::Tape& T = ctx->tape;
   auto rel = [&](void* p) {
@@ -22,6 +29,7 @@ int adj_free(diablo_ctx* ctx) {
   T.ckpt.clear();
   T.sub.clear();
   T.ready = 0;
+  T.sub_seg = -1;
   return 0;
 }
 
@@ -115,6 +123,7 @@ int adj_alloc(diablo_ctx* ctx, int nsteps, int every) {
     T.ckpt_time.assign(T.nseg + 1, 0.0);
   }
   T.ready = 0;
+  T.sub_seg = -1;
   if (!T.work_ready) {
 #define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
     const int nfs = 3 + ctx->nth;
@@ -177,7 +186,7 @@ int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
     a.ncol = ctx->nkx1 * ctx->nk2;
     a.jstart = ctx->jstart; a.jend = ctx->jend; a.rk = rk;
     Prof pr(ctx, K_OTHER);
-    const int warps = 4;
+    const int warps = ADJ_COLUMN_WARPS;
     dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
     switch (rows_per_lane(ctx->nyp2)) {
 #define X(r) case r: k_adj_column<r><<<grd, blk, 0, ctx->stream>>>(a); break;
@@ -209,7 +218,7 @@ int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
     a.ncol = ctx->nkx1 * ctx->nk2;
     a.jst = ctx->jst[s]; a.jet = ctx->jet[s];
     Prof pr(ctx, K_OTHER);
-    const int warps = 4;
+    const int warps = ADJ_COLUMN_WARPS;
     dim3 blk(32 * warps), grd((a.ncol + warps - 1) / warps);
     switch (rows_per_lane(ctx->nyp2)) {
 #define X(r) case r: k_adj_scalar<r><<<grd, blk, 0, ctx->stream>>>(a); break;
@@ -231,8 +240,14 @@ int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
     Prof pr(ctx, K_OTHER);
     k_adj_nl_prep<<<grid1d(ftot), 256, 0, ctx->stream>>>(a);
   }
-  if ((rc = ifft_batch(ctx, T.pf, T.pp, nprod))) return rc;
-  if ((rc = ifft_batch(ctx, u_in, T.up, nfs))) return rc;
+  {
+    // the product adjoints and the substep's input fields in one batch
+    const double2* src[8 + 3 * DIABLO_MAX_TH + 3 + DIABLO_MAX_TH];
+    double* dst[8 + 3 * DIABLO_MAX_TH + 3 + DIABLO_MAX_TH];
+    for (int q = 0; q < nprod; ++q) { src[q] = T.pf[q]; dst[q] = T.pp[q]; }
+    for (int q = 0; q < nfs; ++q) { src[nprod + q] = u_in[q]; dst[nprod + q] = T.up[q]; }
+    if ((rc = ifft_batch(ctx, src, dst, nprod + nfs))) return rc;
+  }
   {
     AdjNlPointArgs a;
     memset(&a, 0, sizeof(a));
@@ -274,7 +289,8 @@ int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every) {
   if ((rc = ensure_scratch(ctx)) || (rc = ensure_xs64(ctx))) return rc;
   if ((rc = adj_alloc(ctx, nsteps, every))) return rc;
   diablo_ctx::Tape& T = ctx->tape;
-  const int ns = 4 + ctx->nth;   // u1, u2, u3, p, th..
+  const int ns = 4 + ctx->nth, nfs = 3 + ctx->nth;   // u1, u2, u3, p, th..
+  const int slast = (T.nseg - 1) * every;             // first step of the last segment
   for (int s = 0; s < nsteps; ++s) {
     if (s % every == 0) {
       const int k = s / every;
@@ -282,8 +298,23 @@ int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every) {
       T.ckpt_step[k] = ctx->time_step;
       T.ckpt_time[k] = ctx->time;
     }
-    if ((rc = one_step(ctx))) return rc;
+    if (s < slast) {
+      if ((rc = one_step(ctx))) return rc;
+      continue;
+    }
+    // the last segment keeps each substep's input fields as it goes, so that
+    // the adjoint starts on it without recomputing it
+    ctx->time_step += 1;
+    for (int rk = 1; rk <= 3; ++rk) {
+      double2* cu[3 + DIABLO_MAX_TH];
+      for (int q = 0; q < 3; ++q) cu[q] = ctx->st[ctx->cur][q];
+      for (int q = 0; q < ctx->nth; ++q) cu[3 + q] = ctx->st[ctx->cur][4 + q];
+      if ((rc = copy_fields(ctx, &T.sub[((size_t)(s - slast) * 3 + (rk - 1)) * nfs], cu, nfs))) return rc;
+      if ((rc = substep(ctx, rk))) return rc;
+    }
+    ctx->time += ctx->delta_t;
   }
+  T.sub_seg = T.nseg - 1;
   if ((rc = copy_fields(ctx, &T.ckpt[(size_t)T.nseg * ns], ctx->st[ctx->cur], ns))) return rc;
   T.ckpt_step[T.nseg] = ctx->time_step;
   T.ckpt_time[T.nseg] = ctx->time;
@@ -307,22 +338,27 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam) {
     if ((rc = four_in(ctx, lam[q], T.lu[q], false))) return rc;
   for (int q = 0; q < nfs; ++q) CK(cudaMemsetAsync(T.lF[q], 0, fe, ctx->stream));
   for (int k = T.nseg - 1; k >= 0; --k) {
-    // recompute the segment from its checkpoint, keeping each substep's input velocities and scalars
-    if ((rc = copy_fields(ctx, ctx->st[ctx->cur], &T.ckpt[(size_t)k * ns], ns))) return rc;
-    ctx->time_step = T.ckpt_step[k];
-    ctx->time = T.ckpt_time[k];
+    // recompute the segment from its checkpoint, keeping each substep's input
+    // velocities and scalars (the segment whose inputs `sub` already holds --
+    // the last one, straight after the record -- is not recomputed)
     const int s0 = k * T.every, s1 = std::min(T.nsteps, s0 + T.every);
-    for (int s = s0; s < s1; ++s) {
-      ctx->time_step += 1;
-      for (int rk = 1; rk <= 3; ++rk) {
-        double2** keep = &T.sub[((size_t)(s - s0) * 3 + (rk - 1)) * nfs];
-        double2* cu[3 + DIABLO_MAX_TH];
-        for (int q = 0; q < 3; ++q) cu[q] = ctx->st[ctx->cur][q];
-        for (int q = 0; q < ctx->nth; ++q) cu[3 + q] = ctx->st[ctx->cur][4 + q];
-        if ((rc = copy_fields(ctx, keep, cu, nfs))) return rc;
-        if ((rc = substep(ctx, rk))) return rc;
+    if (T.sub_seg != k) {
+      if ((rc = copy_fields(ctx, ctx->st[ctx->cur], &T.ckpt[(size_t)k * ns], ns))) return rc;
+      ctx->time_step = T.ckpt_step[k];
+      ctx->time = T.ckpt_time[k];
+      for (int s = s0; s < s1; ++s) {
+        ctx->time_step += 1;
+        for (int rk = 1; rk <= 3; ++rk) {
+          double2** keep = &T.sub[((size_t)(s - s0) * 3 + (rk - 1)) * nfs];
+          double2* cu[3 + DIABLO_MAX_TH];
+          for (int q = 0; q < 3; ++q) cu[q] = ctx->st[ctx->cur][q];
+          for (int q = 0; q < ctx->nth; ++q) cu[3 + q] = ctx->st[ctx->cur][4 + q];
+          if ((rc = copy_fields(ctx, keep, cu, nfs))) return rc;
+          if ((rc = substep(ctx, rk))) return rc;
+        }
+        ctx->time += ctx->delta_t;
       }
-      ctx->time += ctx->delta_t;
+      T.sub_seg = k;
     }
     for (int s = s1 - 1; s >= s0; --s)
       for (int rk = 3; rk >= 1; --rk)

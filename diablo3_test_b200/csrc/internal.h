@@ -147,6 +147,7 @@ struct diablo_ctx {
   // discrete adjoint: checkpoints of the recorded steps and adjoint work arrays
   struct Tape {
     int ready, nsteps, every, nseg;
+    int sub_seg;                      // segment whose substep inputs `sub` holds (-1: none)
     int step_end, gen_end;
     double time_end;
     std::vector<double2*> ckpt;       // (nseg + 1) x (4 + nth) fields (u1, u2, u3, p, th..); the last is the final state

@@ -268,11 +268,13 @@ int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, do
  * LES, the 'Front' forcing, the scalar filter and mixed precision get
  * DIABLO_ERR_UNSUPPORTED.
  * diablo_adjoint_record advances nsteps steps exactly as diablo_step does and
- * keeps the state (u1, u2, u3, p, th_0..) every `every` steps on the device.
+ * keeps the state (u1, u2, u3, p, th_0..) every `every` steps on the device,
+ * and the input fields of every substep of the last segment.
  * diablo_adjoint_run takes lam[0..3+n_th] = dJ/d(u1, u2, u3, p, th_0..) of the
  * recorded final state for any objective J and overwrites them with dJ/d of the state
  * the recording started from.  It recomputes each segment of `every` steps
- * from its checkpoint and runs the hand-written adjoint of every RK substep
+ * from its checkpoint (not the last one after a fresh record: its substep
+ * inputs are at hand) and runs the hand-written adjoint of every RK substep
  * backwards through it (transposed tridiagonal solves, adjoint transforms,
  * adjoint nonlinear products), and leaves the context at the recorded final
  * state.  lam arrays use the reference Fourier layout (host or device); each

@@ -254,3 +254,30 @@ def test_adjoint_rejects_unsupported_and_stale(cuda_device):
         assert e.value.status == _lib.ERR_STATE
     finally:
         ch.close()
+
+
+def test_adjoint_run_repeats_bit_identically(cuda_device):
+    """The record keeps the last segment's substep inputs, so the first run
+    recomputes every segment but that one; a second run over the same record
+    recomputes all of them.  Both must give the same gradient, bit for bit,
+    with one segment and with several."""
+    p = small_params(nx=32, ny=33, nz=24, re=300.0, n_th=1, grav_y=0.5)
+    gy = grid_for(p)
+    ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=2))
+    try:
+        rng = np.random.default_rng(3)
+        shape = (p.ny + 2, p.nz + 2, p.nx + 2)
+        for nsteps, every in ((5, 2), (3, 3)):
+            x0 = [ch.download(f) for f in _state_fields(p)]
+            ch.adjoint_record(nsteps, every)
+            lam0 = [rng.standard_normal(shape) for _ in x0]
+            a = [l.copy() for l in lam0]
+            b = [l.copy() for l in lam0]
+            ch.adjoint_run(a)
+            ch.adjoint_run(b)
+            for q in range(len(a)):
+                assert np.array_equal(a[q], b[q]), (nsteps, every, q)
+            for f, x in zip(_state_fields(p), x0):
+                ch.upload(f, x, _lib.LAYOUT_FOURIER)
+    finally:
+        ch.close()
