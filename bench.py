@@ -570,16 +570,38 @@ def e2e_round_trip(ch, torch, k, stream, dist=None, world=1):
 
 def profile_other(args, torch):
     """Profiling runs (no JSON line), for launch lists and ncu sections, at
-    --grid: the adjoint with the adjoint workload's parameters (velocity-only
-    FP64; diablo_adjoint_record over --steps steps, a checkpoint every step,
-    then diablo_adjoint_run), and the statistics (diablo_stats --steps times)
-    on the Re_tau = 180 workload's state."""
+    --grid: the adjoint with the adjoint workload's parameters (FP64;
+    diablo_adjoint_record over --steps steps, a checkpoint every step, then
+    diablo_adjoint_run; with --adjoint-scalars N, N scalars with buoyancy and
+    background gradients), the statistics (diablo_stats --steps times) on the
+    Re_tau = 180 workload's state, and the 48-member ensemble (--steps
+    ensemble steps in its default mode)."""
     import dataclasses
     from diablo3_test_b200 import ics, _lib
-    from diablo3_test_b200.config import FP64, MIXED
+    from diablo3_test_b200.config import FP64, MIXED, ChannelParams
     from diablo3_test_b200.grid import create_grid, TANH_ENDS_SYMMETRIC
+    if args.profile_ensemble:
+        from diablo3_test_b200.channel import Ensemble
+        members = [setup_channel(p, gy, f, MIXED) for p, gy, f in ics.config_c5()]
+        ens = Ensemble(members)
+        ens.step(args.warmup)
+        ens.synchronize()
+        t0 = time.perf_counter()
+        ens.step(args.steps)
+        ens.synchronize()
+        print(f"profiling run ensemble (mode {ens.mode}): {time.perf_counter() - t0:.3f} s")
+        ens.close()
+        for ch in members:
+            ch.close()
+        return
     if args.profile_adjoint:
         p, gy, _ = ics.config_c4()      # velocity-only FP64 parameters
+        if args.adjoint_scalars:
+            kw = {f.name: getattr(p, f.name) for f in dataclasses.fields(p)
+                  if f.name not in ("n_th", "pr", "ri", "th_bc_ymin", "th_bc_ymax", "th_bc_ymin_c1",
+                                    "th_bc_ymax_c1", "dthdx", "dthdz", "filter_th", "filter_int")}
+            kw.update(grav_y=0.5, grav_x=0.2)
+            p = ChannelParams.with_scalars(args.adjoint_scalars, **kw)
     else:
         p, gy = ics.config_c2()
     if args.grid:
@@ -592,7 +614,7 @@ def profile_other(args, torch):
     ch.step(args.warmup)
     t0 = time.perf_counter()
     if args.profile_adjoint:
-        ids = (_lib.U1, _lib.U2, _lib.U3, _lib.P)
+        ids = (_lib.U1, _lib.U2, _lib.U3, _lib.P) + tuple(_lib.TH + n for n in range(p.n_th))
         lam = [torch.randn(ch.shape_phys, dtype=torch.float64, device="cuda") for _ in ids]
         ch.adjoint_record(args.steps, 1)
         ch.adjoint_run(lam)
@@ -623,7 +645,7 @@ def run_ours(args):
     else:
         torch.cuda.set_device(local)
     torch.cuda.init()
-    if args.profile_adjoint or args.profile_stats:
+    if args.profile_adjoint or args.profile_stats or args.profile_ensemble:
         profile_other(args, torch)
         return
     if args.profile_les:
@@ -820,6 +842,10 @@ def main():
                     help="profiling: time the dynamic-LES workload instead (mixed unless --precision fp64)")
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="profiling: record and run the adjoint on the --grid workload (velocities, FP64)")
+    ap.add_argument("--profile-ensemble", action="store_true",
+                    help="profiling: --steps steps of the 48-member ensemble")
+    ap.add_argument("--adjoint-scalars", type=int, default=0,
+                    help="profiling: scalars in the --profile-adjoint case")
     ap.add_argument("--profile-stats", action="store_true",
                     help="profiling: save_stats_chan on the --grid workload state")
     args = ap.parse_args()
