@@ -415,6 +415,36 @@ def ensemble_bench(torch, k, warmup=3):
             "kernel_launches_total": launches}
 
 
+def c1_bench(torch, k=200, warmup=5, cpu_steps=2):
+    """Config 1, plain FP64 DNS at the reference test-case shape (64 x 193 x 32,
+    one scalar, Re 1000, dt 1e-3, laminar parabola plus seeded 1% noise):
+    k steps on the GPU (CUDA events on the context's stream), and the CPU
+    oracle on all host cores for cpu_steps whole steps after one warm-up."""
+    from diablo3_test_b200 import ics
+    from diablo3_test_b200.config import FP64
+    from tests.helpers import setup_oracle
+    p, gy = ics.config_c1()
+    fields = ics.laminar_dns(p, gy, seed=1, amp=0.01)
+    ch = setup_channel(p, gy, fields, FP64)
+    stream = torch.cuda.Stream()
+    ch.set_stream(stream.cuda_stream)
+    ch.step(warmup)
+    ms = timed_steps(ch, torch, stream, k)
+    ch.close()
+    pts = p.nx * p.ny * p.nz
+    cores = os.cpu_count() or 1
+    o = setup_oracle(p, gy, fields, workers=cores)
+    o.step(1)
+    t = time.perf_counter()
+    o.step(cpu_steps)
+    t_cpu = (time.perf_counter() - t) / cpu_steps
+    return {"workload": "plain FP64 DNS 64x193x32, one scalar, Re 1000, Pr 1, dt 1e-3, tanh 1.8, "
+                        "laminar parabola + 1% seeded noise",
+            "steps": k, "value": pts * k / (ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms / k,
+            "cpu_oracle": {"value": pts / t_cpu / 1e6, "unit": UNIT, "cores": cores, "s_per_step": t_cpu,
+                           "steps": cpu_steps, "kind": "port"}}
+
+
 def les_bench(torch, k=5, warmup=2):
     """LES workload (config 3: dynamic Smagorinsky, 128 x 129 x 128, Re_tau =
     1000, k^-5/3 random-phase start, LES active from step 1) in FP64 and in
@@ -529,10 +559,14 @@ def stats_bench(ch, p, peak, reps=5):
 def e2e_round_trip(ch, torch, k, stream, dist=None, world=1):
     """End to end through the C ABI with pinned host buffers: each step
     uploads the state (u1, u2, u3, p, scalars) from the host in the reference
-    layout, advances one step and downloads the state again.  Every copy runs
-    on the context's stream, so CUDA events on that stream bracket the copies
-    and the steps; under torchrun every rank runs its replica between barriers
-    and the time is the maximum over ranks."""
+    layout, advances one step and downloads the state into the same host
+    arrays.  The value is diablo_step_host, which overlaps each field's
+    download with the next step's upload of the field before it (the two link
+    directions at once); beside it, the same round trip as separate
+    diablo_upload_state / diablo_step / diablo_download_state calls.  The work
+    is ordered on the context's stream, so CUDA events on that stream bracket
+    the copies and the steps; under torchrun every rank runs its replica
+    between barriers and the time is the maximum over ranks."""
     from diablo3_test_b200 import _lib
     p = ch.params
     ids = [_lib.U1, _lib.U2, _lib.U3, _lib.P] + [_lib.TH + n for n in range(p.n_th)]
@@ -541,30 +575,47 @@ def e2e_round_trip(ch, torch, k, stream, dist=None, world=1):
     for b, fid in zip(bufs, ids):
         ch.download(fid, out=b)
     ch.synchronize()
-    box = (p.ny + 2) * (2 * (p.nz // 3) + 1) * (p.nx // 2) * 16
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
+    # bytes a field moves: its rows k <= 2Nkz of every plane; uploads carry
+    # each row's pad entry (Nx/2 + 1 complex), downloads the Nx/2 modes
+    rows = (p.ny + 2) * (2 * (p.nz // 3) + 1)
+    h2d, d2h = rows * (p.nx // 2 + 1) * 16, rows * (p.nx // 2) * 16
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(k):
-        for b, fid in zip(bufs, ids):
-            ch.upload(fid, b)
-        ch.step(1)
-        for b, fid in zip(bufs, ids):
-            ch.download(fid, out=b)
-    e1.record(stream)
-    e1.synchronize()
-    ch.synchronize()
-    ms = max_over_ranks([e0.elapsed_time(e1)], torch, dist)[0]
+
+    def timed(fn):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ch.synchronize()
+        return max_over_ranks([e0.elapsed_time(e1)], torch, dist)[0]
+
+    ch.step_host(bufs, 1)          # warm-up: the copy streams and staging arrays
+
+    def per_call():
+        for _ in range(k):
+            for b, fid in zip(bufs, ids):
+                ch.upload(fid, b)
+            ch.step(1)
+            for b, fid in zip(bufs, ids):
+                ch.download(fid, out=b)
+
+    ms = timed(lambda: ch.step_host(bufs, k))
+    ms_calls = timed(per_call)
     if dist is not None:
         dist.barrier()
     pts = p.nx * p.ny * p.nz
     return {"value": aggregate_rate(pts, world, k, ms), "unit": UNIT,
-            "h2d_bytes_per_step": box * len(ids) * world,
-            "d2h_bytes_per_step": box * len(ids) * world, "ms_per_step": ms / k,
-            "path": "diablo_upload_state x6 (host, pinned) + diablo_step + diablo_download_state x6",
+            "h2d_bytes_per_step": h2d * len(ids) * world,
+            "d2h_bytes_per_step": d2h * len(ids) * world, "ms_per_step": ms / k,
+            "path": f"diablo_step_host (host, pinned; {len(ids)} fields up and down per step, "
+                    "each field's download overlapping the next step's upload of the field before it)",
+            "separate_calls": {"value": aggregate_rate(pts, world, k, ms_calls), "ms_per_step": ms_calls / k,
+                               "path": f"diablo_upload_state x{len(ids)} + diablo_step + "
+                                       f"diablo_download_state x{len(ids)}"},
             "timing": "CUDA events on the context's stream, max over ranks"}
 
 
@@ -782,6 +833,8 @@ def run_ours(args):
     out["stats"] = stats_bench(chm, p, peak)
     chm.close()
     chd.close()
+    if world == 1 and not args.no_c1:
+        out["c1"] = c1_bench(torch)
     if world == 1 and not args.no_les:
         out["les"] = les_bench(torch)
     if world == 1 and not args.no_adjoint:
@@ -828,6 +881,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost section")
     ap.add_argument("--no-les", action="store_true", help="skip the LES section")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 64x193x32 FP64 DNS section")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default transform tiles")
     ap.add_argument("--ensemble-steps", type=int, default=20,
                     help="timed steps of the 48-member ensemble section (0: skip)")

@@ -58,6 +58,7 @@ SIGNATURES = {
     "diablo_ensemble_stream": (_vp, [_vp]),
     "diablo_ensemble_autotune": (_i, [_vp, _i]),
     "diablo_ensemble_set_mode": (_i, [_vp, _i]),
+    "diablo_step_host": (_i, [_vp, _vp, _i]),
     "diablo_ensemble_mode": (_i, [_vp]),
     "diablo_ensemble_destroy": (_i, [_vp]),
     "diablo_fft_xz_to_fourier": (_i, [_vp, _vp, _vp]),

@@ -119,6 +119,17 @@ class Channel:
         _lib.check(self.lib.diablo_autotune(self.ctx, t), "autotune")
         return tuple(t)
 
+    def step_host(self, bufs, nsteps: int = 1):
+        """nsteps host round trips (diablo_step_host): upload the state from
+        the host arrays bufs (u1, u2, u3, p, then one per scalar; reference
+        Fourier layout, pinned for the full link rate), step, download into
+        the same arrays; field downloads overlap the next uploads."""
+        ns = 4 + self.params.n_th
+        if len(bufs) != ns:
+            raise ValueError(f"{ns} host arrays: u1, u2, u3, p and one per scalar")
+        arr = (ctypes.c_void_p * ns)(*[_ptr(b) for b in bufs])
+        _lib.check(self.lib.diablo_step_host(self.ctx, arr, nsteps), "step_host")
+
     def adjoint_record(self, nsteps: int, every: int):
         """Advance nsteps steps, keeping checkpoints every `every` steps for
         adjoint_run (DNS with velocities and scalars in FP64)."""

@@ -388,6 +388,19 @@ diablo_ctx* diablo_create(const diablo_params* p, const double* gy, int* status)
 int diablo_destroy(diablo_ctx* ctx) {
   if (!ctx) return DIABLO_ERR_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->xfer.ready) {
+    diablo_ctx::Xfer& X = ctx->xfer;
+    cudaStreamSynchronize(X.up);
+    cudaStreamSynchronize(X.down);
+    cudaStreamDestroy(X.up);
+    cudaStreamDestroy(X.down);
+    cudaEventDestroy(X.start);
+    for (int f = 0; f < 4 + DIABLO_MAX_TH; ++f) {
+      if (X.e_up[f]) cudaEventDestroy(X.e_up[f]);
+      if (X.e_conv[f]) cudaEventDestroy(X.e_conv[f]);
+      if (X.e_down[f]) cudaEventDestroy(X.e_down[f]);
+    }
+  }
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& t : ctx->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
   for (auto e : ctx->pool) cudaEventDestroy(e);
@@ -545,6 +558,85 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout) {
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   return 0;
+}
+
+// Streams, events and staging arrays of diablo_step_host (once per context).
+static int ensure_xfer(diablo_ctx* ctx) {
+  diablo_ctx::Xfer& X = ctx->xfer;
+  if (X.ready) return 0;
+  const int ns = 4 + ctx->nth;
+  const size_t stage = (size_t)ctx->nyp2 * ctx->nk2 * (ctx->nxp + 1) * sizeof(double2);
+  int rc;
+  for (int f = 0; f < ns; ++f) {
+    if ((rc = dev_alloc(ctx, (void**)&X.up_stage[f], stage))) return rc;
+    if ((rc = dev_alloc(ctx, (void**)&X.down_stage[f], stage))) return rc;
+  }
+  CK(cudaStreamCreateWithFlags(&X.up, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&X.down, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&X.start, cudaEventDisableTiming));
+  for (int f = 0; f < ns; ++f) {
+    CK(cudaEventCreateWithFlags(&X.e_up[f], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&X.e_conv[f], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&X.e_down[f], cudaEventDisableTiming));
+  }
+  X.ready = 1;
+  return 0;
+}
+
+int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps) {
+  if (!ctx || !bufs || nsteps < 0) return DIABLO_ERR_ARG;
+  const int ns = 4 + ctx->nth;
+  for (int f = 0; f < ns; ++f)
+    if (!bufs[f] || is_device_ptr(bufs[f])) return DIABLO_ERR_ARG;
+  int rc;
+  if ((rc = ensure_bscratch(ctx)) || (rc = ensure_xfer(ctx))) return rc;
+  diablo_ctx::Xfer& X = ctx->xfer;
+  const size_t rowb = (size_t)(ctx->nxp + 1) * sizeof(double2);
+  const size_t tot = (size_t)ctx->nyp2 * ctx->nk2 * ctx->nxp;
+  // the copy streams start after the work already queued on the context's stream
+  CK(cudaEventRecord(X.start, ctx->stream));
+  CK(cudaStreamWaitEvent(X.up, X.start, 0));
+  CK(cudaStreamWaitEvent(X.down, X.start, 0));
+  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    // uploads: field f after its own download of the step before
+    for (int f = 0; f < ns; ++f) {
+      if (s > 0) CK(cudaStreamWaitEvent(X.up, X.e_down[f], 0));
+      CK(cudaMemcpy2DAsync(X.up_stage[f], rowb * ctx->nk2, bufs[f], rowb * (ctx->nz + 2), rowb * ctx->nk2,
+                           ctx->nyp2, cudaMemcpyHostToDevice, X.up));
+      CK(cudaEventRecord(X.e_up[f], X.up));
+    }
+    for (int f = 0; f < ns; ++f) {
+      CK(cudaStreamWaitEvent(ctx->stream, X.e_up[f], 0));
+      Prof pr(ctx, K_OTHER);
+      k_ref_to_four<<<grid1d(tot), 256, 0, ctx->stream>>>(X.up_stage[f], ctx->st[ctx->cur][f], ctx->g,
+                                                           ctx->nxp, ctx->nxp + 1, ctx->nk2, ctx->d_flag);
+    }
+    if ((rc = one_step(ctx))) return rc;
+    // downloads: each field's device-to-host copy as soon as it is packed,
+    // overlapping the next step's upload of the fields before it
+    for (int f = 0; f < ns; ++f) {
+      {
+        Prof pr(ctx, K_OTHER);
+        k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->st[ctx->cur][f], X.down_stage[f], ctx->g,
+                                                             ctx->nxp, ctx->nxp, ctx->nk2);
+      }
+      CK(cudaEventRecord(X.e_conv[f], ctx->stream));
+      CK(cudaStreamWaitEvent(X.down, X.e_conv[f], 0));
+      cudaMemcpy3DParms m = box_parms(bufs[f], rowb, ctx->nz + 2, X.down_stage[f], ctx->nxp * sizeof(double2),
+                                      ctx->nk2, ctx->nxp * sizeof(double2), ctx->nk2, ctx->nyp2,
+                                      cudaMemcpyDeviceToHost);
+      CK(cudaMemcpy3DAsync(&m, X.down));
+      CK(cudaEventRecord(X.e_down[f], X.down));
+    }
+  }
+  // the context's stream ends after the last download
+  for (int f = 0; f < ns && nsteps > 0; ++f) CK(cudaStreamWaitEvent(ctx->stream, X.e_down[f], 0));
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaGetLastError());
+  return bad ? DIABLO_ERR_STATE : 0;
 }
 
 int diablo_download_nu_t(diablo_ctx* ctx, double* buf) {

@@ -162,6 +162,14 @@ struct diablo_ctx {
     double *pp[8 + 3 * DIABLO_MAX_TH], *up[3 + DIABLO_MAX_TH], *lp3[3 + DIABLO_MAX_TH];
     double *d_cn, *d_rmask, *d_pa;    // [3 rk][3 + nth field][3][n], [3 + nth][n], [3][n]
   } tape;
+  // diablo_step_host: copy streams (host-to-device, device-to-host), per-field
+  // staging arrays in the reference layout and their events
+  struct Xfer {
+    cudaStream_t up, down;
+    cudaEvent_t start, e_up[4 + DIABLO_MAX_TH], e_conv[4 + DIABLO_MAX_TH], e_down[4 + DIABLO_MAX_TH];
+    double2 *up_stage[4 + DIABLO_MAX_TH], *down_stage[4 + DIABLO_MAX_TH];
+    int ready;
+  } xfer;
   struct Timed { int slot; cudaEvent_t a, b; };
   std::vector<Timed> timed;        // pending (recorded, not yet read)
   std::vector<cudaEvent_t> pool;   // free events

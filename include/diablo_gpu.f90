@@ -291,6 +291,15 @@ module diablo_gpu
       integer(c_int) :: diablo_tiles
     end function diablo_tiles
 
+    ! ---- the host round trip: bufs(1:4+N_th) hold the addresses of the
+    ! host Fourier arrays u1, u2, u3, p, th_1, ..
+    function diablo_step_host(ctx, bufs, nsteps) bind(C, name="diablo_step_host")
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ctx
+      type(c_ptr), intent(in) :: bufs(*)
+      integer(c_int), value :: nsteps
+      integer(c_int) :: diablo_step_host
+    end function diablo_step_host
     ! ---- ensembles of independent channels
     function diablo_ensemble_create(members, n, status) bind(C, name="diablo_ensemble_create")
       import :: c_ptr, c_int

@@ -120,6 +120,22 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
  * (module array of for/flow.f90:50, set by les_chan, for/les.f90:235-241 and
  * :2241-2262) in the reference's physical layout; host or device `buf`.
  * All zero before the first LES substep, as the reference's array is. */
+/*
+ * The host-authoritative round trip, nsteps times: every step uploads the
+ * state (u1, u2, u3, p, th_0..) from bufs[0..3+n_th], advances one step as
+ * diablo_step does, and downloads the new state into the same arrays -- the
+ * mode in which the Fortran arrays stay authoritative on the host between
+ * steps.  bufs are HOST arrays in the reference Fourier layout (pinned memory
+ * for the full link rate; device pointers return DIABLO_ERR_ARG).  Each
+ * field's download goes out as soon as the field is packed, and the next
+ * step's upload of that field follows it, so the two link directions work at
+ * once on different fields.  The work is ordered after what is already queued
+ * on the context's stream, and the call returns when the last download has
+ * landed; DIABLO_ERR_STATE if an uploaded array broke the layout contract
+ * (nonzero modes Nkx < i < Nxp).  No reference counterpart: the reference's
+ * state never leaves the host.
+ */
+int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps);
 int diablo_download_nu_t(diablo_ctx* ctx, double* buf);
 
 /* for/fft.f90:247-315.  v: physical array, vv: Fourier array, both full
