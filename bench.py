@@ -575,10 +575,10 @@ def e2e_round_trip(ch, torch, k, stream, dist=None, world=1):
     for b, fid in zip(bufs, ids):
         ch.download(fid, out=b)
     ch.synchronize()
-    # bytes a field moves: its rows k <= 2Nkz of every plane; uploads carry
-    # each row's pad entry (Nx/2 + 1 complex), downloads the Nx/2 modes
+    # bytes a field moves each way: its rows k <= 2Nkz of every plane, with
+    # each row's pad entry (Nx/2 + 1 complex)
     rows = (p.ny + 2) * (2 * (p.nz // 3) + 1)
-    h2d, d2h = rows * (p.nx // 2 + 1) * 16, rows * (p.nx // 2) * 16
+    h2d = d2h = rows * (p.nx // 2 + 1) * 16
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 

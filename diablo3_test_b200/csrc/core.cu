@@ -398,7 +398,8 @@ int diablo_destroy(diablo_ctx* ctx) {
     for (int f = 0; f < 4 + DIABLO_MAX_TH; ++f) {
       if (X.e_up[f]) cudaEventDestroy(X.e_up[f]);
       if (X.e_conv[f]) cudaEventDestroy(X.e_conv[f]);
-      if (X.e_down[f]) cudaEventDestroy(X.e_down[f]);
+      for (int c = 0; c < 4; ++c)
+        if (X.e_down[f][c]) cudaEventDestroy(X.e_down[f][c]);
     }
   }
   for (void* p : ctx->allocs) cudaFree(p);
@@ -570,6 +571,9 @@ static int ensure_xfer(diablo_ctx* ctx) {
   for (int f = 0; f < ns; ++f) {
     if ((rc = dev_alloc(ctx, (void**)&X.up_stage[f], stage))) return rc;
     if ((rc = dev_alloc(ctx, (void**)&X.down_stage[f], stage))) return rc;
+    // the rows' pad entries (i = Nxp) are never written by the packing
+    // kernel: zero, as the reference's zeroed modes above Nkx
+    CK(cudaMemsetAsync(X.down_stage[f], 0, stage, ctx->stream));
   }
   CK(cudaStreamCreateWithFlags(&X.up, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&X.down, cudaStreamNonBlocking));
@@ -577,7 +581,7 @@ static int ensure_xfer(diablo_ctx* ctx) {
   for (int f = 0; f < ns; ++f) {
     CK(cudaEventCreateWithFlags(&X.e_up[f], cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&X.e_conv[f], cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&X.e_down[f], cudaEventDisableTiming));
+    for (int c = 0; c < 4; ++c) CK(cudaEventCreateWithFlags(&X.e_down[f][c], cudaEventDisableTiming));
   }
   X.ready = 1;
   return 0;
@@ -598,12 +602,24 @@ int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps) {
   CK(cudaStreamWaitEvent(X.up, X.start, 0));
   CK(cudaStreamWaitEvent(X.down, X.start, 0));
   CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  // Each field moves in four chunks of planes, so that a chunk's upload can
+  // follow its own download while the next chunks are still coming back: the
+  // pipeline fills and drains by a quarter field, not a whole one.
+  constexpr int NCH = 4;
+  auto chunk = [&](int c) { return (ctx->nyp2 * c) / NCH; };   // first plane of chunk c
+  const size_t hplane = (size_t)(ctx->nz + 2) * (ctx->nxp + 1);  // complex entries per host plane
+  const size_t dplane = (size_t)ctx->nk2 * (ctx->nxp + 1);       // ... per staging plane
   for (int s = 0; s < nsteps; ++s) {
-    // uploads: field f after its own download of the step before
+    // uploads: each chunk after its own download of the step before
     for (int f = 0; f < ns; ++f) {
-      if (s > 0) CK(cudaStreamWaitEvent(X.up, X.e_down[f], 0));
-      CK(cudaMemcpy2DAsync(X.up_stage[f], rowb * ctx->nk2, bufs[f], rowb * (ctx->nz + 2), rowb * ctx->nk2,
-                           ctx->nyp2, cudaMemcpyHostToDevice, X.up));
+      for (int c = 0; c < NCH; ++c) {
+        const int j0 = chunk(c), nj = chunk(c + 1) - j0;
+        if (nj <= 0) continue;
+        if (s > 0) CK(cudaStreamWaitEvent(X.up, X.e_down[f][c], 0));
+        CK(cudaMemcpy2DAsync(X.up_stage[f] + (size_t)j0 * dplane, rowb * ctx->nk2,
+                             reinterpret_cast<const double2*>(bufs[f]) + (size_t)j0 * hplane,
+                             rowb * (ctx->nz + 2), rowb * ctx->nk2, nj, cudaMemcpyHostToDevice, X.up));
+      }
       CK(cudaEventRecord(X.e_up[f], X.up));
     }
     for (int f = 0; f < ns; ++f) {
@@ -613,25 +629,33 @@ int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps) {
                                                            ctx->nxp, ctx->nxp + 1, ctx->nk2, ctx->d_flag);
     }
     if ((rc = one_step(ctx))) return rc;
-    // downloads: each field's device-to-host copy as soon as it is packed,
-    // overlapping the next step's upload of the fields before it
+    // downloads: each field's chunks as soon as the field is packed,
+    // overlapping the next step's uploads of the chunks before them
     for (int f = 0; f < ns; ++f) {
       {
         Prof pr(ctx, K_OTHER);
         k_four_to_ref<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->st[ctx->cur][f], X.down_stage[f], ctx->g,
-                                                             ctx->nxp, ctx->nxp, ctx->nk2);
+                                                             ctx->nxp, ctx->nxp + 1, ctx->nk2);
       }
       CK(cudaEventRecord(X.e_conv[f], ctx->stream));
       CK(cudaStreamWaitEvent(X.down, X.e_conv[f], 0));
-      cudaMemcpy3DParms m = box_parms(bufs[f], rowb, ctx->nz + 2, X.down_stage[f], ctx->nxp * sizeof(double2),
-                                      ctx->nk2, ctx->nxp * sizeof(double2), ctx->nk2, ctx->nyp2,
-                                      cudaMemcpyDeviceToHost);
-      CK(cudaMemcpy3DAsync(&m, X.down));
-      CK(cudaEventRecord(X.e_down[f], X.down));
+      // rows k <= 2Nkz of a plane, pad entries included, are contiguous in
+      // the host array: 2D copies of such blocks (the upload's form)
+      for (int c = 0; c < NCH; ++c) {
+        const int j0 = chunk(c), nj = chunk(c + 1) - j0;
+        if (nj <= 0) continue;
+        CK(cudaMemcpy2DAsync(reinterpret_cast<double2*>(bufs[f]) + (size_t)j0 * hplane, rowb * (ctx->nz + 2),
+                             X.down_stage[f] + (size_t)j0 * dplane, rowb * ctx->nk2, rowb * ctx->nk2, nj,
+                             cudaMemcpyDeviceToHost, X.down));
+        CK(cudaEventRecord(X.e_down[f][c], X.down));
+      }
     }
   }
   // the context's stream ends after the last download
-  for (int f = 0; f < ns && nsteps > 0; ++f) CK(cudaStreamWaitEvent(ctx->stream, X.e_down[f], 0));
+  if (nsteps > 0) {
+    CK(cudaEventRecord(X.start, X.down));
+    CK(cudaStreamWaitEvent(ctx->stream, X.start, 0));
+  }
   int bad = 0;
   CK(cudaMemcpyAsync(&bad, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));

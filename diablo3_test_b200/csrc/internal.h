@@ -166,7 +166,8 @@ struct diablo_ctx {
   // staging arrays in the reference layout and their events
   struct Xfer {
     cudaStream_t up, down;
-    cudaEvent_t start, e_up[4 + DIABLO_MAX_TH], e_conv[4 + DIABLO_MAX_TH], e_down[4 + DIABLO_MAX_TH];
+    cudaEvent_t start, e_up[4 + DIABLO_MAX_TH], e_conv[4 + DIABLO_MAX_TH];
+    cudaEvent_t e_down[4 + DIABLO_MAX_TH][4];   // per field and plane chunk
     double2 *up_stage[4 + DIABLO_MAX_TH], *down_stage[4 + DIABLO_MAX_TH];
     int ready;
   } xfer;

@@ -132,8 +132,9 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
  * once on different fields.  The work is ordered after what is already queued
  * on the context's stream, and the call returns when the last download has
  * landed; DIABLO_ERR_STATE if an uploaded array broke the layout contract
- * (nonzero modes Nkx < i < Nxp).  No reference counterpart: the reference's
- * state never leaves the host.
+ * (nonzero modes Nkx < i < Nxp).  The downloads write the rows' pad entries
+ * (i = Nxp) as zero, as the reference's transform leaves its modes above Nkx.
+ * No reference counterpart: the reference's state never leaves the host.
  */
 int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps);
 int diablo_download_nu_t(diablo_ctx* ctx, double* buf);
