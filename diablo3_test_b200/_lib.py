@@ -34,7 +34,7 @@ STAT_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw",
                  "uu_dudx", "vv_dvdy", "wu_dwdx", "vu_dvdx", "uv_dudy", "wv_dwdy",
                  "dudy", "dwdy", "cp", "shear", "omega_x", "omega_y", "omega_z",
                  "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
-STAT_TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
+STAT_TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss", "kappa_sgs")
 STAT_SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b", "bpe")
 STAT_ZSTAR = ("shear2", "thw", "chi", "epsilon", "TKE", "KE")
 

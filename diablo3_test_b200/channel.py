@@ -51,7 +51,7 @@ MEAN_H5_NAMES = {
     "omega_x": "omega_x", "omega_y": "omega_z", "omega_z": "omega_y", "epsilon": "epsilon",
     "epsilon_m": "epsilon_m", "nu_sgs": "nu_sgs", "eps_sgs2": "eps_sgs2",
     "thme": "thme{:02d}", "dthdy": "dthdz{:02d}", "thrms": "thrms{:02d}", "thv": "thw{:02d}",
-    "thv_m": "thw{:02d}_m", "pe_diss": "pe_diss{:02d}", "spectrum": "FTx_uu",
+    "thv_m": "thw{:02d}_m", "pe_diss": "pe_diss{:02d}", "kappa_sgs": "kappa_sgs", "spectrum": "FTx_uu",
     "u1y_left_b": "u1z_x0", "time": "time", "bpe": "BPE", "th1_pdf": "th1PDF",
     "th1_bin": "th1bin", "zstar": "<name>_zstar",
 }

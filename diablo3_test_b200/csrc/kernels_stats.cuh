@@ -199,23 +199,30 @@ __global__ void __launch_bounds__(STAT_THREADS) k_stats_modes(const __grid_const
   block_sum_store<NQ>(acc, nq, a.part + ((size_t)j * a.nslice + blockIdx.x) * STAT_NQ);
 }
 
-// compute_TKE_diss_les (for/statistics.f90:2054-2120) and the plane mean of
-// nu_t (nu_t_mean, for/les.f90:927-937) from physical u1, u2, u3 and nu_t
+// compute_TKE_diss_les (for/statistics.f90:2054-2120), the plane mean of
+// nu_t (nu_t_mean, for/les.f90:927-937) and of each scalar's kappa_t
+// (kappa_t_mean, :1420-1448) from physical u1, u2, u3, nu_t and kappa_t
 // ([j][k][i], Nz x Nx per plane).  Slot 0: sum of nu_t over plane j
-// (1 <= j <= Ny); slot 1: sum of the GY dissipation term `temp` (2 <= j <= Ny).
+// (1 <= j <= Ny); slot 1: sum of the GY dissipation term `temp` (2 <= j <= Ny);
+// slot 2 + n: sum of scalar n's kappa_t (FP32 arrays when kap32 is set).
+#define STAT_LQ (2 + DIABLO_MAX_TH)
 struct StatsLesArgs {
   const double* u[3];
   const double* nu_t;
+  const void* kap[DIABLO_MAX_TH];
+  int nth, kap32;
   const double* dy;
   const double* dyf;
   int nyp, nslice;
   size_t pn;            // Nz * Nx
-  double* part;         // [Ny+2][nslice][2]
+  double* part;         // [Ny+2][nslice][STAT_LQ]
 };
 
 static __global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_constant__ StatsLesArgs a) {
   const int j = blockIdx.y;
-  double acc[2] = {0.0, 0.0};
+  double acc[STAT_LQ];
+#pragma unroll
+  for (int q = 0; q < STAT_LQ; ++q) acc[q] = 0.0;
   if (j >= 1 && j <= a.nyp) {
     const size_t pn = a.pn;
     const double* u1 = a.u[0];
@@ -232,6 +239,11 @@ static __global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < pn; i += (size_t)a.nslice * blockDim.x) {
       const size_t o = (size_t)j * pn + i, op = o + pn, om = o - pn;
       acc[0] += nt[o];
+#pragma unroll
+      for (int n = 0; n < DIABLO_MAX_TH; ++n)
+        if (n < a.nth)
+          acc[2 + n] += a.kap32 ? (double)static_cast<const float*>(a.kap[n])[o]
+                                : static_cast<const double*>(a.kap[n])[o];
       if (j >= 2) {
         const double t2 = u2[o] * ((0.5 * (nt[o] + nt[op]) * (u2[op] - u2[o]) / a.dyf[j] -
                                     0.5 * (nt[o] + nt[om]) * (u2[o] - u2[om]) / a.dyf[j - 1]) /
@@ -240,7 +252,7 @@ static __global__ void __launch_bounds__(STAT_THREADS) k_stats_les(const __grid_
       }
     }
   }
-  block_sum_store<2>(acc, 2, a.part + ((size_t)j * a.nslice + blockIdx.x) * 2);
+  block_sum_store<STAT_LQ>(acc, 2 + a.nth, a.part + ((size_t)j * a.nslice + blockIdx.x) * STAT_LQ);
 }
 
 // Z-line statistics of the x-inhomogeneous branch from physical u1, u2, u3

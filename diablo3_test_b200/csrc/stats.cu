@@ -38,7 +38,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   // every sub-buffer (the double2 rows among them) starts 16-byte aligned
   auto even = [](size_t v) { return (v + 1) & ~(size_t)1; };
   const size_t n_part = even((size_t)nyp2 * nslice * STAT_NQ), n_means = even((size_t)nyp2 * (4 + nth));
-  const size_t n_spec = even((size_t)nyp2 * nkx1), n_les = even((size_t)nyp2 * lslice * 2);
+  const size_t n_spec = even((size_t)nyp2 * nkx1), n_les = even((size_t)nyp2 * lslice * STAT_LQ);
   const size_t n_rows = (size_t)nyp2 * (3 + nth) * nkx1 * 2, n_bpe = even((size_t)nx);
   const size_t n_zs = even((size_t)(1 + ZS_N) * nx);
   const size_t n_xy = (size_t)XY_N * nyp2 * nx;
@@ -133,6 +133,12 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
     memset(&b, 0, sizeof(b));
     for (int q = 0; q < 3; ++q) b.u[q] = uphys[q];
     b.nu_t = nt;
+    // kappa_t: the AMD scalar model's own (model 5, in the LES precision),
+    // else nu_t (for/les.f90:1130-1146)
+    b.nth = nth;
+    const bool amd = p.les_model_type == 5;
+    b.kap32 = (amd && L.nu_t_fp32) ? 1 : 0;
+    for (int n = 0; n < nth; ++n) b.kap[n] = amd ? (const void*)L.kap[n] : (const void*)nt;
     b.dy = ctx->d_dy;
     b.dyf = ctx->d_dyf;
     b.nyp = ny;
@@ -295,7 +301,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   };
   auto LQ = [&](int j, int q) {
     double s = 0.0;
-    for (int sl = 0; sl < lslice; ++sl) s += lpart[((size_t)j * lslice + sl) * 2 + q];
+    for (int sl = 0; sl < lslice; ++sl) s += lpart[((size_t)j * lslice + sl) * STAT_LQ + q];
     return s;
   };
   const std::vector<double>&gy = ctx->h_gy, &gyf = ctx->h_gyf, &dy = ctx->h_dy, &dyf = ctx->h_dyf;
@@ -464,6 +470,7 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
       tset(DIABLO_STAT_THRMS, j, sqrt(Q(j, q0)));
       tset(DIABLO_STAT_THV, j, Q(j, q0 + 1));
       tset(DIABLO_STAT_PE_DISS, j, Q(j, q0 + 2));
+      tset(DIABLO_STAT_KAPPA_SGS, j, les ? LQ(j, 2 + n) / nn : 0.0);
       // thv_m (:377-385), gx(i) = i Lx / Nx
       double s = 0.0;
       for (int i = 0; i < nx; ++i)

@@ -182,7 +182,9 @@ int diablo_filter_chan(diablo_ctx* ctx, int n);
  * last scalar's stand; empty bins are NaN, 0/0 as in the reference).  Not
  * computed: HDF5/movie output.  nu_sgs is the
  * plane mean of the nu_t of the most recent LES substep and eps_sgs2 uses that
- * nu_t, as compute_TKE_diss_les does; both are 0 without LES.
+ * nu_t, as compute_TKE_diss_les does; a scalar's kappa_sgs is the plane mean
+ * of its kappa_t of that substep (les_chan_th's kappa_t_mean,
+ * for/les.f90:1420-1448, which writes scalar 1's); all are 0 without LES.
  * Layout of `out` (diablo_stats_size doubles):
  *   profile q of the velocity set at out[q*Ny + j-1], q < DIABLO_STAT_NPROF;
  *   then, for scalar n, profile r at out[(NPROF + n*NTHPROF + r)*Ny + j-1];
@@ -204,7 +206,7 @@ enum {
 };
 enum {
   DIABLO_STAT_THME = 0, DIABLO_STAT_DTHDY, DIABLO_STAT_THRMS, DIABLO_STAT_THV,
-  DIABLO_STAT_THV_M, DIABLO_STAT_PE_DISS, DIABLO_STAT_NTHPROF
+  DIABLO_STAT_THV_M, DIABLO_STAT_PE_DISS, DIABLO_STAT_KAPPA_SGS, DIABLO_STAT_NTHPROF
 };
 enum {
   DIABLO_STAT_TIME = 0, DIABLO_STAT_DT, DIABLO_STAT_UBULK, DIABLO_STAT_URMS_B,

@@ -44,7 +44,7 @@ VEL_PROFILES = ("ume", "vme", "wme", "mke", "urms", "vrms", "wrms", "uv", "uw", 
                 "uu_dudx", "vv_dvdy", "wu_dwdx", "vu_dvdx", "uv_dudy", "wv_dwdy",
                 "dudy", "dwdy", "cp", "shear", "omega_x", "omega_y", "omega_z",
                 "epsilon", "epsilon_m", "nu_sgs", "eps_sgs2")
-TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss")
+TH_PROFILES = ("thme", "dthdy", "thrms", "thv", "thv_m", "pe_diss", "kappa_sgs")
 SCALARS = ("time", "dt", "ubulk", "urms_b", "vrms_b", "wrms_b", "u1y_left_b")
 
 
@@ -82,11 +82,13 @@ def _krows(kfac, k0):
     return kfac if kfac.shape[1] == 1 else kfac[:, k0:, :]
 
 
-def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> dict:
+def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True, kappa_t=None) -> dict:
     """Statistics of the oracle's current (Fourier) state.  Applies the
     velocity and scalar wall values first, as the reference does (:63-64),
     which changes the oracle's state the same way.  ``nu_t`` (reference
-    physical layout) enables the LES rows nu_sgs and eps_sgs2.
+    physical layout) enables the LES rows nu_sgs and eps_sgs2; ``kappa_t`` (one
+    such array per scalar) each scalar's kappa_sgs, the plane mean of its
+    kappa_t (kappa_t_mean, for/les.f90:1420-1448).
     ``homogeneous_x = False`` is the branch of IC types 5-8: z-line averages
     ume_xy(x, y) etc. as the means (when Nz > 1), the x derivatives of epsilon
     without the kz = 0 row, compute_MKE_diss and the production terms that use
@@ -331,6 +333,10 @@ def save_stats_chan(o: OracleChannel, nu_t=None, homogeneous_x: bool = True) -> 
             prof["pe_diss"][j] = np.sum((r1[j] + p.dthdx[n]) ** 2 + r2[j] ** 2
                                         + (r3[j] + p.dthdz[n]) ** 2) / NN
         prof["thme"][:] = tm
+        if kappa_t is not None:
+            kt = kappa_t[n][:, :Nz, :Nx]
+            for j in range(1, Nyp + 1):
+                prof["kappa_sgs"][j] = np.sum(kt[j]) / NN
         if n == 0:
             u1y_left = np.zeros(ny2)
             for j in range(1, Nyp + 1):

@@ -113,8 +113,10 @@ def test_stats_les_match_oracle(cuda_device, model, precision):
         nu_t = ch.download_nu_t()
         o = _oracle_from_gpu(ch, p, gy)
         sg = ch.stats()
-        so = save_stats_chan(o, nu_t=nu_t)
+        # kappa_t = nu_t for the Smagorinsky models (for/les.f90:1130-1146)
+        so = save_stats_chan(o, nu_t=nu_t, kappa_t=[nu_t] * p.n_th)
         _compare(sg, so, p)
+        assert np.abs(sg["th"][0]["kappa_sgs"]).max() > 0
         assert np.abs(sg["profiles"]["nu_sgs"]).max() > 0
         assert np.abs(sg["profiles"]["eps_sgs2"]).max() > 0
     finally:
@@ -160,7 +162,7 @@ def test_stats_nonhomogeneous_les_matches_oracle(cuda_device):
         nu_t = ch.download_nu_t()
         o = _oracle_from_gpu(ch, p, gy)
         sg = ch.stats(homogeneous_x=False)
-        so = save_stats_chan(o, nu_t=nu_t, homogeneous_x=False)
+        so = save_stats_chan(o, nu_t=nu_t, homogeneous_x=False, kappa_t=[nu_t] * p.n_th)
         _compare(sg, so, p)
     finally:
         ch.close()
