@@ -128,7 +128,7 @@ int adj_alloc(diablo_ctx* ctx, int nsteps, int every) {
 #define AL(ptr, bytes) if ((rc = dev_alloc(ctx, (void**)&(ptr), (bytes)))) return rc
     const int nfs = 3 + ctx->nth;
     for (int q = 0; q < nfs + 1; ++q) { AL(T.lu[q], fe); AL(T.ou[q], fe); }
-    for (int q = 0; q < nfs; ++q) { AL(T.lF[q], fe); AL(T.oF[q], fe); AL(T.lnl[q], fe); AL(T.lf3[q], fe);
+    for (int q = 0; q < nfs; ++q) { AL(T.lF[q], fe); AL(T.oF[q], fe); AL(T.lnl[q], fe);
                                     AL(T.up[q], pe); AL(T.lp3[q], pe); }
     for (int q = 0; q < 8 + 3 * ctx->nth; ++q) { AL(T.pf[q], fe); AL(T.pp[q], pe); }
     AL(T.d_cn, (size_t)9 * nfs * ctx->nyp2 * sizeof(double));
@@ -262,17 +262,13 @@ int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
     Prof pr(ctx, K_OTHER);
     k_adj_nl_point<<<grid1d(ptot), 256, 0, ctx->stream>>>(a);
   }
-  if ((rc = fft_batch(ctx, T.lp3, T.lf3, nfs))) return rc;
   {
-    AdjAccArgs a;
-    memset(&a, 0, sizeof(a));
-    for (int f = 0; f < 3; ++f) { a.ou[f] = T.ou[f]; a.add[f] = T.lf3[f]; }
-    for (int s = 0; s < nth; ++s) { a.ou[3 + s] = T.ou[4 + s]; a.add[3 + s] = T.lf3[3 + s]; }
-    a.scale = (double)ctx->nx * ctx->nz;
-    a.g = fg;
-    a.nf = nfs;
-    Prof pr(ctx, K_OTHER);
-    k_adj_acc<<<grid1d(ftot), 256, 0, ctx->stream>>>(a);
+    // ou += w(m) Nx Nz F(lambda physical): the inverse transform's transpose,
+    // accumulated by the z forward transform itself
+    double2* acc[3 + DIABLO_MAX_TH];
+    for (int f = 0; f < 3; ++f) acc[f] = T.ou[f];
+    for (int s = 0; s < nth; ++s) acc[3 + s] = T.ou[4 + s];
+    if ((rc = fft_batch_t<double>(ctx, T.lp3, acc, nfs, (double)ctx->nx * ctx->nz))) return rc;
   }
   CK(cudaGetLastError());
   for (int q = 0; q < nfs + 1; ++q) std::swap(T.lu[q], T.ou[q]);

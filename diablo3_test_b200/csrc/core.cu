@@ -190,7 +190,7 @@ int ifft_batch_t(diablo_ctx* ctx, const double2* const* four, P* const* phys, in
 }
 
 template <typename P>
-int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int nf) {
+int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int nf, double acc_scale) {
   typedef typename CT<P>::C C;
   const C* tz = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tz64 : (const void*)ctx->tz32);
   const C* tm = (const C*)(sizeof(P) == 8 ? (const void*)ctx->tm64 : (const void*)ctx->tm32);
@@ -218,6 +218,7 @@ int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int
     za.tw = tz;
     za.kz = ctx->d_kz;
     za.scale = 1.0 / ctx->nz;
+    za.acc_scale = acc_scale;
     int rc;
     { Prof pr(ctx, K_OTHER); if ((rc = launch_xfwd<P, false>(xa, ctx->M, ctx->nyp2, m, ctx->stream))) return rc; }
     { Prof pr(ctx, K_OTHER); if ((rc = launch_zfwd<C, double2, false>(za, ctx->nz, m, ctx->stream))) return rc; }
@@ -227,8 +228,8 @@ int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int
 
 template int ifft_batch_t<double>(diablo_ctx*, const double2* const*, double* const*, int);
 template int ifft_batch_t<float>(diablo_ctx*, const double2* const*, float* const*, int);
-template int fft_batch_t<double>(diablo_ctx*, const double* const*, double2* const*, int);
-template int fft_batch_t<float>(diablo_ctx*, const float* const*, double2* const*, int);
+template int fft_batch_t<double>(diablo_ctx*, const double* const*, double2* const*, int, double);
+template int fft_batch_t<float>(diablo_ctx*, const float* const*, double2* const*, int, double);
 
 int ifft_batch(diablo_ctx* ctx, const double2* const* four, double* const* phys, int nf) {
   return ifft_batch_t<double>(ctx, four, phys, nf);

@@ -157,7 +157,7 @@ struct diablo_ctx {
     // lambdas of the state [u1, u2, u3, p, th..], of cf and NL [u1, u2, u3, th..],
     // the product adjoints (8 + 3 nth) and the physical fields of the substep
     double2 *lu[4 + DIABLO_MAX_TH], *ou[4 + DIABLO_MAX_TH], *lF[3 + DIABLO_MAX_TH], *oF[3 + DIABLO_MAX_TH];
-    double2 *lnl[3 + DIABLO_MAX_TH], *pf[8 + 3 * DIABLO_MAX_TH], *lf3[3 + DIABLO_MAX_TH];
+    double2 *lnl[3 + DIABLO_MAX_TH], *pf[8 + 3 * DIABLO_MAX_TH];
     int work_ready;
     double *pp[8 + 3 * DIABLO_MAX_TH], *up[3 + DIABLO_MAX_TH], *lp3[3 + DIABLO_MAX_TH];
     double *d_cn, *d_rmask, *d_pa;    // [3 rk][3 + nth field][3][n], [3 + nth][n], [3][n]
@@ -238,8 +238,10 @@ bool is_device_ptr(const void* p);
 // element type P (double or float); instantiated for both in core.cu
 template <typename P>
 int ifft_batch_t(diablo_ctx* ctx, const double2* const* four, P* const* phys, int nf);
+// acc_scale != 0 (FP64 output only): four[f] += w(m) acc_scale F(phys[f])
+// instead of four[f] = F(phys[f]), w(0) = 1, w(m > 0) = 2
 template <typename P>
-int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int nf);
+int fft_batch_t(diablo_ctx* ctx, const P* const* phys, double2* const* four, int nf, double acc_scale = 0.0);
 int ifft_batch(diablo_ctx* ctx, const double2* const* four, double* const* phys, int nf);
 int fft_batch(diablo_ctx* ctx, const double* const* phys, double2* const* four, int nf);
 int les_active(const diablo_ctx* ctx);

@@ -459,22 +459,3 @@ static __global__ void k_adj_nl_point(const __grid_constant__ AdjNlPointArgs a) 
   a.o3[idx] = l3;
 }
 
-// ou[f] += w(m) Nx Nz * F(lambda u_f physical)  (the inverse transform's transpose)
-struct AdjAccArgs {
-  double2* ou[3 + DIABLO_MAX_TH];
-  const double2* add[3 + DIABLO_MAX_TH];
-  double scale;     // Nx Nz
-  FGeom g;
-  int nf;
-};
-
-static __global__ void k_adj_acc(const __grid_constant__ AdjAccArgs a) {
-  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const size_t tot = (size_t)a.g.n * a.g.ps;
-  if (idx >= tot) return;
-  const int kq = idx % a.g.kp;
-  if (kq >= a.g.nk2) return;
-  const int m = (idx / a.g.kp) % a.g.nkx1;
-  const double w = a.scale * (m > 0 ? 2.0 : 1.0);
-  for (int f = 0; f < a.nf; ++f) a.ou[f][idx] = a.ou[f][idx] + w * a.add[f][idx];
-}

@@ -95,6 +95,11 @@ template <typename C, typename CO> struct ZFwdArgs {
   const double* dyf;
   double* prof;
   size_t fps;
+  // plain form, FP64 output: nonzero makes the kernel accumulate,
+  // dst[kp] += w(m) acc_scale X^[k] / Nz with w(0) = 1, w(m > 0) = 2 (the
+  // transpose of the dealiased inverse transform, which the discrete adjoint
+  // adds into its lambdas)
+  double acc_scale;
 };
 
 // Blocks per SM the FP32 z-forward and x-inverse kernels' register caps are
@@ -211,6 +216,23 @@ __global__ void __launch_bounds__(N2* S, sizeof(C) == 8 ? ZFWD32_MIN_BLOCKS : 1)
             v.y += ((Up + U0) * vp.y - (U0 + Um) * vc.y) * id;
             dst64[kp] = v;
           }
+        }
+      }
+    }
+    return;
+  }
+  if (!COMBINE && a.acc_scale != 0.0) {
+    const int m = (a.q0 + q) % a.g.nkx1;
+    const double w = a.acc_scale * (m > 0 ? 2.0 : 1.0);
+    double2* dacc = reinterpret_cast<double2*>(dst);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      int k1 = t + r * N2;
+      if (k1 < N1) {
+#pragma unroll
+        for (int k2 = 0; k2 < N2; ++k2) {
+          int kp = z_pack(k1 + N1 * k2, a.g.nz, a.g.nkz);
+          if (kp >= 0) dacc[kp] = dacc[kp] + w * cvt<double2>(sc * ra[r][k2]);
         }
       }
     }
