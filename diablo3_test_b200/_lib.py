@@ -70,6 +70,7 @@ SIGNATURES = {
     "diablo_filter_chan": (_i, [_vp, _i]),
     "diablo_stats_size": (_i, [_vp]),
     "diablo_stats": (_i, [_vp, _i, ctypes.POINTER(_d), _i]),
+    "diablo_les_eps_sgs1": (_i, [_vp, ctypes.POINTER(_d), _i]),
     "diablo_set_precision": (_i, [_vp, _i]),
     "diablo_get_time": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_i), ctypes.POINTER(_d)]),
     "diablo_set_time": (_i, [_vp, _d, _i, _d]),

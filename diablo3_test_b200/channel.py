@@ -192,6 +192,17 @@ class Channel:
             del res["scalars"]["bpe"]
         return res
 
+    def les_eps_sgs1(self) -> np.ndarray:
+        """eps_sgs1 of les_chan (for/les.f90:924-1068), (Ny,) on GY points:
+        requested by :meth:`stats` on an LES channel and formed at the first
+        substep of the next step, as the reference's flag_save_LES does.
+        Raises DiabloError (DIABLO_ERR_STATE) when no step has run since the
+        request."""
+        out = np.zeros(self.params.ny)
+        _lib.check(self.lib.diablo_les_eps_sgs1(self.ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                out.size), "les_eps_sgs1")
+        return out
+
     # -- reference surface ---------------------------------------------
     def fft_xz_to_fourier(self, v, vv):
         _lib.check(self.lib.diablo_fft_xz_to_fourier(self.ctx, _ptr(v), _ptr(vv)), "fft_xz_to_fourier")

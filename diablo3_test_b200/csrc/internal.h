@@ -143,6 +143,10 @@ struct diablo_ctx {
     double* dp[DYN_NF];
     double2* df[DYN_NF];
     double* dsums;
+    // eps_sgs1 (for/les.f90:924-1068): requested by a statistics save, formed
+    // at the next step's first substep; blank when the LES gate is still off
+    double* d_eps;
+    int eps_req, eps_ready, eps_blank;
   } les;
   // discrete adjoint: checkpoints of the recorded steps and adjoint work arrays
   struct Tape {

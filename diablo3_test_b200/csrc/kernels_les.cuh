@@ -329,6 +329,89 @@ static __global__ void k_les_div(LesDivArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// eps_sgs1 (for/les.f90:924-1068): the plane mean of u_i times the SGS force
+// F_i that k_les_div adds to cf_i, formed at the first substep of a step that
+// follows a statistics save.  The reference transforms each F_i to physical
+// space and sums u_i F_i over the plane; both factors are band-limited, so the
+// plane mean is the Parseval sum over the retained modes (weight 2 for kx > 0,
+// the kx = 0 column through the Hermitian part of u).  F1 and F3 live on GYF
+// planes and are averaged onto GY plane j from planes j and j - 1; F2 (with
+// the explicit cross terms ikx T5 + ikz T6) is on GY.  One block per plane,
+// out[j] for j = 2..Nyp and 0 elsewhere.
+struct EpsSgsArgs {
+  const double2* cu[3];
+  const double2* T[7];
+  const double* kx;
+  const double* kz;
+  const double* dyf;
+  const double* sf;   // delta_yf
+  const double* sg;   // delta_y
+  FGeom g;
+  double* out;
+};
+
+static constexpr int EPS_THREADS = 256;
+
+static __global__ void __launch_bounds__(EPS_THREADS) k_eps_sgs1(EpsSgsArgs a) {
+  const int j = blockIdx.x;
+  const int nyp = a.g.nyp;
+  const size_t ps = a.g.ps;
+  double acc = 0.0;
+  if (j >= 2 && j <= nyp) {
+    const int nmodes = a.g.nkx1 * a.g.nk2;
+    for (int idx = threadIdx.x; idx < nmodes; idx += EPS_THREADS) {
+      const int m = idx / a.g.nk2, kq = idx - m * a.g.nk2;
+      const bool m0 = m == 0;
+      const int kqm = kq == 0 ? 0 : a.g.nk2 - kq;
+      const size_t col = (size_t)m * a.g.kp;
+      const double kxm = a.kx[m], kzq = a.kz[kq];
+      auto ld = [&](const double2* f, int jj) -> double2 {
+        const size_t o = (size_t)jj * ps + col;
+        double2 v = f[o + kq];
+        if (m0) {
+          const double2 u = f[o + kqm];
+          v = make_double2(0.5 * (v.x + u.x), 0.5 * (v.y - u.y));
+        }
+        return v;
+      };
+      auto dot = [](double2 p, double2 q) { return p.x * q.x + p.y * q.y; };
+      // F1, F3 on GYF plane jj (the cf1, cf3 terms of k_les_div)
+      auto f13 = [&](int jj, double2& F1, double2& F3) {
+        const size_t o = (size_t)jj * ps + col + kq;
+        const double s = a.sf[jj], g0 = a.sg[jj], g1 = a.sg[jj + 1], idf = a.dyf[jj];
+        const double2 c1 = s * a.T[0][o], c3 = s * a.T[1][o], c5 = s * a.T[3][o];
+        const double2 c4 = g0 * a.T[2][o], c4p = g1 * a.T[2][o + ps];
+        const double2 c6 = g0 * a.T[4][o], c6p = g1 * a.T[4][o + ps];
+        F1 = make_double2(0.0, 0.0) - mul_ik(kxm, c1) - make_double2((c4p.x - c4.x) / idf, (c4p.y - c4.y) / idf) -
+             mul_ik(kzq, c5);
+        F3 = make_double2(0.0, 0.0) - mul_ik(kxm, c5) - make_double2((c6p.x - c6.x) / idf, (c6p.y - c6.y) / idf) -
+             mul_ik(kzq, c3);
+      };
+      double2 F1, F3, F1m, F3m;
+      f13(j, F1, F3);
+      f13(j - 1, F1m, F3m);
+      const size_t o = (size_t)j * ps + col + kq;
+      const double2 c4 = a.sg[j] * a.T[2][o], c6 = a.sg[j] * a.T[4][o];
+      const double2 F2 = make_double2(0.0, 0.0) - mul_ik(kxm, c4) - mul_ik(kzq, c6) + mul_ik(kxm, a.T[5][o]) +
+                         mul_ik(kzq, a.T[6][o]);
+      const double w = m0 ? 1.0 : 2.0;
+      acc += w * (0.5 * (dot(ld(a.cu[0], j), F1) + dot(ld(a.cu[0], j - 1), F1m)) +
+                  0.5 * (dot(ld(a.cu[2], j), F3) + dot(ld(a.cu[2], j - 1), F3m)) + dot(ld(a.cu[1], j), F2));
+    }
+  }
+  // fixed-order block reduction: the result does not depend on scheduling
+  __shared__ double red[EPS_THREADS / 32];
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < EPS_THREADS / 32; ++w) s += red[w];
+    a.out[j] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // scalar SGS flux (:1144-1200): out_x = ikx cth, out_z = ikz cth on planes 1..Nyp+1
 struct ThGradArgs {
   const double2* cth[8];

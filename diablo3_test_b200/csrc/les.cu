@@ -42,6 +42,7 @@ int ensure_les(diablo_ctx* ctx) {
   AL(L.d_d2f, n * sizeof(double)); AL(L.d_d2g, n * sizeof(double));
   AL(L.d_sclf, n * sizeof(double)); AL(L.d_sclg, n * sizeof(double));
   AL(L.d_idy, n * sizeof(double)); AL(L.d_idyf, n * sizeof(double));
+  AL(L.d_eps, n * sizeof(double));
 #undef AL
   // filter widths Delta^2 and the constant-model scalings (for/les.f90:224-245)
   std::vector<double> d2f(n, 0.0), d2g(n, 0.0), cf(n, 0.0), cg(n, 0.0), sclf(n, 1.0), sclg(n, 1.0);
@@ -264,6 +265,22 @@ int substep_les_t(diablo_ctx* ctx, int rk) {
     da.j1 = ctx->jstart; da.j2 = ctx->ny - 1;
     Prof pr(ctx, K_OTHER);
     k_les_div<<<grid1d(ftot), 256, 0, ctx->stream>>>(da);
+  }
+  // eps_sgs1 after a statistics save, from the stresses just formed and the
+  // state with the LES wall values (for/les.f90:924-1068)
+  if (rk == 1 && L.eps_req) {
+    EpsSgsArgs ea;
+    for (int q = 0; q < 3; ++q) ea.cu[q] = ctx->st[c][q];
+    for (int i = 0; i < 7; ++i) ea.T[i] = L.T[i];
+    ea.kx = ctx->d_kx; ea.kz = ctx->d_kz; ea.dyf = ctx->d_dyf;
+    ea.sf = L.d_sclf; ea.sg = L.d_sclg; ea.g = fg; ea.out = L.d_eps;
+    {
+      Prof pr(ctx, K_OTHER);
+      k_eps_sgs1<<<ctx->nyp2, EPS_THREADS, 0, ctx->stream>>>(ea);
+    }
+    L.eps_req = 0;
+    L.eps_ready = 1;
+    L.eps_blank = 0;
   }
   // 7. scalar SGS flux: the AMD scalar model (model 5, for/les.f90:1219-1412)
   // or kappa_t = nu_t (for/les.f90:1130-1200)
@@ -503,6 +520,22 @@ int dynamic_coefficient(diablo_ctx* ctx) {
 
 // mixed precision: the LES model and its transforms in FP32, the
 // Crank-Nicolson solves, projection and state in FP64
+int diablo_les_eps_sgs1(diablo_ctx* ctx, double* out, int len) {
+  if (!ctx || !out || len < ctx->ny) return DIABLO_ERR_ARG;
+  diablo_ctx::Les& L = ctx->les;
+  if (!L.eps_ready) return DIABLO_ERR_STATE;
+  if (L.eps_blank) {
+    for (int j = 0; j < ctx->ny; ++j) out[j] = 0.0;
+    return 0;
+  }
+  std::vector<double> h(ctx->nyp2);
+  CK(cudaMemcpyAsync(h.data(), L.d_eps, ctx->nyp2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  // plane sums over the retained modes are already plane means
+  for (int j = 1; j <= ctx->ny; ++j) out[j - 1] = h[j];
+  return 0;
+}
+
 int substep_les(diablo_ctx* ctx, int rk) {
   return ctx->precision == DIABLO_FP64 ? substep_les_t<double>(ctx, rk) : substep_les_t<float>(ctx, rk);
 }

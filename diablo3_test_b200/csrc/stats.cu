@@ -16,6 +16,12 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len) {
   if (!ctx || !out) return DIABLO_ERR_ARG;
   if (len < diablo_stats_size(ctx)) return DIABLO_ERR_ARG;
   const diablo_params& p = ctx->p;
+  // flag_save_LES: eps_sgs1 is formed at the next step's first substep
+  // (for/control.f90:95, for/les.f90:924)
+  if (p.use_les) {
+    ctx->les.eps_req = 1;
+    ctx->les.eps_ready = 0;
+  }
   int rc;
   // apply_BC_vel_mpi_post / apply_BC_th_mpi_post on the state (:63-64)
   if ((rc = bc_post(ctx, 1, 1))) return rc;

@@ -434,6 +434,13 @@ int substep(diablo_ctx* ctx, int rk) {
     if (m != 1 && m != 2 && m != 4 && m != 5) return DIABLO_ERR_UNSUPPORTED;
     return substep_les(ctx, rk);
   }
+  // LES gated off (a new flow's first 100 steps): a pending LES statistics
+  // request is answered with blanks (for/channel.f90:271-274)
+  if (ctx->p.use_les && rk == 1 && ctx->les.eps_req) {
+    ctx->les.eps_req = 0;
+    ctx->les.eps_ready = 1;
+    ctx->les.eps_blank = 1;
+  }
   int rc = ensure_scratch(ctx);
   if (rc) return rc;
   update_transient(ctx);

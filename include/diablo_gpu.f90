@@ -176,6 +176,15 @@ module diablo_gpu
       integer(c_int), value :: len
       integer(c_int) :: diablo_stats
     end function diablo_stats
+    ! eps_sgs1 of les_chan (for/les.f90:924-1068), formed at the step after a
+    ! diablo_stats call on an LES context
+    function diablo_les_eps_sgs1(ctx, out, len) bind(C, name="diablo_les_eps_sgs1")
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(out) :: out(*)
+      integer(c_int), value :: len
+      integer(c_int) :: diablo_les_eps_sgs1
+    end function diablo_les_eps_sgs1
 
     ! ---- run control
     function diablo_set_precision(ctx, precision) bind(C, name="diablo_set_precision")

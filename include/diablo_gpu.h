@@ -120,6 +120,8 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
  * (module array of for/flow.f90:50, set by les_chan, for/les.f90:235-241 and
  * :2241-2262) in the reference's physical layout; host or device `buf`.
  * All zero before the first LES substep, as the reference's array is. */
+int diablo_download_nu_t(diablo_ctx* ctx, double* buf);
+
 /*
  * The host-authoritative round trip, nsteps times: every step uploads the
  * state (u1, u2, u3, p, th_0..) from bufs[0..3+n_th], advances one step as
@@ -137,7 +139,6 @@ int diablo_download_state(diablo_ctx* ctx, int field, double* buf, int layout);
  * No reference counterpart: the reference's state never leaves the host.
  */
 int diablo_step_host(diablo_ctx* ctx, double* const* bufs, int nsteps);
-int diablo_download_nu_t(diablo_ctx* ctx, double* buf);
 
 /* for/fft.f90:247-315.  v: physical array, vv: Fourier array, both full
  * reference-size buffers (host or device); v == vv is allowed, as in the
@@ -214,6 +215,17 @@ enum {
 };
 int diablo_stats_size(diablo_ctx* ctx);
 int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len);
+
+/* eps_sgs1 of les_chan (for/les.f90:924-1068), the plane mean of u_i times
+ * the SGS stress force added to cf_i (interpolated onto GY points; written to
+ * mean.h5 with sign opposite to the usual dissipation convention, as the
+ * reference notes).  As in the reference, a diablo_stats call on an LES
+ * context requests it (flag_save_LES, for/control.f90:95) and the next step's
+ * first substep forms it from that substep's stresses; this call then copies
+ * Ny values (j = 1..Ny; j = 1 is 0) into host `out` (len >= Ny).  All zero
+ * when the LES gate was still off at that step (for/channel.f90:271-274);
+ * DIABLO_ERR_STATE when no step has run since the request. */
+int diablo_les_eps_sgs1(diablo_ctx* ctx, double* out, int len);
 
 int diablo_set_precision(diablo_ctx* ctx, int precision);
 int diablo_get_time(diablo_ctx* ctx, double* time, int* time_step, double* delta_t);

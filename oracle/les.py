@@ -1,6 +1,7 @@
 """numpy restatement of the reference's LES closures (test infrastructure only).
 
 * Type 1, constant Smagorinsky: ``les_chan`` (for/les.f90:20-270, 850-925)
+  and its ``eps_sgs1`` statistic (:924-1068),
   and ``les_chan_th`` (for/les.f90:1091-1200), with ``compute_strain_chan``
   (:1463-1510), ``apply_BC_les``/``apply_BC_th_les`` (:2001-2105),
   ``ghost_les_mpi`` and ``ghost_CS2_mpi`` at one y-rank (:2107-2270, :2444-2530).
@@ -471,6 +472,49 @@ def les_chan(o):
         temp.r[J2, :Nz, :Nx] = nt[J2, :Nz, :Nx] * (u[J2, :Nz, :Nx] - u[1:Nyp, :Nz, :Nx]) / o.dy[J2, None, None]
         o.fft_xz_to_fourier(temp)
         cf2[J2, K, I] = cf2[J2, K, I] + ck * temp.c[J2, K, I]
+    if getattr(o, "flag_save_les", False) and o.rk_step == 1:     # :924
+        o.eps_sgs1 = eps_sgs1(o, C1, C3, C4, C5, C6, nt)
+        o.flag_save_les = False
+
+
+def eps_sgs1(o, C1, C3, C4, C5, C6, nt):
+    """eps_sgs1_mean of les_chan (for/les.f90:940-1068): the plane mean of
+    u_i times the SGS force of cf_i, evaluated as the reference does, each force
+    transformed to physical space and multiplied point by point; the u1 and u3
+    parts are averaged from GYF onto GY.  Velocities are the physical fields of
+    les_chan (after the LES wall values).  Returns (Ny,) for j = 1..Nyp."""
+    Nyp, Nx, Nz, K, I = o.Nyp, o.Nx, o.Nz, slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    cikx, cikz = o.cikx[None, None, :o.Nxp], o.cikz[None, :, None]
+    u1, u2, u3 = (f.r[:, :Nz, :Nx] for f in (o.u1, o.u2, o.u3))
+    eps = np.zeros(o.Ny + 2)
+    tmp = Field(o.Ny, o.Nz, o.Nx)
+    R, RP, J2 = slice(1, Nyp + 1), slice(2, Nyp + 2), slice(2, Nyp + 1)
+    dyf = o.dyf[R, None, None]
+    # parts of CF1 and CF3 on GYF, interpolated onto GY (:944-984)
+    for u, first, pair, last in ((u1, C1, C4, C5), (u3, C5, C6, C3)):
+        tmp.buf[:] = 0.0
+        tmp.c[R, K, I] = -cikx * first[R, K, I] - (pair[RP, K, I] - pair[R, K, I]) / dyf - cikz * last[R, K, I]
+        o.fft_xz_to_physical(tmp)
+        t = tmp.r[:, :Nz, :Nx]
+        for j in range(2, Nyp + 1):
+            eps[j] += np.sum(0.5 * (u[j] * t[j] + u[j - 1] * t[j - 1]))
+    # part of CF2 on GY (:986-1003)
+    tmp.buf[:] = 0.0
+    tmp.c[J2, K, I] = -cikx * C4[J2, K, I] - cikz * C6[J2, K, I]
+    o.fft_xz_to_physical(tmp)
+    for j in range(2, Nyp + 1):
+        eps[j] += np.sum(tmp.r[j, :Nz, :Nx] * u2[j])
+    # the explicit cross terms of CF2 (:1004-1052)
+    for u, ck in ((u1, cikx), (u3, cikz)):
+        tmp.buf[:] = 0.0
+        tmp.r[J2, :Nz, :Nx] = nt[J2, :Nz, :Nx] * (u[J2] - u[1:Nyp]) / o.dy[J2, None, None]
+        o.fft_xz_to_fourier(tmp)
+        tmp.c[J2, K, I] = ck * tmp.c[J2, K, I]
+        o.fft_xz_to_physical(tmp)
+        for j in range(2, Nyp + 1):
+            eps[j] += np.sum(tmp.r[j, :Nz, :Nx] * u2[j])
+    eps /= float(Nx * Nz)                                          # :1064-1068
+    return eps[1:Nyp + 1].copy()
 
 
 def _amd_scalar(o, F, n):

@@ -135,3 +135,84 @@ def test_les_mixed_precision_close_to_fp64(cuda_device, model):
     finally:
         a.close()
         b.close()
+
+
+EPS_CASES = {
+    "smagorinsky": dict(les_model_type=LES_SMAGORINSKY),
+    "smagorinsky_neumann_top": dict(les_model_type=LES_SMAGORINSKY, u_bc_ymax=1, w_bc_ymax=1,
+                                    u_bc_ymax_c1=0.1),
+    "dynamic": dict(les_model_type=LES_DYNAMIC_SMAGORINSKY),
+    "amd_rozema": dict(les_model_type=LES_AMD_ROZEMA),
+    "amd_verstappen": dict(les_model_type=LES_AMD_VERSTAPPEN, n_th=2, pr=[0.71, 1.0]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(EPS_CASES))
+def test_les_eps_sgs1_matches_oracle(cuda_device, case):
+    """eps_sgs1 (for/les.f90:924-1068): a statistics save requests it, the
+    next step's first substep forms it.  The GPU's Parseval sums against the
+    oracle's physical-space loops, relative to the profile's largest value."""
+    p = _les_params(EPS_CASES[case])
+    gy = grid_for(p)
+    fields = initial_fields(p, gy, kind="turbulent", seed=9)
+    o = setup_oracle(p, gy, fields)
+    ch = setup_gpu(p, gy, fields)
+    try:
+        o.step(1)
+        ch.step(1)
+        with pytest.raises(_lib.DiabloError) as e:       # nothing requested yet
+            ch.les_eps_sgs1()
+        assert e.value.status == _lib.ERR_STATE
+        ch.stats()                                       # flag_save_LES
+        o.apply_bc_vel_post()                            # what save_stats_chan applies
+        o.apply_bc_th_post()
+        o.flag_save_les = True
+        with pytest.raises(_lib.DiabloError):            # requested, not yet formed
+            ch.les_eps_sgs1()
+        o.step(1)
+        ch.step(1)
+        eg, eo = ch.les_eps_sgs1(), o.eps_sgs1
+        scale = np.abs(eo).max()
+        assert scale > 0
+        assert np.abs(eg - eo).max() <= TOL * scale, np.abs(eg - eo).max() / scale
+        assert eg[0] == 0.0
+        _compare(o, ch, "after the eps_sgs1 step")
+        # formed once per request: a further step leaves the value in place
+        ch.step(1)
+        assert np.array_equal(ch.les_eps_sgs1(), eg)
+    finally:
+        ch.close()
+
+
+def test_les_eps_sgs1_mixed_close_to_fp64(cuda_device):
+    p = _les_params(dict(les_model_type=LES_DYNAMIC_SMAGORINSKY))
+    gy = grid_for(p)
+    fields = initial_fields(p, gy, kind="turbulent", seed=10)
+    a = setup_gpu(p, gy, fields)
+    b = setup_gpu(p, gy, fields)
+    try:
+        b.set_precision(MIXED)
+        for ch in (a, b):
+            ch.step(1)
+            ch.stats()
+            ch.step(1)
+        ea, eb = a.les_eps_sgs1(), b.les_eps_sgs1()
+        assert np.abs(eb - ea).max() <= 1e-4 * np.abs(ea).max()
+    finally:
+        a.close()
+        b.close()
+
+
+def test_les_eps_sgs1_blank_while_gate_closed(cuda_device):
+    # a new flow's first 100 steps skip the LES term; the request is answered
+    # with blanks (for/channel.f90:271-274)
+    p = _les_params(dict(les_model_type=LES_SMAGORINSKY), create_new_flow=True)
+    gy = grid_for(p)
+    ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=6))
+    try:
+        ch.step(1)
+        ch.stats()
+        ch.step(1)
+        assert np.all(ch.les_eps_sgs1() == 0.0)
+    finally:
+        ch.close()

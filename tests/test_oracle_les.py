@@ -131,3 +131,64 @@ def test_amd_viscosity_is_linear_in_velocity(model):
     assert np.abs(out[0][0]).max() > 0 and np.abs(out[0][1]).max() > 0
     np.testing.assert_allclose(out[1][0], 2.0 * out[0][0], rtol=1e-9, atol=1e-14)
     np.testing.assert_allclose(out[1][1], 2.0 * out[0][1], rtol=1e-9, atol=1e-14)
+
+
+def _parseval_mean(o, a, b):
+    """Plane means of the product of two band-limited fields from their packed
+    Fourier coefficients: weight 1 on the kx = 0 column, 2 elsewhere."""
+    K, I = slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    w = np.full(o.Nxp, 2.0)
+    w[0] = 1.0
+    return np.sum(w * np.real(a[:, K, I] * np.conj(b[:, K, I])), axis=(1, 2))
+
+
+def test_eps_sgs1_physical_loops_equal_parseval_sums():
+    """eps_sgs1 (for/les.f90:940-1068) as the reference forms it (forces to
+    physical space, point products, plane sums) against the Parseval sums over
+    the retained modes that the CUDA kernel evaluates: one and the same number
+    for band-limited fields.  Random Hermitian-consistent stresses from real
+    fields, random velocities and nu_t."""
+    from oracle.channel import Field
+    from oracle.les import eps_sgs1
+    o = _oracle(LES_SMAGORINSKY)
+    rng = np.random.default_rng(3)
+    Nx, Nz, Ny = o.Nx, o.Nz, o.Ny
+
+    def real_field():
+        f = Field(Ny, Nz, Nx)
+        f.r[:, :Nz, :Nx] = rng.standard_normal((Ny + 2, Nz, Nx))
+        o.fft_xz_to_fourier(f)          # band-limited from here on
+        return f
+
+    C = [real_field() for _ in range(5)]
+    U = [real_field() for _ in range(3)]
+    uc = [u.c.copy() for u in U]
+    for u in U:
+        o.fft_xz_to_physical(u)
+    o.u1, o.u2, o.u3 = U
+    nt = np.zeros((Ny + 2, Nz + 2, Nx + 2))
+    nt[2:Ny, :Nz, :Nx] = rng.random((Ny - 2, Nz, Nx))
+    C1, C3, C4, C5, C6 = (c.c for c in C)
+    got = eps_sgs1(o, C1, C3, C4, C5, C6, nt)
+
+    K, I = slice(0, o.twoNkz + 1), slice(0, o.Nxp)
+    ikx, ikz = 1j * o.kx[None, None, :o.Nxp], 1j * o.kz[None, :o.twoNkz + 1, None]
+    R, RP = slice(1, Ny + 1), slice(2, Ny + 2)
+    F1 = np.zeros_like(C1); F3 = np.zeros_like(C1); F2 = np.zeros_like(C1)
+    dyf = o.dyf[R, None, None]
+    F1[R, K, I] = -ikx * C1[R, K, I] - (C4[RP, K, I] - C4[R, K, I]) / dyf - ikz * C5[R, K, I]
+    F3[R, K, I] = -ikx * C5[R, K, I] - (C6[RP, K, I] - C6[R, K, I]) / dyf - ikz * C3[R, K, I]
+    t1, t3 = Field(Ny, Nz, Nx), Field(Ny, Nz, Nx)
+    u1p, u3p = U[0].r[:, :Nz, :Nx], U[2].r[:, :Nz, :Nx]
+    t1.r[2:Ny + 1, :Nz, :Nx] = nt[2:Ny + 1, :Nz, :Nx] * (u1p[2:Ny + 1] - u1p[1:Ny]) / o.dy[2:Ny + 1, None, None]
+    t3.r[2:Ny + 1, :Nz, :Nx] = nt[2:Ny + 1, :Nz, :Nx] * (u3p[2:Ny + 1] - u3p[1:Ny]) / o.dy[2:Ny + 1, None, None]
+    o.fft_xz_to_fourier(t1)
+    o.fft_xz_to_fourier(t3)
+    J2 = slice(2, Ny + 1)
+    F2[J2, K, I] = (-ikx * C4[J2, K, I] - ikz * C6[J2, K, I] + ikx * t1.c[J2, K, I] + ikz * t3.c[J2, K, I])
+    p1, p3, p2 = _parseval_mean(o, uc[0], F1), _parseval_mean(o, uc[2], F3), _parseval_mean(o, uc[1], F2)
+    ref = np.zeros(Ny + 2)
+    for j in range(2, Ny + 1):
+        ref[j] = 0.5 * (p1[j] + p1[j - 1]) + 0.5 * (p3[j] + p3[j - 1]) + p2[j]
+    assert got[0] == 0.0
+    assert np.abs(got - ref[1:Ny + 1]).max() <= 1e-12 * np.abs(ref).max()
