@@ -9,8 +9,9 @@ reals, the layout of ``vv(0:Nxp, 0:Nz+1, 0:Nyp+1)``), one tensor per scalar
 after p.  The forward advances `channel` by nsteps steps keeping checkpoints
 every `every` steps; backward recomputes each segment from its checkpoint and
 runs the adjoint substeps backwards (no autograd graph of the step is built).
-DNS in FP64 with velocities and scalars (for/channel.f90:rk_chan_1 without
-LES, 'Front' forcing or the scalar filter).
+DNS in FP64 with velocities and scalars, the scalar filter of
+filter_scalars included (for/channel.f90:rk_chan_1 without LES or 'Front'
+forcing).
 """
 from __future__ import annotations
 

@@ -100,8 +100,6 @@ void adj_rows(diablo_ctx* ctx, std::vector<double>& cn, std::vector<double>& rma
 int adj_supported(const diablo_ctx* ctx) {
   if (ctx->p.use_les || ctx->precision != DIABLO_FP64 || ctx->p.variable_dt || ctx->p.flavor_front)
     return DIABLO_ERR_UNSUPPORTED;
-  for (int s = 0; s < ctx->nth; ++s)
-    if (ctx->p.filter_th[s]) return DIABLO_ERR_UNSUPPORTED;
   return 0;
 }
 
@@ -295,7 +293,7 @@ int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every) {
       T.ckpt_time[k] = ctx->time;
     }
     if (s < slast) {
-      if ((rc = one_step(ctx))) return rc;
+      if ((rc = one_step(ctx)) || (rc = filter_scalars(ctx))) return rc;
       continue;
     }
     // the last segment keeps each substep's input fields as it goes, so that
@@ -309,6 +307,7 @@ int diablo_adjoint_record(diablo_ctx* ctx, int nsteps, int every) {
       if ((rc = substep(ctx, rk))) return rc;
     }
     ctx->time += ctx->delta_t;
+    if ((rc = filter_scalars(ctx))) return rc;
   }
   T.sub_seg = T.nseg - 1;
   if ((rc = copy_fields(ctx, &T.ckpt[(size_t)T.nseg * ns], ctx->st[ctx->cur], ns))) return rc;
@@ -353,12 +352,19 @@ int diablo_adjoint_run(diablo_ctx* ctx, double* const* lam) {
           if ((rc = substep(ctx, rk))) return rc;
         }
         ctx->time += ctx->delta_t;
+        if ((rc = filter_scalars(ctx))) return rc;
       }
       T.sub_seg = k;
     }
-    for (int s = s1 - 1; s >= s0; --s)
+    for (int s = s1 - 1; s >= s0; --s) {
+      // the scalar filter that ended step s (a real factor per mode, its own
+      // transpose) acts on the scalar lambdas first
+      const int ts = T.ckpt_step[k] + (s - s0) + 1;
+      for (int n = 0; n < ctx->nth; ++n)
+        if (filter_due(ctx, n, ts) && (rc = filter_field(ctx, n, T.lu[4 + n]))) return rc;
       for (int rk = 3; rk >= 1; --rk)
         if ((rc = adj_substep(ctx, rk, &T.sub[((size_t)(s - s0) * 3 + (rk - 1)) * nfs]))) return rc;
+    }
   }
   // back to the recorded final state
   if ((rc = copy_fields(ctx, ctx->st[ctx->cur], &T.ckpt[(size_t)T.nseg * ns], ns))) return rc;

@@ -715,7 +715,10 @@ int diablo_rk_substep(diablo_ctx* ctx, int rk_step) {
   return rc ? rc : sched_status(ctx);
 }
 
-static int filter_chan(diablo_ctx* ctx, int n) {
+// filter_chan's transfer function applied to scalar n's planes jst..jet of
+// the Fourier field f: a real factor per (kx, kz) mode, so the operation is
+// its own adjoint (the discrete adjoint applies it to the scalar's lambda)
+extern "C++" int filter_field(diablo_ctx* ctx, int n, double2* f) {
   if (!ctx->d_sigma) {
     const int nkx1 = ctx->nkx1, nk2 = ctx->nk2;
     std::vector<double> sg((size_t)nkx1 * nk2), kx(nkx1), kz(nk2);
@@ -736,16 +739,23 @@ static int filter_chan(diablo_ctx* ctx, int n) {
   const int j0 = ctx->jst[n], j1 = ctx->jet[n];
   const size_t tot = (size_t)(j1 - j0 + 1) * ctx->nkx1 * ctx->kp;
   Prof pr(ctx, K_OTHER);
-  k_filter_th<<<grid1d(tot), 256, 0, ctx->stream>>>(ctx->st[ctx->cur][4 + n], ctx->d_sigma, j0, j1, ctx->nkx1,
-                                                    ctx->nk2, ctx->kp);
+  k_filter_th<<<grid1d(tot), 256, 0, ctx->stream>>>(f, ctx->d_sigma, j0, j1, ctx->nkx1, ctx->nk2, ctx->kp);
   CK(cudaGetLastError());
   return 0;
+}
+
+static int filter_chan(diablo_ctx* ctx, int n) { return filter_field(ctx, n, ctx->st[ctx->cur][4 + n]); }
+
+// scalars filter_scalars filters after the step that brought the counter to
+// time_step (for/advance.f90:161-173)
+extern "C++" bool filter_due(const diablo_ctx* ctx, int n, int time_step) {
+  return ctx->p.filter_th[n] && ctx->p.filter_int[n] > 0 && time_step % ctx->p.filter_int[n] == 0;
 }
 
 // filter_scalars (for/advance.f90:161-173), after each step
 extern "C++" int filter_scalars(diablo_ctx* ctx) {
   for (int n = 0; n < ctx->nth; ++n)
-    if (ctx->p.filter_th[n] && ctx->p.filter_int[n] > 0 && ctx->time_step % ctx->p.filter_int[n] == 0) {
+    if (filter_due(ctx, n, ctx->time_step)) {
       int rc = filter_chan(ctx, n);
       if (rc) return rc;
     }

@@ -253,6 +253,8 @@ int four_in(diablo_ctx* ctx, const double* buf, double2* dst, bool check);
 int four_out(diablo_ctx* ctx, const double2* src, double* buf);
 int bc_post(diablo_ctx* ctx, int do_vel, int do_th);
 int filter_scalars(diablo_ctx* ctx);
+int filter_field(diablo_ctx* ctx, int n, double2* f);
+bool filter_due(const diablo_ctx* ctx, int n, int time_step);
 
 // ---- column solve launchers (column_launch.cu) ----------------------------
 int launch_tiles(const Solve2Args& A, cudaStream_t s);

@@ -102,13 +102,17 @@ def test_adjoint_matches_torch_autograd(cuda_device, case):
         ch.close()
 
 
-def test_adjoint_finite_differences_scalars(cuda_device):
+@pytest.mark.parametrize("filtered", [False, True])
+def test_adjoint_finite_differences_scalars(cuda_device, filtered):
     """Two scalars with buoyancy and background gradients, 48 x 65 x 32,
     20 steps with checkpoints every 5: the directional derivative of
     J = 1/2 <u.u> + 1/2 <th.th> from the adjoint against central finite
     differences along 4 seeded directions (perturbing velocities and
-    scalars)."""
-    p = small_params(nx=48, ny=65, nz=32, re=500.0, delta_t=1e-3, n_th=2, **SCALARS)
+    scalars).  `filtered`: filter_scalars filters the scalars every 2 and 4
+    steps (for/advance.f90:161-173); 20 is a multiple of both, so every
+    evaluation meets the filter at the same steps of its run."""
+    extra = dict(filter_th=[True, True], filter_int=[2, 4]) if filtered else {}
+    p = small_params(nx=48, ny=65, nz=32, re=500.0, delta_t=1e-3, n_th=2, **SCALARS, **extra)
     gy = grid_for(p)
     _, _, dy, dyf = metrics(gy)
     ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=6))
@@ -234,10 +238,12 @@ def test_adjoint_finite_differences_c4(cuda_device):
 
 
 def test_adjoint_rejects_unsupported_and_stale(cuda_device):
-    p = small_params(n_th=1, filter_th=[True], filter_int=[2])
+    from diablo3_test_b200.config import MIXED
+    p = small_params(n_th=1)
     gy = grid_for(p)
     ch = setup_gpu(p, gy, initial_fields(p, gy))
     try:
+        ch.set_precision(MIXED)
         with pytest.raises(_lib.DiabloError) as e:
             ch.adjoint_record(2, 1)
         assert e.value.status == _lib.ERR_UNSUPPORTED
