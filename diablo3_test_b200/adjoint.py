@@ -10,8 +10,8 @@ after p.  The forward advances `channel` by nsteps steps keeping checkpoints
 every `every` steps; backward recomputes each segment from its checkpoint and
 runs the adjoint substeps backwards (no autograd graph of the step is built).
 DNS in FP64 with velocities and scalars, the scalar filter of
-filter_scalars included (for/channel.f90:rk_chan_1 without LES or 'Front'
-forcing).
+filter_scalars and the 'Front' thermal-wind advection included
+(for/channel.f90:rk_chan_1 without LES).
 """
 from __future__ import annotations
 

@@ -98,8 +98,7 @@ void adj_rows(diablo_ctx* ctx, std::vector<double>& cn, std::vector<double>& rma
 }
 
 int adj_supported(const diablo_ctx* ctx) {
-  if (ctx->p.use_les || ctx->precision != DIABLO_FP64 || ctx->p.variable_dt || ctx->p.flavor_front)
-    return DIABLO_ERR_UNSUPPORTED;
+  if (ctx->p.use_les || ctx->precision != DIABLO_FP64 || ctx->p.variable_dt) return DIABLO_ERR_UNSUPPORTED;
   return 0;
 }
 
@@ -224,6 +223,22 @@ int adj_substep(diablo_ctx* ctx, int rk, double2* const* u_in) {
 #undef X
       default: return DIABLO_ERR_SIZE;
     }
+  }
+  if (p.flavor_front && ctx->ro_inv != 0.0 && nth > 0) {
+    // thermal-wind advection (for/forcing.f90:37-113), after every lambda cf
+    // of this substep is known
+    AdjFrontArgs a;
+    memset(&a, 0, sizeof(a));
+    for (int f = 0; f < 3; ++f) { a.onl[f] = T.lnl[f]; a.ou[f] = T.ou[f]; }
+    for (int s = 0; s < nth; ++s) {
+      a.onl[3 + s] = T.lnl[3 + s]; a.ou[3 + s] = T.ou[4 + s];
+      a.dthdx[s] = p.dthdx[s]; a.dthdz[s] = p.dthdz[s];
+    }
+    a.kx = ctx->d_kx; a.kz = ctx->d_kz; a.gy = ctx->d_gy; a.gyf = ctx->d_gyf;
+    a.ly = p.ly; a.coef = p.delta / ctx->ro_inv;
+    a.nth = nth; a.n = ctx->nyp2; a.nkx1 = ctx->nkx1; a.nk2 = ctx->nk2; a.kp = ctx->kp;
+    Prof pr(ctx, K_OTHER);
+    k_adj_front<<<grid1d((size_t)ctx->nyp2 * ctx->nkx1 * ctx->kp), 256, 0, ctx->stream>>>(a);
   }
   const int nprod = 8 + 3 * nth;
   {

@@ -340,6 +340,60 @@ __global__ void __launch_bounds__(128) k_adj_scalar(const __grid_constant__ AdjS
   for (int r = 0; r < R; ++r) st(a.oth, j0 + r, OU[r]);
 }
 
+// Adjoint of the thermal-wind advection of the 'Front' flavor
+// (user_rhs_chan_fourier, for/forcing.f90:37-113), after k_adj_column and
+// k_adj_scalar have written lambda cf = -onl on each field's cf rows (zero
+// elsewhere).  Forward, per scalar n with c = delta / Ro_inv and
+// s_n(y) = c (y - Ly/2) (dTHdX_n kz - dTHdZ_n kx):
+//   cf1 -= i s_n(gyf) u1 + c (-dTHdZ_n) (u2(j) + u2(j+1)) / 2
+//   cf3 -= i s_n(gyf) u3 + c dTHdX_n (u2(j) + u2(j+1)) / 2
+//   cf2 -= i s_n(gy) u2,   cfth_n -= i s_n(gyf) th_n
+// so lambda u += i s lambda cf (the conjugate of -i s), and lambda u2(j)
+// takes -c/2 (sum -dTHdZ) (lcf1(j) + lcf1(j-1)) - c/2 (sum dTHdX) (lcf3(j) + lcf3(j-1)).
+// One thread per (j, m, kq) entry; adds into the lambdas of the old state.
+struct AdjFrontArgs {
+  const double2* onl[3 + DIABLO_MAX_TH];   // -lambda cf of u1, u2, u3, th..
+  double2* ou[3 + DIABLO_MAX_TH];          // lambda of the old u1, u2, u3, th..
+  const double* kx;
+  const double* kz;
+  const double* gy;
+  const double* gyf;
+  double ly, coef;                         // Ly, delta / Ro_inv
+  double dthdx[DIABLO_MAX_TH], dthdz[DIABLO_MAX_TH];
+  int nth, n, nkx1, nk2, kp;
+};
+
+static __global__ void k_adj_front(const __grid_constant__ AdjFrontArgs a) {
+  const size_t ps = (size_t)a.nkx1 * a.kp;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)a.n * ps) return;
+  const int kq = idx % a.kp;
+  if (kq >= a.nk2) return;
+  const int m = (idx / a.kp) % a.nkx1;
+  const int j = idx / ps;
+  const double kxm = a.kx[m], kzq = a.kz[kq];
+  const double gf = a.gyf[j] - 0.5 * a.ly, gg = a.gy[j] - 0.5 * a.ly;
+  double sx = 0.0, sz = 0.0;
+  for (int t = 0; t < a.nth; ++t) { sx += a.dthdx[t]; sz += a.dthdz[t]; }
+  // velocities: s summed over the scalars
+  const double sf = a.coef * gf * (sx * kzq - sz * kxm), sg = a.coef * gg * (sx * kzq - sz * kxm);
+  const double2 l1 = -1.0 * a.onl[0][idx], l2 = -1.0 * a.onl[1][idx], l3 = -1.0 * a.onl[2][idx];
+  a.ou[0][idx] = a.ou[0][idx] + mul_ik(sf, l1);
+  a.ou[2][idx] = a.ou[2][idx] + mul_ik(sf, l3);
+  double2 o2 = a.ou[1][idx] + mul_ik(sg, l2);
+  double2 s1 = l1, s3 = l3;
+  if (j >= 1) {
+    s1 = s1 - a.onl[0][idx - ps];
+    s3 = s3 - a.onl[2][idx - ps];
+  }
+  o2 = o2 - (0.5 * a.coef * (-sz)) * s1 - (0.5 * a.coef * sx) * s3;
+  a.ou[1][idx] = o2;
+  for (int t = 0; t < a.nth; ++t) {
+    const double st = a.coef * gf * (a.dthdx[t] * kzq - a.dthdz[t] * kxm);
+    a.ou[3 + t][idx] = a.ou[3 + t][idx] + mul_ik(st, -1.0 * a.onl[3 + t][idx]);
+  }
+}
+
 // lambda NL -> the eight physical-space product adjoints, in Fourier space,
 // scaled by the forward transform's transpose (1/(NxNz), halved for kx > 0):
 //   0 u1u3: -ikz l1 - ikx l3   1 u1u1: -ikx l1   2 u3u3: -ikz l3

@@ -296,9 +296,9 @@ int diablo_fft_xz_to_fourier_noalloc(int nx, int ny, int nz, const double* v, do
  * Discrete adjoint of diablo_step.  No reference counterpart: the reference
  * has no adjoint.  For DNS contexts in FP64 with velocities and any number of
  * scalars (buoyancy, background gradients, scalar transport, the filter of
- * filter_scalars, whose real per-mode factor is its own transpose), fixed
- * delta_t; LES, the 'Front' forcing and mixed precision get
- * DIABLO_ERR_UNSUPPORTED.
+ * filter_scalars, whose real per-mode factor is its own transpose, and the
+ * 'Front' flavor's thermal-wind advection), fixed delta_t; LES, mixed
+ * precision and variable_dt get DIABLO_ERR_UNSUPPORTED.
  * diablo_adjoint_record advances nsteps steps exactly as diablo_step does and
  * keeps the state (u1, u2, u3, p, th_0..) every `every` steps on the device,
  * and the input fields of every substep of the last segment.

@@ -102,17 +102,26 @@ def test_adjoint_matches_torch_autograd(cuda_device, case):
         ch.close()
 
 
-@pytest.mark.parametrize("filtered", [False, True])
-def test_adjoint_finite_differences_scalars(cuda_device, filtered):
+FD_VARIANTS = {
+    "plain": {},
+    "filtered": dict(filter_th=[True, True], filter_int=[2, 4]),
+    "front": dict(flavor="Front", ro=4.0, delta=0.8),
+}
+
+
+@pytest.mark.parametrize("variant", sorted(FD_VARIANTS))
+def test_adjoint_finite_differences_scalars(cuda_device, variant):
     """Two scalars with buoyancy and background gradients, 48 x 65 x 32,
     20 steps with checkpoints every 5: the directional derivative of
     J = 1/2 <u.u> + 1/2 <th.th> from the adjoint against central finite
     differences along 4 seeded directions (perturbing velocities and
-    scalars).  `filtered`: filter_scalars filters the scalars every 2 and 4
+    scalars).  "filtered": filter_scalars filters the scalars every 2 and 4
     steps (for/advance.f90:161-173); 20 is a multiple of both, so every
-    evaluation meets the filter at the same steps of its run."""
-    extra = dict(filter_th=[True, True], filter_int=[2, 4]) if filtered else {}
-    p = small_params(nx=48, ny=65, nz=32, re=500.0, delta_t=1e-3, n_th=2, **SCALARS, **extra)
+    evaluation meets the filter at the same steps of its run.  "front": the
+    'Front' flavor's thermal-wind advection of velocities and scalars
+    (for/forcing.f90:37-113) with rotation."""
+    p = small_params(nx=48, ny=65, nz=32, re=500.0, delta_t=1e-3, n_th=2, **SCALARS,
+                     **FD_VARIANTS[variant])
     gy = grid_for(p)
     _, _, dy, dyf = metrics(gy)
     ch = setup_gpu(p, gy, initial_fields(p, gy, kind="turbulent", seed=6))
