@@ -669,8 +669,19 @@ struct XFwdSmem {
 #define XR2C_WARP_SYNC 1
 #endif
 
+// The FP64 products kernel (8 z-rows of 64 threads a block) holds 252
+// registers unbounded, four blocks per SM.  A cap for six blocks (168
+// registers, no spills) took it from 1.546 to 1.200 ms per launch at
+// 256 x 257 x 256 with bit-identical output, and eight blocks (128 registers,
+// 176 bytes spilled) measured 1.239 ms.  The same caps on the FP64 z forward
+// combine and x inverse (168/128 registers) moved them by +-2% and are not set.
+#ifndef XR2C64_MIN_BLOCKS
+#define XR2C64_MIN_BLOCKS 6
+#endif
+
 template <typename T, int N1, int N2, int KT, bool NL>
-__global__ void __launch_bounds__(N2* KT, (NL && sizeof(T) == 4) ? XR2C32_MIN_BLOCKS : 1) k_xr2c(XFwdArgs<T> a) {
+__global__ void __launch_bounds__(N2* KT, NL ? (sizeof(T) == 4 ? XR2C32_MIN_BLOCKS : XR2C64_MIN_BLOCKS) : 1)
+    k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   typedef XFwdSmem<T, N1, N2, KT, NL> L;
   constexpr int M = N1 * N2;
