@@ -675,12 +675,16 @@ struct XFwdSmem {
 // 256 x 257 x 256 with bit-identical output, and eight blocks (128 registers,
 // 176 bytes spilled) measured 1.239 ms.  The same caps on the FP64 z forward
 // combine and x inverse (168/128 registers) moved them by +-2% and are not set.
+// The cap applies to that measured shape (Nx = 256, 8 rows a block) only: on
+// other lengths and row counts it makes the compiler spill.
 #ifndef XR2C64_MIN_BLOCKS
 #define XR2C64_MIN_BLOCKS 6
 #endif
 
 template <typename T, int N1, int N2, int KT, bool NL>
-__global__ void __launch_bounds__(N2* KT, NL ? (sizeof(T) == 4 ? XR2C32_MIN_BLOCKS : XR2C64_MIN_BLOCKS) : 1)
+__global__ void __launch_bounds__(N2* KT, NL ? (sizeof(T) == 4 ? XR2C32_MIN_BLOCKS
+                                                   : (N1 == 16 && N2 == 8 && KT == 8 ? XR2C64_MIN_BLOCKS : 1))
+                                             : 1)
     k_xr2c(XFwdArgs<T> a) {
   typedef typename CT<T>::C C;
   typedef XFwdSmem<T, N1, N2, KT, NL> L;
