@@ -224,7 +224,9 @@ int diablo_stats(diablo_ctx* ctx, int homogeneous_x, double* out, int len);
  * first substep forms it from that substep's stresses; this call then copies
  * Ny values (j = 1..Ny; j = 1 is 0) into host `out` (len >= Ny).  All zero
  * when the LES gate was still off at that step (for/channel.f90:271-274);
- * DIABLO_ERR_STATE when no step has run since the request. */
+ * DIABLO_ERR_STATE when no step of the context's own (diablo_step,
+ * diablo_step_host, diablo_rk_substep with rk 1) has run since the request:
+ * ensemble graph replays do not answer it. */
 int diablo_les_eps_sgs1(diablo_ctx* ctx, double* out, int len);
 
 int diablo_set_precision(diablo_ctx* ctx, int precision);
